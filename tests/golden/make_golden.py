@@ -1,0 +1,121 @@
+"""Regenerate tests/golden/reference_golden.json from the reference's own tests.
+
+Reads the reference checkout as text only (nothing is compiled or run):
+
+* src/test_su.cpp   - per test function, every `double|uint32_t NAME[] = {...}`
+                      array, every `std::vector<...> NAME = {...}` literal,
+                      every newick string given to su::BPTree and every
+                      `to_keep = {...}` set;
+* test/capi_inmem_test.c - the inline CSR copy of test.biom (obs ids, sample
+                      ids, indices, indptr, data);
+* src/test*.tre     - the newick trees the API tests load.
+
+Usage: python tests/golden/make_golden.py [/path/to/reference]
+"""
+import json
+import os
+import re
+import sys
+
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
+
+
+def _numbers(body):
+    """Parse a C initialiser list of numbers; None if it holds anything else."""
+    body = re.sub(r"//[^\n]*", "", body)
+    vals = []
+    try:
+        for tok in body.replace("\n", " ").split(","):
+            tok = tok.strip()
+            if not tok:
+                continue
+            if "/" in tok:  # e.g. 1.0/3
+                a, b = tok.split("/")
+                vals.append(float(a) / float(b))
+            else:
+                vals.append(float(tok))
+    except ValueError:
+        return None
+    return vals
+
+
+def _split_functions(text):
+    funcs = {}
+    for m in re.finditer(r"^void (test_\w+)\(\)\s*\{", text, flags=re.M):
+        start = m.end()
+        depth = 1
+        i = start
+        while depth and i < len(text):
+            if text[i] == "{":
+                depth += 1
+            elif text[i] == "}":
+                depth -= 1
+            i += 1
+        funcs[m.group(1)] = text[start:i]
+    return funcs
+
+
+def parse_test_su(path):
+    text = open(path).read()
+    out = {}
+    for name, body in _split_functions(text).items():
+        entry = {"arrays": {}, "vectors": {}, "newick": [], "to_keep": []}
+        for m in re.finditer(r"(?:const\s+)?(double|uint32_t)\s+(\w+)\s*\[\d*\]\s*=\s*\{([^}]*)\}", body):
+            vals = _numbers(m.group(3))
+            if vals is not None:
+                entry["arrays"].setdefault(m.group(2), []).append(vals)
+        for m in re.finditer(r"std::vector<(bool|double|std::string)>\s+(\w+)\s*=\s*\{([^}]*)\}", body):
+            kind, vname, content = m.groups()
+            if kind == "bool":
+                vals = [t.strip() == "true" for t in content.split(",") if t.strip()]
+            elif kind == "double":
+                vals = _numbers(content)
+            else:
+                vals = re.findall(r'"([^"]*)"', content)
+            entry["vectors"][vname] = vals
+        entry["newick"] = re.findall(r'su::BPTree\s+\w+\("([^"]*)"\)', body)
+        for m in re.finditer(r"to_keep\s*=\s*\{([^}]*)\}", body):
+            entry["to_keep"].append(re.findall(r'"([^"]*)"', m.group(1)))
+        if any(entry.values()):
+            out[name] = entry
+    return out
+
+
+def parse_capi_inmem(path):
+    text = open(path).read()
+
+    def strings(var):
+        m = re.search(var + r"\[\]\s*=\s*\{([^}]*)\}", text)
+        return re.findall(r'"([^"]*)"', m.group(1))
+
+    def nums(var):
+        m = re.search(var + r"\[\]\s*=\s*\{([^}]*)\}", text)
+        return _numbers(m.group(1))
+
+    return {
+        "obs_ids": strings("obs_ids"),
+        "sample_ids": strings("samp_ids"),
+        "indices": [int(v) for v in nums("indices")],
+        "indptr": [int(v) for v in nums("indptr")],
+        "data": nums("data"),
+    }
+
+
+def main():
+    golden = {
+        "source": "biocore/unifrac-binaries tests, read as text by tests/golden/make_golden.py",
+        "test_su": parse_test_su(os.path.join(REF, "src", "test_su.cpp")),
+        "table_csr": parse_capi_inmem(os.path.join(REF, "test", "capi_inmem_test.c")),
+        "trees": {},
+    }
+    for fn in sorted(os.listdir(os.path.join(REF, "src"))):
+        if fn.endswith(".tre"):
+            golden["trees"][fn] = open(os.path.join(REF, "src", fn)).read().strip()
+    with open(OUT, "w") as f:
+        json.dump(golden, f, indent=1, sort_keys=True)
+    print("wrote", OUT)
+
+
+if __name__ == "__main__":
+    main()
