@@ -1,0 +1,314 @@
+/*
+ * unifrac_b200.h - C ABI of the B200 Strided State UniFrac engine.
+ *
+ * The first part of this header is a drop-in for the in-memory and tree
+ * entry points of biocore/unifrac-binaries' C API (src/api.hpp).  Types have
+ * the same layout, enums the same values, functions the same names,
+ * signatures, ownership rules and status codes; each declaration cites the
+ * reference declaration it replaces.  Results are allocated by the library
+ * with malloc and released only through the matching destroy_*() call.
+ *
+ * The file-based entry points (one_off, partial, faith_pd_one_off, ...) read
+ * BIOM-HDF5 tables.  This build has no HDF5 library: they check that both
+ * files exist (table_missing / tree_missing as the reference), parse the
+ * newick tree, and report table_missing for the table with a message on
+ * stderr.  The in-memory entry points carry the whole compute path.
+ *
+ * The second part (ssu_b200_*) has no counterpart in the reference: in-memory
+ * forms of one_off / partial / faith_pd, and a device-resident plan for
+ * callers that keep the table on the GPU between calls.
+ *
+ * Every compute call runs on the current CUDA device (or ACC_DEVICE_NUM when
+ * set, as the reference's OpenACC runtime honours it).  Calls are
+ * thread-safe: each one owns its stream and device buffers.  No call exits
+ * the process; failures come back as a status.
+ */
+#ifndef UNIFRAC_B200_H
+#define UNIFRAC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define SSU_EXTERN extern "C"
+#else
+#include <stdbool.h>
+#define SSU_EXTERN extern
+#endif
+
+/* ------------------------------------------------------------------ types */
+
+/* src/status_enum.hpp:4-6 */
+typedef enum compute_status {
+    okay = 0, tree_missing, table_missing, table_empty, unknown_method,
+    table_and_tree_do_not_overlap, output_error, invalid_method, grouping_missing
+} ComputeStatus;
+typedef enum io_status {
+    read_okay = 0, write_okay, open_error, read_error, magic_incompatible, bad_header, unexpected_end, write_error
+} IOStatus;
+typedef enum merge_status {
+    merge_okay = 0, incomplete_stripe_set, sample_id_consistency, square_mismatch, partials_mismatch, stripes_overlap
+} MergeStatus;
+
+/* Condensed (scipy squareform) result, src/api.hpp:40-46. */
+typedef struct mat {
+    unsigned int n_samples;
+    unsigned int cf_size;
+    bool is_upper_triangle;
+    double *condensed_form;
+    char **sample_ids;
+} mat_t;
+
+/* Full row-major n x n result, src/api.hpp:54-72.  flags bit 0x1000 marks a
+ * matrix backed by an unlinked temp file under mmap_dir (low 12 bits: fd). */
+typedef struct mat_full_fp64 {
+    uint32_t n_samples;
+    uint32_t flags;
+    double *matrix;
+    char **sample_ids;
+} mat_full_fp64_t;
+
+typedef struct mat_full_fp32 {
+    uint32_t n_samples;
+    uint32_t flags;
+    float *matrix;
+    char **sample_ids;
+} mat_full_fp32_t;
+
+/* Per-sample vector (Faith PD), src/api.hpp:82-86. */
+typedef struct results_vec {
+    unsigned int n_samples;
+    double *values;
+    char **sample_ids;
+} r_vec;
+
+/* Stripes [stripe_start, stripe_stop) of the distance matrix, each of
+ * n_samples values: stripes[s - stripe_start][k] = d(k, (k + s + 1) % n),
+ * src/api.hpp:99-107. */
+typedef struct partial_mat {
+    uint32_t n_samples;
+    char **sample_ids;
+    double **stripes;
+    uint32_t stripe_start;
+    uint32_t stripe_stop;
+    uint32_t stripe_total;
+    bool is_upper_triangle;
+} partial_mat_t;
+
+/* src/api.hpp:123-133 */
+typedef struct partial_dyn_mat {
+    uint32_t n_samples;
+    char **sample_ids;
+    uint64_t *offsets;
+    double **stripes;
+    uint32_t stripe_start;
+    uint32_t stripe_stop;
+    uint32_t stripe_total;
+    bool is_upper_triangle;
+    char *filename;
+} partial_dyn_mat_t;
+
+/* Observation-major CSR table, borrowed for the call: row i (feature
+ * obs_ids[i]) spans indptr[i]..indptr[i+1] of indices (sample positions) and
+ * data (counts).  src/api.hpp:145-154 */
+typedef struct support_biom {
+    char **obs_ids;
+    char **sample_ids;
+    uint32_t *indices;
+    uint32_t *indptr;
+    double *data;
+    int n_obs;
+    int n_samples;
+    int nnz;
+} support_biom_t;
+
+/* Balanced-parentheses tree: structure[i] true for '(' ; the length and name
+ * of a node sit at its opening index.  src/api.hpp:163-168 */
+typedef struct support_bptree {
+    bool *structure;
+    double *lengths;
+    char **names;
+    int n_parens;
+} support_bptree_t;
+
+/* Opaque parsed tree, src/api.hpp:173-175. */
+typedef struct opaque_bptree {
+    int dummy;
+} opaque_bptree_t;
+
+/* --------------------------------------------- reference-compatible calls */
+
+/* src/api.hpp:28 - seeds the rarefaction generator. */
+SSU_EXTERN void ssu_set_random_seed(unsigned int new_seed);
+
+/* src/api.hpp:188-206 */
+SSU_EXTERN IOStatus read_bptree_opaque(const char *tree_filename, opaque_bptree_t **tree_data);
+SSU_EXTERN void load_bptree_opaque(const char *newick, opaque_bptree_t **tree_data);
+SSU_EXTERN void convert_bptree_opaque(const support_bptree_t *in_tree, opaque_bptree_t **tree_data);
+SSU_EXTERN void destroy_bptree_opaque(opaque_bptree_t **tree_data);
+/* Number of tips of the tree (the reference returns this too, whatever its comment says). */
+SSU_EXTERN int get_bptree_opaque_els(opaque_bptree_t *tree_data);
+
+/* src/api.hpp:196-201 */
+SSU_EXTERN void destroy_mat(mat_t **result);
+SSU_EXTERN void destroy_mat_full_fp64(mat_full_fp64_t **result);
+SSU_EXTERN void destroy_mat_full_fp32(mat_full_fp32_t **result);
+SSU_EXTERN void destroy_partial_mat(partial_mat_t **result);
+SSU_EXTERN void destroy_partial_dyn_mat(partial_dyn_mat_t **result);
+SSU_EXTERN void destroy_results_vec(r_vec **result);
+
+/* In-memory full-matrix UniFrac, fp64 and fp32 results.  src/api.hpp:268-323.
+ * The fp64 form rejects fp32 method names (and vice versa) with
+ * invalid_method, as src/api.cpp:775-829.  A non-NULL *result is filled in
+ * place (the caller pre-allocated it), as src/api.cpp:675-677.
+ * subsample_depth > 0 rarefies every sample without replacement first
+ * (samples below the depth are dropped); only without-replacement is
+ * supported, as the reference. */
+SSU_EXTERN ComputeStatus one_off_matrix_inmem_v3(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                                 const char *unifrac_method, bool variance_adjust, double alpha,
+                                                 bool bypass_tips, bool normalize_sample_counts, unsigned int n_substeps,
+                                                 unsigned int subsample_depth, bool subsample_with_replacement,
+                                                 const char *mmap_dir, mat_full_fp64_t **result);
+SSU_EXTERN ComputeStatus one_off_matrix_inmem_v2(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                                 const char *unifrac_method, bool variance_adjust, double alpha,
+                                                 bool bypass_tips, unsigned int n_substeps, unsigned int subsample_depth,
+                                                 bool subsample_with_replacement, const char *mmap_dir,
+                                                 mat_full_fp64_t **result);
+SSU_EXTERN ComputeStatus one_off_inmem(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                       const char *unifrac_method, bool variance_adjust, double alpha,
+                                       bool bypass_tips, unsigned int n_substeps, mat_full_fp64_t **result);
+SSU_EXTERN ComputeStatus one_off_matrix_inmem_fp32_v3(const support_biom_t *table_data,
+                                                      const support_bptree_t *tree_data, const char *unifrac_method,
+                                                      bool variance_adjust, double alpha, bool bypass_tips,
+                                                      bool normalize_sample_counts, unsigned int n_substeps,
+                                                      unsigned int subsample_depth, bool subsample_with_replacement,
+                                                      const char *mmap_dir, mat_full_fp32_t **result);
+SSU_EXTERN ComputeStatus one_off_matrix_inmem_fp32_v2(const support_biom_t *table_data,
+                                                      const support_bptree_t *tree_data, const char *unifrac_method,
+                                                      bool variance_adjust, double alpha, bool bypass_tips,
+                                                      unsigned int n_substeps, unsigned int subsample_depth,
+                                                      bool subsample_with_replacement, const char *mmap_dir,
+                                                      mat_full_fp32_t **result);
+SSU_EXTERN ComputeStatus one_off_inmem_fp32(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                            const char *unifrac_method, bool variance_adjust, double alpha,
+                                            bool bypass_tips, unsigned int n_substeps, mat_full_fp32_t **result);
+
+/* UniFrac between two dense sample vectors over n_obs features.
+ * src/api.hpp:456-478 */
+SSU_EXTERN ComputeStatus one_dense_pair_v3t(unsigned int n_obs, const char **obs_ids, const double *sample1,
+                                            const double *sample2, const opaque_bptree_t *tree_data,
+                                            const char *unifrac_method, bool variance_adjust, double alpha,
+                                            bool bypass_tips, bool normalize_sample_counts, double *result);
+SSU_EXTERN ComputeStatus one_dense_pair_v3(unsigned int n_obs, const char **obs_ids, const double *sample1,
+                                           const double *sample2, const support_bptree_t *tree_data,
+                                           const char *unifrac_method, bool variance_adjust, double alpha,
+                                           bool bypass_tips, bool normalize_sample_counts, double *result);
+SSU_EXTERN ComputeStatus one_dense_pair_v2t(unsigned int n_obs, const char **obs_ids, const double *sample1,
+                                            const double *sample2, const opaque_bptree_t *tree_data,
+                                            const char *unifrac_method, bool variance_adjust, double alpha,
+                                            bool bypass_tips, double *result);
+SSU_EXTERN ComputeStatus one_dense_pair_v2(unsigned int n_obs, const char **obs_ids, const double *sample1,
+                                           const double *sample2, const support_bptree_t *tree_data,
+                                           const char *unifrac_method, bool variance_adjust, double alpha,
+                                           bool bypass_tips, double *result);
+
+/* File-based entry points (BIOM-HDF5 table + newick tree).
+ * src/api.hpp:228-244, 348-436, 492-493, 805-814 */
+SSU_EXTERN ComputeStatus one_off_v3(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                                    bool variance_adjust, double alpha, bool bypass_tips,
+                                    bool normalize_sample_counts, unsigned int n_substeps, mat_t **result);
+SSU_EXTERN ComputeStatus one_off_wtree_v3(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                          const char *unifrac_method, bool variance_adjust, double alpha,
+                                          bool bypass_tips, bool normalize_sample_counts, unsigned int n_substeps,
+                                          mat_t **result);
+SSU_EXTERN ComputeStatus one_off(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                                 bool variance_adjust, double alpha, bool bypass_tips, unsigned int n_substeps,
+                                 mat_t **result);
+SSU_EXTERN ComputeStatus one_off_wtree(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                       const char *unifrac_method, bool variance_adjust, double alpha,
+                                       bool bypass_tips, unsigned int n_substeps, mat_t **result);
+SSU_EXTERN ComputeStatus one_off_matrix_v3(const char *biom_filename, const char *tree_filename,
+                                           const char *unifrac_method, bool variance_adjust, double alpha,
+                                           bool bypass_tips, bool normalize_sample_counts, unsigned int n_substeps,
+                                           unsigned int subsample_depth, bool subsample_with_replacement,
+                                           const char *mmap_dir, mat_full_fp64_t **result);
+SSU_EXTERN ComputeStatus one_off_matrix_fp32_v3(const char *biom_filename, const char *tree_filename,
+                                                const char *unifrac_method, bool variance_adjust, double alpha,
+                                                bool bypass_tips, bool normalize_sample_counts,
+                                                unsigned int n_substeps, unsigned int subsample_depth,
+                                                bool subsample_with_replacement, const char *mmap_dir,
+                                                mat_full_fp32_t **result);
+SSU_EXTERN ComputeStatus faith_pd_one_off(const char *biom_filename, const char *tree_filename, r_vec **result);
+SSU_EXTERN ComputeStatus partial_v3(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                                    bool variance_adjust, double alpha, bool bypass_tips,
+                                    bool normalize_sample_count, unsigned int n_substeps, unsigned int stripe_start,
+                                    unsigned int stripe_stop, partial_mat_t **result);
+SSU_EXTERN ComputeStatus partial(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                                 bool variance_adjust, double alpha, bool bypass_tips, unsigned int n_substeps,
+                                 unsigned int stripe_start, unsigned int stripe_stop, partial_mat_t **result);
+
+/* ------------------------------------------- extensions (no reference twin) */
+
+/* one_off / partial / faith_pd_one_off over in-memory inputs: the compute
+ * paths of the file-based calls above without the file parsing.  Method names,
+ * statuses and result layouts are those of the file-based calls.  An
+ * out-of-range stripe_stop returns output_error (the reference exits). */
+SSU_EXTERN ComputeStatus ssu_b200_one_off_inmem_v3(const support_biom_t *table_data,
+                                                   const support_bptree_t *tree_data, const char *unifrac_method,
+                                                   bool variance_adjust, double alpha, bool bypass_tips,
+                                                   bool normalize_sample_counts, unsigned int n_substeps,
+                                                   mat_t **result);
+SSU_EXTERN ComputeStatus ssu_b200_partial_inmem_v3(const support_biom_t *table_data,
+                                                   const support_bptree_t *tree_data, const char *unifrac_method,
+                                                   bool variance_adjust, double alpha, bool bypass_tips,
+                                                   bool normalize_sample_counts, unsigned int n_substeps,
+                                                   unsigned int stripe_start, unsigned int stripe_stop,
+                                                   partial_mat_t **result);
+SSU_EXTERN ComputeStatus ssu_b200_faith_pd_inmem(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                                 r_vec **result);
+
+/* Host-side tree helpers used by the tests (no device work): `in_tree`
+ * sheared to the tips named in names[0..n_names) (names == NULL keeps every
+ * tip) and, when do_collapse, collapsed; written into caller buffers of
+ * n_parens slots, *out_n gets its size.  Names are pointers into
+ * in_tree->names.  Returns 0 on success. */
+SSU_EXTERN int ssu_b200_shear_collapse(const support_bptree_t *in_tree, const char *const *names, int n_names,
+                                       int do_collapse, bool *out_structure, double *out_lengths,
+                                       const char **out_names, int *out_n);
+/* Newick -> BP arrays into caller buffers of `capacity` slots (lengths read
+ * through single precision, as the reference's parser).  Names point into a
+ * buffer owned by the opaque tree; free it with destroy_bptree_opaque. */
+SSU_EXTERN int ssu_b200_tree_arrays(const opaque_bptree_t *tree_data, int capacity, bool *out_structure,
+                                    double *out_lengths, const char **out_names, int *out_n);
+
+/* Device-resident plan: the table and tree are prepared and uploaded once;
+ * every execute recomputes the full n x n matrix into device memory from the
+ * resident inputs.  stream (a cudaStream_t, may be NULL) orders the work. */
+typedef struct ssu_b200_plan ssu_b200_plan_t;
+SSU_EXTERN ComputeStatus ssu_b200_plan_create(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                              const char *unifrac_method, bool variance_adjust, double alpha,
+                                              bool bypass_tips, bool normalize_sample_counts,
+                                              ssu_b200_plan_t **plan);
+SSU_EXTERN ComputeStatus ssu_b200_plan_execute(ssu_b200_plan_t *plan, void *stream);
+/* Device pointer to the n x n result (double for *_fp64 methods, else float). */
+SSU_EXTERN const void *ssu_b200_plan_device_result(const ssu_b200_plan_t *plan);
+SSU_EXTERN ComputeStatus ssu_b200_plan_copy_result(ssu_b200_plan_t *plan, void *host_out, void *stream);
+/* n(n-1)/2 * embedded branches: the pair-branch updates one execute performs. */
+SSU_EXTERN uint64_t ssu_b200_plan_work_units(const ssu_b200_plan_t *plan);
+SSU_EXTERN uint32_t ssu_b200_plan_n_samples(const ssu_b200_plan_t *plan);
+SSU_EXTERN uint64_t ssu_b200_plan_n_embedded(const ssu_b200_plan_t *plan);
+/* Kernel launches one execute issues. */
+SSU_EXTERN uint32_t ssu_b200_plan_launches(const ssu_b200_plan_t *plan);
+/* When enabled, execute brackets each stage with CUDA events on its stream;
+ * ssu_b200_plan_stage_ms then reports {embed, pair-kernel, finalize} in ms for
+ * the last execute (synchronising the stream), and the pair kernel's
+ * algorithmic bytes per launch. */
+SSU_EXTERN void ssu_b200_plan_set_timing(ssu_b200_plan_t *plan, int enable);
+SSU_EXTERN int ssu_b200_plan_stage_ms(ssu_b200_plan_t *plan, float *embed_ms, float *pair_ms, float *finalize_ms);
+SSU_EXTERN void ssu_b200_plan_destroy(ssu_b200_plan_t **plan);
+
+/* Name of the kernel family the plan's pair stage launches (for profiling). */
+SSU_EXTERN const char *ssu_b200_plan_pair_kernel(const ssu_b200_plan_t *plan);
+/* Library version string. */
+SSU_EXTERN const char *ssu_b200_version(void);
+
+#endif /* UNIFRAC_B200_H */

@@ -65,6 +65,10 @@ def parse_test_su(path):
             vals = _numbers(m.group(3))
             if vals is not None:
                 entry["arrays"].setdefault(m.group(2), []).append(vals)
+        for m in re.finditer(r"bool\s+(\w+)\s*\[\d*\]\s*=\s*\{([^}]*)\}", body):
+            toks = [t.strip() for t in m.group(2).split(",") if t.strip()]
+            if all(t in ("0", "1", "true", "false") for t in toks):
+                entry["arrays"].setdefault(m.group(1), []).append([1.0 if t in ("1", "true") else 0.0 for t in toks])
         for m in re.finditer(r"std::vector<(bool|double|std::string)>\s+(\w+)\s*=\s*\{([^}]*)\}", body):
             kind, vname, content = m.groups()
             if kind == "bool":

@@ -1,0 +1,240 @@
+"""Parity of the CUDA path (through the C ABI of libssu_b200.so) with the
+oracle, on seeded inputs.
+
+Bars: fp64 methods within 1e-12 relative of the oracle (1e-13 absolute where
+the oracle value is 0); fp32 methods within 4x the reference fp32 build's own
+error against fp64 on the same input (measured with the oracle's fp32 mode),
+floored at 1e-6; NaN patterns identical."""
+import numpy as np
+import pytest
+
+import ssu_synth
+from conftest import matrix_from_stripes, rel_err, stripes_from_golden
+
+pytestmark = pytest.mark.gpu
+
+METHODS = ["unweighted", "unweighted_unnormalized", "weighted_normalized", "weighted_unnormalized", "generalized"]
+FP64_REL = 1e-12
+FP64_ABS = 1e-13
+
+
+def _case(seed, n_tips=90, n_samples=37, density=0.12, drop=7):
+    tree = ssu_synth.random_binary_tree(n_tips, 0.1, seed)
+    table = ssu_synth.geometric_table(tree.tip_names()[: n_tips - drop], n_samples, density, 10.0, seed + 3)
+    return tree, table
+
+
+def check_fp64(gpu, ref):
+    r, z = rel_err(gpu, ref)
+    assert r <= FP64_REL, f"max rel err {r:.3e}"
+    assert z <= FP64_ABS, f"max abs err at zeros {z:.3e}"
+
+
+def check_fp32(gpu32, oracle, tree, table, method, **kw):
+    o64 = oracle.oracle_one_off(tree, table, method + "_fp64", **kw)["matrix"]
+    o32 = oracle.oracle_one_off(tree, table, method + "_fp32", **kw)["matrix"]
+    ref_err, ref_zero = rel_err(o32, o64)
+    ours, ours_zero = rel_err(gpu32, o64)
+    assert ours <= max(4 * ref_err, 1e-6), (ours, ref_err)
+    assert ours_zero <= max(4 * ref_zero, 1e-6)
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("vaw", [False, True])
+@pytest.mark.parametrize("bypass", [False, True])
+def test_fp64_matches_oracle(ssu, oracle_mod, method, vaw, bypass):
+    tree, table = _case(21)
+    kw = dict(variance_adjust=vaw, bypass_tips=bypass, alpha=0.5)
+    gpu, ids = ssu.one_off_matrix(tree, table, method + "_fp64", **kw)
+    assert ids == table.sample_ids
+    check_fp64(gpu, oracle_mod.oracle_one_off(tree, table, method + "_fp64", **kw)["matrix"])
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("vaw", [False, True])
+def test_fp32_within_reference_fp32_error(ssu, oracle_mod, method, vaw):
+    tree, table = _case(22)
+    kw = dict(variance_adjust=vaw, alpha=0.5)
+    gpu, _ = ssu.one_off_matrix(tree, table, method + "_fp32", **kw)
+    assert gpu.dtype == np.float32
+    check_fp32(gpu, oracle_mod, tree, table, method, **kw)
+
+
+@pytest.mark.parametrize("alpha", [0.0, 0.25, 0.5, 1.0, 1.5])
+def test_generalized_alphas(ssu, oracle_mod, alpha):
+    tree, table = _case(23)
+    for vaw in (False, True):
+        gpu, _ = ssu.one_off_matrix(tree, table, "generalized_fp64", variance_adjust=vaw, alpha=alpha)
+        check_fp64(gpu, oracle_mod.oracle_one_off(tree, table, "generalized_fp64", variance_adjust=vaw,
+                                                  alpha=alpha)["matrix"])
+
+
+@pytest.mark.parametrize("n", [2, 3, 5, 63, 64, 65, 127, 128, 129, 200, 255, 256, 257])
+@pytest.mark.parametrize("method", ["unweighted_fp64", "weighted_normalized_fp64", "generalized_fp64"])
+def test_tile_boundaries(ssu, oracle_mod, n, method):
+    tree, table = _case(100 + n, n_tips=70, n_samples=n, density=0.2, drop=0)
+    gpu, _ = ssu.one_off_matrix(tree, table, method, alpha=0.5)
+    check_fp64(gpu, oracle_mod.oracle_one_off(tree, table, method, alpha=0.5)["matrix"])
+    assert np.all(np.diag(gpu) == 0)
+    np.testing.assert_array_equal(gpu, gpu.T)
+
+
+GOLDEN_CASES = [
+    ("test_unweighted_unifrac", "", "unweighted_fp64", {}),
+    ("test_unweighted_unifrac", "", "unweighted_fp32", {}),
+    ("test_unweighted_unifrac_fast", "", "unweighted_fp64", {"bypass_tips": True}),
+    ("test_unnormalized_unweighted_unifrac", "", "unweighted_unnormalized_fp64", {}),
+    ("test_unnormalized_weighted_unifrac", "", "weighted_unnormalized_fp64", {}),
+    ("test_normalized_weighted_unifrac", "", "weighted_normalized_fp64", {}),
+    ("test_normalized_weighted_unifrac", "", "weighted_normalized_fp32", {}),
+    ("test_generalized_unifrac", "w_", "generalized_fp64", {"alpha": 1.0}),
+    ("test_generalized_unifrac", "d0_", "generalized_fp64", {"alpha": 0.0}),
+    ("test_generalized_unifrac", "d05_", "generalized_fp64", {"alpha": 0.5}),
+    ("test_vaw_unifrac_weighted_normalized", "w_", "weighted_normalized_fp64", {"variance_adjust": True}),
+]
+
+
+@pytest.mark.parametrize("func,prefix,method,kw", GOLDEN_CASES)
+def test_reference_goldens_through_c_abi(ssu, golden, test_tree, test_table, func, prefix, method, kw):
+    exp = stripes_from_golden(golden["test_su"][func], prefix)
+    gpu, _ = ssu.one_off_matrix(test_tree, test_table, method, **kw)
+    np.testing.assert_allclose(gpu, matrix_from_stripes(exp, 6), atol=1e-6, rtol=0)
+    stripes, meta = ssu.partial(test_tree, test_table, method, 0, 3, **kw)
+    np.testing.assert_allclose(stripes, exp, atol=1e-6, rtol=0)
+    assert meta["total"] == 3 and meta["upper"]
+
+
+def test_faith_goldens_through_c_abi(ssu, golden, test_table):
+    exp = golden["test_su"]["test_faith_pd"]["arrays"]["exp"][0]
+    for tre in ("test_faith.tre", "test_faith_shear.tre"):
+        tree = ssu_synth.parse_newick(golden["trees"][tre])
+        vals, ids = ssu.faith_pd(tree, test_table)
+        np.testing.assert_allclose(vals, exp, atol=1e-6, rtol=0)
+        assert ids == test_table.sample_ids
+
+
+@pytest.mark.parametrize("n", [6, 7, 40, 41, 300])
+def test_partial_windows_and_condensed(ssu, oracle_mod, n):
+    tree, table = _case(40 + n, n_tips=80, n_samples=n, density=0.2, drop=0)
+    method = "weighted_normalized_fp64"
+    s_total = (n + 1) // 2
+    windows = [(0, s_total), (0, 1), (s_total - 1, s_total), (s_total // 3, max(s_total // 3 + 1, 2 * s_total // 3))]
+    for start, stop in windows:
+        gpu, meta = ssu.partial(tree, table, method, start, stop)
+        ref = oracle_mod.oracle_one_off(tree, table, method, stripe_start=start, stripe_stop=stop)["stripes"]
+        check_fp64(gpu, ref)
+        assert (meta["start"], meta["stop"], meta["total"]) == (start, stop, s_total)
+    cf, ids, upper = ssu.one_off(tree, table, method)
+    full = oracle_mod.oracle_one_off(tree, table, method)["matrix"]
+    iu = np.triu_indices(n, 1)
+    check_fp64(cf, full[iu])
+    assert upper and len(cf) == n * (n - 1) // 2
+
+
+def test_partial_out_of_range_is_an_error_not_an_exit(ssu, test_tree, test_table):
+    with pytest.raises(ssu.SSUError) as e:
+        ssu.partial(test_tree, test_table, "unweighted_fp64", 0, 4)
+    assert e.value.status == 6
+
+
+def test_faith_filters_empty_samples(ssu, oracle_mod):
+    tree, table = _case(51, n_samples=30)
+    dense = table.dense()
+    dense[:, [0, 7]] = 0
+    flat = np.flatnonzero(dense.ravel() > 0)
+    t2 = ssu_synth.make_table(table.obs_ids, table.n_samples, flat, dense.ravel()[flat])
+    vals, ids = ssu.faith_pd(tree, t2)
+    ref = oracle_mod.oracle_faith_pd(tree, t2)
+    assert ids == [t2.sample_ids[i] for i in ref["kept"]]
+    np.testing.assert_allclose(vals, ref["values"], rtol=1e-12, atol=0)
+
+
+def test_empty_samples_give_reference_nan_pattern(ssu, oracle_mod):
+    tree, table = _case(52, n_samples=20)
+    dense = table.dense()
+    dense[:, [3, 4]] = 0
+    flat = np.flatnonzero(dense.ravel() > 0)
+    t2 = ssu_synth.make_table(table.obs_ids, table.n_samples, flat, dense.ravel()[flat])
+    for m in METHODS:
+        gpu, _ = ssu.one_off_matrix(tree, t2, m + "_fp64", alpha=0.5)
+        ref = oracle_mod.oracle_one_off(tree, t2, m + "_fp64", alpha=0.5)["matrix"]
+        assert np.array_equal(np.isnan(gpu), np.isnan(ref)), m
+        check_fp64(gpu, ref)
+
+
+def test_dense_pair(ssu, golden, oracle_mod):
+    tree = ssu_synth.parse_newick(golden["trees"]["test.tre"])
+    obs = ["GG_OTU_1", "GG_OTU_2", "GG_OTU_3", "GG_OTU_4", "GG_OTU_5"]
+    s1, s3 = [0, 5, 0, 2, 0], [1, 0, 1, 1, 1]
+    d = ssu.dense_pair(tree, obs, s1, s3, "unweighted_fp64")
+    flat = [i * 2 + j for i in range(5) for j, v in enumerate((s1[i], s3[i])) if v > 0]
+    vals = [(s1, s3)[f % 2][f // 2] for f in flat]
+    t = ssu_synth.make_table(obs, 2, np.array(flat), np.array(vals, dtype=float))
+    exp = oracle_mod.oracle_one_off(tree, t, "unweighted_fp64")["matrix"][0, 1]
+    assert abs(d - exp) <= 1e-12 * abs(exp)
+    d32 = ssu.dense_pair(tree, obs, s1, s3, "unweighted")
+    assert abs(d32 - 0.57142857) < 1e-6  # test/capi_inmem_test.c exp13
+
+
+def test_unnormalized_sample_counts(ssu, oracle_mod):
+    tree, table = _case(53)
+    for m in ("weighted_unnormalized_fp64", "weighted_normalized_fp64", "generalized_fp64"):
+        gpu, _ = ssu.one_off_matrix(tree, table, m, normalize=False, alpha=0.5)
+        check_fp64(gpu, oracle_mod.oracle_one_off(tree, table, m, normalize=False, alpha=0.5)["matrix"])
+
+
+def test_plan_api_matches_one_off(ssu):
+    tree, table = _case(54, n_samples=150)
+    for m in ("weighted_normalized_fp64", "unweighted_fp32"):
+        plan = ssu.Plan(tree, table, m)
+        plan.set_timing(True)
+        plan.execute()
+        out = plan.result()
+        e, p, f = plan.stage_ms()
+        assert p > 0 and e >= 0
+        ref, _ = ssu.one_off_matrix(tree, table, m)
+        np.testing.assert_array_equal(out, ref)
+        assert plan.work_units() == 150 * 149 // 2 * plan.n_embedded()
+        assert plan.launches() >= 2
+        plan.close()
+
+
+def test_mmap_backed_result(ssu, tmp_path):
+    tree, table = _case(55)
+    a, _ = ssu.one_off_matrix(tree, table, "weighted_unnormalized_fp64", mmap_dir=str(tmp_path))
+    b, _ = ssu.one_off_matrix(tree, table, "weighted_unnormalized_fp64")
+    np.testing.assert_array_equal(a, b)
+
+
+def test_rarefaction_keeps_deep_samples(ssu):
+    tree, table = _case(56, n_samples=25, density=0.5)
+    totals = table.dense().sum(axis=0)
+    depth = int(np.percentile(totals, 40))
+    ssu.lib().ssu_set_random_seed(7)
+    m, ids = ssu.one_off_matrix(tree, table, "unweighted_fp64", subsample_depth=depth)
+    keep = [table.sample_ids[j] for j in range(table.n_samples) if totals[j] >= depth]
+    assert ids == keep
+    assert m.shape == (len(keep), len(keep))
+    assert np.all(np.isfinite(m))
+
+
+def test_config2_full_size_stripe_windows(ssu, oracle_mod):
+    """Full 20,000-tip x 2,048-sample config-2 input: the GPU matrix against
+    the oracle on the first and last stripes, plus matrix properties."""
+    tree, table = ssu_synth.config2()
+    n = table.n_samples
+    s_total = (n + 1) // 2
+    for m in ("weighted_normalized_fp64", "weighted_unnormalized_fp64"):
+        gpu, _ = ssu.one_off_matrix(tree, table, m)
+        assert np.all(np.diag(gpu) == 0)
+        np.testing.assert_array_equal(gpu, gpu.T)
+        assert np.all(np.isfinite(gpu))
+        for start, stop in [(0, 2), (s_total - 2, s_total)]:
+            ref = oracle_mod.oracle_one_off(tree, table, m, stripe_start=start, stripe_stop=stop)["stripes"]
+            got = np.array([[gpu[k, (k + s + 1) % n] for k in range(n)] for s in range(start, stop)])
+            check_fp64(got, ref)
+    gpu32, _ = ssu.one_off_matrix(tree, table, "weighted_normalized_fp32")
+    ref = oracle_mod.oracle_one_off(tree, table, "weighted_normalized_fp64", stripe_start=0, stripe_stop=1)["stripes"]
+    got = np.array([gpu32[k, (k + 1) % n] for k in range(n)], dtype=np.float64)
+    r, _ = rel_err(got, ref[0])
+    assert r < 1e-4

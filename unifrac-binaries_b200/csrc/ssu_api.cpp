@@ -1,0 +1,838 @@
+// C ABI of the B200 UniFrac engine (include/unifrac_b200.h).
+//
+// Host orchestration mirrors the reference's API layer (src/api.cpp):
+// validate table and tree, shear and collapse the tree to the table's
+// features, run the device plan, and hand back malloc'ed results that the
+// caller releases through destroy_*().  Nothing here exits the process.
+#include "unifrac_b200.h"
+
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fcntl.h>
+#include <fstream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <sys/mman.h>
+#include <unistd.h>
+#include <unordered_set>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "ssu_engine.hpp"
+#include "ssu_table.hpp"
+#include "ssu_tree.hpp"
+
+namespace {
+
+constexpr uint32_t kMmapFdMask = 0x0fff;  // src/api.cpp:27-28
+constexpr uint32_t kMmapFlag = 0x1000;
+
+std::atomic<uint64_t> g_seed{5489u};
+
+bool env_yes(const char *name) {
+    const char *v = std::getenv(name);
+    if (!v) return false;
+    const std::string s(v);
+    return !(s == "NO" || s == "N" || s == "no" || s == "n" || s == "NEVER" || s == "never");
+}
+
+// UNIFRAC_TIMING_INFO step timer, as the reference's SETUP_TDBG/TDBG_STEP
+// (src/api.cpp:34-49) with millisecond resolution.
+struct StepTimer {
+    const char *what;
+    bool on;
+    std::chrono::steady_clock::time_point t0;
+    explicit StepTimer(const char *w) : what(w), on(env_yes("UNIFRAC_TIMING_INFO")), t0(std::chrono::steady_clock::now()) {
+        if (on) std::printf("INFO (unifrac): Starting %s\n", what);
+    }
+    void step(const char *name) {
+        if (!on) return;
+        auto t1 = std::chrono::steady_clock::now();
+        std::printf("INFO (unifrac): dt %8.3f ms : Completed %s.%s\n",
+                    std::chrono::duration<double, std::milli>(t1 - t0).count(), what, name);
+        t0 = t1;
+    }
+};
+
+// Select the device as the reference's OpenACC runtime does (ACC_DEVICE_NUM).
+bool select_device(std::string &err) {
+    static std::atomic<bool> announced{false};
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        err = "no CUDA device available";
+        return false;
+    }
+    if (const char *d = std::getenv("ACC_DEVICE_NUM")) {
+        const int id = std::atoi(d);
+        if (id >= 0 && id < count && cudaSetDevice(id) != cudaSuccess) {
+            err = "cudaSetDevice failed";
+            return false;
+        }
+    }
+    if (env_yes("UNIFRAC_GPU_INFO") && !announced.exchange(true)) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceProp p;
+        if (cudaGetDeviceProperties(&p, dev) == cudaSuccess)
+            std::printf("INFO (unifrac): Using GPU %d (%s), B200 engine\n", dev, p.name);
+    }
+    return true;
+}
+
+void report(const std::string &where, const std::string &err) {
+    if (!err.empty()) std::fprintf(stderr, "unifrac-b200: %s: %s\n", where.c_str(), err.c_str());
+}
+
+ComputeStatus is_fp64_method(const char *m, bool &fp64) {
+    ssu::Method method;
+    if (!ssu::parse_method(m, method, fp64)) return unknown_method;
+    return okay;
+}
+
+char **copy_ids(const std::vector<std::string> &ids) {
+    char **out = static_cast<char **>(std::malloc(sizeof(char *) * (ids.size() ? ids.size() : 1)));
+    for (size_t i = 0; i < ids.size(); i++) out[i] = strdup(ids[i].c_str());
+    return out;
+}
+
+ssu::Table table_from(const support_biom_t *t) {
+    return ssu::Table::borrow(static_cast<uint32_t>(t->n_obs), static_cast<uint32_t>(t->n_samples), t->indptr,
+                              t->indices, t->data, t->obs_ids, t->sample_ids);
+}
+
+ssu::BPTree tree_from(const support_bptree_t *t) {
+    return ssu::BPTree::from_arrays(t->structure, t->lengths, t->names, t->n_parens);
+}
+
+// VALIDATE_TREE_TABLE (src/api.cpp:94-100)
+ComputeStatus validate(const ssu::Table &table, const ssu::BPTree &tree) {
+    if (table.n_samples == 0 || table.n_obs == 0) return table_empty;
+    const std::unordered_set<std::string> tips = tree.tip_names();
+    for (const std::string &id : table.obs_ids)
+        if (!tips.count(id)) return table_and_tree_do_not_overlap;
+    return okay;
+}
+
+// SYNC_TREE_TABLE (src/api.cpp:90-92) + flattening for the device.
+ssu::FlatTree sync_tree(const ssu::Table &table, const ssu::BPTree &tree, bool bypass_tips) {
+    const std::unordered_set<std::string> keep(table.obs_ids.begin(), table.obs_ids.end());
+    const ssu::BPTree sheared = tree.shear(keep).collapse();
+    return ssu::flatten(sheared, table.obs_index(), bypass_tips);
+}
+
+struct Request {
+    const char *method;
+    bool vaw;
+    double alpha;
+    bool bypass;
+    bool normalize;
+};
+
+ComputeStatus make_plan(const ssu::Table &table, const ssu::BPTree &tree, const Request &r,
+                        std::unique_ptr<ssu::Plan> &plan, StepTimer &timer) {
+    ssu::MethodSpec spec;
+    if (!ssu::parse_method(r.method, spec.method, spec.fp64)) return unknown_method;
+    spec.vaw = r.vaw;
+    spec.alpha = r.alpha;
+    spec.bypass_tips = r.bypass;
+    spec.normalize = r.normalize;
+    std::string err;
+    if (!select_device(err)) {
+        report("device", err);
+        return output_error;
+    }
+    const ssu::FlatTree flat = sync_tree(table, tree, r.bypass);
+    timer.step("sync_tree_table");
+    ssu::Plan *p = nullptr;
+    const int rc = ssu::Plan::create(table, flat, spec, nullptr, &p, err);
+    if (rc) {
+        report("plan", err);
+        return static_cast<ComputeStatus>(rc);
+    }
+    plan.reset(p);
+    timer.step("upload");
+    return okay;
+}
+
+template <class TReal, class TMat>
+bool alloc_full(TMat *&result, const std::vector<std::string> &ids, const char *mmap_dir) {
+    result = static_cast<TMat *>(std::malloc(sizeof(TMat)));
+    result->n_samples = static_cast<uint32_t>(ids.size());
+    result->flags = 0;
+    result->sample_ids = copy_ids(ids);
+    const uint64_t n = ids.size();
+    const uint64_t bytes = sizeof(TReal) * n * n;
+    if (mmap_dir && mmap_dir[0]) {
+        std::string tmpl = std::string(mmap_dir) + "/su_mmap_XXXXXX";
+        int fd = mkstemp(&tmpl[0]);
+        result->matrix = nullptr;
+        if (fd >= 0) {
+            unlink(tmpl.c_str());
+            if (ftruncate(fd, static_cast<off_t>(bytes)) == 0) {
+                void *m = mmap(nullptr, bytes ? bytes : 1, PROT_READ | PROT_WRITE, MAP_SHARED | MAP_NORESERVE, fd, 0);
+                if (m != MAP_FAILED) {
+                    result->matrix = static_cast<TReal *>(m);
+                    result->flags = (static_cast<uint32_t>(fd) & kMmapFdMask) | kMmapFlag;
+                }
+            }
+            if (!result->matrix) close(fd);
+        }
+    } else {
+        result->matrix = static_cast<TReal *>(std::malloc(bytes ? bytes : 1));
+    }
+    return result->matrix != nullptr;
+}
+
+template <class TMat, class TReal>
+void destroy_full(TMat **result) {
+    if (!result || !*result) return;
+    TMat *r = *result;
+    for (uint32_t i = 0; i < r->n_samples; i++) std::free(r->sample_ids[i]);
+    std::free(r->sample_ids);
+    if (r->matrix) {
+        if ((r->flags & kMmapFlag) == 0) {
+            std::free(r->matrix);
+        } else {
+            const uint64_t n = r->n_samples;
+            munmap(r->matrix, sizeof(TReal) * n * n ? sizeof(TReal) * n * n : 1);
+            close(static_cast<int>(r->flags & kMmapFdMask));
+        }
+        r->matrix = nullptr;
+    }
+    std::free(r);
+    *result = nullptr;
+}
+
+// one_off_matrix_T (src/api.cpp:639-696) over an already validated table.
+template <class TReal, class TMat>
+ComputeStatus full_matrix(const ssu::Table &table, const ssu::BPTree &tree, const Request &r, const char *mmap_dir,
+                          TMat **result) {
+    StepTimer timer("one_off_matrix_inmem");
+    std::unique_ptr<ssu::Plan> plan;
+    ComputeStatus st = make_plan(table, tree, r, plan, timer);
+    if (st != okay) return st;
+    bool allocated = false;
+    if (*result == nullptr) {
+        if (!alloc_full<TReal, TMat>(*result, table.sample_ids, mmap_dir)) {
+            destroy_full<TMat, TReal>(result);
+            report("one_off_matrix", "result allocation failed");
+            return output_error;
+        }
+        allocated = true;
+    }
+    if ((*result)->matrix == nullptr || (*result)->n_samples != table.n_samples) {
+        report("one_off_matrix", "caller-provided result does not match the table");
+        return output_error;
+    }
+    std::string err;
+    const int rc = plan->run_full((*result)->matrix, sizeof(TReal) == 8, err);
+    timer.step("stripes_to_matrix");
+    if (rc) {
+        report("one_off_matrix", err);
+        if (allocated) destroy_full<TMat, TReal>(result);
+        return static_cast<ComputeStatus>(rc);
+    }
+    return okay;
+}
+
+// one_off_matrix_v3_T (src/api.cpp:700-717): optional rarefaction first.
+template <class TReal, class TMat>
+ComputeStatus full_matrix_v3(const support_biom_t *table_data, const support_bptree_t *tree_data, const Request &r,
+                             bool want_fp64, unsigned int subsample_depth, bool with_replacement, const char *mmap_dir,
+                             TMat **result) {
+    bool fp64 = false;
+    ComputeStatus st = is_fp64_method(r.method, fp64);
+    if (st != okay) return st;
+    if (fp64 != want_fp64) return invalid_method;
+    if (!table_data || table_data->n_samples <= 0 || table_data->n_obs <= 0) return table_empty;
+    if (!tree_data) return tree_missing;
+    ssu::Table table = table_from(table_data);
+    const ssu::BPTree tree = tree_from(tree_data);
+    st = validate(table, tree);
+    if (st != okay) return st;
+    if (subsample_depth > 0) {
+        ssu::Table sub = table.rarefied(subsample_depth, with_replacement, g_seed.load());
+        if (sub.n_samples == 0 || sub.n_obs == 0) return table_empty;
+        return full_matrix<TReal, TMat>(sub, tree, r, mmap_dir, result);
+    }
+    return full_matrix<TReal, TMat>(table, tree, r, mmap_dir, result);
+}
+
+ComputeStatus condensed(const ssu::Table &table, const ssu::BPTree &tree, const Request &r, mat_t **result) {
+    StepTimer timer("one_off");
+    std::unique_ptr<ssu::Plan> plan;
+    ComputeStatus st = make_plan(table, tree, r, plan, timer);
+    if (st != okay) return st;
+    const uint64_t n = table.n_samples;
+    mat_t *m = static_cast<mat_t *>(std::malloc(sizeof(mat_t)));
+    m->n_samples = table.n_samples;
+    m->cf_size = static_cast<unsigned int>(n * (n - 1) / 2);
+    m->is_upper_triangle = true;
+    m->condensed_form = static_cast<double *>(std::malloc(sizeof(double) * (m->cf_size ? m->cf_size : 1)));
+    m->sample_ids = copy_ids(table.sample_ids);
+    std::string err;
+    const int rc = plan->run_condensed(m->condensed_form, err);
+    timer.step("stripes_to_condensed_form");
+    if (rc) {
+        report("one_off", err);
+        destroy_mat(&m);
+        return static_cast<ComputeStatus>(rc);
+    }
+    *result = m;
+    return okay;
+}
+
+ComputeStatus partial_stripes(const ssu::Table &table, const ssu::BPTree &tree, const Request &r,
+                              unsigned int stripe_start, unsigned int stripe_stop, partial_mat_t **result) {
+    StepTimer timer("partial");
+    const uint32_t n_stripes = (table.n_samples + 1) / 2;
+    if (stripe_stop <= stripe_start) stripe_stop = n_stripes;  // as set_tasks, src/api.cpp:455-456
+    if (stripe_stop > n_stripes || stripe_start >= n_stripes) {
+        report("partial", "stopping stripe is out of bounds, max " + std::to_string(n_stripes));
+        return output_error;
+    }
+    std::unique_ptr<ssu::Plan> plan;
+    ComputeStatus st = make_plan(table, tree, r, plan, timer);
+    if (st != okay) return st;
+    partial_mat_t *p = static_cast<partial_mat_t *>(std::malloc(sizeof(partial_mat_t)));
+    p->n_samples = table.n_samples;
+    p->sample_ids = copy_ids(table.sample_ids);
+    p->stripe_start = stripe_start;
+    p->stripe_stop = stripe_stop;
+    p->stripe_total = n_stripes;
+    p->is_upper_triangle = true;
+    p->stripes = static_cast<double **>(std::malloc(sizeof(double *) * (stripe_stop - stripe_start)));
+    for (uint32_t s = 0; s < stripe_stop - stripe_start; s++)
+        p->stripes[s] = static_cast<double *>(std::calloc(table.n_samples, sizeof(double)));
+    std::string err;
+    const int rc = plan->run_stripes(stripe_start, stripe_stop, p->stripes, err);
+    timer.step("process_stripes");
+    if (rc) {
+        report("partial", err);
+        destroy_partial_mat(&p);
+        return static_cast<ComputeStatus>(rc);
+    }
+    *result = p;
+    return okay;
+}
+
+ComputeStatus inmem_common(const support_biom_t *table_data, const support_bptree_t *tree_data, ssu::Table &table,
+                           ssu::BPTree &tree) {
+    if (!table_data || table_data->n_samples <= 0 || table_data->n_obs <= 0) return table_empty;
+    if (!tree_data) return tree_missing;
+    table = table_from(table_data);
+    tree = tree_from(tree_data);
+    return validate(table, tree);
+}
+
+// faith_pd_one_off (src/api.cpp:569-603) over an in-memory table.
+ComputeStatus faith_pd(const ssu::Table &table, const ssu::BPTree &tree, r_vec **result) {
+    StepTimer timer("faith_pd");
+    ssu::Table nz = table.filtered(1.0);
+    r_vec *rv = static_cast<r_vec *>(std::malloc(sizeof(r_vec)));
+    if (nz.n_samples == 0 || nz.n_obs == 0) {
+        std::fprintf(stderr, "WARNING: All samples had zero counts. Forcing zero result.\n");
+        rv->n_samples = table.n_samples;
+        rv->values = static_cast<double *>(std::calloc(table.n_samples ? table.n_samples : 1, sizeof(double)));
+        rv->sample_ids = copy_ids(table.sample_ids);
+        *result = rv;
+        return okay;
+    }
+    if (nz.n_samples != table.n_samples || nz.n_obs != table.n_obs)
+        std::fprintf(stderr, "WARNING: Some samples had zero counts and were filtered out.\n");
+    rv->n_samples = nz.n_samples;
+    rv->values = static_cast<double *>(std::calloc(nz.n_samples, sizeof(double)));
+    rv->sample_ids = copy_ids(nz.sample_ids);
+    std::string err;
+    if (!select_device(err)) {
+        report("faith_pd", err);
+        destroy_results_vec(&rv);
+        return output_error;
+    }
+    const ssu::FlatTree flat = sync_tree(nz, tree, false);
+    timer.step("sync_tree_table");
+    ssu::Plan *p = nullptr;
+    int rc = ssu::Plan::create_faith(nz, flat, nullptr, &p, err);
+    if (!rc) {
+        std::unique_ptr<ssu::Plan> plan(p);
+        rc = plan->run_faith(rv->values, err);
+    }
+    timer.step("faith_pd");
+    if (rc) {
+        report("faith_pd", err);
+        destroy_results_vec(&rv);
+        return static_cast<ComputeStatus>(rc);
+    }
+    *result = rv;
+    return okay;
+}
+
+bool file_exists(const char *path) {
+    if (!path) return false;
+    std::ifstream f(path);
+    return f.good();
+}
+
+bool read_text(const char *path, std::string &out) {
+    std::ifstream f(path);
+    if (!f.good()) return false;
+    std::stringstream ss;
+    ss << f.rdbuf();
+    out = ss.str();
+    return true;
+}
+
+// BIOM-HDF5 tables need an HDF5 reader, which this build does not carry.
+ComputeStatus load_biom(const char *biom_filename) {
+    std::fprintf(stderr,
+                 "unifrac-b200: %s: BIOM-HDF5 input is not available in this build; use the in-memory "
+                 "entry points\n",
+                 biom_filename);
+    return table_missing;
+}
+
+struct OpaqueTree {
+    ssu::BPTree tree;
+};
+
+ComputeStatus file_front(const char *biom_filename, const char *tree_filename) {
+    if (!file_exists(biom_filename)) return table_missing;
+    if (!file_exists(tree_filename)) return tree_missing;
+    std::string text;
+    ssu::BPTree tree;
+    if (!read_text(tree_filename, text) || !ssu::BPTree::from_newick(text, tree)) return tree_missing;
+    return load_biom(biom_filename);
+}
+
+}  // namespace
+
+// =================================================== reference-compatible
+
+extern "C" {
+
+void ssu_set_random_seed(unsigned int new_seed) { g_seed.store(new_seed); }
+
+IOStatus read_bptree_opaque(const char *tree_filename, opaque_bptree_t **tree_data) {
+    if (tree_data == nullptr) return unexpected_end;
+    std::string text;
+    if (!read_text(tree_filename, text)) return open_error;
+    OpaqueTree *t = new OpaqueTree();
+    if (!ssu::BPTree::from_newick(text, t->tree)) {
+        delete t;
+        return unexpected_end;
+    }
+    *tree_data = reinterpret_cast<opaque_bptree_t *>(t);
+    return read_okay;
+}
+
+void load_bptree_opaque(const char *newick, opaque_bptree_t **tree_data) {
+    OpaqueTree *t = new OpaqueTree();
+    if (!newick || !ssu::BPTree::from_newick(newick, t->tree)) t->tree = ssu::BPTree();
+    *tree_data = reinterpret_cast<opaque_bptree_t *>(t);
+}
+
+void convert_bptree_opaque(const support_bptree_t *in_tree, opaque_bptree_t **tree_data) {
+    OpaqueTree *t = new OpaqueTree();
+    t->tree = tree_from(in_tree);
+    *tree_data = reinterpret_cast<opaque_bptree_t *>(t);
+}
+
+void destroy_bptree_opaque(opaque_bptree_t **tree_data) {
+    if (tree_data && *tree_data) {
+        delete reinterpret_cast<OpaqueTree *>(*tree_data);
+        *tree_data = nullptr;
+    }
+}
+
+int get_bptree_opaque_els(opaque_bptree_t *tree_data) {
+    if (!tree_data) return 0;
+    return static_cast<int>(reinterpret_cast<OpaqueTree *>(tree_data)->tree.tip_names().size());
+}
+
+void destroy_mat(mat_t **result) {
+    if (!result || !*result) return;
+    mat_t *m = *result;
+    for (unsigned int i = 0; i < m->n_samples; i++) std::free(m->sample_ids[i]);
+    std::free(m->sample_ids);
+    std::free(m->condensed_form);
+    std::free(m);
+    *result = nullptr;
+}
+
+void destroy_mat_full_fp64(mat_full_fp64_t **result) { destroy_full<mat_full_fp64_t, double>(result); }
+void destroy_mat_full_fp32(mat_full_fp32_t **result) { destroy_full<mat_full_fp32_t, float>(result); }
+
+void destroy_partial_mat(partial_mat_t **result) {
+    if (!result || !*result) return;
+    partial_mat_t *p = *result;
+    if (p->sample_ids) {
+        for (uint32_t i = 0; i < p->n_samples; i++) std::free(p->sample_ids[i]);
+        std::free(p->sample_ids);
+    }
+    if (p->stripes) {
+        for (uint32_t s = 0; s < p->stripe_stop - p->stripe_start; s++) std::free(p->stripes[s]);
+        std::free(p->stripes);
+    }
+    std::free(p);
+    *result = nullptr;
+}
+
+void destroy_partial_dyn_mat(partial_dyn_mat_t **result) {
+    if (!result || !*result) return;
+    partial_dyn_mat_t *p = *result;
+    if (p->sample_ids) {
+        for (uint32_t i = 0; i < p->n_samples; i++) std::free(p->sample_ids[i]);
+        std::free(p->sample_ids);
+    }
+    if (p->stripes) {
+        for (uint32_t s = 0; s < p->stripe_stop - p->stripe_start; s++) std::free(p->stripes[s]);
+        std::free(p->stripes);
+    }
+    std::free(p->offsets);
+    std::free(p->filename);
+    std::free(p);
+    *result = nullptr;
+}
+
+void destroy_results_vec(r_vec **result) {
+    if (!result || !*result) return;
+    r_vec *r = *result;
+    for (unsigned int i = 0; i < r->n_samples; i++) std::free(r->sample_ids[i]);
+    std::free(r->sample_ids);
+    std::free(r->values);
+    std::free(r);
+    *result = nullptr;
+}
+
+ComputeStatus one_off_matrix_inmem_v3(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                      const char *unifrac_method, bool variance_adjust, double alpha,
+                                      bool bypass_tips, bool normalize_sample_counts, unsigned int,
+                                      unsigned int subsample_depth, bool subsample_with_replacement,
+                                      const char *mmap_dir, mat_full_fp64_t **result) {
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return full_matrix_v3<double, mat_full_fp64_t>(table_data, tree_data, r, true, subsample_depth,
+                                                    subsample_with_replacement, mmap_dir, result);
+}
+
+ComputeStatus one_off_matrix_inmem_v2(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                      const char *unifrac_method, bool variance_adjust, double alpha,
+                                      bool bypass_tips, unsigned int n_substeps, unsigned int subsample_depth,
+                                      bool subsample_with_replacement, const char *mmap_dir,
+                                      mat_full_fp64_t **result) {
+    return one_off_matrix_inmem_v3(table_data, tree_data, unifrac_method, variance_adjust, alpha, bypass_tips, true,
+                                   n_substeps, subsample_depth, subsample_with_replacement, mmap_dir, result);
+}
+
+ComputeStatus one_off_inmem(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                            const char *unifrac_method, bool variance_adjust, double alpha, bool bypass_tips,
+                            unsigned int n_substeps, mat_full_fp64_t **result) {
+    return one_off_matrix_inmem_v3(table_data, tree_data, unifrac_method, variance_adjust, alpha, bypass_tips, true,
+                                   n_substeps, 0, false, nullptr, result);
+}
+
+ComputeStatus one_off_matrix_inmem_fp32_v3(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                           const char *unifrac_method, bool variance_adjust, double alpha,
+                                           bool bypass_tips, bool normalize_sample_counts, unsigned int,
+                                           unsigned int subsample_depth, bool subsample_with_replacement,
+                                           const char *mmap_dir, mat_full_fp32_t **result) {
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return full_matrix_v3<float, mat_full_fp32_t>(table_data, tree_data, r, false, subsample_depth,
+                                                   subsample_with_replacement, mmap_dir, result);
+}
+
+ComputeStatus one_off_matrix_inmem_fp32_v2(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                           const char *unifrac_method, bool variance_adjust, double alpha,
+                                           bool bypass_tips, unsigned int n_substeps, unsigned int subsample_depth,
+                                           bool subsample_with_replacement, const char *mmap_dir,
+                                           mat_full_fp32_t **result) {
+    return one_off_matrix_inmem_fp32_v3(table_data, tree_data, unifrac_method, variance_adjust, alpha, bypass_tips,
+                                        true, n_substeps, subsample_depth, subsample_with_replacement, mmap_dir,
+                                        result);
+}
+
+ComputeStatus one_off_inmem_fp32(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                 const char *unifrac_method, bool variance_adjust, double alpha, bool bypass_tips,
+                                 unsigned int n_substeps, mat_full_fp32_t **result) {
+    return one_off_matrix_inmem_fp32_v3(table_data, tree_data, unifrac_method, variance_adjust, alpha, bypass_tips,
+                                        true, n_substeps, 0, false, nullptr, result);
+}
+
+// one_dense_pair (src/api.cpp:729-766)
+static ComputeStatus dense_pair(unsigned int n_obs, const char **obs_ids, const double *sample1,
+                                const double *sample2, const ssu::BPTree &tree, const char *unifrac_method,
+                                bool variance_adjust, double alpha, bool bypass_tips, bool normalize,
+                                double *result) {
+    bool fp64 = false;
+    ComputeStatus st = is_fp64_method(unifrac_method, fp64);
+    if (st != okay) return st;
+    ssu::Table table = ssu::Table::dense_pair(n_obs, obs_ids, sample1, sample2);
+    st = validate(table, tree);
+    if (st != okay) return st;
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize};
+    if (fp64) {
+        mat_full_fp64_t *m = nullptr;
+        st = full_matrix<double, mat_full_fp64_t>(table, tree, r, nullptr, &m);
+        if (st == okay) {
+            *result = m->matrix[1];
+            destroy_mat_full_fp64(&m);
+        }
+    } else {
+        mat_full_fp32_t *m = nullptr;
+        st = full_matrix<float, mat_full_fp32_t>(table, tree, r, nullptr, &m);
+        if (st == okay) {
+            *result = m->matrix[1];
+            destroy_mat_full_fp32(&m);
+        }
+    }
+    return st;
+}
+
+ComputeStatus one_dense_pair_v3t(unsigned int n_obs, const char **obs_ids, const double *sample1,
+                                 const double *sample2, const opaque_bptree_t *tree_data, const char *unifrac_method,
+                                 bool variance_adjust, double alpha, bool bypass_tips, bool normalize_sample_counts,
+                                 double *result) {
+    if (!tree_data) return tree_missing;
+    const ssu::BPTree &tree = reinterpret_cast<const OpaqueTree *>(tree_data)->tree;
+    return dense_pair(n_obs, obs_ids, sample1, sample2, tree, unifrac_method, variance_adjust, alpha, bypass_tips,
+                      normalize_sample_counts, result);
+}
+
+ComputeStatus one_dense_pair_v3(unsigned int n_obs, const char **obs_ids, const double *sample1,
+                                const double *sample2, const support_bptree_t *tree_data, const char *unifrac_method,
+                                bool variance_adjust, double alpha, bool bypass_tips, bool normalize_sample_counts,
+                                double *result) {
+    if (!tree_data) return tree_missing;
+    const ssu::BPTree tree = tree_from(tree_data);
+    return dense_pair(n_obs, obs_ids, sample1, sample2, tree, unifrac_method, variance_adjust, alpha, bypass_tips,
+                      normalize_sample_counts, result);
+}
+
+ComputeStatus one_dense_pair_v2t(unsigned int n_obs, const char **obs_ids, const double *sample1,
+                                 const double *sample2, const opaque_bptree_t *tree_data, const char *unifrac_method,
+                                 bool variance_adjust, double alpha, bool bypass_tips, double *result) {
+    return one_dense_pair_v3t(n_obs, obs_ids, sample1, sample2, tree_data, unifrac_method, variance_adjust, alpha,
+                              bypass_tips, true, result);
+}
+
+ComputeStatus one_dense_pair_v2(unsigned int n_obs, const char **obs_ids, const double *sample1,
+                                const double *sample2, const support_bptree_t *tree_data, const char *unifrac_method,
+                                bool variance_adjust, double alpha, bool bypass_tips, double *result) {
+    return one_dense_pair_v3(n_obs, obs_ids, sample1, sample2, tree_data, unifrac_method, variance_adjust, alpha,
+                             bypass_tips, true, result);
+}
+
+ComputeStatus one_off_v3(const char *biom_filename, const char *tree_filename, const char *, bool, double, bool,
+                         bool, unsigned int, mat_t **) {
+    return file_front(biom_filename, tree_filename);
+}
+
+ComputeStatus one_off_wtree_v3(const char *biom_filename, const opaque_bptree_t *tree_data, const char *, bool,
+                               double, bool, bool, unsigned int, mat_t **) {
+    if (!tree_data) return tree_missing;
+    if (!file_exists(biom_filename)) return table_missing;
+    return load_biom(biom_filename);
+}
+
+ComputeStatus one_off(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                      bool variance_adjust, double alpha, bool bypass_tips, unsigned int n_substeps, mat_t **result) {
+    return one_off_v3(biom_filename, tree_filename, unifrac_method, variance_adjust, alpha, bypass_tips, true,
+                      n_substeps, result);
+}
+
+ComputeStatus one_off_wtree(const char *biom_filename, const opaque_bptree_t *tree_data, const char *unifrac_method,
+                            bool variance_adjust, double alpha, bool bypass_tips, unsigned int n_substeps,
+                            mat_t **result) {
+    return one_off_wtree_v3(biom_filename, tree_data, unifrac_method, variance_adjust, alpha, bypass_tips, true,
+                            n_substeps, result);
+}
+
+ComputeStatus one_off_matrix_v3(const char *biom_filename, const char *tree_filename, const char *, bool, double,
+                                bool, bool, unsigned int, unsigned int, bool, const char *, mat_full_fp64_t **) {
+    return file_front(biom_filename, tree_filename);
+}
+
+ComputeStatus one_off_matrix_fp32_v3(const char *biom_filename, const char *tree_filename, const char *, bool,
+                                     double, bool, bool, unsigned int, unsigned int, bool, const char *,
+                                     mat_full_fp32_t **) {
+    return file_front(biom_filename, tree_filename);
+}
+
+ComputeStatus faith_pd_one_off(const char *biom_filename, const char *tree_filename, r_vec **) {
+    return file_front(biom_filename, tree_filename);
+}
+
+ComputeStatus partial_v3(const char *biom_filename, const char *tree_filename, const char *, bool, double, bool,
+                         bool, unsigned int, unsigned int, unsigned int, partial_mat_t **) {
+    return file_front(biom_filename, tree_filename);
+}
+
+ComputeStatus partial(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                      bool variance_adjust, double alpha, bool bypass_tips, unsigned int n_substeps,
+                      unsigned int stripe_start, unsigned int stripe_stop, partial_mat_t **result) {
+    return partial_v3(biom_filename, tree_filename, unifrac_method, variance_adjust, alpha, bypass_tips, true,
+                      n_substeps, stripe_start, stripe_stop, result);
+}
+
+// ================================================================ extensions
+
+ComputeStatus ssu_b200_one_off_inmem_v3(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                        const char *unifrac_method, bool variance_adjust, double alpha,
+                                        bool bypass_tips, bool normalize_sample_counts, unsigned int,
+                                        mat_t **result) {
+    bool fp64 = false;
+    ComputeStatus st = is_fp64_method(unifrac_method, fp64);
+    if (st != okay) return st;
+    ssu::Table table;
+    ssu::BPTree tree;
+    st = inmem_common(table_data, tree_data, table, tree);
+    if (st != okay) return st;
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return condensed(table, tree, r, result);
+}
+
+ComputeStatus ssu_b200_partial_inmem_v3(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                        const char *unifrac_method, bool variance_adjust, double alpha,
+                                        bool bypass_tips, bool normalize_sample_counts, unsigned int,
+                                        unsigned int stripe_start, unsigned int stripe_stop,
+                                        partial_mat_t **result) {
+    bool fp64 = false;
+    ComputeStatus st = is_fp64_method(unifrac_method, fp64);
+    if (st != okay) return st;
+    ssu::Table table;
+    ssu::BPTree tree;
+    st = inmem_common(table_data, tree_data, table, tree);
+    if (st != okay) return st;
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return partial_stripes(table, tree, r, stripe_start, stripe_stop, result);
+}
+
+ComputeStatus ssu_b200_faith_pd_inmem(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                      r_vec **result) {
+    ssu::Table table;
+    ssu::BPTree tree;
+    const ComputeStatus st = inmem_common(table_data, tree_data, table, tree);
+    if (st != okay) return st;
+    return faith_pd(table, tree, result);
+}
+
+int ssu_b200_shear_collapse(const support_bptree_t *in_tree, const char *const *names, int n_names,
+                            int do_collapse, bool *out_structure, double *out_lengths, const char **out_names,
+                            int *out_n) {
+    if (!in_tree || !out_n) return 1;
+    const ssu::BPTree tree = tree_from(in_tree);
+    std::unordered_set<std::string> keep;
+    if (names)
+        for (int i = 0; i < n_names; i++) keep.insert(names[i]);
+    else
+        keep = tree.tip_names();
+    const ssu::BPTree sheared = tree.shear(keep);
+    const ssu::BPTree r = do_collapse ? sheared.collapse() : sheared;
+    // names are handed back as pointers into the input tree's strings
+    std::unordered_map<std::string, const char *> by_name;
+    for (int i = 0; i < in_tree->n_parens; i++) by_name.emplace(in_tree->names[i], in_tree->names[i]);
+    *out_n = static_cast<int>(r.size());
+    for (uint32_t i = 0; i < r.size(); i++) {
+        out_structure[i] = r.open[i] != 0;
+        out_lengths[i] = r.length[i];
+        auto it = by_name.find(r.name[i]);
+        out_names[i] = it != by_name.end() ? it->second : "";
+    }
+    return 0;
+}
+
+int ssu_b200_tree_arrays(const opaque_bptree_t *tree_data, int capacity, bool *out_structure, double *out_lengths,
+                         const char **out_names, int *out_n) {
+    if (!tree_data || !out_n) return 1;
+    const ssu::BPTree &t = reinterpret_cast<const OpaqueTree *>(tree_data)->tree;
+    *out_n = static_cast<int>(t.size());
+    if (static_cast<int>(t.size()) > capacity) return 2;
+    for (uint32_t i = 0; i < t.size(); i++) {
+        out_structure[i] = t.open[i] != 0;
+        out_lengths[i] = t.length[i];
+        out_names[i] = t.name[i].c_str();
+    }
+    return 0;
+}
+
+struct ssu_b200_plan {
+    std::unique_ptr<ssu::Plan> plan;
+};
+
+ComputeStatus ssu_b200_plan_create(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                   const char *unifrac_method, bool variance_adjust, double alpha, bool bypass_tips,
+                                   bool normalize_sample_counts, ssu_b200_plan_t **plan) {
+    bool fp64 = false;
+    ComputeStatus st = is_fp64_method(unifrac_method, fp64);
+    if (st != okay) return st;
+    ssu::Table table;
+    ssu::BPTree tree;
+    st = inmem_common(table_data, tree_data, table, tree);
+    if (st != okay) return st;
+    StepTimer timer("plan_create");
+    auto *h = new ssu_b200_plan();
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    st = make_plan(table, tree, r, h->plan, timer);
+    if (st != okay) {
+        delete h;
+        return st;
+    }
+    // the plan owns copies of everything it needs on the device
+    if (h->plan->synchronize()) {
+        delete h;
+        return output_error;
+    }
+    *plan = h;
+    return okay;
+}
+
+ComputeStatus ssu_b200_plan_execute(ssu_b200_plan_t *plan, void *stream) {
+    if (!plan) return output_error;
+    return plan->plan->execute(stream) ? output_error : okay;
+}
+
+const void *ssu_b200_plan_device_result(const ssu_b200_plan_t *plan) {
+    return plan ? plan->plan->device_result() : nullptr;
+}
+
+ComputeStatus ssu_b200_plan_copy_result(ssu_b200_plan_t *plan, void *host_out, void *stream) {
+    if (!plan) return output_error;
+    return plan->plan->copy_result(host_out, stream) ? output_error : okay;
+}
+
+uint64_t ssu_b200_plan_work_units(const ssu_b200_plan_t *plan) { return plan ? plan->plan->work_units() : 0; }
+uint32_t ssu_b200_plan_n_samples(const ssu_b200_plan_t *plan) { return plan ? plan->plan->n_samples() : 0; }
+uint64_t ssu_b200_plan_n_embedded(const ssu_b200_plan_t *plan) { return plan ? plan->plan->n_embedded() : 0; }
+uint32_t ssu_b200_plan_launches(const ssu_b200_plan_t *plan) { return plan ? plan->plan->launches() : 0; }
+void ssu_b200_plan_set_timing(ssu_b200_plan_t *plan, int enable) {
+    if (plan) plan->plan->set_timing(enable != 0);
+}
+
+int ssu_b200_plan_stage_ms(ssu_b200_plan_t *plan, float *embed_ms, float *pair_ms, float *finalize_ms) {
+    if (!plan) return 1;
+    ssu::StageTimes t;
+    if (plan->plan->stage_times(t)) return 1;
+    if (embed_ms) *embed_ms = t.embed_ms;
+    if (pair_ms) *pair_ms = t.pair_ms;
+    if (finalize_ms) *finalize_ms = t.finalize_ms;
+    return 0;
+}
+
+void ssu_b200_plan_destroy(ssu_b200_plan_t **plan) {
+    if (plan && *plan) {
+        delete *plan;
+        *plan = nullptr;
+    }
+}
+
+const char *ssu_b200_plan_pair_kernel(const ssu_b200_plan_t *plan) {
+    return plan ? plan->plan->pair_kernel_name() : "";
+}
+
+const char *ssu_b200_version(void) { return "unifrac-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

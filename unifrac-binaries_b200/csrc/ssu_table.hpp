@@ -1,0 +1,59 @@
+// Host-side feature table for the B200 UniFrac engine: an observation-major
+// CSR (the reference's biom_inmem sparse layout, src/biom_inmem.cpp:130-157),
+// borrowed from the caller or owned after filtering / rarefaction.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+namespace ssu {
+
+struct Table {
+    Table() = default;
+    Table(const Table &) = delete;  // owned arrays are referenced by pointer
+    Table &operator=(const Table &) = delete;
+    Table(Table &&) = default;
+    Table &operator=(Table &&) = default;
+
+    uint32_t n_obs = 0;
+    uint32_t n_samples = 0;
+    const uint32_t *indptr = nullptr;   // n_obs + 1
+    const uint32_t *indices = nullptr;  // sample positions
+    const double *data = nullptr;
+    std::vector<std::string> obs_ids;
+    std::vector<std::string> sample_ids;
+    std::vector<double> totals;  // per-sample sum, accumulated in observation order
+
+    // storage when the table owns its arrays
+    std::vector<uint32_t> own_indptr, own_indices;
+    std::vector<double> own_data;
+
+    uint64_t nnz() const { return n_obs ? indptr[n_obs] : 0; }
+
+    // Borrow a caller's CSR (not copied, as src/biom_inmem.cpp:129-157).
+    static Table borrow(uint32_t n_obs, uint32_t n_samples, const uint32_t *indptr, const uint32_t *indices,
+                        const double *data, const char *const *obs_ids, const char *const *sample_ids);
+    // Two dense samples; only strictly positive values are kept
+    // (src/biom_inmem.cpp:160-190).
+    static Table dense_pair(uint32_t n_obs, const char *const *obs_ids, const double *s1, const double *s2);
+
+    // Samples with total >= min_total, re-numbered, and observations that
+    // keep at least one entry (src/biom_inmem.cpp:284-338).  Totals are the
+    // parent's.
+    Table filtered(double min_total) const;
+    // Every sample with total >= depth subsampled to `depth` counts (without
+    // or with replacement); lighter samples and observations left without a
+    // positive count are dropped (src/biom_subsampled.cpp:287-353).  The
+    // random stream is this library's own.
+    Table rarefied(uint32_t depth, bool with_replacement, uint64_t seed) const;
+
+    void compute_totals();
+    std::unordered_map<std::string, uint32_t> obs_index() const;
+
+  private:
+    void adopt_owned();
+};
+
+}  // namespace ssu

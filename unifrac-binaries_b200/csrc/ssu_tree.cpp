@@ -1,0 +1,287 @@
+// Host-side phylogeny handling: BP trees, newick, shear, collapse, flatten.
+#include "ssu_tree.hpp"
+
+#include <algorithm>
+#include <cstdlib>
+
+namespace ssu {
+
+void BPTree::pair_parentheses() {
+    match.assign(open.size(), 0);
+    std::vector<uint32_t> stack;
+    stack.reserve(64);
+    for (uint32_t i = 0; i < open.size(); i++) {
+        if (open[i]) {
+            stack.push_back(i);
+        } else if (!stack.empty()) {
+            uint32_t o = stack.back();
+            stack.pop_back();
+            match[o] = i;
+            match[i] = o;
+        }
+    }
+}
+
+BPTree BPTree::from_arrays(const bool *structure, const double *lengths, const char *const *names, int n) {
+    BPTree t;
+    const uint32_t m = n > 0 ? static_cast<uint32_t>(n) : 0;
+    t.open.resize(m);
+    t.length.resize(m);
+    t.name.resize(m);
+    for (uint32_t i = 0; i < m; i++) {
+        t.open[i] = structure[i] ? 1 : 0;
+        t.length[i] = lengths[i];
+        t.name[i] = names[i] ? names[i] : "";
+    }
+    t.pair_parentheses();
+    return t;
+}
+
+namespace {
+
+// Rooted tree as child lists, the intermediate form of the newick parser.
+struct ChildTree {
+    std::vector<std::vector<uint32_t>> children;
+    std::vector<double> length;
+    std::vector<std::string> name;
+    uint32_t add() {
+        children.emplace_back();
+        length.push_back(0.0);
+        name.emplace_back();
+        return static_cast<uint32_t>(children.size() - 1);
+    }
+};
+
+BPTree serialise(const ChildTree &ct, uint32_t root) {
+    BPTree t;
+    const size_t n = 2 * ct.children.size();
+    t.open.reserve(n);
+    t.length.reserve(n);
+    t.name.reserve(n);
+    // explicit stack: (node, next child index)
+    std::vector<std::pair<uint32_t, uint32_t>> stack;
+    stack.emplace_back(root, 0);
+    t.open.push_back(1);
+    t.length.push_back(ct.length[root]);
+    t.name.push_back(ct.name[root]);
+    while (!stack.empty()) {
+        auto &top = stack.back();
+        const auto &kids = ct.children[top.first];
+        if (top.second < kids.size()) {
+            uint32_t c = kids[top.second++];
+            t.open.push_back(1);
+            t.length.push_back(ct.length[c]);
+            t.name.push_back(ct.name[c]);
+            stack.emplace_back(c, 0);
+        } else {
+            t.open.push_back(0);
+            t.length.push_back(0.0);
+            t.name.emplace_back();
+            stack.pop_back();
+        }
+    }
+    t.pair_parentheses();
+    return t;
+}
+
+void apply_label(ChildTree &ct, uint32_t node, const std::string &label) {
+    if (label.empty()) return;
+    const size_t colon = label.find_last_of(':');
+    if (colon == std::string::npos) {
+        ct.name[node] = label;
+        ct.length[node] = 0.0;
+        return;
+    }
+    ct.name[node] = label.substr(0, colon);
+    // single precision, as std::stof in the reference parser
+    ct.length[node] = static_cast<double>(std::strtof(label.c_str() + colon + 1, nullptr));
+}
+
+}  // namespace
+
+bool BPTree::from_newick(const std::string &text, BPTree &out) {
+    size_t end = text.size();
+    while (end > 0 && (text[end - 1] == ' ' || text[end - 1] == '\t' || text[end - 1] == '\n' ||
+                       text[end - 1] == '\r'))
+        end--;
+    ChildTree ct;
+    const uint32_t root = ct.add();
+    std::vector<uint32_t> stack;
+    uint32_t cur = root;
+    std::string label;
+    bool in_quote = false;
+    for (size_t i = 0; i < end; i++) {
+        const char c = text[i];
+        if (c == '\n') continue;
+        if (c == '\'') {
+            in_quote = !in_quote;
+            continue;
+        }
+        if (in_quote) {
+            label.push_back(c);
+            continue;
+        }
+        if (c == '(') {
+            apply_label(ct, cur, label);
+            label.clear();
+            stack.push_back(cur);
+            cur = ct.add();
+            ct.children[stack.back()].push_back(cur);
+        } else if (c == ',') {
+            apply_label(ct, cur, label);
+            label.clear();
+            if (stack.empty()) return false;
+            cur = ct.add();
+            ct.children[stack.back()].push_back(cur);
+        } else if (c == ')') {
+            apply_label(ct, cur, label);
+            label.clear();
+            if (stack.empty()) return false;
+            cur = stack.back();
+            stack.pop_back();
+        } else if (c == ';') {
+            break;
+        } else {
+            label.push_back(c);
+        }
+    }
+    apply_label(ct, cur, label);
+    if (!stack.empty()) return false;
+    out = serialise(ct, root);
+    return true;
+}
+
+BPTree BPTree::masked(const std::vector<uint8_t> &keep, const std::vector<double> &lengths) const {
+    BPTree r;
+    size_t m = 0;
+    for (uint8_t k : keep) m += k;
+    r.open.reserve(m);
+    r.length.reserve(m);
+    r.name.reserve(m);
+    for (uint32_t i = 0; i < size(); i++) {
+        if (!keep[i]) continue;
+        r.open.push_back(open[i]);
+        r.length.push_back(lengths[i]);
+        r.name.push_back(name[i]);
+    }
+    r.pair_parentheses();
+    return r;
+}
+
+BPTree BPTree::shear(const std::unordered_set<std::string> &keep) const {
+    const uint32_t n = size();
+    std::vector<uint8_t> mask(n, 0);
+    std::vector<uint32_t> parent(n, UINT32_MAX);
+    std::vector<uint32_t> stack;
+    for (uint32_t i = 0; i < n; i++) {
+        if (open[i]) {
+            parent[i] = stack.empty() ? UINT32_MAX : stack.back();
+            stack.push_back(i);
+        } else if (!stack.empty()) {
+            stack.pop_back();
+        }
+    }
+    for (uint32_t i = 0; i + 1 < n; i++) {
+        if (!leaf(i) || keep.count(name[i]) == 0) continue;
+        mask[i] = mask[i + 1] = 1;
+        for (uint32_t p = parent[i]; p != UINT32_MAX && !mask[p]; p = parent[p]) mask[p] = mask[match[p]] = 1;
+    }
+    return masked(mask, length);
+}
+
+BPTree BPTree::collapse() const {
+    const uint32_t n = size();
+    std::vector<uint8_t> mask(n, 0);
+    std::vector<double> len(length);
+    for (uint32_t cur = 0; cur < n; cur++) {  // opening parentheses in index order = preorder
+        if (!open[cur]) continue;
+        if (leaf(cur) || cur == 0) {
+            mask[cur] = mask[match[cur]] = 1;
+            continue;
+        }
+        const uint32_t first = cur + 1;
+        const uint32_t last = match[match[cur] - 1];
+        if (first == last)
+            len[first] = len[first] + len[cur];
+        else
+            mask[cur] = mask[match[cur]] = 1;
+    }
+    return masked(mask, len);
+}
+
+std::unordered_set<std::string> BPTree::tip_names() const {
+    std::unordered_set<std::string> out;
+    for (uint32_t i = 0; i + 1 < size(); i++)
+        if (leaf(i)) out.insert(name[i]);
+    return out;
+}
+
+uint32_t BPTree::n_tips() const {
+    uint32_t c = 0;
+    for (uint32_t i = 0; i + 1 < size(); i++) c += leaf(i);
+    return c;
+}
+
+FlatTree flatten(const BPTree &t, const std::unordered_map<std::string, uint32_t> &obs_index, bool bypass_tips) {
+    FlatTree f;
+    const uint32_t n = t.size();
+    const uint32_t total = n / 2;
+    f.n_nodes = total > 0 ? total - 1 : 0;
+    // postorder: the k-th closing parenthesis closes the k-th postorder node;
+    // the root closes last and is not a row (src/unifrac_cmp.cpp:97-100)
+    std::vector<uint32_t> post_open;
+    post_open.reserve(f.n_nodes);
+    for (uint32_t i = 0; i < n && post_open.size() < f.n_nodes; i++)
+        if (!t.open[i]) post_open.push_back(t.match[i]);
+    std::vector<uint32_t> row_of_open(n, UINT32_MAX);
+    uint32_t r = 0;
+    for (uint32_t k = 0; k < f.n_nodes; k++)
+        if (!(bypass_tips && t.leaf(post_open[k]))) row_of_open[post_open[k]] = r++;
+    f.n_embedded = r;
+    for (uint32_t k = 0; k < f.n_nodes; k++)
+        if (row_of_open[post_open[k]] == UINT32_MAX) row_of_open[post_open[k]] = r++;
+
+    f.length.assign(f.n_nodes, 0.0);
+    f.leaf_obs.assign(f.n_nodes, -1);
+    f.postorder_row.resize(f.n_nodes);
+    std::vector<uint32_t> height(f.n_nodes, 0);
+    std::vector<std::vector<uint32_t>> kids(f.n_nodes);
+    uint32_t max_height = 0;
+    for (uint32_t k = 0; k < f.n_nodes; k++) {
+        const uint32_t o = post_open[k];
+        const uint32_t row = row_of_open[o];
+        f.postorder_row[k] = row;
+        f.length[row] = t.length[o];
+        if (t.leaf(o)) {
+            f.leaf_rows.push_back(row);
+            auto it = obs_index.find(t.name[o]);
+            if (it != obs_index.end()) f.leaf_obs[row] = static_cast<int32_t>(it->second);
+        } else {
+            uint32_t h = 0;
+            for (uint32_t c = o + 1; c < n && t.open[c]; c = t.match[c] + 1) {
+                const uint32_t cr = row_of_open[c];
+                kids[row].push_back(cr);
+                h = std::max(h, height[cr] + 1);
+            }
+            height[row] = h;
+            max_height = std::max(max_height, h);
+        }
+    }
+    f.child_ptr.assign(f.n_nodes + 1, 0);
+    for (uint32_t row = 0; row < f.n_nodes; row++) f.child_ptr[row + 1] = f.child_ptr[row] + kids[row].size();
+    f.child_rows.reserve(f.child_ptr[f.n_nodes]);
+    for (uint32_t row = 0; row < f.n_nodes; row++)
+        f.child_rows.insert(f.child_rows.end(), kids[row].begin(), kids[row].end());
+    // internal rows bucketed by height 1..max_height
+    f.level_ptr.assign(max_height + 1, 0);
+    for (uint32_t row = 0; row < f.n_nodes; row++)
+        if (height[row] > 0) f.level_ptr[height[row]]++;
+    for (uint32_t h = 1; h <= max_height; h++) f.level_ptr[h] += f.level_ptr[h - 1];
+    f.level_rows.assign(f.level_ptr[max_height], 0);
+    std::vector<uint32_t> fill(f.level_ptr.begin(), f.level_ptr.end());
+    for (uint32_t row = 0; row < f.n_nodes; row++)
+        if (height[row] > 0) f.level_rows[fill[height[row] - 1]++] = row;
+    return f;
+}
+
+}  // namespace ssu

@@ -1,0 +1,66 @@
+// Host-side phylogeny handling for the B200 UniFrac engine: balanced-
+// parentheses trees, newick parsing, shear/collapse and the flattened
+// postorder that the device embedding consumes.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+
+namespace ssu {
+
+// A rooted tree in balanced-parentheses form.  open[i] is true for '(' and
+// the length and name of a node live at its opening index, as the
+// reference's BPTree (src/tree.hpp:21-153).  match[i] pairs every
+// parenthesis with its partner.
+struct BPTree {
+    std::vector<uint8_t> open;
+    std::vector<double> length;
+    std::vector<std::string> name;
+    std::vector<uint32_t> match;
+
+    uint32_t size() const { return static_cast<uint32_t>(open.size()); }
+    bool leaf(uint32_t i) const { return open[i] && i + 1 < open.size() && !open[i + 1]; }
+    void pair_parentheses();
+
+    // src/tree.cpp:72-99 (arrays are copied).
+    static BPTree from_arrays(const bool *structure, const double *lengths, const char *const *names, int n);
+    // Newick text -> tree, following the reference parser's rules
+    // (src/tree.cpp:315-455): quotes group a label and are dropped, newlines
+    // are skipped, a label's last ':' splits name and length, and lengths are
+    // read in single precision (std::stof, src/tree.cpp:446,449).
+    static bool from_newick(const std::string &text, BPTree &out);
+
+    // Keep the tips named in `keep` and all their ancestors (src/tree.cpp:145-163).
+    BPTree shear(const std::unordered_set<std::string> &keep) const;
+    // Remove non-root nodes with a single child, adding their length to the
+    // child, in preorder (src/tree.cpp:165-191).
+    BPTree collapse() const;
+    BPTree masked(const std::vector<uint8_t> &keep, const std::vector<double> &lengths) const;
+
+    std::unordered_set<std::string> tip_names() const;
+    uint32_t n_tips() const;
+};
+
+// The sheared tree flattened for the device.  Non-root nodes are numbered by
+// rows: the embedded nodes (postorder, minus tips when bypass_tips) take rows
+// [0, n_embedded), bypassed tips follow.  Children of a row are listed left
+// to right, the order the reference sums them in (src/unifrac_internal.cpp:249-257).
+struct FlatTree {
+    uint32_t n_nodes = 0;      // non-root nodes
+    uint32_t n_embedded = 0;   // rows that enter the pair sums
+    std::vector<double> length;        // per row
+    std::vector<int32_t> leaf_obs;     // per row: table row of a tip, -1 for internal nodes
+    std::vector<uint32_t> child_ptr;   // per row, CSR into child_rows
+    std::vector<uint32_t> child_rows;
+    std::vector<uint32_t> leaf_rows;   // rows of tips
+    std::vector<uint32_t> level_ptr;   // internal rows grouped by height (1, 2, ...)
+    std::vector<uint32_t> level_rows;
+    std::vector<uint32_t> postorder_row;  // postorder index -> row
+};
+
+FlatTree flatten(const BPTree &tree, const std::unordered_map<std::string, uint32_t> &obs_index, bool bypass_tips);
+
+}  // namespace ssu

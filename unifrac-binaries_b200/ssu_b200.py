@@ -1,0 +1,427 @@
+"""ctypes binding of libssu_b200.so (include/unifrac_b200.h).
+
+Mirrors the reference's C API for Python callers and tests: tables and trees
+are passed as `support_biom_t` / `support_bptree_t` built from the
+`ssu_synth.Table` / `ssu_synth.BPTree` containers (or any object with the
+same attributes), results come back as numpy arrays after the library's
+destroy_*() has been called.  The library must be built (`make` in this
+directory, or `__graft_entry__.build()`); loading fails loudly otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libssu_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "unifrac_b200.h")
+
+STATUS = ["okay", "tree_missing", "table_missing", "table_empty", "unknown_method",
+          "table_and_tree_do_not_overlap", "output_error", "invalid_method", "grouping_missing"]
+IO_STATUS = ["read_okay", "write_okay", "open_error", "read_error", "magic_incompatible", "bad_header",
+             "unexpected_end", "write_error"]
+
+_strpp = C.POINTER(C.c_char_p)
+
+
+class SupportBiom(C.Structure):
+    _fields_ = [("obs_ids", _strpp), ("sample_ids", _strpp), ("indices", C.POINTER(C.c_uint32)),
+                ("indptr", C.POINTER(C.c_uint32)), ("data", C.POINTER(C.c_double)), ("n_obs", C.c_int),
+                ("n_samples", C.c_int), ("nnz", C.c_int)]
+
+
+class SupportBPTree(C.Structure):
+    _fields_ = [("structure", C.POINTER(C.c_bool)), ("lengths", C.POINTER(C.c_double)), ("names", _strpp),
+                ("n_parens", C.c_int)]
+
+
+class MatFull64(C.Structure):
+    _fields_ = [("n_samples", C.c_uint32), ("flags", C.c_uint32), ("matrix", C.POINTER(C.c_double)),
+                ("sample_ids", _strpp)]
+
+
+class MatFull32(C.Structure):
+    _fields_ = [("n_samples", C.c_uint32), ("flags", C.c_uint32), ("matrix", C.POINTER(C.c_float)),
+                ("sample_ids", _strpp)]
+
+
+class Mat(C.Structure):
+    _fields_ = [("n_samples", C.c_uint), ("cf_size", C.c_uint), ("is_upper_triangle", C.c_bool),
+                ("condensed_form", C.POINTER(C.c_double)), ("sample_ids", _strpp)]
+
+
+class RVec(C.Structure):
+    _fields_ = [("n_samples", C.c_uint), ("values", C.POINTER(C.c_double)), ("sample_ids", _strpp)]
+
+
+class PartialMat(C.Structure):
+    _fields_ = [("n_samples", C.c_uint32), ("sample_ids", _strpp), ("stripes", C.POINTER(C.POINTER(C.c_double))),
+                ("stripe_start", C.c_uint32), ("stripe_stop", C.c_uint32), ("stripe_total", C.c_uint32),
+                ("is_upper_triangle", C.c_bool)]
+
+
+class SSUError(RuntimeError):
+    def __init__(self, status, where=""):
+        self.status = status
+        name = STATUS[status] if 0 <= status < len(STATUS) else str(status)
+        super().__init__(f"{where}: {name}" if where else name)
+
+
+def declared_functions(header=HEADER):
+    """Names of every function the public header declares."""
+    text = open(header).read()
+    return sorted(set(re.findall(r"SSU_EXTERN[^;(]*?\b(\w+)\s*\(", text, flags=re.S)))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is not built; run `make` in {HERE}")
+        L = C.CDLL(LIB_PATH)
+        P, PP = C.POINTER, C.POINTER
+        common = [P(SupportBiom), P(SupportBPTree), C.c_char_p, C.c_bool, C.c_double, C.c_bool, C.c_bool, C.c_uint]
+        L.one_off_matrix_inmem_v3.argtypes = common + [C.c_uint, C.c_bool, C.c_char_p, PP(P(MatFull64))]
+        L.one_off_matrix_inmem_fp32_v3.argtypes = common + [C.c_uint, C.c_bool, C.c_char_p, PP(P(MatFull32))]
+        L.ssu_b200_one_off_inmem_v3.argtypes = common + [PP(P(Mat))]
+        L.ssu_b200_partial_inmem_v3.argtypes = common + [C.c_uint, C.c_uint, PP(P(PartialMat))]
+        L.ssu_b200_faith_pd_inmem.argtypes = [P(SupportBiom), P(SupportBPTree), PP(P(RVec))]
+        L.one_dense_pair_v3.argtypes = [C.c_uint, _strpp, P(C.c_double), P(C.c_double), P(SupportBPTree), C.c_char_p,
+                                        C.c_bool, C.c_double, C.c_bool, C.c_bool, P(C.c_double)]
+        L.one_dense_pair_v3t.argtypes = [C.c_uint, _strpp, P(C.c_double), P(C.c_double), C.c_void_p, C.c_char_p,
+                                         C.c_bool, C.c_double, C.c_bool, C.c_bool, P(C.c_double)]
+        L.load_bptree_opaque.argtypes = [C.c_char_p, P(C.c_void_p)]
+        L.load_bptree_opaque.restype = None
+        L.read_bptree_opaque.argtypes = [C.c_char_p, P(C.c_void_p)]
+        L.convert_bptree_opaque.argtypes = [P(SupportBPTree), P(C.c_void_p)]
+        L.convert_bptree_opaque.restype = None
+        L.destroy_bptree_opaque.argtypes = [P(C.c_void_p)]
+        L.destroy_bptree_opaque.restype = None
+        L.get_bptree_opaque_els.argtypes = [C.c_void_p]
+        L.ssu_b200_tree_arrays.argtypes = [C.c_void_p, C.c_int, P(C.c_bool), P(C.c_double), _strpp, P(C.c_int)]
+        L.ssu_b200_shear_collapse.argtypes = [P(SupportBPTree), _strpp, C.c_int, C.c_int, P(C.c_bool),
+                                              P(C.c_double), _strpp, P(C.c_int)]
+        for name, typ in [("destroy_mat_full_fp64", MatFull64), ("destroy_mat_full_fp32", MatFull32),
+                          ("destroy_mat", Mat), ("destroy_results_vec", RVec), ("destroy_partial_mat", PartialMat)]:
+            f = getattr(L, name)
+            f.argtypes = [PP(P(typ))]
+            f.restype = None
+        for name in ["one_off_v3", "one_off_matrix_v3", "faith_pd_one_off", "partial_v3"]:
+            getattr(L, name).restype = C.c_int
+        L.faith_pd_one_off.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p]
+        L.ssu_set_random_seed.argtypes = [C.c_uint]
+        L.ssu_set_random_seed.restype = None
+        L.ssu_b200_plan_create.argtypes = common[:-1] + [P(C.c_void_p)]
+        L.ssu_b200_plan_execute.argtypes = [C.c_void_p, C.c_void_p]
+        L.ssu_b200_plan_device_result.argtypes = [C.c_void_p]
+        L.ssu_b200_plan_device_result.restype = C.c_void_p
+        L.ssu_b200_plan_copy_result.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ssu_b200_plan_work_units.argtypes = [C.c_void_p]
+        L.ssu_b200_plan_work_units.restype = C.c_uint64
+        L.ssu_b200_plan_n_samples.argtypes = [C.c_void_p]
+        L.ssu_b200_plan_n_samples.restype = C.c_uint32
+        L.ssu_b200_plan_n_embedded.argtypes = [C.c_void_p]
+        L.ssu_b200_plan_n_embedded.restype = C.c_uint64
+        L.ssu_b200_plan_launches.argtypes = [C.c_void_p]
+        L.ssu_b200_plan_launches.restype = C.c_uint32
+        L.ssu_b200_plan_set_timing.argtypes = [C.c_void_p, C.c_int]
+        L.ssu_b200_plan_set_timing.restype = None
+        L.ssu_b200_plan_stage_ms.argtypes = [C.c_void_p, P(C.c_float), P(C.c_float), P(C.c_float)]
+        L.ssu_b200_plan_destroy.argtypes = [P(C.c_void_p)]
+        L.ssu_b200_plan_destroy.restype = None
+        L.ssu_b200_plan_pair_kernel.argtypes = [C.c_void_p]
+        L.ssu_b200_plan_pair_kernel.restype = C.c_char_p
+        L.ssu_b200_version.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+# ------------------------------------------------------------ marshalling
+
+def _strarr(strings):
+    arr = (C.c_char_p * max(len(strings), 1))()
+    arr[:len(strings)] = [s.encode() for s in strings]
+    return arr
+
+
+class Inputs:
+    """support_biom_t + support_bptree_t views of a (tree, table) pair; keeps
+    the backing numpy arrays alive while the call runs."""
+
+    def __init__(self, tree, table):
+        self.indptr = np.ascontiguousarray(table.indptr, dtype=np.uint32)
+        self.indices = np.ascontiguousarray(table.indices, dtype=np.uint32)
+        self.data = np.ascontiguousarray(table.data, dtype=np.float64)
+        self.obs = _strarr(table.obs_ids)
+        self.samples = _strarr(table.sample_ids)
+        self.biom = SupportBiom(self.obs, self.samples, self.indices.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                self.indptr.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                self.data.ctypes.data_as(C.POINTER(C.c_double)), len(table.obs_ids),
+                                len(table.sample_ids), int(self.indptr[-1]) if len(self.indptr) else 0)
+        self.structure = np.ascontiguousarray(tree.structure, dtype=np.bool_)
+        self.lengths = np.ascontiguousarray(tree.lengths, dtype=np.float64)
+        self.names = _strarr(tree.names)
+        self.tree = SupportBPTree(self.structure.ctypes.data_as(C.POINTER(C.c_bool)),
+                                  self.lengths.ctypes.data_as(C.POINTER(C.c_double)), self.names,
+                                  len(tree.names))
+
+
+def _ids(ptr, n):
+    return [ptr[i].decode() for i in range(n)]
+
+
+def is_fp64(method):
+    return method.endswith("_fp64")
+
+
+# ------------------------------------------------------------ entry points
+
+def one_off_matrix(tree, table, method, variance_adjust=False, alpha=1.0, bypass_tips=False, normalize=True,
+                   subsample_depth=0, with_replacement=False, mmap_dir=None):
+    """Full n x n matrix through one_off_matrix_inmem_v3 (fp64 methods) or
+    one_off_matrix_inmem_fp32_v3 (fp32 methods).  Returns (matrix, ids)."""
+    L = lib()
+    x = Inputs(tree, table)
+    md = mmap_dir.encode() if mmap_dir else None
+    if is_fp64(method):
+        res = C.POINTER(MatFull64)()
+        st = L.one_off_matrix_inmem_v3(C.byref(x.biom), C.byref(x.tree), method.encode(), variance_adjust, alpha,
+                                       bypass_tips, normalize, 1, subsample_depth, with_replacement, md,
+                                       C.byref(res))
+        if st != 0:
+            raise SSUError(st, "one_off_matrix_inmem_v3")
+        n = res.contents.n_samples
+        out = np.ctypeslib.as_array(res.contents.matrix, shape=(n, n)).copy()
+        ids = _ids(res.contents.sample_ids, n)
+        L.destroy_mat_full_fp64(C.byref(res))
+    else:
+        res = C.POINTER(MatFull32)()
+        st = L.one_off_matrix_inmem_fp32_v3(C.byref(x.biom), C.byref(x.tree), method.encode(), variance_adjust,
+                                            alpha, bypass_tips, normalize, 1, subsample_depth, with_replacement, md,
+                                            C.byref(res))
+        if st != 0:
+            raise SSUError(st, "one_off_matrix_inmem_fp32_v3")
+        n = res.contents.n_samples
+        out = np.ctypeslib.as_array(res.contents.matrix, shape=(n, n)).copy()
+        ids = _ids(res.contents.sample_ids, n)
+        L.destroy_mat_full_fp32(C.byref(res))
+    return out, ids
+
+
+def status_of_matrix_call(tree, table, method, fp32_entry=False, **kw):
+    """Status code of a full-matrix call (no exception), for error-path tests."""
+    L = lib()
+    x = Inputs(tree, table)
+    if fp32_entry:
+        res = C.POINTER(MatFull32)()
+        st = L.one_off_matrix_inmem_fp32_v3(C.byref(x.biom), C.byref(x.tree), method.encode(), False, 1.0, False,
+                                            True, 1, 0, False, None, C.byref(res))
+        if st == 0:
+            L.destroy_mat_full_fp32(C.byref(res))
+    else:
+        res = C.POINTER(MatFull64)()
+        st = L.one_off_matrix_inmem_v3(C.byref(x.biom), C.byref(x.tree), method.encode(), False, 1.0, False, True,
+                                       1, 0, False, None, C.byref(res))
+        if st == 0:
+            L.destroy_mat_full_fp64(C.byref(res))
+    return st
+
+
+def one_off(tree, table, method, variance_adjust=False, alpha=1.0, bypass_tips=False, normalize=True):
+    """Condensed form (mat_t) through ssu_b200_one_off_inmem_v3."""
+    L = lib()
+    x = Inputs(tree, table)
+    res = C.POINTER(Mat)()
+    st = L.ssu_b200_one_off_inmem_v3(C.byref(x.biom), C.byref(x.tree), method.encode(), variance_adjust, alpha,
+                                     bypass_tips, normalize, 1, C.byref(res))
+    if st != 0:
+        raise SSUError(st, "ssu_b200_one_off_inmem_v3")
+    m = res.contents
+    cf = np.ctypeslib.as_array(m.condensed_form, shape=(m.cf_size,)).copy() if m.cf_size else np.zeros(0)
+    ids = _ids(m.sample_ids, m.n_samples)
+    upper = bool(m.is_upper_triangle)
+    L.destroy_mat(C.byref(res))
+    return cf, ids, upper
+
+
+def partial(tree, table, method, stripe_start, stripe_stop, variance_adjust=False, alpha=1.0, bypass_tips=False,
+            normalize=True):
+    """Stripes [start, stop) (partial_mat_t) through ssu_b200_partial_inmem_v3."""
+    L = lib()
+    x = Inputs(tree, table)
+    res = C.POINTER(PartialMat)()
+    st = L.ssu_b200_partial_inmem_v3(C.byref(x.biom), C.byref(x.tree), method.encode(), variance_adjust, alpha,
+                                     bypass_tips, normalize, 1, stripe_start, stripe_stop, C.byref(res))
+    if st != 0:
+        raise SSUError(st, "ssu_b200_partial_inmem_v3")
+    p = res.contents
+    rows = p.stripe_stop - p.stripe_start
+    stripes = np.zeros((rows, p.n_samples))
+    for s in range(rows):
+        stripes[s] = np.ctypeslib.as_array(p.stripes[s], shape=(p.n_samples,))
+    meta = {"start": p.stripe_start, "stop": p.stripe_stop, "total": p.stripe_total,
+            "upper": bool(p.is_upper_triangle), "ids": _ids(p.sample_ids, p.n_samples)}
+    L.destroy_partial_mat(C.byref(res))
+    return stripes, meta
+
+
+def faith_pd(tree, table):
+    L = lib()
+    x = Inputs(tree, table)
+    res = C.POINTER(RVec)()
+    st = L.ssu_b200_faith_pd_inmem(C.byref(x.biom), C.byref(x.tree), C.byref(res))
+    if st != 0:
+        raise SSUError(st, "ssu_b200_faith_pd_inmem")
+    r = res.contents
+    vals = np.ctypeslib.as_array(r.values, shape=(r.n_samples,)).copy()
+    ids = _ids(r.sample_ids, r.n_samples)
+    L.destroy_results_vec(C.byref(res))
+    return vals, ids
+
+
+def dense_pair(tree, obs_ids, s1, s2, method, variance_adjust=False, alpha=1.0, bypass_tips=False, normalize=True):
+    L = lib()
+    x = Inputs(tree, _EmptyTable())
+    ids = _strarr(obs_ids)
+    a = np.ascontiguousarray(s1, dtype=np.float64)
+    b = np.ascontiguousarray(s2, dtype=np.float64)
+    out = C.c_double(0.0)
+    st = L.one_dense_pair_v3(len(obs_ids), ids, a.ctypes.data_as(C.POINTER(C.c_double)),
+                             b.ctypes.data_as(C.POINTER(C.c_double)), C.byref(x.tree), method.encode(),
+                             variance_adjust, alpha, bypass_tips, normalize, C.byref(out))
+    if st != 0:
+        raise SSUError(st, "one_dense_pair_v3")
+    return out.value
+
+
+class _EmptyTable:
+    obs_ids, sample_ids = [], []
+    indptr = np.zeros(1, np.uint32)
+    indices = np.zeros(0, np.uint32)
+    data = np.zeros(0)
+
+
+class OpaqueTree:
+    """opaque_bptree_t from a newick string (load_bptree_opaque) or file."""
+
+    def __init__(self, newick=None, path=None):
+        self.ptr = C.c_void_p()
+        if path is not None:
+            st = lib().read_bptree_opaque(path.encode(), C.byref(self.ptr))
+            if st != 0:
+                raise RuntimeError(f"read_bptree_opaque: {IO_STATUS[st]}")
+        else:
+            lib().load_bptree_opaque(newick.encode(), C.byref(self.ptr))
+
+    def arrays(self):
+        n = C.c_int(0)
+        lib().ssu_b200_tree_arrays(self.ptr, 0, None, None, None, C.byref(n))
+        cap = n.value
+        s = np.zeros(cap, dtype=np.bool_)
+        ln = np.zeros(cap, dtype=np.float64)
+        nm = (C.c_char_p * max(cap, 1))()
+        rc = lib().ssu_b200_tree_arrays(self.ptr, cap, s.ctypes.data_as(C.POINTER(C.c_bool)),
+                                        ln.ctypes.data_as(C.POINTER(C.c_double)), nm, C.byref(n))
+        assert rc == 0
+        return s, ln, [nm[i].decode() for i in range(cap)]
+
+    def n_tips(self):
+        return lib().get_bptree_opaque_els(self.ptr)
+
+    def close(self):
+        if self.ptr:
+            lib().destroy_bptree_opaque(C.byref(self.ptr))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def shear_collapse(tree, names=None, collapse=True):
+    """Host-side shear(names) [+ collapse()] of the library (no device work);
+    names=None keeps every tip."""
+    x = Inputs(tree, _EmptyTable())
+    n = len(tree.names)
+    s = np.zeros(n, dtype=np.bool_)
+    ln = np.zeros(n, dtype=np.float64)
+    nm = (C.c_char_p * max(n, 1))()
+    keep = _strarr(names) if names is not None else None
+    out_n = C.c_int(0)
+    rc = lib().ssu_b200_shear_collapse(C.byref(x.tree), keep, len(names) if names is not None else 0,
+                                       1 if collapse else 0, s.ctypes.data_as(C.POINTER(C.c_bool)),
+                                       ln.ctypes.data_as(C.POINTER(C.c_double)), nm, C.byref(out_n))
+    assert rc == 0
+    m = out_n.value
+    return s[:m].copy(), ln[:m].copy(), [nm[i].decode() for i in range(m)]
+
+
+class Plan:
+    """Device-resident plan: inputs uploaded once, execute() recomputes the
+    full matrix in HBM."""
+
+    def __init__(self, tree, table, method, variance_adjust=False, alpha=1.0, bypass_tips=False, normalize=True):
+        L = lib()
+        self._x = Inputs(tree, table)
+        self.ptr = C.c_void_p()
+        st = L.ssu_b200_plan_create(C.byref(self._x.biom), C.byref(self._x.tree), method.encode(), variance_adjust,
+                                    alpha, bypass_tips, normalize, C.byref(self.ptr))
+        if st != 0:
+            raise SSUError(st, "ssu_b200_plan_create")
+        self.method = method
+        self.n = L.ssu_b200_plan_n_samples(self.ptr)
+
+    def execute(self, stream=None):
+        st = lib().ssu_b200_plan_execute(self.ptr, C.c_void_p(stream) if stream else None)
+        if st != 0:
+            raise SSUError(st, "ssu_b200_plan_execute")
+
+    def result(self, stream=None):
+        dt = np.float64 if is_fp64(self.method) else np.float32
+        out = np.empty((self.n, self.n), dtype=dt)
+        st = lib().ssu_b200_plan_copy_result(self.ptr, out.ctypes.data_as(C.c_void_p),
+                                             C.c_void_p(stream) if stream else None)
+        if st != 0:
+            raise SSUError(st, "ssu_b200_plan_copy_result")
+        return out
+
+    def device_result(self):
+        return lib().ssu_b200_plan_device_result(self.ptr)
+
+    def work_units(self):
+        return int(lib().ssu_b200_plan_work_units(self.ptr))
+
+    def n_embedded(self):
+        return int(lib().ssu_b200_plan_n_embedded(self.ptr))
+
+    def launches(self):
+        return int(lib().ssu_b200_plan_launches(self.ptr))
+
+    def pair_kernel(self):
+        return lib().ssu_b200_plan_pair_kernel(self.ptr).decode()
+
+    def set_timing(self, on=True):
+        lib().ssu_b200_plan_set_timing(self.ptr, 1 if on else 0)
+
+    def stage_ms(self):
+        e, p, f = C.c_float(), C.c_float(), C.c_float()
+        if lib().ssu_b200_plan_stage_ms(self.ptr, C.byref(e), C.byref(p), C.byref(f)) != 0:
+            raise RuntimeError("stage timing unavailable")
+        return e.value, p.value, f.value
+
+    def close(self):
+        if self.ptr:
+            lib().ssu_b200_plan_destroy(C.byref(self.ptr))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
