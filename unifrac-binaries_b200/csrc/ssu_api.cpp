@@ -94,9 +94,13 @@ ComputeStatus is_fp64_method(const char *m, bool &fp64) {
     return okay;
 }
 
-char **copy_ids(const std::vector<std::string> &ids) {
+char **copy_ids(const std::vector<std::string_view> &ids) {
     char **out = static_cast<char **>(std::malloc(sizeof(char *) * (ids.size() ? ids.size() : 1)));
-    for (size_t i = 0; i < ids.size(); i++) out[i] = strdup(ids[i].c_str());
+    for (size_t i = 0; i < ids.size(); i++) {
+        out[i] = static_cast<char *>(std::malloc(ids[i].size() + 1));
+        std::memcpy(out[i], ids[i].data(), ids[i].size());
+        out[i][ids[i].size()] = '\0';
+    }
     return out;
 }
 
@@ -105,22 +109,23 @@ ssu::Table table_from(const support_biom_t *t) {
                               t->indices, t->data, t->obs_ids, t->sample_ids);
 }
 
-ssu::BPTree tree_from(const support_bptree_t *t) {
-    return ssu::BPTree::from_arrays(t->structure, t->lengths, t->names, t->n_parens);
+// The caller's arrays outlive the call: names are viewed, not copied.
+ssu::BPTree tree_from(const support_bptree_t *t, bool copy_names = false) {
+    return ssu::BPTree::from_arrays(t->structure, t->lengths, t->names, t->n_parens, copy_names);
 }
 
 // VALIDATE_TREE_TABLE (src/api.cpp:94-100)
 ComputeStatus validate(const ssu::Table &table, const ssu::BPTree &tree) {
     if (table.n_samples == 0 || table.n_obs == 0) return table_empty;
-    const std::unordered_set<std::string> tips = tree.tip_names();
-    for (const std::string &id : table.obs_ids)
+    const ssu::NameSet tips = tree.tip_names();
+    for (const std::string_view &id : table.obs_ids)
         if (!tips.count(id)) return table_and_tree_do_not_overlap;
     return okay;
 }
 
 // SYNC_TREE_TABLE (src/api.cpp:90-92) + flattening for the device.
 ssu::FlatTree sync_tree(const ssu::Table &table, const ssu::BPTree &tree, bool bypass_tips) {
-    const std::unordered_set<std::string> keep(table.obs_ids.begin(), table.obs_ids.end());
+    const ssu::NameSet keep(table.obs_ids.begin(), table.obs_ids.end());
     const ssu::BPTree sheared = tree.shear(keep).collapse();
     return ssu::flatten(sheared, table.obs_index(), bypass_tips);
 }
@@ -160,7 +165,7 @@ ComputeStatus make_plan(const ssu::Table &table, const ssu::BPTree &tree, const 
 }
 
 template <class TReal, class TMat>
-bool alloc_full(TMat *&result, const std::vector<std::string> &ids, const char *mmap_dir) {
+bool alloc_full(TMat *&result, const std::vector<std::string_view> &ids, const char *mmap_dir) {
     result = static_cast<TMat *>(std::malloc(sizeof(TMat)));
     result->n_samples = static_cast<uint32_t>(ids.size());
     result->flags = 0;
@@ -438,7 +443,7 @@ void load_bptree_opaque(const char *newick, opaque_bptree_t **tree_data) {
 
 void convert_bptree_opaque(const support_bptree_t *in_tree, opaque_bptree_t **tree_data) {
     OpaqueTree *t = new OpaqueTree();
-    t->tree = tree_from(in_tree);
+    t->tree = tree_from(in_tree, true);
     *tree_data = reinterpret_cast<opaque_bptree_t *>(t);
 }
 
@@ -725,7 +730,7 @@ int ssu_b200_shear_collapse(const support_bptree_t *in_tree, const char *const *
                             int *out_n) {
     if (!in_tree || !out_n) return 1;
     const ssu::BPTree tree = tree_from(in_tree);
-    std::unordered_set<std::string> keep;
+    ssu::NameSet keep;
     if (names)
         for (int i = 0; i < n_names; i++) keep.insert(names[i]);
     else
@@ -733,14 +738,11 @@ int ssu_b200_shear_collapse(const support_bptree_t *in_tree, const char *const *
     const ssu::BPTree sheared = tree.shear(keep);
     const ssu::BPTree r = do_collapse ? sheared.collapse() : sheared;
     // names are handed back as pointers into the input tree's strings
-    std::unordered_map<std::string, const char *> by_name;
-    for (int i = 0; i < in_tree->n_parens; i++) by_name.emplace(in_tree->names[i], in_tree->names[i]);
     *out_n = static_cast<int>(r.size());
     for (uint32_t i = 0; i < r.size(); i++) {
         out_structure[i] = r.open[i] != 0;
         out_lengths[i] = r.length[i];
-        auto it = by_name.find(r.name[i]);
-        out_names[i] = it != by_name.end() ? it->second : "";
+        out_names[i] = r.name[i].data();  // a view into in_tree->names
     }
     return 0;
 }
@@ -754,7 +756,7 @@ int ssu_b200_tree_arrays(const opaque_bptree_t *tree_data, int capacity, bool *o
     for (uint32_t i = 0; i < t.size(); i++) {
         out_structure[i] = t.open[i] != 0;
         out_lengths[i] = t.length[i];
-        out_names[i] = t.name[i].c_str();
+        out_names[i] = t.name[i].data();  // owned, NUL-terminated strings
     }
     return 0;
 }

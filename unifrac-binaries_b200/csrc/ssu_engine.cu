@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <cuda_runtime.h>
+#include <mutex>
 
 #include "ssu_kernels.cuh"
 
@@ -48,6 +49,28 @@ bool parse_method(const char *name, Method &method, bool &fp64) {
 namespace {
 
 constexpr int kOutputError = 6;  // ComputeStatus output_error
+
+// One stream-ordered memory pool per device, owned by the library, that
+// keeps freed blocks cached (no release threshold): repeated calls reuse the
+// embedding and result buffers instead of re-mapping them.
+cudaMemPool_t device_pool(int dev) {
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    if (pools.size() <= static_cast<size_t>(dev)) pools.resize(dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+        uint64_t threshold = UINT64_MAX;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &threshold);
+        pools[dev] = p;
+    }
+    return pools[dev];
+}
 
 #define SSU_CK(call)                                                                                  \
     do {                                                                                              \
@@ -259,10 +282,13 @@ struct PlanImpl {
     uint32_t launches = 0;
     std::vector<void *> allocations;
 
+    cudaMemPool_t pool = nullptr;
+
     template <typename P>
     cudaError_t alloc(P **p, size_t bytes) {
         void *q = nullptr;
-        cudaError_t e = cudaMallocAsync(&q, std::max<size_t>(bytes, 256), stream);
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(&q, std::max<size_t>(bytes, 256), pool, stream)
+                             : cudaMallocAsync(&q, std::max<size_t>(bytes, 256), stream);
         if (e == cudaSuccess) {
             allocations.push_back(q);
             *p = static_cast<P *>(q);
@@ -309,6 +335,7 @@ int PlanImpl::setup(const Table &table, const FlatTree &tree) {
     int dev_id = 0;
     SSU_CK(cudaGetDevice(&dev_id));
     SSU_CK(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, dev_id));
+    pool = device_pool(dev_id);
     if (!stream) {
         SSU_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;

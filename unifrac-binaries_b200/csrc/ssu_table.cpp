@@ -147,8 +147,8 @@ Table Table::rarefied(uint32_t depth, bool with_replacement, uint64_t seed) cons
     return t;
 }
 
-std::unordered_map<std::string, uint32_t> Table::obs_index() const {
-    std::unordered_map<std::string, uint32_t> m;
+std::unordered_map<std::string_view, uint32_t> Table::obs_index() const {
+    std::unordered_map<std::string_view, uint32_t> m;
     m.reserve(n_obs * 2 + 1);
     for (uint32_t i = 0; i < n_obs; i++) m[obs_ids[i]] = i;
     return m;

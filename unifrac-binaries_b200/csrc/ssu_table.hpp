@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <string_view>
 #include <unordered_map>
 #include <vector>
 
@@ -22,8 +23,9 @@ struct Table {
     const uint32_t *indptr = nullptr;   // n_obs + 1
     const uint32_t *indices = nullptr;  // sample positions
     const double *data = nullptr;
-    std::vector<std::string> obs_ids;
-    std::vector<std::string> sample_ids;
+    // views into the caller's id strings (valid for the call)
+    std::vector<std::string_view> obs_ids;
+    std::vector<std::string_view> sample_ids;
     std::vector<double> totals;  // per-sample sum, accumulated in observation order
 
     // storage when the table owns its arrays
@@ -50,7 +52,7 @@ struct Table {
     Table rarefied(uint32_t depth, bool with_replacement, uint64_t seed) const;
 
     void compute_totals();
-    std::unordered_map<std::string, uint32_t> obs_index() const;
+    std::unordered_map<std::string_view, uint32_t> obs_index() const;
 
   private:
     void adopt_owned();

@@ -22,16 +22,24 @@ void BPTree::pair_parentheses() {
     }
 }
 
-BPTree BPTree::from_arrays(const bool *structure, const double *lengths, const char *const *names, int n) {
+BPTree BPTree::from_arrays(const bool *structure, const double *lengths, const char *const *names, int n,
+                           bool copy_names) {
     BPTree t;
     const uint32_t m = n > 0 ? static_cast<uint32_t>(n) : 0;
     t.open.resize(m);
     t.length.resize(m);
     t.name.resize(m);
+    if (copy_names) t.storage = std::make_shared<std::deque<std::string>>();
     for (uint32_t i = 0; i < m; i++) {
         t.open[i] = structure[i] ? 1 : 0;
         t.length[i] = lengths[i];
-        t.name[i] = names[i] ? names[i] : "";
+        const char *nm = names[i] ? names[i] : "";
+        if (copy_names) {
+            t.storage->emplace_back(nm);
+            t.name[i] = t.storage->back();
+        } else {
+            t.name[i] = nm;
+        }
     }
     t.pair_parentheses();
     return t;
@@ -54,6 +62,8 @@ struct ChildTree {
 
 BPTree serialise(const ChildTree &ct, uint32_t root) {
     BPTree t;
+    t.storage = std::make_shared<std::deque<std::string>>(ct.name.begin(), ct.name.end());
+    const std::deque<std::string> &names = *t.storage;
     const size_t n = 2 * ct.children.size();
     t.open.reserve(n);
     t.length.reserve(n);
@@ -63,7 +73,7 @@ BPTree serialise(const ChildTree &ct, uint32_t root) {
     stack.emplace_back(root, 0);
     t.open.push_back(1);
     t.length.push_back(ct.length[root]);
-    t.name.push_back(ct.name[root]);
+    t.name.push_back(names[root]);
     while (!stack.empty()) {
         auto &top = stack.back();
         const auto &kids = ct.children[top.first];
@@ -71,12 +81,12 @@ BPTree serialise(const ChildTree &ct, uint32_t root) {
             uint32_t c = kids[top.second++];
             t.open.push_back(1);
             t.length.push_back(ct.length[c]);
-            t.name.push_back(ct.name[c]);
+            t.name.push_back(names[c]);
             stack.emplace_back(c, 0);
         } else {
             t.open.push_back(0);
             t.length.push_back(0.0);
-            t.name.emplace_back();
+            t.name.emplace_back("");  // a NUL-terminated empty name
             stack.pop_back();
         }
     }
@@ -153,6 +163,7 @@ bool BPTree::from_newick(const std::string &text, BPTree &out) {
 
 BPTree BPTree::masked(const std::vector<uint8_t> &keep, const std::vector<double> &lengths) const {
     BPTree r;
+    r.storage = storage;
     size_t m = 0;
     for (uint8_t k : keep) m += k;
     r.open.reserve(m);
@@ -168,7 +179,7 @@ BPTree BPTree::masked(const std::vector<uint8_t> &keep, const std::vector<double
     return r;
 }
 
-BPTree BPTree::shear(const std::unordered_set<std::string> &keep) const {
+BPTree BPTree::shear(const NameSet &keep) const {
     const uint32_t n = size();
     std::vector<uint8_t> mask(n, 0);
     std::vector<uint32_t> parent(n, UINT32_MAX);
@@ -209,8 +220,9 @@ BPTree BPTree::collapse() const {
     return masked(mask, len);
 }
 
-std::unordered_set<std::string> BPTree::tip_names() const {
-    std::unordered_set<std::string> out;
+NameSet BPTree::tip_names() const {
+    NameSet out;
+    out.reserve(size() / 2 + 1);
     for (uint32_t i = 0; i + 1 < size(); i++)
         if (leaf(i)) out.insert(name[i]);
     return out;
@@ -222,7 +234,7 @@ uint32_t BPTree::n_tips() const {
     return c;
 }
 
-FlatTree flatten(const BPTree &t, const std::unordered_map<std::string, uint32_t> &obs_index, bool bypass_tips) {
+FlatTree flatten(const BPTree &t, const NameIndex &obs_index, bool bypass_tips) {
     FlatTree f;
     const uint32_t n = t.size();
     const uint32_t total = n / 2;

@@ -4,29 +4,39 @@
 #pragma once
 
 #include <cstdint>
+#include <deque>
+#include <memory>
 #include <string>
+#include <string_view>
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
 
 namespace ssu {
 
+using NameSet = std::unordered_set<std::string_view>;
+using NameIndex = std::unordered_map<std::string_view, uint32_t>;
+
 // A rooted tree in balanced-parentheses form.  open[i] is true for '(' and
 // the length and name of a node live at its opening index, as the
 // reference's BPTree (src/tree.hpp:21-153).  match[i] pairs every
-// parenthesis with its partner.
+// parenthesis with its partner.  Names are views: into `storage` when the
+// tree owns them, else into the caller's arrays for the duration of a call.
 struct BPTree {
     std::vector<uint8_t> open;
     std::vector<double> length;
-    std::vector<std::string> name;
+    std::vector<std::string_view> name;
     std::vector<uint32_t> match;
+    std::shared_ptr<std::deque<std::string>> storage;
 
     uint32_t size() const { return static_cast<uint32_t>(open.size()); }
     bool leaf(uint32_t i) const { return open[i] && i + 1 < open.size() && !open[i + 1]; }
     void pair_parentheses();
 
-    // src/tree.cpp:72-99 (arrays are copied).
-    static BPTree from_arrays(const bool *structure, const double *lengths, const char *const *names, int n);
+    // src/tree.cpp:72-99.  With copy_names the tree owns its names;
+    // otherwise it views the caller's strings.
+    static BPTree from_arrays(const bool *structure, const double *lengths, const char *const *names, int n,
+                              bool copy_names);
     // Newick text -> tree, following the reference parser's rules
     // (src/tree.cpp:315-455): quotes group a label and are dropped, newlines
     // are skipped, a label's last ':' splits name and length, and lengths are
@@ -34,13 +44,13 @@ struct BPTree {
     static bool from_newick(const std::string &text, BPTree &out);
 
     // Keep the tips named in `keep` and all their ancestors (src/tree.cpp:145-163).
-    BPTree shear(const std::unordered_set<std::string> &keep) const;
+    BPTree shear(const NameSet &keep) const;
     // Remove non-root nodes with a single child, adding their length to the
     // child, in preorder (src/tree.cpp:165-191).
     BPTree collapse() const;
     BPTree masked(const std::vector<uint8_t> &keep, const std::vector<double> &lengths) const;
 
-    std::unordered_set<std::string> tip_names() const;
+    NameSet tip_names() const;
     uint32_t n_tips() const;
 };
 
@@ -61,6 +71,6 @@ struct FlatTree {
     std::vector<uint32_t> postorder_row;  // postorder index -> row
 };
 
-FlatTree flatten(const BPTree &tree, const std::unordered_map<std::string, uint32_t> &obs_index, bool bypass_tips);
+FlatTree flatten(const BPTree &tree, const NameIndex &obs_index, bool bypass_tips);
 
 }  // namespace ssu

@@ -144,9 +144,26 @@ def lib():
 
 # ------------------------------------------------------------ marshalling
 
+class _StrArray:
+    """char** over one NUL-separated buffer (built without a per-string
+    ctypes conversion); keeps its buffers alive."""
+
+    def __init__(self, strings):
+        n = len(strings)
+        blob = ("\0".join(strings) + "\0").encode()
+        self.buf = C.create_string_buffer(blob, len(blob))
+        nul = np.flatnonzero(np.frombuffer(blob, dtype=np.uint8) == 0)
+        off = np.zeros(max(n, 1), dtype=np.uint64)
+        if n > 1:
+            off[1:n] = nul[: n - 1] + 1
+        self.ptrs = off + np.uint64(C.addressof(self.buf))
+        self.arr = (C.c_char_p * max(n, 1)).from_buffer(self.ptrs)
+
+
 def _strarr(strings):
-    arr = (C.c_char_p * max(len(strings), 1))()
-    arr[:len(strings)] = [s.encode() for s in strings]
+    holder = _StrArray(strings)
+    arr = holder.arr
+    arr._holder = holder  # the array keeps its buffers alive
     return arr
 
 
