@@ -306,6 +306,28 @@ SSU_EXTERN void ssu_b200_plan_set_timing(ssu_b200_plan_t *plan, int enable);
 SSU_EXTERN int ssu_b200_plan_stage_ms(ssu_b200_plan_t *plan, float *embed_ms, float *pair_ms, float *finalize_ms);
 SSU_EXTERN void ssu_b200_plan_destroy(ssu_b200_plan_t **plan);
 
+/* Weighted UniFrac (normalized when `normalized` != 0, else unnormalized)
+ * for callers that cannot allocate device memory - code running inside a
+ * framework that owns all device memory through its own arena, or under a
+ * fixed device-memory budget handed out up front.  No counterpart in the
+ * reference.  The caller passes device buffers: d_embedding holds
+ * n_embedded rows of ld doubles (ld a multiple of 128, >= n_samples), row e
+ * the proportions of embedded branch e per sample; d_lengths the n_embedded
+ * branch lengths; d_out receives the full n_samples x n_samples fp64 matrix.
+ * The call allocates nothing: its scratch (split-K partial tiles, per-sample
+ * weighted sums, tile list) lives in one 32 MiB file-scope device array that
+ * every GPU loading the library holds until exit.  n_samples is limited to
+ * 100000 and a call whose scratch needs exceed the array returns
+ * output_error with a message.  All calls share that array and it keeps the
+ * last call's contents (nothing in it needs to start at zero); calls that
+ * overlap on the GPU race on it.  The first call on a device resolves the
+ * array's address and sets kernel limits, so it should come before any
+ * stream capture.  Work is queued on `stream` (a cudaStream_t, may be NULL)
+ * and not synchronised. */
+SSU_EXTERN ComputeStatus ssu_b200_weighted_pairs_noalloc(const double *d_embedding, const double *d_lengths,
+                                                         uint32_t n_embedded, uint32_t n_samples, uint64_t ld,
+                                                         int normalized, double *d_out, void *stream);
+
 /* Name of the kernel family the plan's pair stage launches (for profiling). */
 SSU_EXTERN const char *ssu_b200_plan_pair_kernel(const ssu_b200_plan_t *plan);
 /* Library version string. */

@@ -166,7 +166,7 @@ __global__ void build_lut_kernel(const T *__restrict__ len, uint32_t E, T *__res
 
 // Faith PD: per sample sum of L over non-root nodes with u > 0
 // (src/unifrac.cpp:362-387), rows visited in postorder within fixed chunks.
-__global__ void faith_partial_kernel(const double *__restrict__ U, const double *__restrict__ len_by_row,
+static __global__ void faith_partial_kernel(const double *__restrict__ U, const double *__restrict__ len_by_row,
                                      const uint32_t *__restrict__ post_rows, uint32_t K, uint64_t ld,
                                      uint32_t chunk, double *__restrict__ partial) {
     const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -181,7 +181,7 @@ __global__ void faith_partial_kernel(const double *__restrict__ U, const double 
     partial[static_cast<uint64_t>(blockIdx.y) * ld + j] = s;
 }
 
-__global__ void zero_diagonal_kernel(void *out, uint32_t n, int fp64) {
+static __global__ void zero_diagonal_kernel(void *out, uint32_t n, int fp64) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     if (fp64)
