@@ -58,6 +58,30 @@ def dist_init():
     return world, rank, local
 
 
+def stripe_window(n_samples, rank, world):
+    """Balanced split of the (n+1)/2 stripes over ranks, as the reference's
+    set_tasks splits them over substeps (src/api.cpp:447-491)."""
+    total = (n_samples + 1) // 2
+    big, small = -(-total // world), total // world
+    n_big = total % world or world
+    start = sum(big if r < n_big else small for r in range(rank))
+    return start, start + (big if rank < n_big else small)
+
+
+def combine_ranks(values, world, device):
+    """[step_ms, e2e_ms, units, pair_ms] -> max-over-ranks times and summed units."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if world == 1:
+        return values[0], values[1], values[2], values[3]
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tsum = t.clone()
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    return tmax[0].item(), tmax[1].item(), tsum[2].item(), tmax[3].item()
+
+
 def make_workload(seed, args):
     import ssu_synth
     return ssu_synth.config2(seed=seed, n_samples=args.samples, n_tips=args.tips)
@@ -254,17 +278,8 @@ def main():
               tree.lengths.nbytes)
     d2h = int(args.samples) ** 2 * 8
 
-    t = torch.tensor([total_ms, sum(e2e_ms), float(units), mean_pair_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        tmax = t.clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t.clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        total_ms, e2e_total, mean_pair_ms = tmax[0].item(), tmax[1].item(), tmax[3].item()
-        all_units = tsum[2].item()
-    else:
-        e2e_total = sum(e2e_ms)
-        all_units = float(units)
+    total_ms, e2e_total, all_units, mean_pair_ms = combine_ranks(
+        [total_ms, sum(e2e_ms), float(units), mean_pair_ms], world, "cuda")
 
     if rank == 0:
         value = all_units * args.steps / (total_ms / 1e3)

@@ -1,0 +1,83 @@
+"""N > 1 paths on CPU with gloo, world size 2: the rank aggregation bench.py
+uses (max time, summed units), and one matrix split into disjoint stripe
+windows, one per rank, computed independently and gathered — no exchange
+during compute — equal to the single-process matrix."""
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _worker(rank, world, port, out_q):
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    for p in ("unifrac-binaries_b200", "oracle"):
+        sys.path.insert(0, os.path.join(ROOT, p))
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import bench
+        import oracle_py
+        import ssu_synth
+        step, e2e, units, pair = bench.combine_ranks([10.0 + rank, 5.0 * (rank + 1), 100.0, 2.0 - rank], world, "cpu")
+        tree = ssu_synth.random_binary_tree(80, 0.1, 5)
+        table = ssu_synth.geometric_table(tree.tip_names(), 45, 0.15, 8.0, 6)
+        start, stop = bench.stripe_window(table.n_samples, rank, world)
+        part = oracle_py.oracle_one_off(tree, table, "weighted_normalized_fp64", stripe_start=start,
+                                        stripe_stop=stop)["stripes"]
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (start, stop, part))
+        if rank == 0:
+            out_q.put({"agg": (step, e2e, units, pair), "gathered": gathered})
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.fixture(scope="module")
+def two_rank_result():
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return res
+
+
+def test_rank_aggregation_is_max_time_and_summed_units(two_rank_result):
+    step, e2e, units, pair = two_rank_result["agg"]
+    assert step == 11.0 and e2e == 10.0 and units == 200.0 and pair == 2.0
+
+
+def test_stripe_windows_partition_and_gather_to_the_full_matrix(two_rank_result, oracle_mod):
+    import ssu_synth
+    gathered = sorted(two_rank_result["gathered"], key=lambda g: g[0])
+    assert gathered[0][0] == 0 and gathered[0][1] == gathered[1][0] and gathered[1][1] == 23
+    stripes = np.concatenate([g[2] for g in gathered])
+    tree = ssu_synth.random_binary_tree(80, 0.1, 5)
+    table = ssu_synth.geometric_table(tree.tip_names(), 45, 0.15, 8.0, 6)
+    full = oracle_mod.oracle_one_off(tree, table, "weighted_normalized_fp64")["stripes"]
+    np.testing.assert_array_equal(stripes, full)
+
+
+@pytest.mark.parametrize("n,world", [(6, 2), (7, 3), (2048, 8), (25000, 8), (5, 4)])
+def test_stripe_window_covers_every_stripe_once(n, world):
+    sys.path.insert(0, ROOT)
+    import bench
+    total = (n + 1) // 2
+    windows = [bench.stripe_window(n, r, world) for r in range(world)]
+    assert windows[0][0] == 0 and windows[-1][1] == total
+    assert all(windows[i][1] == windows[i + 1][0] for i in range(world - 1))
