@@ -146,6 +146,11 @@ ComputeStatus make_plan(const ssu::Table &table, const ssu::BPTree &tree, const 
     spec.alpha = r.alpha;
     spec.bypass_tips = r.bypass;
     spec.normalize = r.normalize;
+    // UNIFRAC_B200_UNWEIGHTED_MODE=gemm selects the tensor-core contraction
+    // for unweighted methods (max relative error ~1e-7 instead of the stripe
+    // form's bit-level agreement)
+    if (const char *mode = std::getenv("UNIFRAC_B200_UNWEIGHTED_MODE"))
+        spec.unweighted_gemm = std::string(mode) == "gemm";
     std::string err;
     if (!select_device(err)) {
         report("device", err);

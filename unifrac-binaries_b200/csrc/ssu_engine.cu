@@ -6,9 +6,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <mutex>
 
+#include "ssu_gemm.cuh"
 #include "ssu_kernels.cuh"
 
 namespace ssu {
@@ -80,6 +83,39 @@ cudaMemPool_t device_pool(int dev) {
             return kOutputError;                                                                      \
         }                                                                                             \
     } while (0)
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no
+// link-time dependency on libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// 2-D fp16 tensor map over a row-major [rows][cols] matrix with a
+// 64-column x 128-row box and 128-byte swizzle (the UMMA K-major layout).
+bool make_fp16_map(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols) {
+    EncodeTiledFn f = encode_tiled();
+    if (!f) return false;
+    const cuuint64_t dims[2] = {cols, rows};
+    const cuuint64_t strides[1] = {cols * 2};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(tc::BLOCK_K), static_cast<cuuint32_t>(tc::BLOCK_M)};
+    const cuuint32_t estr[2] = {1, 1};
+    return f(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 // Type-erased pair stage: one kernel family with its tile shape.
 template <typename T>
@@ -273,6 +309,18 @@ struct PlanImpl {
     size_t partial_bytes = 0;
 
     std::vector<double> host_totals;  // per-sample totals, padded to ld
+
+    // tensor-core unweighted path
+    bool gemm = false;
+    uint32_t n_pad = 0, k_pad = 0, n_chunks = 0;
+    __half *d_A = nullptr, *d_Bh = nullptr, *d_Bl = nullptr, *d_lhi = nullptr, *d_llo = nullptr;
+    double *d_r = nullptr, *d_lsorted = nullptr, *d_chunk_scale = nullptr, *d_G = nullptr;
+    int32_t *d_parent_col = nullptr, *d_start_col = nullptr;
+    uint32_t *d_sample_ptr = nullptr;
+    int *d_error = nullptr;
+    CUtensorMap map_A{}, map_Bh{}, map_Bl{};
+    int setup_gemm(const Table &table, const FlatTree &tree);
+    int execute_gemm(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t ntiles);
 
     template <typename T>
     PairKernel<T> &kern();
@@ -574,11 +622,16 @@ int PlanImpl::execute_T(cudaStream_t s, const dev::OutSpec &out, const uint2 *ti
 }
 
 int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop) {
+    if (gemm) {
+        dev::OutSpec o{mode, d_out, start, stop};
+        return execute_gemm(stream, o, d_tiles, n_tiles);
+    }
     const int BM = spec.fp64 ? kd.BM : kf.BM, BN = spec.fp64 ? kd.BN : kf.BN;
     std::vector<uint2> tiles = make_tiles(n, BM, BN, mode == 1, start, stop);
     uint2 *d_t = nullptr;
     SSU_CK(upload(&d_t, tiles.data(), sizeof(uint2) * tiles.size()));
     uint32_t s = 1, rows = 0;
+    (void)s;
     if (spec.fp64)
         choose_splits<double>(static_cast<uint32_t>(tiles.size()), s, rows);
     else
@@ -596,6 +649,146 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
     return rc;
 }
 
+// --------------------------------------------------- tensor-core unweighted
+
+int PlanImpl::setup_gemm(const Table &table, const FlatTree &tree) {
+    const uint32_t chunk_nodes = tc::CHUNK_KB * tc::BLOCK_K;
+    n_pad = ((n + tc::BLOCK_M - 1) / tc::BLOCK_M) * tc::BLOCK_M;
+    k_pad = std::max<uint32_t>(chunk_nodes, ((E + chunk_nodes - 1) / chunk_nodes) * chunk_nodes);
+    n_chunks = k_pad / chunk_nodes;
+    // embedded nodes sorted by decreasing length
+    std::vector<uint32_t> order(E);
+    for (uint32_t e = 0; e < E; e++) order[e] = e;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return tree.length[a] > tree.length[b]; });
+    std::vector<int32_t> col_of_row(tree.n_nodes, -1);
+    for (uint32_t c = 0; c < E; c++) col_of_row[order[c]] = static_cast<int32_t>(c);
+    std::vector<double> lsorted(k_pad, 0.0), scale(n_chunks, 1.0);
+    std::vector<__half> lhi(k_pad, __float2half(0.0f)), llo(k_pad, __float2half(0.0f));
+    for (uint32_t c = 0; c < E; c++) lsorted[c] = tree.length[order[c]];
+    for (uint32_t ch = 0; ch < n_chunks; ch++) {
+        const double mx = lsorted[ch * chunk_nodes];
+        int sig = 0;
+        if (mx > 0) sig = 14 - static_cast<int>(std::floor(std::log2(mx)));
+        scale[ch] = std::ldexp(1.0, -sig);
+        for (uint32_t c = ch * chunk_nodes; c < (ch + 1) * chunk_nodes; c++) {
+            const double x = std::ldexp(lsorted[c], sig);
+            const __half h = __double2half(x);
+            lhi[c] = h;
+            llo[c] = __double2half(x - static_cast<double>(__half2float(h)));
+        }
+    }
+    // parents among embedded nodes
+    std::vector<int32_t> parent_row(tree.n_nodes, -1);
+    for (uint32_t r = 0; r < tree.n_nodes; r++)
+        for (uint32_t c = tree.child_ptr[r]; c < tree.child_ptr[r + 1]; c++) parent_row[tree.child_rows[c]] = r;
+    std::vector<int32_t> parent_col(k_pad, -1);
+    for (uint32_t c = 0; c < E; c++) {
+        const int32_t p = parent_row[order[c]];
+        parent_col[c] = (p >= 0 && static_cast<uint32_t>(p) < E) ? col_of_row[p] : -1;
+    }
+    // sample-major list of starting columns (tip, or its parent when tips are bypassed)
+    std::vector<int32_t> start_of_obs(table.n_obs, -1);
+    for (uint32_t r : tree.leaf_rows) {
+        const int32_t obs = tree.leaf_obs[r];
+        if (obs < 0) continue;
+        int32_t node = static_cast<int32_t>(r);
+        if (r >= E) node = parent_row[r];
+        start_of_obs[obs] = (node >= 0 && static_cast<uint32_t>(node) < E) ? col_of_row[node] : -1;
+    }
+    std::vector<uint32_t> sample_ptr(n + 1, 0);
+    for (uint32_t i = 0; i < table.n_obs; i++)
+        for (uint32_t q = table.indptr[i]; q < table.indptr[i + 1]; q++)
+            if (table.data[q] > 0.0 && start_of_obs[i] >= 0) sample_ptr[table.indices[q] + 1]++;
+    for (uint32_t j = 0; j < n; j++) sample_ptr[j + 1] += sample_ptr[j];
+    std::vector<int32_t> start_col(std::max<uint32_t>(sample_ptr[n], 1));
+    std::vector<uint32_t> fill(sample_ptr.begin(), sample_ptr.end() - 1);
+    for (uint32_t i = 0; i < table.n_obs; i++)
+        for (uint32_t q = table.indptr[i]; q < table.indptr[i + 1]; q++)
+            if (table.data[q] > 0.0 && start_of_obs[i] >= 0) start_col[fill[table.indices[q]]++] = start_of_obs[i];
+
+    const size_t op_bytes = sizeof(__half) * static_cast<size_t>(n_pad) * k_pad;
+    SSU_CK(alloc(&d_A, op_bytes));
+    SSU_CK(alloc(&d_Bh, op_bytes));
+    SSU_CK(alloc(&d_Bl, op_bytes));
+    SSU_CK(alloc(&d_r, sizeof(double) * n_pad));
+    SSU_CK(alloc(&d_G, sizeof(double) * static_cast<size_t>(n_pad) * n_pad));
+    SSU_CK(upload(&d_lhi, lhi.data(), sizeof(__half) * k_pad));
+    SSU_CK(upload(&d_llo, llo.data(), sizeof(__half) * k_pad));
+    SSU_CK(upload(&d_lsorted, lsorted.data(), sizeof(double) * k_pad));
+    SSU_CK(upload(&d_chunk_scale, scale.data(), sizeof(double) * n_chunks));
+    SSU_CK(upload(&d_parent_col, parent_col.data(), sizeof(int32_t) * k_pad));
+    SSU_CK(upload(&d_sample_ptr, sample_ptr.data(), sizeof(uint32_t) * (n + 1)));
+    SSU_CK(upload(&d_start_col, start_col.data(), sizeof(int32_t) * start_col.size()));
+    SSU_CK(alloc(&d_error, sizeof(int)));
+    SSU_CK(cudaMemsetAsync(d_error, 0, sizeof(int), stream));
+    if (!make_fp16_map(&map_A, d_A, n_pad, k_pad) || !make_fp16_map(&map_Bh, d_Bh, n_pad, k_pad) ||
+        !make_fp16_map(&map_Bl, d_Bl, n_pad, k_pad)) {
+        last_error = "cuTensorMapEncodeTiled failed";
+        return kOutputError;
+    }
+    SSU_CK(cudaFuncSetAttribute(tc::unweighted_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(tc::SMEM_BYTES)));
+    const size_t bits_smem = sizeof(uint32_t) * (k_pad / 32);
+    if (bits_smem > 200 * 1024) {
+        last_error = "tree too large for the tensor-core presence kernel";
+        return kOutputError;
+    }
+    SSU_CK(cudaFuncSetAttribute(tc::presence_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(bits_smem)));
+    // every ordered tile of G, grouped 12 x 12 so concurrent CTAs share row
+    // blocks in L2
+    std::vector<uint2> tiles;
+    const uint32_t nb = n_pad / tc::BLOCK_M;
+    for (uint32_t gk = 0; gk < nb; gk += 12)
+        for (uint32_t gl = 0; gl < nb; gl += 12)
+            for (uint32_t kb = gk; kb < std::min(nb, gk + 12); kb++)
+                for (uint32_t lb = gl; lb < std::min(nb, gl + 12); lb++) tiles.push_back(make_uint2(kb, lb));
+    n_tiles = static_cast<uint32_t>(tiles.size());
+    SSU_CK(upload(&d_tiles, tiles.data(), sizeof(uint2) * tiles.size()));
+    gemm = true;
+    return 0;
+}
+
+int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t ntiles) {
+    launches = 0;
+    if (timing) SSU_CK(cudaEventRecord(ev[0], s));
+    const size_t bits_smem = sizeof(uint32_t) * (k_pad / 32);
+    tc::presence_rows_kernel<<<n_pad, 256, bits_smem, s>>>(d_sample_ptr, d_start_col, d_parent_col, d_lhi, d_llo,
+                                                           d_lsorted, n, k_pad, d_A, d_Bh, d_Bl, d_r);
+    launches++;
+    if (timing) SSU_CK(cudaEventRecord(ev[1], s));
+    if (ntiles) {
+        tc::GemmArgs g{};
+        g.tiles = tiles;
+        g.n_tiles = ntiles;
+        g.n = n;
+        g.n_kblocks = k_pad / tc::BLOCK_K;
+        g.chunk_scale = d_chunk_scale;
+        g.G = d_G;
+        g.ldg = n_pad;
+        g.error = d_error;
+        g.wait_cycles = 2000000000LL;  // about one second per wait at B200 clocks
+        tc::unweighted_tc_kernel<<<ntiles, tc::THREADS, tc::SMEM_BYTES, s>>>(map_A, map_Bh, map_Bl, g);
+        launches++;
+    }
+    if (timing) SSU_CK(cudaEventRecord(ev[2], s));
+    if (n) {
+        const dim3 grid((n + 31) / 32, (n + 31) / 32);
+        tc::finish_unweighted_kernel<<<grid, dim3(32, 8), 0, s>>>(d_G, n_pad, d_r, n,
+                                                                  spec.method == Method::unweighted ? 1 : 0,
+                                                                  spec.fp64 ? 1 : 0, out);
+        launches++;
+    }
+    if (out.mode == 0 && n) {
+        dev::zero_diagonal_kernel<<<(n + 255) / 256, 256, 0, s>>>(out.ptr, n, spec.fp64 ? 1 : 0);
+        launches++;
+    }
+    if (timing) SSU_CK(cudaEventRecord(ev[3], s));
+    SSU_CK(cudaGetLastError());
+    return 0;
+}
+
 // ------------------------------------------------------------------ Plan
 
 int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spec, void *stream, Plan **out,
@@ -606,7 +799,22 @@ int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spe
     m.spec = spec;
     m.stream = static_cast<cudaStream_t>(stream);
     int rc = m.setup(table, tree);
-    if (!rc) rc = spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
+    bool want_gemm = spec.unweighted_gemm && !spec.vaw &&
+                     (spec.method == Method::unweighted || spec.method == Method::unweighted_unnormalized);
+    // presence is "proportion > 0": with no negative count it is the OR of
+    // the tips below a node; other inputs keep the stripe kernel
+    for (uint64_t q = 0; want_gemm && q < table.nnz(); q++)
+        if (!(table.data[q] >= 0.0)) want_gemm = false;
+    if (!rc && want_gemm) {
+        rc = m.setup_gemm(table, tree);
+        if (!rc && m.alloc(&m.d_full, (spec.fp64 ? sizeof(double) : sizeof(float)) * static_cast<uint64_t>(m.n) * m.n) !=
+                       cudaSuccess) {
+            m.last_error = "device allocation failed";
+            rc = kOutputError;
+        }
+    } else if (!rc) {
+        rc = spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
+    }
     if (rc) {
         err = m.last_error;
         delete p;
@@ -658,8 +866,20 @@ int Plan::execute(void *stream) {
     PlanImpl &m = *impl_;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : m.stream;
     dev::OutSpec o{0, m.d_full, 0, 0};
+    if (m.gemm) return m.execute_gemm(s, o, m.d_tiles, m.n_tiles);
     return m.spec.fp64 ? m.execute_T<double>(s, o, m.d_tiles, m.n_tiles, m.splits)
                        : m.execute_T<float>(s, o, m.d_tiles, m.n_tiles, m.splits);
+}
+
+int Plan::device_error() {
+    PlanImpl &m = *impl_;
+    if (!m.d_error) return 0;
+    int h = 0;
+    if (cudaMemcpyAsync(&h, m.d_error, sizeof(int), cudaMemcpyDeviceToHost, m.stream) != cudaSuccess ||
+        cudaStreamSynchronize(m.stream) != cudaSuccess)
+        return kOutputError;
+    if (h) cudaMemsetAsync(m.d_error, 0, sizeof(int), m.stream);
+    return h;
 }
 
 int Plan::run_full(void *host_out, bool out_fp64, std::string &err) {
@@ -675,6 +895,9 @@ int Plan::run_full(void *host_out, bool out_fp64, std::string &err) {
         if (e == cudaSuccess) e = cudaStreamSynchronize(m.stream);
         if (e != cudaSuccess) {
             m.last_error = cudaGetErrorString(e);
+            rc = kOutputError;
+        } else if (const int de = device_error()) {
+            m.last_error = "device wait expired (code " + std::to_string(de) + ")";
             rc = kOutputError;
         }
     }
@@ -698,6 +921,9 @@ int Plan::run_stripes(uint32_t start, uint32_t stop, double *const *host_stripes
         if (e == cudaSuccess) e = cudaStreamSynchronize(m.stream);
         if (e != cudaSuccess) {
             m.last_error = cudaGetErrorString(e);
+            rc = kOutputError;
+        } else if (const int de = device_error()) {
+            m.last_error = "device wait expired (code " + std::to_string(de) + ")";
             rc = kOutputError;
         } else {
             for (uint32_t s = start; s < stop; s++)
@@ -723,6 +949,9 @@ int Plan::run_condensed(double *host_cf, std::string &err) {
         if (e == cudaSuccess) e = cudaStreamSynchronize(m.stream);
         if (e != cudaSuccess) {
             m.last_error = cudaGetErrorString(e);
+            rc = kOutputError;
+        } else if (const int de = device_error()) {
+            m.last_error = "device wait expired (code " + std::to_string(de) + ")";
             rc = kOutputError;
         }
     }
@@ -769,7 +998,8 @@ int Plan::copy_result(void *host_out, void *stream) {
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : m.stream;
     const size_t bytes = (m.spec.fp64 ? sizeof(double) : sizeof(float)) * static_cast<size_t>(m.n) * m.n;
     if (cudaMemcpyAsync(host_out, m.d_full, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess) return kOutputError;
-    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : kOutputError;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return kOutputError;
+    return device_error() ? kOutputError : 0;
 }
 
 int Plan::synchronize() { return cudaStreamSynchronize(impl_->stream) == cudaSuccess ? 0 : kOutputError; }
@@ -781,7 +1011,10 @@ uint64_t Plan::work_units() const {
     return n * (n - (n ? 1 : 0)) / 2 * impl_->E;
 }
 uint32_t Plan::launches() const { return impl_->launches; }
-const char *Plan::pair_kernel_name() const { return impl_->spec.fp64 ? impl_->kd.name : impl_->kf.name; }
+const char *Plan::pair_kernel_name() const {
+    if (impl_->gemm) return "unweighted_tc_kernel";
+    return impl_->spec.fp64 ? impl_->kd.name : impl_->kf.name;
+}
 void Plan::set_timing(bool on) { impl_->timing = on; }
 
 int Plan::stage_times(StageTimes &out) {

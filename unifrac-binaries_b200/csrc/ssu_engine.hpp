@@ -21,6 +21,9 @@ struct MethodSpec {
     double alpha = 1.0;
     bool bypass_tips = false;
     bool normalize = true;
+    // unweighted (non variance-adjusted) only: run the tcgen05 contraction
+    // instead of the presence-word stripe kernel
+    bool unweighted_gemm = false;
 };
 
 // Method-name table of the reference (src/api.cpp:55-88): bare names are fp32.
@@ -64,6 +67,9 @@ class Plan {
     const void *device_result() const;
     int copy_result(void *host_out, void *stream);
     int synchronize();
+    // Error code raised by a device-side bounded wait since the last check
+    // (0 = none); synchronises the plan's stream.
+    int device_error();
 
     uint32_t n_samples() const;
     uint64_t n_embedded() const;
