@@ -381,7 +381,7 @@ def main():
     for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         barrier()
         t0 = time.perf_counter()
-        m, _ = ssu_b200.one_off_matrix(tree, table, args.method)
+        m, _ = ssu_b200.one_off_matrix(tree, table, args.method, copy=False)
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) * 1e3
         if i > 0:

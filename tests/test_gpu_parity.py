@@ -238,3 +238,16 @@ def test_config2_full_size_stripe_windows(ssu, oracle_mod):
     got = np.array([gpu32[k, (k + 1) % n] for k in range(n)], dtype=np.float64)
     r, _ = rel_err(got, ref[0])
     assert r < 1e-4
+
+
+def test_zero_copy_result_view_outlives_its_parent(ssu):
+    import gc
+    tree, table = _case(57, n_samples=64)
+    ref, _ = ssu.one_off_matrix(tree, table, "weighted_normalized_fp64")
+    view, _ = ssu.one_off_matrix(tree, table, "weighted_normalized_fp64", copy=False)
+    row = view[3]
+    del view
+    gc.collect()
+    np.testing.assert_array_equal(row, ref[3])
+    v32, _ = ssu.one_off_matrix(tree, table, "weighted_normalized_fp32", copy=False)
+    assert v32.dtype == np.float32 and v32.shape == (64, 64)

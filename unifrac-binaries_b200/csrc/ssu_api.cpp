@@ -17,6 +17,7 @@
 #include <sstream>
 #include <string>
 #include <sys/mman.h>
+#include <thread>
 #include <unistd.h>
 #include <unordered_set>
 #include <vector>
@@ -31,6 +32,7 @@ namespace {
 
 constexpr uint32_t kMmapFdMask = 0x0fff;  // src/api.cpp:27-28
 constexpr uint32_t kMmapFlag = 0x1000;
+constexpr size_t kHugeAlign = size_t(2) << 20;
 
 std::atomic<uint64_t> g_seed{5489u};
 
@@ -114,20 +116,32 @@ ssu::BPTree tree_from(const support_bptree_t *t, bool copy_names = false) {
     return ssu::BPTree::from_arrays(t->structure, t->lengths, t->names, t->n_parens, copy_names);
 }
 
-// VALIDATE_TREE_TABLE (src/api.cpp:94-100)
-ComputeStatus validate(const ssu::Table &table, const ssu::BPTree &tree) {
-    if (table.n_samples == 0 || table.n_obs == 0) return table_empty;
-    const ssu::NameSet tips = tree.tip_names();
-    for (const std::string_view &id : table.obs_ids)
-        if (!tips.count(id)) return table_and_tree_do_not_overlap;
-    return okay;
+// Observation name -> row (the last row wins for a repeated name, as the
+// reference's obs_id_index map); *distinct gets the number of distinct names.
+ssu::NameMap obs_map(const ssu::Table &table, uint32_t *distinct) {
+    ssu::NameMap m(table.n_obs);
+    for (uint32_t i = 0; i < table.n_obs; i++) m.set(table.obs_ids[i], i);
+    uint32_t d = 0;
+    for (uint32_t i = 0; i < table.n_obs; i++) d += m.find(table.obs_ids[i]) == static_cast<int64_t>(i);
+    *distinct = d;
+    return m;
 }
 
-// SYNC_TREE_TABLE (src/api.cpp:90-92) + flattening for the device.
+// VALIDATE_TREE_TABLE (src/api.cpp:94-100): every table id is a tip name.
+ComputeStatus validate(const ssu::Table &table, const ssu::BPTree &tree) {
+    if (table.n_samples == 0 || table.n_obs == 0) return table_empty;
+    uint32_t distinct = 0;
+    const ssu::NameMap obs = obs_map(table, &distinct);
+    return tree.count_matched(obs, table.n_obs) == distinct ? okay : table_and_tree_do_not_overlap;
+}
+
+// SYNC_TREE_TABLE (src/api.cpp:90-92) + flattening for the device; the
+// shear tags the kept tips with their table rows.
 ssu::FlatTree sync_tree(const ssu::Table &table, const ssu::BPTree &tree, bool bypass_tips) {
-    const ssu::NameSet keep(table.obs_ids.begin(), table.obs_ids.end());
-    const ssu::BPTree sheared = tree.shear(keep).collapse();
-    return ssu::flatten(sheared, table.obs_index(), bypass_tips);
+    uint32_t distinct = 0;
+    const ssu::NameMap obs = obs_map(table, &distinct);
+    const ssu::BPTree sheared = tree.shear_to(obs, table.n_obs, nullptr).collapse();
+    return ssu::flatten(sheared, bypass_tips);
 }
 
 struct Request {
@@ -192,10 +206,35 @@ bool alloc_full(TMat *&result, const std::vector<std::string_view> &ids, const c
             }
             if (!result->matrix) close(fd);
         }
+    } else if (bytes >= kHugeAlign) {
+        // 2 MiB-aligned with transparent huge pages: ~500x fewer page faults
+        // when the result is written; still released with free()
+        void *p = nullptr;
+        if (posix_memalign(&p, kHugeAlign, bytes) == 0) {
+            madvise(p, bytes, MADV_HUGEPAGE);
+            result->matrix = static_cast<TReal *>(p);
+        } else {
+            result->matrix = nullptr;
+        }
     } else {
         result->matrix = static_cast<TReal *>(std::malloc(bytes ? bytes : 1));
     }
     return result->matrix != nullptr;
+}
+
+// Touch every page of a fresh host buffer on a few threads (run while the
+// GPU computes, so the copy-out finds resident pages).
+void prefault(void *p, size_t bytes) {
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const size_t slice = ((bytes / hw) + kHugeAlign - 1) / kHugeAlign * kHugeAlign;
+    std::vector<std::thread> threads;
+    for (unsigned t = 0; t < hw; t++) {
+        const size_t a = t * slice;
+        if (a >= bytes) break;
+        const size_t len = std::min(slice, bytes - a);
+        threads.emplace_back([p, a, len] { std::memset(static_cast<char *>(p) + a, 0, len); });
+    }
+    for (auto &th : threads) th.join();
 }
 
 template <class TMat, class TReal>
@@ -240,7 +279,15 @@ ComputeStatus full_matrix(const ssu::Table &table, const ssu::BPTree &tree, cons
         return output_error;
     }
     std::string err;
-    const int rc = plan->run_full((*result)->matrix, sizeof(TReal) == 8, err);
+    int rc = plan->execute(nullptr);
+    if (rc == 0) {
+        const bool fresh = allocated && (*result)->flags == 0;
+        const size_t bytes = sizeof(TReal) * static_cast<size_t>(table.n_samples) * table.n_samples;
+        if (fresh && bytes >= kHugeAlign) prefault((*result)->matrix, bytes);  // overlaps the device work
+        rc = plan->download_full((*result)->matrix, fresh, err);
+    } else {
+        err = "launch failed";
+    }
     timer.step("stripes_to_matrix");
     if (rc) {
         report("one_off_matrix", err);

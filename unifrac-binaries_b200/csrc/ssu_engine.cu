@@ -905,6 +905,27 @@ int Plan::run_full(void *host_out, bool out_fp64, std::string &err) {
     return rc;
 }
 
+int Plan::download_full(void *host_out, bool pin, std::string &err) {
+    PlanImpl &m = *impl_;
+    const size_t bytes = (m.spec.fp64 ? sizeof(double) : sizeof(float)) * static_cast<size_t>(m.n) * m.n;
+    bool registered = false;
+    if (pin && bytes >= (size_t(1) << 20))
+        registered = cudaHostRegister(host_out, bytes, cudaHostRegisterDefault) == cudaSuccess;
+    if (pin && !registered) cudaGetLastError();  // a refused registration only means a pageable copy
+    cudaError_t e = cudaMemcpyAsync(host_out, m.d_full, bytes, cudaMemcpyDeviceToHost, m.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m.stream);
+    if (registered) cudaHostUnregister(host_out);
+    if (e != cudaSuccess) {
+        err = cudaGetErrorString(e);
+        return kOutputError;
+    }
+    if (const int de = device_error()) {
+        err = "device wait expired (code " + std::to_string(de) + ")";
+        return kOutputError;
+    }
+    return 0;
+}
+
 int Plan::run_stripes(uint32_t start, uint32_t stop, double *const *host_stripes, std::string &err) {
     PlanImpl &m = *impl_;
     const size_t count = static_cast<size_t>(stop - start) * m.n;

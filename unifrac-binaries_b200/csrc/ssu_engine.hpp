@@ -64,6 +64,11 @@ class Plan {
     // Faith PD values of every sample (plan from create_faith).
     int run_faith(double *host_values, std::string &err);
 
+    // Copy the full result of the last execute into host memory; with
+    // `pin`, the destination is page-locked for the copy (cudaHostRegister)
+    // and released after.  Synchronises and checks device-side errors.
+    int download_full(void *host_out, bool pin, std::string &err);
+
     const void *device_result() const;
     int copy_result(void *host_out, void *stream);
     int synchronize();

@@ -8,14 +8,13 @@ namespace ssu {
 
 void BPTree::pair_parentheses() {
     match.assign(open.size(), 0);
-    std::vector<uint32_t> stack;
-    stack.reserve(64);
+    std::vector<uint32_t> stack(open.size() / 2 + 1);
+    size_t top = 0;
     for (uint32_t i = 0; i < open.size(); i++) {
         if (open[i]) {
-            stack.push_back(i);
-        } else if (!stack.empty()) {
-            uint32_t o = stack.back();
-            stack.pop_back();
+            stack[top++] = i;
+        } else if (top > 0) {
+            const uint32_t o = stack[--top];
             match[o] = i;
             match[i] = o;
         }
@@ -161,7 +160,8 @@ bool BPTree::from_newick(const std::string &text, BPTree &out) {
     return true;
 }
 
-BPTree BPTree::masked(const std::vector<uint8_t> &keep, const std::vector<double> &lengths) const {
+BPTree BPTree::masked(const std::vector<uint8_t> &keep, const std::vector<double> &lengths,
+                      const std::vector<int32_t> *tags) const {
     BPTree r;
     r.storage = storage;
     size_t m = 0;
@@ -169,14 +169,55 @@ BPTree BPTree::masked(const std::vector<uint8_t> &keep, const std::vector<double
     r.open.reserve(m);
     r.length.reserve(m);
     r.name.reserve(m);
+    const std::vector<int32_t> &tg = tags ? *tags : tag;
+    const bool tagged = !tg.empty();
+    r.open.resize(m);
+    r.length.resize(m);
+    r.name.resize(m);
+    if (tagged) r.tag.resize(m);
+    size_t j = 0;
     for (uint32_t i = 0; i < size(); i++) {
         if (!keep[i]) continue;
-        r.open.push_back(open[i]);
-        r.length.push_back(lengths[i]);
-        r.name.push_back(name[i]);
+        r.open[j] = open[i];
+        r.length[j] = lengths[i];
+        r.name[j] = name[i];
+        if (tagged) r.tag[j] = tg[i];
+        j++;
     }
     r.pair_parentheses();
     return r;
+}
+
+BPTree BPTree::shear_to(const NameMap &obs, uint32_t n_obs, uint32_t *n_rows_matched) const {
+    const uint32_t n = size();
+    std::vector<uint8_t> mask(n, 0);
+    std::vector<uint32_t> parent(n, UINT32_MAX);
+    std::vector<uint32_t> stack;
+    for (uint32_t i = 0; i < n; i++) {
+        if (open[i]) {
+            parent[i] = stack.empty() ? UINT32_MAX : stack.back();
+            stack.push_back(i);
+        } else if (!stack.empty()) {
+            stack.pop_back();
+        }
+    }
+    std::vector<int32_t> tags(n, -1);
+    std::vector<uint8_t> seen(n_obs, 0);
+    uint32_t matched = 0;
+    for (uint32_t i = 0; i + 1 < n; i++) {
+        if (!leaf(i)) continue;
+        const int64_t row = obs.find(name[i]);
+        if (row < 0) continue;
+        tags[i] = static_cast<int32_t>(row);
+        if (!seen[row]) {
+            seen[row] = 1;
+            matched++;
+        }
+        mask[i] = mask[i + 1] = 1;
+        for (uint32_t p = parent[i]; p != UINT32_MAX && !mask[p]; p = parent[p]) mask[p] = mask[match[p]] = 1;
+    }
+    if (n_rows_matched) *n_rows_matched = matched;
+    return masked(mask, length, &tags);
 }
 
 BPTree BPTree::shear(const NameSet &keep) const {
@@ -228,13 +269,30 @@ NameSet BPTree::tip_names() const {
     return out;
 }
 
+uint32_t BPTree::count_matched(const NameMap &obs, uint32_t n_obs) const {
+    std::vector<uint8_t> seen(n_obs, 0);
+    uint32_t matched = 0;
+    for (uint32_t i = 0; i + 1 < size(); i++) {
+        if (!leaf(i)) continue;
+        const int64_t row = obs.find(name[i]);
+        if (row >= 0 && !seen[row]) {
+            seen[row] = 1;
+            matched++;
+        }
+    }
+    return matched;
+}
+
 uint32_t BPTree::n_tips() const {
     uint32_t c = 0;
     for (uint32_t i = 0; i + 1 < size(); i++) c += leaf(i);
     return c;
 }
 
-FlatTree flatten(const BPTree &t, const NameIndex &obs_index, bool bypass_tips) {
+namespace {
+
+template <class ObsOf>
+FlatTree flatten_impl(const BPTree &t, bool bypass_tips, ObsOf obs_of) {
     FlatTree f;
     const uint32_t n = t.size();
     const uint32_t total = n / 2;
@@ -257,7 +315,7 @@ FlatTree flatten(const BPTree &t, const NameIndex &obs_index, bool bypass_tips) 
     f.leaf_obs.assign(f.n_nodes, -1);
     f.postorder_row.resize(f.n_nodes);
     std::vector<uint32_t> height(f.n_nodes, 0);
-    std::vector<std::vector<uint32_t>> kids(f.n_nodes);
+    std::vector<uint32_t> n_kids(f.n_nodes, 0);
     uint32_t max_height = 0;
     for (uint32_t k = 0; k < f.n_nodes; k++) {
         const uint32_t o = post_open[k];
@@ -266,24 +324,28 @@ FlatTree flatten(const BPTree &t, const NameIndex &obs_index, bool bypass_tips) 
         f.length[row] = t.length[o];
         if (t.leaf(o)) {
             f.leaf_rows.push_back(row);
-            auto it = obs_index.find(t.name[o]);
-            if (it != obs_index.end()) f.leaf_obs[row] = static_cast<int32_t>(it->second);
+            f.leaf_obs[row] = obs_of(o);
         } else {
-            uint32_t h = 0;
+            uint32_t h = 0, nk = 0;
             for (uint32_t c = o + 1; c < n && t.open[c]; c = t.match[c] + 1) {
-                const uint32_t cr = row_of_open[c];
-                kids[row].push_back(cr);
-                h = std::max(h, height[cr] + 1);
+                h = std::max(h, height[row_of_open[c]] + 1);
+                nk++;
             }
+            n_kids[row] = nk;
             height[row] = h;
             max_height = std::max(max_height, h);
         }
     }
+    // children as CSR, left to right
     f.child_ptr.assign(f.n_nodes + 1, 0);
-    for (uint32_t row = 0; row < f.n_nodes; row++) f.child_ptr[row + 1] = f.child_ptr[row] + kids[row].size();
-    f.child_rows.reserve(f.child_ptr[f.n_nodes]);
-    for (uint32_t row = 0; row < f.n_nodes; row++)
-        f.child_rows.insert(f.child_rows.end(), kids[row].begin(), kids[row].end());
+    for (uint32_t row = 0; row < f.n_nodes; row++) f.child_ptr[row + 1] = f.child_ptr[row] + n_kids[row];
+    f.child_rows.assign(f.child_ptr[f.n_nodes], 0);
+    for (uint32_t k = 0; k < f.n_nodes; k++) {
+        const uint32_t o = post_open[k];
+        if (t.leaf(o)) continue;
+        uint32_t w = f.child_ptr[row_of_open[o]];
+        for (uint32_t c = o + 1; c < n && t.open[c]; c = t.match[c] + 1) f.child_rows[w++] = row_of_open[c];
+    }
     // internal rows bucketed by height 1..max_height
     f.level_ptr.assign(max_height + 1, 0);
     for (uint32_t row = 0; row < f.n_nodes; row++)
@@ -294,6 +356,19 @@ FlatTree flatten(const BPTree &t, const NameIndex &obs_index, bool bypass_tips) 
     for (uint32_t row = 0; row < f.n_nodes; row++)
         if (height[row] > 0) f.level_rows[fill[height[row] - 1]++] = row;
     return f;
+}
+
+}  // namespace
+
+FlatTree flatten(const BPTree &t, const NameIndex &obs_index, bool bypass_tips) {
+    return flatten_impl(t, bypass_tips, [&](uint32_t o) -> int32_t {
+        auto it = obs_index.find(t.name[o]);
+        return it != obs_index.end() ? static_cast<int32_t>(it->second) : -1;
+    });
+}
+
+FlatTree flatten(const BPTree &t, bool bypass_tips) {
+    return flatten_impl(t, bypass_tips, [&](uint32_t o) -> int32_t { return t.tag.empty() ? -1 : t.tag[o]; });
 }
 
 }  // namespace ssu

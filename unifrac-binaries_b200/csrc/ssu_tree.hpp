@@ -12,6 +12,8 @@
 #include <unordered_set>
 #include <vector>
 
+#include "ssu_names.hpp"
+
 namespace ssu {
 
 using NameSet = std::unordered_set<std::string_view>;
@@ -28,6 +30,9 @@ struct BPTree {
     std::vector<std::string_view> name;
     std::vector<uint32_t> match;
     std::shared_ptr<std::deque<std::string>> storage;
+    // optional per-parenthesis tag carried through shear/collapse: the table
+    // row of each kept tip (-1 elsewhere)
+    std::vector<int32_t> tag;
 
     uint32_t size() const { return static_cast<uint32_t>(open.size()); }
     bool leaf(uint32_t i) const { return open[i] && i + 1 < open.size() && !open[i + 1]; }
@@ -45,12 +50,21 @@ struct BPTree {
 
     // Keep the tips named in `keep` and all their ancestors (src/tree.cpp:145-163).
     BPTree shear(const NameSet &keep) const;
+    // The same shear for the observation names of a table (`obs` maps a name
+    // to its row): kept tips are tagged with their row.  *n_rows_matched, when
+    // given, receives how many distinct rows some tip carries.
+    BPTree shear_to(const NameMap &obs, uint32_t n_obs, uint32_t *n_rows_matched) const;
     // Remove non-root nodes with a single child, adding their length to the
     // child, in preorder (src/tree.cpp:165-191).
     BPTree collapse() const;
-    BPTree masked(const std::vector<uint8_t> &keep, const std::vector<double> &lengths) const;
+    // The parentheses flagged in `keep`, with `lengths` (and `tags`, or this
+    // tree's own tags) carried along.
+    BPTree masked(const std::vector<uint8_t> &keep, const std::vector<double> &lengths,
+                  const std::vector<int32_t> *tags = nullptr) const;
 
     NameSet tip_names() const;
+    // Distinct rows of `obs` that some tip's name maps to.
+    uint32_t count_matched(const NameMap &obs, uint32_t n_obs) const;
     uint32_t n_tips() const;
 };
 
@@ -72,5 +86,7 @@ struct FlatTree {
 };
 
 FlatTree flatten(const BPTree &tree, const NameIndex &obs_index, bool bypass_tips);
+// Flatten a tree whose tips carry table rows in `tag` (from shear_to).
+FlatTree flatten(const BPTree &tree, bool bypass_tips);
 
 }  // namespace ssu

@@ -12,6 +12,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import re
+import weakref
 
 import numpy as np
 
@@ -199,10 +200,26 @@ def is_fp64(method):
 
 # ------------------------------------------------------------ entry points
 
+def _owned_view(res, destroy, ctype, n):
+    """numpy view of a C result matrix; the C result is destroyed when the
+    last array referring to it is gone (the ctypes buffer is the base)."""
+    buf = (ctype * (n * n)).from_address(C.addressof(res.contents.matrix.contents)) if n else (ctype * 1)()
+    holder = res
+
+    def release(h=holder):
+        destroy(C.byref(h))
+
+    weakref.finalize(buf, release)
+    dt = np.float64 if ctype is C.c_double else np.float32
+    return np.frombuffer(buf, dtype=dt, count=n * n).reshape(n, n)
+
+
 def one_off_matrix(tree, table, method, variance_adjust=False, alpha=1.0, bypass_tips=False, normalize=True,
-                   subsample_depth=0, with_replacement=False, mmap_dir=None):
+                   subsample_depth=0, with_replacement=False, mmap_dir=None, copy=True):
     """Full n x n matrix through one_off_matrix_inmem_v3 (fp64 methods) or
-    one_off_matrix_inmem_fp32_v3 (fp32 methods).  Returns (matrix, ids)."""
+    one_off_matrix_inmem_fp32_v3 (fp32 methods).  Returns (matrix, ids).
+    copy=False returns a zero-copy view of the library's result, released
+    when no array refers to it any more."""
     L = lib()
     x = Inputs(tree, table)
     md = mmap_dir.encode() if mmap_dir else None
@@ -214,8 +231,10 @@ def one_off_matrix(tree, table, method, variance_adjust=False, alpha=1.0, bypass
         if st != 0:
             raise SSUError(st, "one_off_matrix_inmem_v3")
         n = res.contents.n_samples
-        out = np.ctypeslib.as_array(res.contents.matrix, shape=(n, n)).copy()
         ids = _ids(res.contents.sample_ids, n)
+        if not copy:
+            return _owned_view(res, L.destroy_mat_full_fp64, C.c_double, n), ids
+        out = np.ctypeslib.as_array(res.contents.matrix, shape=(n, n)).copy()
         L.destroy_mat_full_fp64(C.byref(res))
     else:
         res = C.POINTER(MatFull32)()
@@ -225,8 +244,10 @@ def one_off_matrix(tree, table, method, variance_adjust=False, alpha=1.0, bypass
         if st != 0:
             raise SSUError(st, "one_off_matrix_inmem_fp32_v3")
         n = res.contents.n_samples
-        out = np.ctypeslib.as_array(res.contents.matrix, shape=(n, n)).copy()
         ids = _ids(res.contents.sample_ids, n)
+        if not copy:
+            return _owned_view(res, L.destroy_mat_full_fp32, C.c_float, n), ids
+        out = np.ctypeslib.as_array(res.contents.matrix, shape=(n, n)).copy()
         L.destroy_mat_full_fp32(C.byref(res))
     return out, ids
 
