@@ -48,7 +48,9 @@ def parse():
     p.add_argument("--method", default=METHOD)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="config2", choices=["config2", "config3"],
+    p.add_argument("--replicates", type=int, default=100)
+    p.add_argument("--tables5", type=int, default=64)
+    p.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
                    help="config3: unweighted fp64, tensor-core contraction vs the plain stripe form")
     p.add_argument("--samples3", type=int, default=25000)
     p.add_argument("--tips3", type=int, default=100000)
@@ -317,6 +319,198 @@ def run_config3(args):
     print(json.dumps(line), flush=True)
 
 
+def _time_batch(torch, plan, stream, steps, warmup, flush):
+    """Per-step device time (ms) of a batch plan replayed as a CUDA graph."""
+    plan.set_graph(True)
+    for _ in range(max(warmup, 1)):
+        plan.execute(stream.cuda_stream)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.execute(stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return sum(ms) / len(ms)
+
+
+def _unbatched_ms(torch, ssu_b200, tree, tables, method, stream, **kw):
+    """Device time of the same tables run one plan per table (no batching)."""
+    total = 0.0
+    for t in tables:
+        p = ssu_b200.Plan(tree, t, method, **kw)
+        p.execute(stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        p.execute(stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+        p.close()
+    return total
+
+
+def _rel_err(a, b):
+    import numpy as np
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nz = b != 0
+    r = float(np.max(np.abs(a[nz] - b[nz]) / np.abs(b[nz]))) if nz.any() else 0.0
+    z = float(np.max(np.abs(a[~nz]))) if (~nz).any() else 0.0
+    return r, z
+
+
+def _batch_setup():
+    import torch
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    return torch, stream, flush
+
+
+def run_config4(args):
+    """100 rarefied replicates (depth 1,000) of a 10,000-feature x 5,000-sample
+    table on a 10,000-tip tree, unweighted and weighted-normalized fp32, every
+    replicate of a method in one batch plan replayed as one CUDA graph."""
+    torch, stream, flush = _batch_setup()
+    import ssu_b200
+    import ssu_synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    t0 = time.perf_counter()
+    tree, base, reps = ssu_synth.config4(n_replicates=args.replicates)
+    gen_s = time.perf_counter() - t0
+    methods = ["unweighted_fp32", "weighted_normalized_fp32"]
+    per, total_units, total_ms, launches = {}, 0, 0.0, 0
+    clocks = ClockSampler(0)
+    for m in methods:
+        t0 = time.perf_counter()
+        plan = ssu_b200.BatchPlan(tree, reps, m)
+        create_s = time.perf_counter() - t0
+        units = plan.work_units()
+        clocks.start()
+        ms = _time_batch(torch, plan, stream, args.steps, args.warmup, flush)
+        clk = clocks.stop()
+        launches += plan.launches()
+        total_units += units
+        total_ms += ms
+        r0 = plan.results()[0]
+        per_table_ms = _unbatched_ms(torch, ssu_b200, tree, reps, m, stream)
+        single = ssu_b200.Plan(tree, reps[0], m)
+        single.execute()
+        s0 = single.result()
+        single.close()
+        per[m] = {"ms_per_step": ms, "value": units / (ms / 1e3), "units": units, "groups": plan.n_groups(),
+                  "tuning": plan.tuning(), "kernel": plan.pair_kernel(), "launches_per_step": plan.launches(),
+                  "plan_create_s": create_s, "clocks": clk, "one_plan_per_replicate_ms": per_table_ms,
+                  "batched_speedup": per_table_ms / ms,
+                  "replicate0_vs_one_table_plan_max_rel": _rel_err(r0, s0)[0]}
+        plan.close()
+        # parity of replicate 0 with the reference's own CPU build (fp32 and fp64)
+        if oracle_py.ref_available():
+            ref64 = oracle_py.ref_one_off(tree, reps[0], m.replace("_fp32", "_fp64"), with_timing=True)
+            ref32 = oracle_py.ref_one_off(tree, reps[0], m, with_timing=True)
+            per[m]["replicate0_parity"] = {"ours_vs_ref_fp64_max_rel": _rel_err(r0, ref64["matrix"])[0],
+                                           "ref_fp32_vs_ref_fp64_max_rel": _rel_err(ref32["matrix"],
+                                                                                    ref64["matrix"])[0]}
+            e = ref32["n_embedded"]
+            n0 = reps[0].n_samples
+            per[m]["cpu_reference_replicate0"] = {"seconds": ref32["seconds"][0],
+                                                  "value": n0 * (n0 - 1) / 2 * e / ref32["seconds"][0],
+                                                  "cores": os.cpu_count()}
+    # end to end through the batch C API: host tables in, host matrices out
+    e2e = {}
+    if args.e2e_steps > 0:
+        for m in methods:
+            t0 = time.perf_counter()
+            out = ssu_b200.one_off_batch(tree, reps, m, copy=False)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            e2e[m] = {"seconds": dt, "value": per[m]["units"] / dt}
+            del out
+    h2d = sum(int(t.indptr.nbytes + t.indices.nbytes + t.data.nbytes) for t in reps)
+    d2h = sum(4 * t.n_samples ** 2 for t in reps)
+    line = {
+        "metric": METRIC, "value": total_units / (total_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-4 generator; replicates rarefied "
+                                                    "on the host, the same tables fed to both engines)",
+        "config": {"workload": f"{args.replicates} rarefied replicates (depth 1000) of 10k features x 5000 samples, "
+                               "10k-tip tree; unweighted_fp32 + weighted_normalized_fp32; full matrices",
+                   "l2": "flushed between steps; embedding > L2", "generation_s": gen_s},
+        "methods": per,
+        "e2e": {"value": (sum(e["value"] * e["seconds"] for e in e2e.values()) / sum(e["seconds"] for e in e2e.values()))
+                if e2e else None, "unit": UNIT, "per_method": e2e, "h2d_bytes_per_step": h2d * len(methods),
+                "d2h_bytes_per_step": d2h * len(methods)},
+        "gpu_launches": launches * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_config5(args):
+    """64 tables of log-uniform sample counts in [64, 4096] on one 50,000-tip
+    tree, generalized (alpha 0.5) and the four variance-adjusted methods in
+    fp64, each method one batch plan replayed as one CUDA graph; per-table
+    parity with the reference's CPU build on the smaller tables."""
+    torch, stream, flush = _batch_setup()
+    import ssu_b200
+    import ssu_synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    t0 = time.perf_counter()
+    tree, tables = ssu_synth.config5(n_tables=args.tables5)
+    gen_s = time.perf_counter() - t0
+    runs = [("generalized_fp64", False), ("unweighted_fp64", True), ("weighted_normalized_fp64", True),
+            ("weighted_unnormalized_fp64", True), ("generalized_fp64", True)]
+    small = sorted(range(len(tables)), key=lambda t: tables[t].n_samples)[:6]
+    per, total_units, total_ms, launches = [], 0, 0.0, 0
+    clocks = ClockSampler(0)
+    for m, vaw in runs:
+        t0 = time.perf_counter()
+        plan = ssu_b200.BatchPlan(tree, tables, m, variance_adjust=vaw, alpha=0.5)
+        create_s = time.perf_counter() - t0
+        units = plan.work_units()
+        clocks.start()
+        ms = _time_batch(torch, plan, stream, args.steps, args.warmup, flush)
+        clk = clocks.stop()
+        launches += plan.launches()
+        total_units += units
+        total_ms += ms
+        res = plan.results()
+        per_table_ms = _unbatched_ms(torch, ssu_b200, tree, tables, m, stream, variance_adjust=vaw, alpha=0.5)
+        entry = {"method": m, "variance_adjust": vaw, "ms_per_step": ms, "value": units / (ms / 1e3),
+                 "one_plan_per_table_ms": per_table_ms, "batched_speedup": per_table_ms / ms,
+                 "units": units, "groups": plan.n_groups(), "tuning": plan.tuning(), "kernel": plan.pair_kernel(),
+                 "launches_per_step": plan.launches(), "plan_create_s": create_s, "clocks": clk}
+        if oracle_py.ref_available():
+            worst = 0.0
+            for t in small:
+                ref = oracle_py.ref_one_off(tree, tables[t], m, variance_adjust=vaw, alpha=0.5)["matrix"]
+                worst = max(worst, _rel_err(res[t], ref)[0])
+            entry["parity_vs_reference_fp64"] = {"tables": [int(tables[t].n_samples) for t in small],
+                                                 "max_rel": worst}
+        per.append(entry)
+        del res
+        plan.close()
+    line = {
+        "metric": METRIC, "value": total_units / (total_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-5 generator)",
+        "config": {"workload": f"{len(tables)} tables, sample counts log-uniform in [64, 4096] "
+                               f"(total {sum(t.n_samples for t in tables)}), 50k-tip tree, 1% non-zero; "
+                               "generalized a=0.5 and VAW unweighted / weighted_normalized / "
+                               "weighted_unnormalized / generalized a=0.5, fp64, full matrices",
+                   "l2": "flushed between steps; embedding > L2", "generation_s": gen_s},
+        "methods": per,
+        "gpu_launches": launches * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def gp_units_e(units, n):
     return int(units // (n * (n - 1) // 2)) if n > 1 else 0
 
@@ -327,6 +521,10 @@ def main():
         return run_reference(args)
     if args.workload == "config3":
         return run_config3(args)
+    if args.workload == "config4":
+        return run_config4(args)
+    if args.workload == "config5":
+        return run_config5(args)
     import torch
     import torch.distributed as dist
     world, rank, local = dist_init()

@@ -292,7 +292,8 @@ SSU_EXTERN ComputeStatus ssu_b200_plan_execute(ssu_b200_plan_t *plan, void *stre
 /* Device pointer to the n x n result (double for *_fp64 methods, else float). */
 SSU_EXTERN const void *ssu_b200_plan_device_result(const ssu_b200_plan_t *plan);
 SSU_EXTERN ComputeStatus ssu_b200_plan_copy_result(ssu_b200_plan_t *plan, void *host_out, void *stream);
-/* n(n-1)/2 * embedded branches: the pair-branch updates one execute performs. */
+/* Sum over tables of n(n-1)/2 * embedded branches: the pair-branch updates
+ * one execute performs. */
 SSU_EXTERN uint64_t ssu_b200_plan_work_units(const ssu_b200_plan_t *plan);
 SSU_EXTERN uint32_t ssu_b200_plan_n_samples(const ssu_b200_plan_t *plan);
 SSU_EXTERN uint64_t ssu_b200_plan_n_embedded(const ssu_b200_plan_t *plan);
@@ -327,6 +328,73 @@ SSU_EXTERN void ssu_b200_plan_destroy(ssu_b200_plan_t **plan);
 SSU_EXTERN ComputeStatus ssu_b200_weighted_pairs_noalloc(const double *d_embedding, const double *d_lengths,
                                                          uint32_t n_embedded, uint32_t n_samples, uint64_t ld,
                                                          int normalized, double *d_out, void *stream);
+
+/* ---- batches: many tables sharing one tree, in one device plan ----------
+ *
+ * The reference computes several rarefied replicates of a table only inside
+ * unifrac_multi_to_file_v2/_v3 (src/api.hpp:565-595), which write them to a
+ * file; it has no in-memory batch call.  These entry points take n_tables
+ * tables (rarefied replicates, or independent tables of uneven sample
+ * counts) that share one tree.  Table t's result equals
+ * one_off_matrix_inmem_v3 (or _fp32_v3) on table t alone - the same
+ * validation, shear and collapse per table - but the whole batch runs as one
+ * plan: tables are embedded together in groups that fit the device, and each
+ * group's pair stage is one persistent kernel launch over the tiles of all
+ * its tables.  results[0..n_tables) receive malloc'ed matrices to release
+ * with destroy_mat_full_fp64 / _fp32; on an error none is left allocated.
+ * Environment: UNIFRAC_B200_GROUP_BYTES caps a group's device bytes,
+ * UNIFRAC_B200_AUTOTUNE=0 keeps the default tile shapes (batches measure
+ * their candidates), UNIFRAC_B200_TUNE_CACHE=<file> keeps tuned choices
+ * across processes. */
+SSU_EXTERN ComputeStatus ssu_b200_one_off_batch_inmem_v3(const support_biom_t *const *tables, unsigned int n_tables,
+                                                         const support_bptree_t *tree_data,
+                                                         const char *unifrac_method, bool variance_adjust,
+                                                         double alpha, bool bypass_tips,
+                                                         bool normalize_sample_counts, mat_full_fp64_t **results);
+SSU_EXTERN ComputeStatus ssu_b200_one_off_batch_inmem_fp32_v3(const support_biom_t *const *tables,
+                                                              unsigned int n_tables,
+                                                              const support_bptree_t *tree_data,
+                                                              const char *unifrac_method, bool variance_adjust,
+                                                              double alpha, bool bypass_tips,
+                                                              bool normalize_sample_counts,
+                                                              mat_full_fp32_t **results);
+/* The compute part of unifrac_multi_to_file_v3 in memory: n_subsamples
+ * replicates of table_data, each rarefied to subsample_depth with this
+ * library's sampler (seeded by ssu_set_random_seed's seed + replicate
+ * index), computed as one batch; results[r] holds replicate r's matrix over
+ * the samples that reached the depth. */
+SSU_EXTERN ComputeStatus ssu_b200_subsample_batch_inmem_v3(const support_biom_t *table_data,
+                                                           const support_bptree_t *tree_data,
+                                                           const char *unifrac_method, bool variance_adjust,
+                                                           double alpha, bool bypass_tips,
+                                                           bool normalize_sample_counts, unsigned int n_subsamples,
+                                                           unsigned int subsample_depth,
+                                                           bool subsample_with_replacement,
+                                                           mat_full_fp64_t **results);
+SSU_EXTERN ComputeStatus ssu_b200_subsample_batch_inmem_fp32_v3(
+    const support_biom_t *table_data, const support_bptree_t *tree_data, const char *unifrac_method,
+    bool variance_adjust, double alpha, bool bypass_tips, bool normalize_sample_counts, unsigned int n_subsamples,
+    unsigned int subsample_depth, bool subsample_with_replacement, mat_full_fp32_t **results);
+/* Device-resident batch plan: results of every table, one after the other,
+ * in device memory (ssu_b200_plan_table_offset elements in).  group_bytes
+ * caps the device bytes of one group's embedding (0: half the free memory);
+ * autotune: -1 default, 0 heuristic tile shapes, 1 measured. */
+SSU_EXTERN ComputeStatus ssu_b200_batch_plan_create(const support_biom_t *const *tables, unsigned int n_tables,
+                                                    const support_bptree_t *tree_data, const char *unifrac_method,
+                                                    bool variance_adjust, double alpha, bool bypass_tips,
+                                                    bool normalize_sample_counts, uint64_t group_bytes,
+                                                    int autotune, ssu_b200_plan_t **plan);
+SSU_EXTERN uint32_t ssu_b200_plan_n_tables(const ssu_b200_plan_t *plan);
+SSU_EXTERN uint32_t ssu_b200_plan_n_groups(const ssu_b200_plan_t *plan);
+SSU_EXTERN uint32_t ssu_b200_plan_table_samples(const ssu_b200_plan_t *plan, uint32_t table);
+SSU_EXTERN uint64_t ssu_b200_plan_table_offset(const ssu_b200_plan_t *plan, uint32_t table);
+/* Embedded branches of the table's own sheared, collapsed tree. */
+SSU_EXTERN uint64_t ssu_b200_plan_table_embedded(const ssu_b200_plan_t *plan, uint32_t table);
+/* With enable != 0, the next execute captures the plan's whole launch
+ * sequence as one CUDA graph and every later execute launches that graph. */
+SSU_EXTERN void ssu_b200_plan_set_graph(ssu_b200_plan_t *plan, int enable);
+/* How the pair kernel's tile shape was chosen, and the shape. */
+SSU_EXTERN const char *ssu_b200_plan_tuning(const ssu_b200_plan_t *plan);
 
 /* Name of the kernel family the plan's pair stage launches (for profiling). */
 SSU_EXTERN const char *ssu_b200_plan_pair_kernel(const ssu_b200_plan_t *plan);

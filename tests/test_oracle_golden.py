@@ -6,6 +6,7 @@ src/test_helper.hpp) except where the golden is an exact small rational."""
 import numpy as np
 import pytest
 
+import ssu_synth
 from conftest import matrix_from_stripes, stripes_from_golden
 
 CASES = [
@@ -63,3 +64,24 @@ def test_golden_sample_totals(golden, test_table):
     exp = golden["test_su"]["test_unifrac_sample_counts"]["arrays"]["exp"][0]
     dense = test_table.dense()
     np.testing.assert_array_equal(dense.sum(axis=0), exp)
+
+
+def test_rarefaction_generator_properties():
+    """The host rarefaction that feeds the batched-replicate workload: every
+    kept sample sums to the depth, no count grows, lighter samples and
+    emptied features are dropped (src/biom_subsampled.cpp:287-353)."""
+    import numpy as np
+    tree = ssu_synth.random_binary_tree(300, 0.1, 1)
+    base = ssu_synth.negbin_table(tree.tip_names(), 80, 0.2, 50.0, 0.5, 2)
+    depth = 150
+    r = ssu_synth.rarefy(base, depth, 3)
+    bd = base.dense()
+    keep = np.flatnonzero(bd.sum(axis=0) >= depth)
+    assert r.sample_ids == [base.sample_ids[j] for j in keep]
+    d = r.dense()
+    rows = [base.obs_ids.index(o) for o in r.obs_ids]
+    assert np.all(d <= bd[rows][:, keep])
+    assert np.all(d.sum(axis=0) == depth)
+    assert np.all(d.sum(axis=1) > 0)
+    again = ssu_synth.rarefy(base, depth, 3)
+    np.testing.assert_array_equal(again.dense(), d)

@@ -320,6 +320,184 @@ ComputeStatus full_matrix_v3(const support_biom_t *table_data, const support_bpt
     return full_matrix<TReal, TMat>(table, tree, r, mmap_dir, result);
 }
 
+// ------------------------------------------------------------------ batches
+
+// Host side of a batch: per-table validation, the tree sheared to the union
+// of the tables' observations and collapsed, each table's rows of the union
+// observations, and each table's own embedded node count.
+struct BatchHost {
+    ssu::FlatTree flat;
+    ssu::TableSet set;
+};
+
+ComputeStatus batch_prepare(const std::vector<const ssu::Table *> &tables, const ssu::BPTree &tree, bool bypass,
+                            BatchHost &bh) {
+    if (tables.empty() || tables.size() > 65535) return table_empty;
+    size_t total_obs = 0;
+    for (const ssu::Table *t : tables) {
+        if (t->n_samples == 0 || t->n_obs == 0) return table_empty;
+        total_obs += t->n_obs;
+    }
+    ssu::NameMap uni(total_obs);
+    std::vector<std::vector<uint32_t>> uid(tables.size());
+    uint32_t n_union = 0;
+    for (size_t t = 0; t < tables.size(); t++) {
+        const ssu::Table &tb = *tables[t];
+        uid[t].resize(tb.n_obs);
+        for (uint32_t i = 0; i < tb.n_obs; i++) {
+            int64_t u = uni.find(tb.obs_ids[i]);
+            if (u < 0) {
+                uni.set(tb.obs_ids[i], n_union);
+                u = n_union++;
+            }
+            uid[t][i] = static_cast<uint32_t>(u);
+        }
+    }
+    // VALIDATE_TREE_TABLE (src/api.cpp:94-100) for every table: each of its
+    // observations names a tip
+    std::vector<uint8_t> in_tree(n_union, 0);
+    for (uint32_t i = 0; i + 1 < tree.size(); i++) {
+        if (!tree.leaf(i)) continue;
+        const int64_t u = uni.find(tree.name[i]);
+        if (u >= 0) in_tree[u] = 1;
+    }
+    for (size_t t = 0; t < tables.size(); t++)
+        for (uint32_t u : uid[t])
+            if (!in_tree[u]) return table_and_tree_do_not_overlap;
+    bh.flat = ssu::flatten(tree.shear_to(uni, n_union, nullptr).collapse(), bypass);
+    bh.set.tables = tables;
+    bh.set.obs_row.assign(tables.size(), std::vector<int32_t>(n_union, -1));
+    bh.set.embedded.resize(tables.size());
+    if (bypass) bh.set.row_active.resize(tables.size());
+    for (size_t t = 0; t < tables.size(); t++) {
+        for (uint32_t i = 0; i < tables[t]->n_obs; i++) bh.set.obs_row[t][uid[t][i]] = static_cast<int32_t>(i);
+        bh.set.embedded[t] =
+            ssu::table_embedded(bh.flat, bh.set.obs_row[t], bypass, bypass ? &bh.set.row_active[t] : nullptr);
+    }
+    return okay;
+}
+
+ComputeStatus batch_plan(const std::vector<const ssu::Table *> &tables, const ssu::BPTree &tree, const Request &r,
+                         const ssu::BatchOptions &opts, std::unique_ptr<ssu::Plan> &plan, StepTimer &timer) {
+    ssu::MethodSpec spec;
+    if (!ssu::parse_method(r.method, spec.method, spec.fp64)) return unknown_method;
+    spec.vaw = r.vaw;
+    spec.alpha = r.alpha;
+    spec.bypass_tips = r.bypass;
+    spec.normalize = r.normalize;
+    std::string err;
+    if (!select_device(err)) {
+        report("device", err);
+        return output_error;
+    }
+    BatchHost bh;
+    ComputeStatus st = batch_prepare(tables, tree, r.bypass, bh);
+    if (st != okay) return st;
+    timer.step("sync_tree_tables");
+    ssu::Plan *p = nullptr;
+    const int rc = ssu::Plan::create_batch(bh.set, bh.flat, spec, opts, nullptr, &p, err);
+    if (rc) {
+        report("batch plan", err);
+        return static_cast<ComputeStatus>(rc);
+    }
+    plan.reset(p);
+    // the caller's CSR arrays are read by the uploads queued above
+    if (plan->synchronize()) return output_error;
+    timer.step("upload");
+    return okay;
+}
+
+template <class TReal, class TMat>
+ComputeStatus batch_matrices(const std::vector<const ssu::Table *> &tables, const ssu::BPTree &tree,
+                             const Request &r, TMat **results) {
+    StepTimer timer("one_off_batch_inmem");
+    std::unique_ptr<ssu::Plan> plan;
+    ComputeStatus st = batch_plan(tables, tree, r, ssu::BatchOptions{}, plan, timer);
+    if (st != okay) return st;
+    const size_t T = tables.size();
+    for (size_t t = 0; t < T; t++) results[t] = nullptr;
+    auto release = [&] {
+        for (size_t t = 0; t < T; t++) destroy_full<TMat, TReal>(&results[t]);
+    };
+    for (size_t t = 0; t < T; t++)
+        if (!alloc_full<TReal, TMat>(results[t], tables[t]->sample_ids, nullptr)) {
+            release();
+            report("one_off_batch", "result allocation failed");
+            return output_error;
+        }
+    std::string err;
+    int rc = plan->execute(nullptr);
+    if (rc == 0) {
+        for (size_t t = 0; t < T; t++) {  // overlaps the device work
+            const size_t bytes = sizeof(TReal) * static_cast<size_t>(tables[t]->n_samples) * tables[t]->n_samples;
+            if (bytes >= kHugeAlign) prefault(results[t]->matrix, bytes);
+        }
+        for (size_t t = 0; t < T && rc == 0; t++) {
+            const uint64_t n = tables[t]->n_samples;
+            rc = plan->download_range(plan->table_offset(static_cast<uint32_t>(t)), n * n, results[t]->matrix, true,
+                                      err);
+        }
+    } else {
+        err = "launch failed";
+    }
+    timer.step("batch_to_matrices");
+    if (rc) {
+        report("one_off_batch", err);
+        release();
+        return static_cast<ComputeStatus>(rc);
+    }
+    return okay;
+}
+
+template <class TReal, class TMat>
+ComputeStatus batch_v3(const support_biom_t *const *tables_data, unsigned int n_tables,
+                       const support_bptree_t *tree_data, const Request &r, bool want_fp64, TMat **results) {
+    bool fp64 = false;
+    ComputeStatus st = is_fp64_method(r.method, fp64);
+    if (st != okay) return st;
+    if (fp64 != want_fp64) return invalid_method;
+    if (!tables_data || n_tables == 0 || !results) return table_empty;
+    if (!tree_data) return tree_missing;
+    std::vector<ssu::Table> tables;
+    tables.reserve(n_tables);
+    for (unsigned int t = 0; t < n_tables; t++) {
+        const support_biom_t *td = tables_data[t];
+        if (!td || td->n_samples <= 0 || td->n_obs <= 0) return table_empty;
+        tables.push_back(table_from(td));
+    }
+    std::vector<const ssu::Table *> ptrs;
+    for (const ssu::Table &t : tables) ptrs.push_back(&t);
+    return batch_matrices<TReal, TMat>(ptrs, tree_from(tree_data), r, results);
+}
+
+template <class TReal, class TMat>
+ComputeStatus subsample_batch_v3(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                 const Request &r, bool want_fp64, unsigned int n_subsamples, unsigned int depth,
+                                 bool with_replacement, TMat **results) {
+    bool fp64 = false;
+    ComputeStatus st = is_fp64_method(r.method, fp64);
+    if (st != okay) return st;
+    if (fp64 != want_fp64) return invalid_method;
+    if (!table_data || table_data->n_samples <= 0 || table_data->n_obs <= 0 || n_subsamples == 0 || depth == 0 ||
+        !results)
+        return table_empty;
+    if (!tree_data) return tree_missing;
+    const ssu::Table table = table_from(table_data);
+    const ssu::BPTree tree = tree_from(tree_data);
+    st = validate(table, tree);
+    if (st != okay) return st;
+    std::vector<ssu::Table> reps;
+    reps.reserve(n_subsamples);
+    const uint64_t seed = g_seed.load();
+    for (unsigned int i = 0; i < n_subsamples; i++) {
+        reps.push_back(table.rarefied(depth, with_replacement, seed + i));
+        if (reps.back().n_samples == 0 || reps.back().n_obs == 0) return table_empty;
+    }
+    std::vector<const ssu::Table *> ptrs;
+    for (const ssu::Table &t : reps) ptrs.push_back(&t);
+    return batch_matrices<TReal, TMat>(ptrs, tree, r, results);
+}
+
 ComputeStatus condensed(const ssu::Table &table, const ssu::BPTree &tree, const Request &r, mat_t **result) {
     StepTimer timer("one_off");
     std::unique_ptr<ssu::Plan> plan;
@@ -882,6 +1060,93 @@ void ssu_b200_plan_destroy(ssu_b200_plan_t **plan) {
         *plan = nullptr;
     }
 }
+
+ComputeStatus ssu_b200_one_off_batch_inmem_v3(const support_biom_t *const *tables, unsigned int n_tables,
+                                              const support_bptree_t *tree_data, const char *unifrac_method,
+                                              bool variance_adjust, double alpha, bool bypass_tips,
+                                              bool normalize_sample_counts, mat_full_fp64_t **results) {
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return batch_v3<double, mat_full_fp64_t>(tables, n_tables, tree_data, r, true, results);
+}
+
+ComputeStatus ssu_b200_one_off_batch_inmem_fp32_v3(const support_biom_t *const *tables, unsigned int n_tables,
+                                                   const support_bptree_t *tree_data, const char *unifrac_method,
+                                                   bool variance_adjust, double alpha, bool bypass_tips,
+                                                   bool normalize_sample_counts, mat_full_fp32_t **results) {
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return batch_v3<float, mat_full_fp32_t>(tables, n_tables, tree_data, r, false, results);
+}
+
+ComputeStatus ssu_b200_subsample_batch_inmem_v3(const support_biom_t *table_data, const support_bptree_t *tree_data,
+                                                const char *unifrac_method, bool variance_adjust, double alpha,
+                                                bool bypass_tips, bool normalize_sample_counts,
+                                                unsigned int n_subsamples, unsigned int subsample_depth,
+                                                bool subsample_with_replacement, mat_full_fp64_t **results) {
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return subsample_batch_v3<double, mat_full_fp64_t>(table_data, tree_data, r, true, n_subsamples, subsample_depth,
+                                                       subsample_with_replacement, results);
+}
+
+ComputeStatus ssu_b200_subsample_batch_inmem_fp32_v3(const support_biom_t *table_data,
+                                                     const support_bptree_t *tree_data, const char *unifrac_method,
+                                                     bool variance_adjust, double alpha, bool bypass_tips,
+                                                     bool normalize_sample_counts, unsigned int n_subsamples,
+                                                     unsigned int subsample_depth, bool subsample_with_replacement,
+                                                     mat_full_fp32_t **results) {
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return subsample_batch_v3<float, mat_full_fp32_t>(table_data, tree_data, r, false, n_subsamples,
+                                                      subsample_depth, subsample_with_replacement, results);
+}
+
+ComputeStatus ssu_b200_batch_plan_create(const support_biom_t *const *tables_data, unsigned int n_tables,
+                                         const support_bptree_t *tree_data, const char *unifrac_method,
+                                         bool variance_adjust, double alpha, bool bypass_tips,
+                                         bool normalize_sample_counts, uint64_t group_bytes, int autotune,
+                                         ssu_b200_plan_t **plan) {
+    bool fp64 = false;
+    ComputeStatus st = is_fp64_method(unifrac_method, fp64);
+    if (st != okay) return st;
+    if (!tables_data || n_tables == 0 || !plan) return table_empty;
+    if (!tree_data) return tree_missing;
+    std::vector<ssu::Table> tables;
+    tables.reserve(n_tables);
+    for (unsigned int t = 0; t < n_tables; t++) {
+        const support_biom_t *td = tables_data[t];
+        if (!td || td->n_samples <= 0 || td->n_obs <= 0) return table_empty;
+        tables.push_back(table_from(td));
+    }
+    std::vector<const ssu::Table *> ptrs;
+    for (const ssu::Table &t : tables) ptrs.push_back(&t);
+    StepTimer timer("batch_plan_create");
+    ssu::BatchOptions opts;
+    opts.group_bytes = group_bytes;
+    opts.autotune = autotune;
+    auto *h = new ssu_b200_plan();
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    st = batch_plan(ptrs, tree_from(tree_data), r, opts, h->plan, timer);
+    if (st != okay) {
+        delete h;
+        return st;
+    }
+    *plan = h;
+    return okay;
+}
+
+uint32_t ssu_b200_plan_n_tables(const ssu_b200_plan_t *plan) { return plan ? plan->plan->n_tables() : 0; }
+uint32_t ssu_b200_plan_n_groups(const ssu_b200_plan_t *plan) { return plan ? plan->plan->n_groups() : 0; }
+uint32_t ssu_b200_plan_table_samples(const ssu_b200_plan_t *plan, uint32_t table) {
+    return plan ? plan->plan->table_samples(table) : 0;
+}
+uint64_t ssu_b200_plan_table_offset(const ssu_b200_plan_t *plan, uint32_t table) {
+    return plan ? plan->plan->table_offset(table) : 0;
+}
+uint64_t ssu_b200_plan_table_embedded(const ssu_b200_plan_t *plan, uint32_t table) {
+    return plan ? plan->plan->table_embedded(table) : 0;
+}
+void ssu_b200_plan_set_graph(ssu_b200_plan_t *plan, int enable) {
+    if (plan) plan->plan->set_graph(enable != 0);
+}
+const char *ssu_b200_plan_tuning(const ssu_b200_plan_t *plan) { return plan ? plan->plan->tuning() : ""; }
 
 const char *ssu_b200_plan_pair_kernel(const ssu_b200_plan_t *plan) {
     return plan ? plan->plan->pair_kernel_name() : "";

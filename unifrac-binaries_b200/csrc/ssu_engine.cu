@@ -1,5 +1,6 @@
 // Device plan of the B200 UniFrac engine: upload, embedding, pair stage,
-// output layouts.  One plan = one table on one GPU, one stream.
+// output layouts.  One plan = one table, or a batch of tables sharing a
+// tree, on one GPU and one stream.
 #include "ssu_engine.hpp"
 
 #include <algorithm>
@@ -9,10 +10,13 @@
 #include <cuda.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
+#include <fstream>
+#include <map>
 #include <mutex>
 
 #include "ssu_gemm.cuh"
 #include "ssu_kernels.cuh"
+#include "ssu_pairs.cuh"
 
 namespace ssu {
 
@@ -117,135 +121,12 @@ bool make_fp16_map(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols) {
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Type-erased pair stage: one kernel family with its tile shape.
-template <typename T>
-struct PairKernel {
-    int BM = 0, BN = 0, threads = 0;
-    int row_quantum = 1;     // node rows (or words) per pipeline stage
-    size_t smem = 0;
-    size_t partial_per_tile = 0;  // accumulator values per tile
-    int blocks_per_sm = 1;
-    const char *name = "";
-    void (*launch)(const dev::PairArgs<T> &, dim3, size_t, cudaStream_t) = nullptr;
-    void (*finalize)(const dev::PairArgs<T> &, uint32_t, cudaStream_t) = nullptr;
-    cudaError_t (*configure)(size_t) = nullptr;
-    cudaError_t (*occupancy)(int *, int, size_t) = nullptr;
-};
-
-template <typename T, class Op, int BM, int BN, int TM, int TN, int KC>
-PairKernel<T> values_kernel(const char *name) {
-    PairKernel<T> k;
-    k.BM = BM;
-    k.BN = BN;
-    k.threads = (BM / TM) * (BN / TN);
-    k.row_quantum = KC;
-    k.smem = dev::pair_values_smem<T, Op, BM, BN, KC>();
-    k.partial_per_tile = static_cast<size_t>(BM) * BN * Op::NACC;
-    k.name = name;
-    k.launch = [](const dev::PairArgs<T> &a, dim3 grid, size_t smem, cudaStream_t s) {
-        dev::pair_values_kernel<T, Op, BM, BN, TM, TN, KC><<<grid, (BM / TM) * (BN / TN), smem, s>>>(a);
-    };
-    k.finalize = [](const dev::PairArgs<T> &a, uint32_t splits, cudaStream_t s) {
-        dev::split_finalize_kernel<T, Op, BM, BN, TM, TN><<<a.n_tiles, (BM / TM) * (BN / TN), 0, s>>>(a, splits);
-    };
-    k.configure = [](size_t smem) {
-        return cudaFuncSetAttribute(dev::pair_values_kernel<T, Op, BM, BN, TM, TN, KC>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    };
-    k.occupancy = [](int *blocks, int threads, size_t smem) {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, dev::pair_values_kernel<T, Op, BM, BN, TM, TN, KC>,
-                                                             threads, smem);
-    };
-    return k;
-}
-
-template <typename T, bool NORM, int BM, int BN, int TM, int TN, int KW>
-PairKernel<T> bits_kernel(const char *name) {
-    using Op = dev::OpUnweightedBits<T, NORM>;
-    PairKernel<T> k;
-    k.BM = BM;
-    k.BN = BN;
-    k.threads = (BM / TM) * (BN / TN);
-    k.row_quantum = KW;
-    k.smem = dev::pair_bits_smem<T, BM, BN, KW>();
-    k.partial_per_tile = static_cast<size_t>(BM) * BN * Op::NACC;
-    k.name = name;
-    k.launch = [](const dev::PairArgs<T> &a, dim3 grid, size_t smem, cudaStream_t s) {
-        dev::pair_bits_kernel<T, NORM, BM, BN, TM, TN, KW><<<grid, (BM / TM) * (BN / TN), smem, s>>>(a);
-    };
-    k.finalize = [](const dev::PairArgs<T> &a, uint32_t splits, cudaStream_t s) {
-        dev::split_finalize_kernel<T, Op, BM, BN, TM, TN><<<a.n_tiles, (BM / TM) * (BN / TN), 0, s>>>(a, splits);
-    };
-    k.configure = [](size_t smem) {
-        return cudaFuncSetAttribute(dev::pair_bits_kernel<T, NORM, BM, BN, TM, TN, KW>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    };
-    k.occupancy = [](int *blocks, int threads, size_t smem) {
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, dev::pair_bits_kernel<T, NORM, BM, BN, TM, TN, KW>,
-                                                             threads, smem);
-    };
-    return k;
-}
-
-// alpha kind: 1 -> sqrt, 2 -> identity, 3 -> constant 1, 0 -> pow
-int alpha_kind(double alpha) {
-    if (alpha == 0.5) return 1;
-    if (alpha == 1.0) return 2;
-    if (alpha == 0.0) return 3;
-    return 0;
-}
-
-template <typename T, template <typename, int> class OpT>
-PairKernel<T> generalized_family(double alpha, const char *name) {
-    switch (alpha_kind(alpha)) {
-    case 1: return values_kernel<T, OpT<T, 1>, 128, 64, 8, 4, 16>(name);
-    case 2: return values_kernel<T, OpT<T, 2>, 128, 64, 8, 4, 16>(name);
-    case 3: return values_kernel<T, OpT<T, 3>, 128, 64, 8, 4, 16>(name);
-    default: return values_kernel<T, OpT<T, 0>, 128, 64, 8, 4, 16>(name);
-    }
-}
-
-template <typename T>
-PairKernel<T> select_kernel(const MethodSpec &s) {
-    constexpr bool D = sizeof(T) == 8;
-    constexpr int KCW = D ? 16 : 32;
-    if (s.vaw) {
-        switch (s.method) {
-        case Method::unweighted:
-            return values_kernel<T, dev::OpVawUnweighted<T, true>, 128, 64, 8, 4, 16>("pair_values<vaw_unweighted>");
-        case Method::unweighted_unnormalized:
-            return values_kernel<T, dev::OpVawUnweighted<T, false>, 128, 64, 8, 4, 16>(
-                "pair_values<vaw_unweighted_unnormalized>");
-        case Method::weighted_normalized:
-            return values_kernel<T, dev::OpVawWeighted<T, true>, 128, 64, 8, 4, 16>(
-                "pair_values<vaw_weighted_normalized>");
-        case Method::weighted_unnormalized:
-            return values_kernel<T, dev::OpVawWeighted<T, false>, 128, 64, 8, 4, 16>(
-                "pair_values<vaw_weighted_unnormalized>");
-        case Method::generalized:
-            return generalized_family<T, dev::OpVawGeneralized>(s.alpha, "pair_values<vaw_generalized>");
-        }
-    }
-    switch (s.method) {
-    case Method::unweighted:
-        return bits_kernel<T, true, 128, 64, 8, 4, D ? 2 : 4>("pair_bits<unweighted>");
-    case Method::unweighted_unnormalized:
-        return bits_kernel<T, false, 128, 64, 8, 4, D ? 2 : 4>("pair_bits<unweighted_unnormalized>");
-    case Method::weighted_normalized:
-        return values_kernel<T, dev::OpWeighted<T, true>, 128, 128, 8, 8, KCW>("pair_values<weighted_normalized>");
-    case Method::weighted_unnormalized:
-        return values_kernel<T, dev::OpWeighted<T, false>, 128, 128, 8, 8, KCW>(
-            "pair_values<weighted_unnormalized>");
-    case Method::generalized:
-        return generalized_family<T, dev::OpGeneralized>(s.alpha, "pair_values<generalized>");
-    }
-    return PairKernel<T>();
-}
-
-// Tiles (kb, lb) holding at least one pair k < l; with a stripe window only
-// those whose pairs reach a stripe in [start, stop).
-std::vector<uint2> make_tiles(uint32_t n, int BM, int BN, bool windowed, uint32_t start, uint32_t stop) {
-    std::vector<uint2> tiles;
+// Tiles of one table (columns [base, base + n) of its group) holding at
+// least one pair k < l; with a stripe window only those whose pairs reach a
+// stripe in [start, stop).  x and y are block indices in the group's
+// columns, z is the table.
+void append_tiles(std::vector<uint4> &tiles, uint32_t table, uint32_t base, uint32_t n, int BM, int BN,
+                  bool windowed, uint32_t start, uint32_t stop) {
     const uint32_t nbk = (n + BM - 1) / BM, nbl = (n + BN - 1) / BN;
     for (uint32_t kb = 0; kb < nbk; kb++) {
         const int64_t kmin = static_cast<int64_t>(kb) * BM;
@@ -262,65 +143,155 @@ std::vector<uint2> make_tiles(uint32_t n, int BM, int BN, bool windowed, uint32_
                 const bool hit2 = s2lo < static_cast<int64_t>(stop) && s2hi >= static_cast<int64_t>(start);
                 if (!hit1 && !hit2) continue;
             }
-            tiles.push_back(make_uint2(kb, lb));
+            tiles.push_back(make_uint4(base / BM + kb, base / BN + lb, table, 0));
         }
     }
-    return tiles;
+}
+
+// Pair-kernel shapes chosen by measurement, per problem class, for the life
+// of the process and, with UNIFRAC_B200_TUNE_CACHE=<file>, across processes
+// (one "key<TAB>shape" line per choice).
+class TuneCache {
+  public:
+    static TuneCache &get() {
+        static TuneCache c;
+        return c;
+    }
+    bool find(const std::string &key, std::string &shape) {
+        std::lock_guard<std::mutex> lock(mu_);
+        load();
+        auto it = entries_.find(key);
+        if (it == entries_.end()) return false;
+        shape = it->second;
+        return true;
+    }
+    void put(const std::string &key, const std::string &shape) {
+        std::lock_guard<std::mutex> lock(mu_);
+        load();
+        entries_[key] = shape;
+        const char *path = std::getenv("UNIFRAC_B200_TUNE_CACHE");
+        if (path && *path) {
+            std::ofstream f(path, std::ios::app);
+            if (f) f << key << '\t' << shape << '\n';
+        }
+    }
+
+  private:
+    void load() {
+        if (loaded_) return;
+        loaded_ = true;
+        const char *path = std::getenv("UNIFRAC_B200_TUNE_CACHE");
+        if (!path || !*path) return;
+        std::ifstream f(path);
+        std::string line;
+        while (std::getline(f, line)) {
+            const size_t tab = line.find('\t');
+            if (tab != std::string::npos) entries_[line.substr(0, tab)] = line.substr(tab + 1);
+        }
+    }
+    std::mutex mu_;
+    bool loaded_ = false;
+    std::map<std::string, std::string> entries_;
+};
+
+int log2_bucket(uint64_t x) {
+    int b = 0;
+    while (x > 1) {
+        x >>= 1;
+        b++;
+    }
+    return b;
+}
+
+int env_int(const char *name, int fallback) {
+    const char *v = std::getenv(name);
+    return (v && *v) ? std::atoi(v) : fallback;
 }
 
 }  // namespace
 
+// Tables that are embedded together: one column slab of the embedding each.
+struct Group {
+    uint32_t t0 = 0, t1 = 0;             // tables [t0, t1)
+    uint64_t ld = 0;                     // columns = row stride of the embedding
+    int32_t *d_tip_obs = nullptr;        // [tip][t1 - t0]: the tip's row in each table, or -1
+    double *d_totals = nullptr;          // per column, fp64
+    void *d_tot = nullptr;               // per column in T (variance adjusted)
+    uint32_t *d_block_table = nullptr;   // per 128 columns: the table (per-table lengths)
+    std::vector<double> totals;
+    uint4 *d_tiles = nullptr;
+    uint32_t n_tiles = 0, splits = 1, rows_per_split = 0;
+};
+
 struct PlanImpl {
     MethodSpec spec;
     bool faith = false;
-    uint32_t n = 0, K = 0, E = 0;
-    uint64_t ld = 0;
+    bool batch = false;
+    uint32_t n = 0;  // samples of all tables
+    uint32_t K = 0, E = 0;
+    uint64_t ld = 0;      // widest group
+    uint32_t max_table_n = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int n_sms = 148;
     std::string last_error;
 
-    // inputs
+    // tables: concatenated CSR, descriptors, groups
+    std::vector<dev::TableDesc> tdesc;
+    dev::TableDesc *d_tdesc = nullptr;
+    std::vector<uint64_t> table_E;
+    std::vector<Group> groups;
     uint32_t *d_indptr = nullptr, *d_indices = nullptr;
-    double *d_data = nullptr, *d_totals = nullptr;
-    uint32_t *d_tip_rows = nullptr;
-    int32_t *d_tip_obs = nullptr;
+    double *d_data = nullptr;
+
+    // tree
     uint32_t n_tips = 0;
+    uint32_t *d_tip_rows = nullptr;
     uint32_t *d_child_ptr = nullptr, *d_child_rows = nullptr, *d_level_rows = nullptr;
     std::vector<uint32_t> level_ptr;
     uint32_t *d_post_rows = nullptr;
     double *d_len_rows = nullptr;
+    void *d_len = nullptr;  // embedded lengths in T; per table when len_stride > 0
+    uint64_t len_stride = 0;
+    std::vector<double> host_len;
+    std::vector<std::vector<uint8_t>> row_active;
 
-    // embedding and method buffers
-    void *d_U = nullptr, *d_C = nullptr, *d_len = nullptr, *d_tot = nullptr;
+    // embedding and method buffers, sized for the widest group
+    void *d_U = nullptr, *d_C = nullptr;
     void *d_W = nullptr, *d_part = nullptr;
     uint32_t n_parts = 0, part_chunk = 0;
     unsigned long long *d_P = nullptr;
     void *d_lut = nullptr;
+    uint64_t lut_stride = 0;
     uint32_t n_words = 0;
     void *d_full = nullptr;
+    uint64_t full_elems = 0;
 
     // pair stage
     PairKernel<double> kd;
     PairKernel<float> kf;
-    uint2 *d_tiles = nullptr;
-    uint32_t n_tiles = 0, splits = 1, rows_per_split = 0;
     void *d_partial = nullptr;
     size_t partial_bytes = 0;
+    int autotune = 0;
+    std::string tuning = "default";
 
-    std::vector<double> host_totals;  // per-sample totals, padded to ld
-
-    // tensor-core unweighted path
+    // tensor-core unweighted path (one table)
     bool gemm = false;
     uint32_t n_pad = 0, k_pad = 0, n_chunks = 0;
     __half *d_A = nullptr, *d_Bh = nullptr, *d_Bl = nullptr, *d_lhi = nullptr, *d_llo = nullptr;
     double *d_r = nullptr, *d_lsorted = nullptr, *d_chunk_scale = nullptr, *d_G = nullptr;
     int32_t *d_parent_col = nullptr, *d_start_col = nullptr;
     uint32_t *d_sample_ptr = nullptr;
+    uint2 *d_gemm_tiles = nullptr;
+    uint32_t n_gemm_tiles = 0;
     int *d_error = nullptr;
     CUtensorMap map_A{}, map_Bh{}, map_Bl{};
     int setup_gemm(const Table &table, const FlatTree &tree);
     int execute_gemm(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t ntiles);
+
+    // CUDA graph of execute()
+    bool graph_on = false, capturing = false;
+    cudaGraphExec_t graph = nullptr;
 
     template <typename T>
     PairKernel<T> &kern();
@@ -350,20 +321,31 @@ struct PlanImpl {
         return cudaMemcpyAsync(*p, src, bytes, cudaMemcpyHostToDevice, stream);
     }
 
-    int setup(const Table &table, const FlatTree &tree);
+    bool bits() const {
+        return !faith && !spec.vaw &&
+               (spec.method == Method::unweighted || spec.method == Method::unweighted_unnormalized);
+    }
+    bool timed() const { return timing && !capturing; }
+
+    int setup(const TableSet &set, const FlatTree &tree, const BatchOptions &opts);
     template <typename T>
     int setup_method();
     template <typename T>
-    int embed(cudaStream_t s);
+    int tune(std::vector<PairKernel<T>> &cands, size_t &chosen);
     template <typename T>
-    int prepare(cudaStream_t s);
+    int embed(cudaStream_t s, const Group &g);
     template <typename T>
-    int pair_stage(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t n_tiles, uint32_t splits);
+    int prepare(cudaStream_t s, const Group &g);
     template <typename T>
-    int choose_splits(uint32_t tiles, uint32_t &splits, uint32_t &rows_per_split);
+    int pair_stage(cudaStream_t s, const Group &g, const dev::OutSpec &out, const uint4 *tiles, uint32_t n_tiles,
+                   uint32_t splits, uint32_t rows_per_split, bool last);
     template <typename T>
-    int execute_T(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t n_tiles, uint32_t splits);
+    void choose_splits(const PairKernel<T> &k, uint32_t tiles, uint32_t &splits, uint32_t &rows_per_split) const;
+    template <typename T>
+    int execute_T(cudaStream_t s, const dev::OutSpec &out);
+    int execute_all(cudaStream_t s);
     int run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop);
+    void zero_diagonal(cudaStream_t s, void *out);
 };
 
 template <>
@@ -375,11 +357,10 @@ PairKernel<float> &PlanImpl::kern<float>() {
     return kf;
 }
 
-int PlanImpl::setup(const Table &table, const FlatTree &tree) {
-    n = table.n_samples;
+int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOptions &opts) {
+    const uint32_t n_tables = static_cast<uint32_t>(set.tables.size());
     K = tree.n_nodes;
     E = faith ? tree.n_nodes : tree.n_embedded;
-    ld = ((static_cast<uint64_t>(n) + 127) / 128) * 128;
     int dev_id = 0;
     SSU_CK(cudaGetDevice(&dev_id));
     SSU_CK(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, dev_id));
@@ -388,20 +369,125 @@ int PlanImpl::setup(const Table &table, const FlatTree &tree) {
         SSU_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         own_stream = true;
     }
-    const uint64_t nnz = table.nnz();
-    SSU_CK(upload(&d_indptr, table.indptr, sizeof(uint32_t) * (table.n_obs + 1)));
-    SSU_CK(upload(&d_indices, table.indices, sizeof(uint32_t) * nnz));
-    SSU_CK(upload(&d_data, table.data, sizeof(double) * nnz));
-    host_totals.assign(ld, 0.0);
-    std::copy(table.totals.begin(), table.totals.end(), host_totals.begin());
-    SSU_CK(upload(&d_totals, host_totals.data(), sizeof(double) * ld));
 
-    std::vector<int32_t> tip_obs;
-    tip_obs.reserve(tree.leaf_rows.size());
-    for (uint32_t r : tree.leaf_rows) tip_obs.push_back(tree.leaf_obs[r]);
+    // table descriptors and the concatenated CSR
+    tdesc.assign(n_tables, dev::TableDesc{});
+    table_E.assign(n_tables, E);
+    uint64_t nnz_total = 0, indptr_total = 0;
+    full_elems = 0;
+    for (uint32_t t = 0; t < n_tables; t++) {
+        const Table &tb = *set.tables[t];
+        dev::TableDesc &d = tdesc[t];
+        d.n = tb.n_samples;
+        d.out_off = full_elems;
+        d.nnz_off = nnz_total;
+        d.indptr_off = static_cast<uint32_t>(indptr_total);
+        full_elems += static_cast<uint64_t>(tb.n_samples) * tb.n_samples;
+        nnz_total += tb.nnz();
+        indptr_total += static_cast<uint64_t>(tb.n_obs) + 1;
+        n += tb.n_samples;
+        max_table_n = std::max(max_table_n, tb.n_samples);
+        if (!set.embedded.empty()) table_E[t] = set.embedded[t];
+    }
+    if (indptr_total > UINT32_MAX) {
+        last_error = "too many observations in one plan";
+        return kOutputError;
+    }
+    SSU_CK(alloc(&d_indptr, sizeof(uint32_t) * indptr_total));
+    SSU_CK(alloc(&d_indices, sizeof(uint32_t) * nnz_total));
+    SSU_CK(alloc(&d_data, sizeof(double) * nnz_total));
+    for (uint32_t t = 0; t < n_tables; t++) {
+        const Table &tb = *set.tables[t];
+        const dev::TableDesc &d = tdesc[t];
+        SSU_CK(cudaMemcpyAsync(d_indptr + d.indptr_off, tb.indptr, sizeof(uint32_t) * (tb.n_obs + 1),
+                               cudaMemcpyHostToDevice, stream));
+        if (tb.nnz()) {
+            SSU_CK(cudaMemcpyAsync(d_indices + d.nnz_off, tb.indices, sizeof(uint32_t) * tb.nnz(),
+                                   cudaMemcpyHostToDevice, stream));
+            SSU_CK(cudaMemcpyAsync(d_data + d.nnz_off, tb.data, sizeof(double) * tb.nnz(), cudaMemcpyHostToDevice,
+                                   stream));
+        }
+    }
+
+    // groups of tables whose embedding fits the budget together
+    const size_t el = (spec.fp64 || faith) ? sizeof(double) : sizeof(float);
+    n_words = bits() ? (E + 63) / 64 : 0;
+    if (!faith && !spec.vaw && spec.method == Method::weighted_normalized) {
+        part_chunk = 512;
+        n_parts = std::max<uint32_t>(1, (E + part_chunk - 1) / part_chunk);
+    }
+    const bool counts = spec.vaw && !faith;
+    const size_t per_col = el * std::max<uint32_t>(K, 1) * (counts ? 2 : 1) + sizeof(double) + (counts ? el : 0) +
+                           sizeof(unsigned long long) * n_words + (n_parts ? el * (n_parts + 1) : 0);
+    size_t budget = opts.group_bytes;
+    if (!budget) {
+        if (const char *b = std::getenv("UNIFRAC_B200_GROUP_BYTES")) budget = std::strtoull(b, nullptr, 10);
+    }
+    if (!budget) {
+        size_t free_b = 0, total_b = 0;
+        SSU_CK(cudaMemGetInfo(&free_b, &total_b));
+        const size_t fixed = el * full_elems + 12 * nnz_total;
+        budget = free_b > fixed ? (free_b - fixed) / 2 : 0;
+    }
+    const uint64_t max_cols = std::max<uint64_t>(128, budget / per_col);
+    groups.clear();
+    uint64_t cols = 0;
+    for (uint32_t t = 0; t < n_tables; t++) {
+        const uint64_t w = std::max<uint64_t>(128, (static_cast<uint64_t>(tdesc[t].n) + 127) / 128 * 128);
+        if (groups.empty() || (cols > 0 && cols + w > max_cols)) {
+            if (!groups.empty()) groups.back().ld = cols;
+            groups.emplace_back();
+            groups.back().t0 = t;
+            cols = 0;
+        }
+        tdesc[t].base = static_cast<uint32_t>(cols);
+        cols += w;
+        groups.back().t1 = t + 1;
+    }
+    if (groups.empty()) groups.emplace_back();
+    groups.back().ld = std::max<uint64_t>(cols, 128);
+    ld = 0;
+    for (const Group &g : groups) ld = std::max(ld, g.ld);
+    if (ld > UINT32_MAX) {
+        last_error = "too many samples in one group";
+        return kOutputError;
+    }
+
+    // per group: the tips' rows in each table, the per-column totals
     n_tips = static_cast<uint32_t>(tree.leaf_rows.size());
+    const bool per_table_len = !faith && !set.row_active.empty();
+    for (Group &g : groups) {
+        const uint32_t tg = g.t1 - g.t0;
+        std::vector<int32_t> tip_obs(static_cast<size_t>(n_tips) * std::max<uint32_t>(tg, 1), -1);
+        for (uint32_t i = 0; i < n_tips; i++) {
+            const int32_t o = tree.leaf_obs[tree.leaf_rows[i]];
+            for (uint32_t j = 0; j < tg; j++) {
+                int32_t v = o;
+                if (!set.obs_row.empty()) {
+                    const std::vector<int32_t> &m = set.obs_row[g.t0 + j];
+                    v = (o >= 0 && static_cast<size_t>(o) < m.size()) ? m[o] : -1;
+                }
+                tip_obs[static_cast<size_t>(i) * tg + j] = v;
+            }
+        }
+        SSU_CK(upload(&g.d_tip_obs, tip_obs.data(), sizeof(int32_t) * tip_obs.size()));
+        g.totals.assign(g.ld, 0.0);
+        for (uint32_t t = g.t0; t < g.t1; t++)
+            std::copy(set.tables[t]->totals.begin(), set.tables[t]->totals.end(), g.totals.begin() + tdesc[t].base);
+        SSU_CK(upload(&g.d_totals, g.totals.data(), sizeof(double) * g.ld));
+        if (per_table_len) {
+            std::vector<uint32_t> bt(g.ld / 128, 0);
+            for (uint32_t t = g.t0; t < g.t1; t++) {
+                const uint64_t w = std::max<uint64_t>(128, (static_cast<uint64_t>(tdesc[t].n) + 127) / 128 * 128);
+                for (uint64_t c = tdesc[t].base / 128; c < (tdesc[t].base + w) / 128; c++) bt[c] = t;
+            }
+            SSU_CK(upload(&g.d_block_table, bt.data(), sizeof(uint32_t) * bt.size()));
+        }
+    }
+    SSU_CK(upload(&d_tdesc, tdesc.data(), sizeof(dev::TableDesc) * std::max<uint32_t>(n_tables, 1)));
+
+    // tree
     SSU_CK(upload(&d_tip_rows, tree.leaf_rows.data(), sizeof(uint32_t) * n_tips));
-    SSU_CK(upload(&d_tip_obs, tip_obs.data(), sizeof(int32_t) * n_tips));
     SSU_CK(upload(&d_child_ptr, tree.child_ptr.data(), sizeof(uint32_t) * tree.child_ptr.size()));
     SSU_CK(upload(&d_child_rows, tree.child_rows.data(), sizeof(uint32_t) * tree.child_rows.size()));
     SSU_CK(upload(&d_level_rows, tree.level_rows.data(), sizeof(uint32_t) * tree.level_rows.size()));
@@ -410,26 +496,33 @@ int PlanImpl::setup(const Table &table, const FlatTree &tree) {
         SSU_CK(upload(&d_post_rows, tree.postorder_row.data(), sizeof(uint32_t) * tree.postorder_row.size()));
         SSU_CK(upload(&d_len_rows, tree.length.data(), sizeof(double) * tree.length.size()));
     }
-    // embedded lengths in T, rows [0, E)
+    // embedded lengths in T, rows [0, E); per table (zero where a row is
+    // not embedded in that table's own tree) with bypassed tips in a batch
+    host_len.assign(tree.length.begin(), tree.length.begin() + E);
+    const uint32_t n_len = per_table_len ? n_tables : 1;
+    len_stride = per_table_len ? E : 0;
     if (spec.fp64 || faith) {
-        std::vector<double> len(tree.length.begin(), tree.length.begin() + E);
-        SSU_CK(upload(reinterpret_cast<double **>(&d_len), len.data(), sizeof(double) * E));
+        std::vector<double> len(static_cast<size_t>(E) * n_len);
+        for (uint32_t t = 0; t < n_len; t++)
+            for (uint32_t e = 0; e < E; e++)
+                len[static_cast<size_t>(t) * E + e] = (!per_table_len || set.row_active[t][e]) ? host_len[e] : 0.0;
+        SSU_CK(upload(reinterpret_cast<double **>(&d_len), len.data(), sizeof(double) * len.size()));
     } else {
-        std::vector<float> len(E);
-        for (uint32_t e = 0; e < E; e++) len[e] = static_cast<float>(tree.length[e]);
-        SSU_CK(upload(reinterpret_cast<float **>(&d_len), len.data(), sizeof(float) * E));
+        std::vector<float> len(static_cast<size_t>(E) * n_len);
+        for (uint32_t t = 0; t < n_len; t++)
+            for (uint32_t e = 0; e < E; e++)
+                len[static_cast<size_t>(t) * E + e] =
+                    (!per_table_len || set.row_active[t][e]) ? static_cast<float>(host_len[e]) : 0.0f;
+        SSU_CK(upload(reinterpret_cast<float **>(&d_len), len.data(), sizeof(float) * len.size()));
     }
     for (auto &e : ev) SSU_CK(cudaEventCreate(&e));
     return 0;
 }
 
 template <typename T>
-int PlanImpl::choose_splits(uint32_t tiles, uint32_t &out_splits, uint32_t &out_rows) {
-    const PairKernel<T> &k = kern<T>();
-    const uint32_t units = (spec.method == Method::unweighted || spec.method == Method::unweighted_unnormalized) &&
-                                   !spec.vaw
-                               ? n_words
-                               : E;
+void PlanImpl::choose_splits(const PairKernel<T> &k, uint32_t tiles, uint32_t &out_splits,
+                             uint32_t &out_rows) const {
+    const uint32_t units = bits() ? n_words : E;
     const uint32_t q = static_cast<uint32_t>(k.row_quantum);
     const uint32_t slots = static_cast<uint32_t>(std::max(1, n_sms * k.blocks_per_sm));
     uint32_t best_s = 1;
@@ -449,73 +542,181 @@ int PlanImpl::choose_splits(uint32_t tiles, uint32_t &out_splits, uint32_t &out_
     out_rows = rows;
     out_splits = rows ? (units + rows - 1) / rows : 1;
     if (out_splits == 0) out_splits = 1;
-    return 0;
 }
 
 template <typename T>
 int PlanImpl::setup_method() {
-    PairKernel<T> k = select_kernel<T>(spec);
-    SSU_CK(k.configure(k.smem));
-    int bps = 0;
-    SSU_CK(k.occupancy(&bps, k.threads, k.smem));
-    if (bps < 1) {
+    std::vector<PairKernel<T>> cands;
+    for (PairKernel<T> k : pair_candidates<T>(spec)) {
+        int bps = 0;
+        if (k.configure(k.smem) != cudaSuccess || k.occupancy(&bps, k.threads, k.smem) != cudaSuccess || bps < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        k.blocks_per_sm = bps;
+        cands.push_back(k);
+    }
+    if (cands.empty()) {
         last_error = "pair kernel does not fit on the device";
         return kOutputError;
     }
-    k.blocks_per_sm = bps;
-    kern<T>() = k;
+    const uint32_t n_tables = static_cast<uint32_t>(tdesc.size());
 
     const size_t rowbytes = sizeof(T) * ld;
     SSU_CK(alloc(&d_U, rowbytes * std::max<uint32_t>(K, 1)));
     if (spec.vaw) {
         SSU_CK(alloc(&d_C, rowbytes * std::max<uint32_t>(K, 1)));
-        std::vector<T> tot(ld, T(0));
-        for (uint64_t j = 0; j < ld; j++) tot[j] = static_cast<T>(host_totals[j]);
-        SSU_CK(upload(reinterpret_cast<T **>(&d_tot), tot.data(), sizeof(T) * ld));
+        for (Group &g : groups) {
+            std::vector<T> tot(g.ld, T(0));
+            for (uint64_t j = 0; j < g.ld; j++) tot[j] = static_cast<T>(g.totals[j]);
+            SSU_CK(upload(reinterpret_cast<T **>(&g.d_tot), tot.data(), sizeof(T) * g.ld));
+        }
     }
-    const bool bits = !spec.vaw && (spec.method == Method::unweighted || spec.method == Method::unweighted_unnormalized);
-    if (bits) {
-        n_words = (E + 63) / 64;
+    if (bits()) {
+        const uint32_t n_lut = len_stride ? n_tables : 1;
+        lut_stride = len_stride ? static_cast<uint64_t>(2048) * n_words : 0;
         SSU_CK(alloc(&d_P, sizeof(unsigned long long) * ld * std::max<uint32_t>(n_words, 1)));
-        SSU_CK(alloc(&d_lut, sizeof(T) * 2048 * std::max<uint32_t>(n_words, 1)));
+        SSU_CK(alloc(&d_lut, sizeof(T) * 2048 * std::max<uint32_t>(n_words, 1) * n_lut));
+        if (n_words) {
+            dev::build_lut_kernel<T><<<dim3(n_words * 8, n_lut), 256, 0, stream>>>(
+                static_cast<const T *>(d_len), E, static_cast<T *>(d_lut), len_stride, lut_stride);
+            SSU_CK(cudaGetLastError());
+        }
     }
-    if (!spec.vaw && spec.method == Method::weighted_normalized) {
-        part_chunk = 512;
-        n_parts = std::max<uint32_t>(1, (E + part_chunk - 1) / part_chunk);
+    if (n_parts) {
         SSU_CK(alloc(&d_W, sizeof(T) * ld));
         SSU_CK(alloc(&d_part, sizeof(T) * ld * n_parts));
     }
-    SSU_CK(alloc(&d_full, sizeof(T) * static_cast<uint64_t>(n) * n));
+    SSU_CK(alloc(&d_full, sizeof(T) * std::max<uint64_t>(full_elems, 1)));
 
-    std::vector<uint2> tiles = make_tiles(n, k.BM, k.BN, false, 0, 0);
-    n_tiles = static_cast<uint32_t>(tiles.size());
-    SSU_CK(upload(&d_tiles, tiles.data(), sizeof(uint2) * tiles.size()));
-    choose_splits<T>(n_tiles, splits, rows_per_split);
-    if (splits > 1) {
-        partial_bytes = sizeof(T) * k.partial_per_tile * n_tiles * splits;
-        SSU_CK(alloc(&d_partial, partial_bytes));
+    size_t chosen = 0;
+    if (cands.size() > 1 && autotune == 1) {
+        const int rc = tune<T>(cands, chosen);
+        if (rc) return rc;
     }
+    kern<T>() = cands[chosen];
+    const PairKernel<T> &k = kern<T>();
+
+    partial_bytes = 0;
+    for (Group &g : groups) {
+        std::vector<uint4> tiles;
+        for (uint32_t t = g.t0; t < g.t1; t++) append_tiles(tiles, t, tdesc[t].base, tdesc[t].n, k.BM, k.BN, false, 0, 0);
+        g.n_tiles = static_cast<uint32_t>(tiles.size());
+        SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * tiles.size()));
+        choose_splits<T>(k, g.n_tiles, g.splits, g.rows_per_split);
+        if (g.splits > 1)
+            partial_bytes = std::max(partial_bytes, sizeof(T) * k.partial_per_tile * g.n_tiles * g.splits);
+    }
+    if (partial_bytes) SSU_CK(alloc(&d_partial, partial_bytes));
+    return 0;
+}
+
+// Pick the tile shape: predicted pair-stage time = waves x (time of one
+// full wave of the shape over a probe of node rows, measured on the plan's
+// own group-0 data) x (rows per split / probe rows).
+template <typename T>
+int PlanImpl::tune(std::vector<PairKernel<T>> &cands, size_t &chosen) {
+    const Group &g = groups[0];
+    const std::string key = std::string(cands[0].name) + (sizeof(T) == 8 ? "|f64" : "|f32") + "|a" +
+                            std::to_string(alpha_kind(spec.alpha)) + "|E" + std::to_string(log2_bucket(E)) + "|c" +
+                            std::to_string(log2_bucket(g.ld)) + "|n" + std::to_string(log2_bucket(max_table_n)) +
+                            "|sm" + std::to_string(n_sms);
+    std::string shape;
+    if (TuneCache::get().find(key, shape)) {
+        for (size_t i = 0; i < cands.size(); i++)
+            if (shape == cands[i].shape) {
+                chosen = i;
+                tuning = "cache " + shape;
+                return 0;
+            }
+    }
+    int rc = embed<T>(stream, g);
+    if (!rc) rc = prepare<T>(stream, g);
+    if (rc) return rc;
+    cudaEvent_t a = nullptr, b = nullptr;
+    SSU_CK(cudaEventCreate(&a));
+    SSU_CK(cudaEventCreate(&b));
+    const uint32_t units = bits() ? n_words : E;
+    double best = 1e300;
+    std::string report;
+    for (size_t i = 0; i < cands.size(); i++) {
+        const PairKernel<T> &k = cands[i];
+        std::vector<uint4> tiles;
+        for (uint32_t t = g.t0; t < g.t1; t++) append_tiles(tiles, t, tdesc[t].base, tdesc[t].n, k.BM, k.BN, false, 0, 0);
+        if (tiles.empty() || units == 0) continue;
+        uint4 *d_t = nullptr;
+        SSU_CK(upload(&d_t, tiles.data(), sizeof(uint4) * tiles.size()));
+        uint32_t splits = 1, rows = 0;
+        choose_splits<T>(k, static_cast<uint32_t>(tiles.size()), splits, rows);
+        const uint32_t slots = static_cast<uint32_t>(std::max(1, n_sms * k.blocks_per_sm));
+        const uint32_t q = static_cast<uint32_t>(k.row_quantum);
+        uint32_t probe = std::min<uint32_t>(units, bits() ? 32 : 2048);
+        probe = std::max<uint32_t>(q, probe / q * q);
+        dev::PairArgs<T> pa{};
+        pa.tiles = d_t;
+        pa.n_tiles = std::min<uint32_t>(static_cast<uint32_t>(tiles.size()), slots);
+        pa.n_splits = 1;
+        pa.tables = d_tdesc;
+        pa.U = static_cast<const T *>(d_U);
+        pa.C = static_cast<const T *>(d_C);
+        pa.len = static_cast<const T *>(d_len);
+        pa.len_stride = len_stride;
+        pa.tot = static_cast<const T *>(g.d_tot);
+        pa.W = static_cast<const T *>(d_W);
+        pa.P = d_P;
+        pa.lut = static_cast<const T *>(d_lut);
+        pa.lut_stride = lut_stride;
+        pa.E = units;
+        pa.ld = g.ld;
+        pa.rows_per_split = probe;
+        pa.alpha = static_cast<T>(spec.alpha);
+        pa.out = dev::OutSpec{0, d_full, 0, 0};
+        pa.partial = nullptr;
+        k.launch(pa, pa.n_tiles, k.smem, stream);
+        SSU_CK(cudaEventRecord(a, stream));
+        for (int r = 0; r < 3; r++) k.launch(pa, pa.n_tiles, k.smem, stream);
+        SSU_CK(cudaEventRecord(b, stream));
+        SSU_CK(cudaEventSynchronize(b));
+        float ms = 0;
+        SSU_CK(cudaEventElapsedTime(&ms, a, b));
+        const double waves = std::ceil(static_cast<double>(tiles.size()) * splits / slots);
+        const double pred = waves * (ms / 3.0) * (static_cast<double>(rows) / probe);
+        char buf[96];
+        std::snprintf(buf, sizeof(buf), "%s%s=%.3gms", report.empty() ? "" : " ", k.shape, pred);
+        report += buf;
+        if (pred < best) {
+            best = pred;
+            chosen = i;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    TuneCache::get().put(key, cands[chosen].shape);
+    tuning = std::string("tuned ") + cands[chosen].shape + " (" + report + ")";
     return 0;
 }
 
 template <typename T>
-int PlanImpl::embed(cudaStream_t s) {
+int PlanImpl::embed(cudaStream_t s, const Group &g) {
     if (K == 0) return 0;
     const bool counts = spec.vaw && !faith;
     T *U = static_cast<T *>(d_U);
     T *C = static_cast<T *>(d_C);
     const bool normalize = faith ? true : spec.normalize;
+    const uint32_t tg = g.t1 - g.t0;
     if (n_tips) {
         const uint32_t grid = std::min<uint32_t>(n_tips, 65535u * 8);
         if (counts)
-            dev::embed_tips_kernel<T, true><<<grid, 256, 0, s>>>(d_tip_rows, d_tip_obs, n_tips, d_indptr, d_indices,
-                                                                 d_data, d_totals, normalize, U, C, ld);
+            dev::embed_tips_kernel<T, true><<<grid, 256, 0, s>>>(d_tip_rows, g.d_tip_obs, n_tips, tg, d_tdesc + g.t0,
+                                                                 d_indptr, d_indices, d_data, g.d_totals, normalize,
+                                                                 U, C, g.ld);
         else
-            dev::embed_tips_kernel<T, false><<<grid, 256, 0, s>>>(d_tip_rows, d_tip_obs, n_tips, d_indptr, d_indices,
-                                                                  d_data, d_totals, normalize, U, C, ld);
+            dev::embed_tips_kernel<T, false><<<grid, 256, 0, s>>>(d_tip_rows, g.d_tip_obs, n_tips, tg,
+                                                                  d_tdesc + g.t0, d_indptr, d_indices, d_data,
+                                                                  g.d_totals, normalize, U, C, g.ld);
         launches++;
     }
-    const uint64_t nvec = ld / dev::Vec16<T>::n;
+    const uint64_t nvec = g.ld / dev::Vec16<T>::n;
     const uint32_t threads = 128;
     const uint32_t col_blocks = static_cast<uint32_t>((nvec + threads - 1) / threads);
     for (size_t h = 1; h < level_ptr.size(); h++) {
@@ -525,10 +726,10 @@ int PlanImpl::embed(cudaStream_t s) {
         const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(blocks, 1u << 20));
         if (counts)
             dev::embed_level_kernel<T, true><<<grid, threads, 0, s>>>(d_level_rows + a, b - a, d_child_ptr,
-                                                                      d_child_rows, U, C, ld, col_blocks);
+                                                                      d_child_rows, U, C, g.ld, col_blocks);
         else
             dev::embed_level_kernel<T, false><<<grid, threads, 0, s>>>(d_level_rows + a, b - a, d_child_ptr,
-                                                                       d_child_rows, U, C, ld, col_blocks);
+                                                                       d_child_rows, U, C, g.ld, col_blocks);
         launches++;
     }
     SSU_CK(cudaGetLastError());
@@ -536,116 +737,140 @@ int PlanImpl::embed(cudaStream_t s) {
 }
 
 template <typename T>
-int PlanImpl::prepare(cudaStream_t s) {
+int PlanImpl::prepare(cudaStream_t s, const Group &g) {
     const T *U = static_cast<const T *>(d_U);
     const T *len = static_cast<const T *>(d_len);
     if (d_W) {
-        dim3 grid(static_cast<uint32_t>((ld + 255) / 256), n_parts);
-        dev::weighted_sums_partial_kernel<T><<<grid, 256, 0, s>>>(U, len, E, ld, part_chunk, static_cast<T *>(d_part));
-        dev::reduce_partials_kernel<T><<<static_cast<uint32_t>((ld + 255) / 256), 256, 0, s>>>(
-            static_cast<const T *>(d_part), n_parts, ld, static_cast<T *>(d_W));
+        dim3 grid(static_cast<uint32_t>((g.ld + 127) / 128), n_parts);
+        dev::weighted_sums_partial_kernel<T><<<grid, 128, 0, s>>>(U, len, E, g.ld, part_chunk,
+                                                                 static_cast<T *>(d_part),
+                                                                 len_stride ? g.d_block_table : nullptr, len_stride);
+        dev::reduce_partials_kernel<T><<<static_cast<uint32_t>((g.ld + 255) / 256), 256, 0, s>>>(
+            static_cast<const T *>(d_part), n_parts, g.ld, static_cast<T *>(d_W));
         launches += 2;
     }
     if (d_P && n_words) {
-        const uint64_t total = static_cast<uint64_t>(n_words) * ld;
+        const uint64_t total = static_cast<uint64_t>(n_words) * g.ld;
         const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((total + 255) / 256, 1u << 20));
-        dev::pack_presence_kernel<T><<<grid, 256, 0, s>>>(U, E, ld, n_words, d_P);
-        dev::build_lut_kernel<T><<<n_words * 8, 256, 0, s>>>(len, E, static_cast<T *>(d_lut));
-        launches += 2;
+        dev::pack_presence_kernel<T><<<grid, 256, 0, s>>>(U, E, g.ld, n_words, d_P);
+        launches++;
     }
     SSU_CK(cudaGetLastError());
     return 0;
 }
 
 template <typename T>
-int PlanImpl::pair_stage(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t ntiles,
-                         uint32_t nsplits) {
+int PlanImpl::pair_stage(cudaStream_t s, const Group &g, const dev::OutSpec &out, const uint4 *tiles,
+                         uint32_t ntiles, uint32_t nsplits, uint32_t rows, bool last) {
     const PairKernel<T> &k = kern<T>();
     if (ntiles == 0) return 0;
     dev::PairArgs<T> a{};
     a.tiles = tiles;
     a.n_tiles = ntiles;
+    a.tables = d_tdesc;
     a.U = static_cast<const T *>(d_U);
     a.C = static_cast<const T *>(d_C);
     a.len = static_cast<const T *>(d_len);
-    a.tot = static_cast<const T *>(d_tot);
+    a.len_stride = len_stride;
+    a.tot = static_cast<const T *>(g.d_tot);
     a.W = static_cast<const T *>(d_W);
     a.P = d_P;
     a.lut = static_cast<const T *>(d_lut);
-    const bool bits = d_P != nullptr;
-    a.E = bits ? n_words : E;
-    a.ld = ld;
-    a.n = n;
+    a.lut_stride = lut_stride;
+    a.E = bits() ? n_words : E;
+    a.ld = g.ld;
     a.alpha = static_cast<T>(spec.alpha);
     a.out = out;
-    uint32_t rows = rows_per_split;
     if (nsplits <= 1) {
         nsplits = 1;
-        rows = bits ? n_words : E;
+        rows = a.E;
         a.partial = nullptr;
     } else {
         a.partial = static_cast<T *>(d_partial);
     }
+    a.n_splits = nsplits;
     a.rows_per_split = rows;
-    dim3 grid(ntiles, nsplits);
-    k.launch(a, grid, k.smem, s);
+    const uint64_t work = static_cast<uint64_t>(ntiles) * nsplits;
+    const uint64_t slots = static_cast<uint64_t>(std::max(1, n_sms * k.blocks_per_sm));
+    k.launch(a, static_cast<uint32_t>(std::min(work, slots)), k.smem, s);
     launches++;
-    if (timing) SSU_CK(cudaEventRecord(ev[2], s));
+    if (last && timed()) SSU_CK(cudaEventRecord(ev[2], s));
     if (nsplits > 1) {
-        k.finalize(a, nsplits, s);
+        k.finalize(a, s);
         launches++;
     }
     SSU_CK(cudaGetLastError());
     return 0;
+}
+
+void PlanImpl::zero_diagonal(cudaStream_t s, void *out) {
+    if (!max_table_n || tdesc.empty()) return;
+    const uint32_t bx = std::min<uint32_t>((max_table_n + 255) / 256, 64);
+    dev::zero_diagonal_kernel<<<dim3(bx, static_cast<uint32_t>(tdesc.size())), 256, 0, s>>>(out, d_tdesc,
+                                                                                          spec.fp64 ? 1 : 0);
+    launches++;
 }
 
 template <typename T>
-int PlanImpl::execute_T(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t ntiles,
-                        uint32_t nsplits) {
+int PlanImpl::execute_T(cudaStream_t s, const dev::OutSpec &out) {
     launches = 0;
-    if (timing) SSU_CK(cudaEventRecord(ev[0], s));
-    int rc = embed<T>(s);
-    if (rc) return rc;
-    rc = prepare<T>(s);
-    if (rc) return rc;
-    if (timing) SSU_CK(cudaEventRecord(ev[1], s));
-    rc = pair_stage<T>(s, out, tiles, ntiles, nsplits);
-    if (rc) return rc;
-    if (timing && ntiles == 0) SSU_CK(cudaEventRecord(ev[2], s));
-    if (out.mode == 0 && n) {
-        dev::zero_diagonal_kernel<<<(n + 255) / 256, 256, 0, s>>>(out.ptr, n, sizeof(T) == 8);
-        launches++;
+    if (timed()) SSU_CK(cudaEventRecord(ev[0], s));
+    for (size_t gi = 0; gi < groups.size(); gi++) {
+        const Group &g = groups[gi];
+        int rc = embed<T>(s, g);
+        if (!rc) rc = prepare<T>(s, g);
+        if (rc) return rc;
+        if (gi == 0 && timed()) SSU_CK(cudaEventRecord(ev[1], s));
+        rc = pair_stage<T>(s, g, out, g.d_tiles, g.n_tiles, g.splits, g.rows_per_split, gi + 1 == groups.size());
+        if (rc) return rc;
+        if (gi + 1 == groups.size() && g.n_tiles == 0 && timed()) SSU_CK(cudaEventRecord(ev[2], s));
     }
-    if (timing) SSU_CK(cudaEventRecord(ev[3], s));
+    if (out.mode == 0) zero_diagonal(s, out.ptr);
+    if (timed()) SSU_CK(cudaEventRecord(ev[3], s));
     SSU_CK(cudaGetLastError());
     return 0;
 }
 
+int PlanImpl::execute_all(cudaStream_t s) {
+    dev::OutSpec o{0, d_full, 0, 0};
+    if (gemm) return execute_gemm(s, o, d_gemm_tiles, n_gemm_tiles);
+    return spec.fp64 ? execute_T<double>(s, o) : execute_T<float>(s, o);
+}
+
+// One table only: its stripes [start, stop) (mode 1) or condensed form (2).
 int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop) {
     if (gemm) {
         dev::OutSpec o{mode, d_out, start, stop};
-        return execute_gemm(stream, o, d_tiles, n_tiles);
+        return execute_gemm(stream, o, d_gemm_tiles, n_gemm_tiles);
     }
+    const Group &g = groups[0];
     const int BM = spec.fp64 ? kd.BM : kf.BM, BN = spec.fp64 ? kd.BN : kf.BN;
-    std::vector<uint2> tiles = make_tiles(n, BM, BN, mode == 1, start, stop);
-    uint2 *d_t = nullptr;
-    SSU_CK(upload(&d_t, tiles.data(), sizeof(uint2) * tiles.size()));
+    std::vector<uint4> tiles;
+    append_tiles(tiles, 0, 0, tdesc[0].n, BM, BN, mode == 1, start, stop);
+    uint4 *d_t = nullptr;
+    SSU_CK(upload(&d_t, tiles.data(), sizeof(uint4) * tiles.size()));
     uint32_t s = 1, rows = 0;
-    (void)s;
     if (spec.fp64)
-        choose_splits<double>(static_cast<uint32_t>(tiles.size()), s, rows);
+        choose_splits<double>(kd, static_cast<uint32_t>(tiles.size()), s, rows);
     else
-        choose_splits<float>(static_cast<uint32_t>(tiles.size()), s, rows);
+        choose_splits<float>(kf, static_cast<uint32_t>(tiles.size()), s, rows);
     // the window never holds more tiles than the full matrix, so the plan's
     // partial buffer is large enough when the split count does not grow
     const size_t per_tile = spec.fp64 ? kd.partial_per_tile * sizeof(double) : kf.partial_per_tile * sizeof(float);
     if (s > 1 && per_tile * tiles.size() * s > partial_bytes) s = 1;
-    const uint32_t saved = rows_per_split;
-    rows_per_split = rows;
     dev::OutSpec o{mode, d_out, start, stop};
-    int rc = spec.fp64 ? execute_T<double>(stream, o, d_t, static_cast<uint32_t>(tiles.size()), s)
-                       : execute_T<float>(stream, o, d_t, static_cast<uint32_t>(tiles.size()), s);
-    rows_per_split = saved;
+    launches = 0;
+    const uint32_t nt = static_cast<uint32_t>(tiles.size());
+    int rc = 0;
+    if (spec.fp64) {
+        rc = embed<double>(stream, g);
+        if (!rc) rc = prepare<double>(stream, g);
+        if (!rc) rc = pair_stage<double>(stream, g, o, d_t, nt, s, rows, true);
+    } else {
+        rc = embed<float>(stream, g);
+        if (!rc) rc = prepare<float>(stream, g);
+        if (!rc) rc = pair_stage<float>(stream, g, o, d_t, nt, s, rows, true);
+    }
     return rc;
 }
 
@@ -744,20 +969,20 @@ int PlanImpl::setup_gemm(const Table &table, const FlatTree &tree) {
         for (uint32_t gl = 0; gl < nb; gl += 12)
             for (uint32_t kb = gk; kb < std::min(nb, gk + 12); kb++)
                 for (uint32_t lb = gl; lb < std::min(nb, gl + 12); lb++) tiles.push_back(make_uint2(kb, lb));
-    n_tiles = static_cast<uint32_t>(tiles.size());
-    SSU_CK(upload(&d_tiles, tiles.data(), sizeof(uint2) * tiles.size()));
+    n_gemm_tiles = static_cast<uint32_t>(tiles.size());
+    SSU_CK(upload(&d_gemm_tiles, tiles.data(), sizeof(uint2) * tiles.size()));
     gemm = true;
     return 0;
 }
 
 int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t ntiles) {
     launches = 0;
-    if (timing) SSU_CK(cudaEventRecord(ev[0], s));
+    if (timed()) SSU_CK(cudaEventRecord(ev[0], s));
     const size_t bits_smem = sizeof(uint32_t) * (k_pad / 32);
     tc::presence_rows_kernel<<<n_pad, 256, bits_smem, s>>>(d_sample_ptr, d_start_col, d_parent_col, d_lhi, d_llo,
                                                            d_lsorted, n, k_pad, d_A, d_Bh, d_Bl, d_r);
     launches++;
-    if (timing) SSU_CK(cudaEventRecord(ev[1], s));
+    if (timed()) SSU_CK(cudaEventRecord(ev[1], s));
     if (ntiles) {
         tc::GemmArgs g{};
         g.tiles = tiles;
@@ -772,7 +997,7 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out, const uint2 
         tc::unweighted_tc_kernel<<<ntiles, tc::THREADS, tc::SMEM_BYTES, s>>>(map_A, map_Bh, map_Bl, g);
         launches++;
     }
-    if (timing) SSU_CK(cudaEventRecord(ev[2], s));
+    if (timed()) SSU_CK(cudaEventRecord(ev[2], s));
     if (n) {
         const dim3 grid((n + 31) / 32, (n + 31) / 32);
         tc::finish_unweighted_kernel<<<grid, dim3(32, 8), 0, s>>>(d_G, n_pad, d_r, n,
@@ -780,16 +1005,22 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out, const uint2 
                                                                   spec.fp64 ? 1 : 0, out);
         launches++;
     }
-    if (out.mode == 0 && n) {
-        dev::zero_diagonal_kernel<<<(n + 255) / 256, 256, 0, s>>>(out.ptr, n, spec.fp64 ? 1 : 0);
-        launches++;
-    }
-    if (timing) SSU_CK(cudaEventRecord(ev[3], s));
+    if (out.mode == 0) zero_diagonal(s, out.ptr);
+    if (timed()) SSU_CK(cudaEventRecord(ev[3], s));
     SSU_CK(cudaGetLastError());
     return 0;
 }
 
 // ------------------------------------------------------------------ Plan
+
+namespace {
+
+int resolve_autotune(int requested, bool batch) {
+    if (requested >= 0) return requested;
+    return env_int("UNIFRAC_B200_AUTOTUNE", batch ? 1 : 0);
+}
+
+}  // namespace
 
 int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spec, void *stream, Plan **out,
                  std::string &err) {
@@ -798,7 +1029,11 @@ int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spe
     PlanImpl &m = *p->impl_;
     m.spec = spec;
     m.stream = static_cast<cudaStream_t>(stream);
-    int rc = m.setup(table, tree);
+    m.autotune = resolve_autotune(-1, false);
+    TableSet set;
+    set.tables.push_back(&table);
+    set.embedded.push_back(tree.n_embedded);
+    int rc = m.setup(set, tree, BatchOptions{});
     bool want_gemm = spec.unweighted_gemm && !spec.vaw &&
                      (spec.method == Method::unweighted || spec.method == Method::unweighted_unnormalized);
     // presence is "proportion > 0": with no negative count it is the OR of
@@ -807,7 +1042,7 @@ int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spe
         if (!(table.data[q] >= 0.0)) want_gemm = false;
     if (!rc && want_gemm) {
         rc = m.setup_gemm(table, tree);
-        if (!rc && m.alloc(&m.d_full, (spec.fp64 ? sizeof(double) : sizeof(float)) * static_cast<uint64_t>(m.n) * m.n) !=
+        if (!rc && m.alloc(&m.d_full, (spec.fp64 ? sizeof(double) : sizeof(float)) * std::max<uint64_t>(m.full_elems, 1)) !=
                        cudaSuccess) {
             m.last_error = "device allocation failed";
             rc = kOutputError;
@@ -815,6 +1050,33 @@ int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spe
     } else if (!rc) {
         rc = spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
     }
+    if (rc) {
+        err = m.last_error;
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return 0;
+}
+
+int Plan::create_batch(const TableSet &set, const FlatTree &tree, const MethodSpec &spec, const BatchOptions &opts,
+                       void *stream, Plan **out, std::string &err) {
+    if (set.tables.empty() || set.tables.size() > 65535 ||
+        (!set.obs_row.empty() && set.obs_row.size() != set.tables.size()) ||
+        (!set.row_active.empty() && set.row_active.size() != set.tables.size())) {
+        err = "bad table set";
+        return kOutputError;
+    }
+    Plan *p = new Plan();
+    p->impl_ = new PlanImpl();
+    PlanImpl &m = *p->impl_;
+    m.spec = spec;
+    m.spec.unweighted_gemm = false;
+    m.batch = true;
+    m.stream = static_cast<cudaStream_t>(stream);
+    m.autotune = resolve_autotune(opts.autotune, true);
+    int rc = m.setup(set, tree, opts);
+    if (!rc) rc = spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
     if (rc) {
         err = m.last_error;
         delete p;
@@ -832,7 +1094,9 @@ int Plan::create_faith(const Table &table, const FlatTree &tree, void *stream, P
     m.spec.fp64 = true;
     m.spec.normalize = true;
     m.stream = static_cast<cudaStream_t>(stream);
-    int rc = m.setup(table, tree);
+    TableSet set;
+    set.tables.push_back(&table);
+    int rc = m.setup(set, tree, BatchOptions{});
     if (!rc) {
         if (m.alloc(&m.d_U, sizeof(double) * m.ld * std::max<uint32_t>(m.K, 1)) != cudaSuccess) {
             err = "device allocation failed";
@@ -852,6 +1116,7 @@ int Plan::create_faith(const Table &table, const FlatTree &tree, void *stream, P
 Plan::~Plan() {
     if (!impl_) return;
     PlanImpl &m = *impl_;
+    if (m.graph) cudaGraphExecDestroy(m.graph);
     if (m.stream) {
         for (void *q : m.allocations) cudaFreeAsync(q, m.stream);
         cudaStreamSynchronize(m.stream);
@@ -862,13 +1127,46 @@ Plan::~Plan() {
     delete impl_;
 }
 
+void Plan::set_graph(bool on) {
+    PlanImpl &m = *impl_;
+    if (!on && m.graph) {
+        cudaGraphExecDestroy(m.graph);
+        m.graph = nullptr;
+    }
+    m.graph_on = on;
+}
+
 int Plan::execute(void *stream) {
     PlanImpl &m = *impl_;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : m.stream;
-    dev::OutSpec o{0, m.d_full, 0, 0};
-    if (m.gemm) return m.execute_gemm(s, o, m.d_tiles, m.n_tiles);
-    return m.spec.fp64 ? m.execute_T<double>(s, o, m.d_tiles, m.n_tiles, m.splits)
-                       : m.execute_T<float>(s, o, m.d_tiles, m.n_tiles, m.splits);
+    if (!m.graph_on) return m.execute_all(s);
+    if (!m.graph) {
+        // capture on a stream of our own so the caller's stream may be the
+        // legacy default stream
+        cudaStream_t cs = m.stream;
+        if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            m.last_error = "stream capture failed";
+            return kOutputError;
+        }
+        m.capturing = true;
+        const int rc = m.execute_all(cs);
+        m.capturing = false;
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(cs, &g);
+        if (rc || e != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            m.last_error = "stream capture failed";
+            return kOutputError;
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&m.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            m.graph = nullptr;
+            m.last_error = cudaGetErrorString(ie);
+            return kOutputError;
+        }
+    }
+    return cudaGraphLaunch(m.graph, s) == cudaSuccess ? 0 : kOutputError;
 }
 
 int Plan::device_error() {
@@ -890,7 +1188,7 @@ int Plan::run_full(void *host_out, bool out_fp64, std::string &err) {
     }
     int rc = execute(nullptr);
     if (!rc) {
-        const size_t bytes = (m.spec.fp64 ? sizeof(double) : sizeof(float)) * static_cast<size_t>(m.n) * m.n;
+        const size_t bytes = (m.spec.fp64 ? sizeof(double) : sizeof(float)) * m.full_elems;
         cudaError_t e = cudaMemcpyAsync(host_out, m.d_full, bytes, cudaMemcpyDeviceToHost, m.stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(m.stream);
         if (e != cudaSuccess) {
@@ -906,13 +1204,24 @@ int Plan::run_full(void *host_out, bool out_fp64, std::string &err) {
 }
 
 int Plan::download_full(void *host_out, bool pin, std::string &err) {
+    return download_range(0, impl_->full_elems, host_out, pin, err);
+}
+
+int Plan::download_range(uint64_t offset, uint64_t count, void *host_out, bool pin, std::string &err) {
     PlanImpl &m = *impl_;
-    const size_t bytes = (m.spec.fp64 ? sizeof(double) : sizeof(float)) * static_cast<size_t>(m.n) * m.n;
+    const size_t el = m.spec.fp64 ? sizeof(double) : sizeof(float);
+    if (offset > m.full_elems || count > m.full_elems - offset) {
+        err = "result range out of bounds";
+        return kOutputError;
+    }
+    const size_t bytes = el * count;
     bool registered = false;
     if (pin && bytes >= (size_t(1) << 20))
         registered = cudaHostRegister(host_out, bytes, cudaHostRegisterDefault) == cudaSuccess;
     if (pin && !registered) cudaGetLastError();  // a refused registration only means a pageable copy
-    cudaError_t e = cudaMemcpyAsync(host_out, m.d_full, bytes, cudaMemcpyDeviceToHost, m.stream);
+    cudaError_t e = bytes ? cudaMemcpyAsync(host_out, static_cast<const char *>(m.d_full) + el * offset, bytes,
+                                            cudaMemcpyDeviceToHost, m.stream)
+                          : cudaSuccess;
     if (e == cudaSuccess) e = cudaStreamSynchronize(m.stream);
     if (registered) cudaHostUnregister(host_out);
     if (e != cudaSuccess) {
@@ -983,7 +1292,8 @@ int Plan::run_condensed(double *host_cf, std::string &err) {
 int Plan::run_faith(double *host_values, std::string &err) {
     PlanImpl &m = *impl_;
     m.launches = 0;
-    int rc = m.embed<double>(m.stream);
+    const Group &g = m.groups[0];
+    int rc = m.embed<double>(m.stream, g);
     if (rc) {
         err = m.last_error;
         return rc;
@@ -991,16 +1301,16 @@ int Plan::run_faith(double *host_values, std::string &err) {
     const uint32_t chunk = 1024;
     const uint32_t parts = std::max<uint32_t>(1, (m.K + chunk - 1) / chunk);
     double *d_part = nullptr, *d_out = nullptr;
-    if (m.alloc(&d_part, sizeof(double) * m.ld * parts) != cudaSuccess ||
-        m.alloc(&d_out, sizeof(double) * m.ld) != cudaSuccess) {
+    if (m.alloc(&d_part, sizeof(double) * g.ld * parts) != cudaSuccess ||
+        m.alloc(&d_out, sizeof(double) * g.ld) != cudaSuccess) {
         err = "device allocation failed";
         return kOutputError;
     }
-    dim3 grid(static_cast<uint32_t>((m.ld + 255) / 256), parts);
+    dim3 grid(static_cast<uint32_t>((g.ld + 255) / 256), parts);
     dev::faith_partial_kernel<<<grid, 256, 0, m.stream>>>(static_cast<const double *>(m.d_U), m.d_len_rows,
-                                                          m.d_post_rows, m.K, m.ld, chunk, d_part);
-    dev::reduce_partials_kernel<double><<<static_cast<uint32_t>((m.ld + 255) / 256), 256, 0, m.stream>>>(
-        d_part, parts, m.ld, d_out);
+                                                          m.d_post_rows, m.K, g.ld, chunk, d_part);
+    dev::reduce_partials_kernel<double><<<static_cast<uint32_t>((g.ld + 255) / 256), 256, 0, m.stream>>>(
+        d_part, parts, g.ld, d_out);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(host_values, d_out, sizeof(double) * m.n, cudaMemcpyDeviceToHost, m.stream);
@@ -1017,7 +1327,7 @@ const void *Plan::device_result() const { return impl_->d_full; }
 int Plan::copy_result(void *host_out, void *stream) {
     PlanImpl &m = *impl_;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : m.stream;
-    const size_t bytes = (m.spec.fp64 ? sizeof(double) : sizeof(float)) * static_cast<size_t>(m.n) * m.n;
+    const size_t bytes = (m.spec.fp64 ? sizeof(double) : sizeof(float)) * m.full_elems;
     if (cudaMemcpyAsync(host_out, m.d_full, bytes, cudaMemcpyDeviceToHost, s) != cudaSuccess) return kOutputError;
     if (cudaStreamSynchronize(s) != cudaSuccess) return kOutputError;
     return device_error() ? kOutputError : 0;
@@ -1026,21 +1336,36 @@ int Plan::copy_result(void *host_out, void *stream) {
 int Plan::synchronize() { return cudaStreamSynchronize(impl_->stream) == cudaSuccess ? 0 : kOutputError; }
 
 uint32_t Plan::n_samples() const { return impl_->n; }
+uint32_t Plan::n_tables() const { return static_cast<uint32_t>(impl_->tdesc.size()); }
+uint32_t Plan::n_groups() const { return static_cast<uint32_t>(impl_->groups.size()); }
+uint32_t Plan::table_samples(uint32_t t) const { return t < impl_->tdesc.size() ? impl_->tdesc[t].n : 0; }
+uint64_t Plan::table_offset(uint32_t t) const { return t < impl_->tdesc.size() ? impl_->tdesc[t].out_off : 0; }
+uint64_t Plan::table_embedded(uint32_t t) const { return t < impl_->table_E.size() ? impl_->table_E[t] : 0; }
 uint64_t Plan::n_embedded() const { return impl_->E; }
 uint64_t Plan::work_units() const {
-    const uint64_t n = impl_->n;
-    return n * (n - (n ? 1 : 0)) / 2 * impl_->E;
+    uint64_t u = 0;
+    for (size_t t = 0; t < impl_->tdesc.size(); t++) {
+        const uint64_t n = impl_->tdesc[t].n;
+        u += n * (n - (n ? 1 : 0)) / 2 * impl_->table_E[t];
+    }
+    return u;
 }
 uint32_t Plan::launches() const { return impl_->launches; }
 const char *Plan::pair_kernel_name() const {
     if (impl_->gemm) return "unweighted_tc_kernel";
     return impl_->spec.fp64 ? impl_->kd.name : impl_->kf.name;
 }
+const char *Plan::tuning() const {
+    if (impl_->gemm) return "fixed";
+    static thread_local std::string s;
+    s = impl_->tuning + " " + (impl_->spec.fp64 ? impl_->kd.shape : impl_->kf.shape);
+    return s.c_str();
+}
 void Plan::set_timing(bool on) { impl_->timing = on; }
 
 int Plan::stage_times(StageTimes &out) {
     PlanImpl &m = *impl_;
-    if (!m.timing) return kOutputError;
+    if (!m.timing || m.graph_on) return kOutputError;
     if (cudaEventSynchronize(m.ev[3]) != cudaSuccess) return kOutputError;
     cudaEventElapsedTime(&out.embed_ms, m.ev[0], m.ev[1]);
     cudaEventElapsedTime(&out.pair_ms, m.ev[1], m.ev[2]);

@@ -1,10 +1,12 @@
 // CUDA kernels of the B200 UniFrac engine (sm_100a).
 //
-// Data layout in HBM (one table):
+// Data layout in HBM (one group of tables sharing the tree):
 //   U[row][j]   proportion embedding, rows = non-root nodes (embedded rows
-//               first, in postorder), j = sample; row stride `ld` = n rounded
-//               up to 128 so every tile load is in bounds and 16-byte aligned;
-//               padding columns are zero.
+//               first, in postorder), j = column.  Table t of the group owns
+//               columns [base_t, base_t + n_t); every base and every table's
+//               width are multiples of 128, so each tile load is in bounds and
+//               16-byte aligned; padding columns are zero.  `ld` = the group's
+//               column count.
 //   C[row][j]   raw-count embedding (variance-adjusted methods only).
 //   P[w][j]     presence bits of 64 consecutive embedded rows (unweighted).
 //   LUT[w][b][v] sum of the lengths selected by the bits of byte value v in
@@ -41,14 +43,27 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // --------------------------------------------------------------- embedding
 
-// Tip rows: zero the row, then scatter the tip's CSR entries; proportions
-// are data / total in fp64 and then rounded to T (src/biom_inmem.cpp:473-497).
+// One table of a group: where its CSR entries, its embedding columns and
+// its result live.
+struct TableDesc {
+    uint64_t out_off;     // first element of the table's result in the output buffer
+    uint64_t nnz_off;     // first CSR entry of the table in the concatenated indices/data
+    uint32_t indptr_off;  // first indptr entry of the table
+    uint32_t base;        // first embedding column of the table in its group
+    uint32_t n;           // samples
+    uint32_t pad;
+};
+
+// Tip rows: zero the row, then scatter the CSR entries of the tip's
+// observation from every table of the group; proportions are data / total in
+// fp64 and then rounded to T (src/biom_inmem.cpp:473-497).
+// tip_obs[t * n_tables + i] = row of tip t's observation in table i, or -1.
 template <typename T, bool COUNTS>
 __global__ void embed_tips_kernel(const uint32_t *__restrict__ tip_rows, const int32_t *__restrict__ tip_obs,
-                                  uint32_t n_tips, const uint32_t *__restrict__ indptr,
-                                  const uint32_t *__restrict__ indices, const double *__restrict__ data,
-                                  const double *__restrict__ totals, bool normalize, T *__restrict__ U,
-                                  T *__restrict__ C, uint64_t ld) {
+                                  uint32_t n_tips, uint32_t n_tables, const TableDesc *__restrict__ tables,
+                                  const uint32_t *__restrict__ indptr, const uint32_t *__restrict__ indices,
+                                  const double *__restrict__ data, const double *__restrict__ totals, bool normalize,
+                                  T *__restrict__ U, T *__restrict__ C, uint64_t ld) {
     for (uint32_t t = blockIdx.x; t < n_tips; t += gridDim.x) {
         const uint64_t row = tip_rows[t];
         T *u = U + row * ld;
@@ -58,11 +73,15 @@ __global__ void embed_tips_kernel(const uint32_t *__restrict__ tip_rows, const i
             if (COUNTS) c[j] = T(0);
         }
         __syncthreads();
-        const int32_t r = tip_obs[t];
-        if (r >= 0) {
-            for (uint32_t q = indptr[r] + threadIdx.x; q < indptr[r + 1]; q += blockDim.x) {
-                const uint32_t j = indices[q];
-                const double v = data[q];
+        for (uint32_t i = 0; i < n_tables; i++) {
+            const int32_t r = tip_obs[static_cast<uint64_t>(t) * n_tables + i];
+            if (r < 0) continue;
+            const TableDesc td = tables[i];
+            const uint32_t *ip = indptr + td.indptr_off;
+            for (uint32_t q = ip[r] + threadIdx.x; q < ip[r + 1]; q += blockDim.x) {
+                const uint64_t qa = td.nnz_off + q;
+                const uint32_t j = td.base + indices[qa];
+                const double v = data[qa];
                 u[j] = normalize ? static_cast<T>(v / totals[j]) : static_cast<T>(v);
                 if (COUNTS) c[j] = static_cast<T>(v);
             }
@@ -112,16 +131,20 @@ __global__ void embed_level_kernel(const uint32_t *__restrict__ rows, uint32_t n
 
 // W[j] = sum_e L_e u_e[j] over embedded rows, in fixed row chunks (partial
 // sums, then an in-order reduction), the one-sided sums of
-// src/unifrac_task_impl.hpp:51-103.
+// src/unifrac_task_impl.hpp:51-103.  With per-table lengths (block_table
+// set, 128 threads per block) a block's columns all belong to the table
+// block_table[blockIdx.x].
 template <typename T>
 __global__ void weighted_sums_partial_kernel(const T *__restrict__ U, const T *__restrict__ len, uint32_t E,
-                                             uint64_t ld, uint32_t chunk, T *__restrict__ partial) {
+                                             uint64_t ld, uint32_t chunk, T *__restrict__ partial,
+                                             const uint32_t *__restrict__ block_table, uint64_t len_stride) {
     const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (j >= ld) return;
+    const T *L = block_table ? len + block_table[blockIdx.x] * len_stride : len;
     const uint32_t e0 = blockIdx.y * chunk;
     const uint32_t e1 = min(E, e0 + chunk);
     T s = T(0);
-    for (uint32_t e = e0; e < e1; e++) s = fma(U[static_cast<uint64_t>(e) * ld + j], len[e], s);
+    for (uint32_t e = e0; e < e1; e++) s = fma(U[static_cast<uint64_t>(e) * ld + j], L[e], s);
     partial[static_cast<uint64_t>(blockIdx.y) * ld + j] = s;
 }
 
@@ -152,16 +175,19 @@ __global__ void pack_presence_kernel(const T *__restrict__ U, uint32_t E, uint64
     }
 }
 
-// 8-bit length tables: LUT[(w*8 + byte)*256 + v] = sum of L over the set bits of v.
+// 8-bit length tables: LUT[(w*8 + byte)*256 + v] = sum of L over the set
+// bits of v; grid.y = table when the lengths are per table.
 template <typename T>
-__global__ void build_lut_kernel(const T *__restrict__ len, uint32_t E, T *__restrict__ lut) {
+__global__ void build_lut_kernel(const T *__restrict__ len, uint32_t E, T *__restrict__ lut, uint64_t len_stride,
+                                 uint64_t lut_stride) {
     const uint32_t wb = blockIdx.x;  // word * 8 + byte
     const uint32_t v = threadIdx.x;  // 0..255
     const uint32_t base = wb * 8;
+    const T *L = len + blockIdx.y * len_stride;
     T s = T(0);
     for (uint32_t i = 0; i < 8; i++)
-        if (((v >> i) & 1u) && base + i < E) s += len[base + i];
-    lut[static_cast<uint64_t>(wb) * 256 + v] = s;
+        if (((v >> i) & 1u) && base + i < E) s += L[base + i];
+    lut[blockIdx.y * lut_stride + static_cast<uint64_t>(wb) * 256 + v] = s;
 }
 
 // Faith PD: per sample sum of L over non-root nodes with u > 0
@@ -181,13 +207,16 @@ static __global__ void faith_partial_kernel(const double *__restrict__ U, const 
     partial[static_cast<uint64_t>(blockIdx.y) * ld + j] = s;
 }
 
-static __global__ void zero_diagonal_kernel(void *out, uint32_t n, int fp64) {
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    if (fp64)
-        static_cast<double *>(out)[static_cast<uint64_t>(k) * n + k] = 0.0;
-    else
-        static_cast<float *>(out)[static_cast<uint64_t>(k) * n + k] = 0.0f;
+// Diagonal of every table's full result (grid.y = table).
+static __global__ void zero_diagonal_kernel(void *out, const TableDesc *__restrict__ tables, int fp64) {
+    const TableDesc td = tables[blockIdx.y];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < td.n; k += gridDim.x * blockDim.x) {
+        const uint64_t at = td.out_off + static_cast<uint64_t>(k) * td.n + k;
+        if (fp64)
+            static_cast<double *>(out)[at] = 0.0;
+        else
+            static_cast<float *>(out)[at] = 0.0f;
+    }
 }
 
 // ---------------------------------------------------------- pair kernels
@@ -223,20 +252,25 @@ __device__ __forceinline__ void emit_pair(const OutSpec &o, uint32_t n, uint32_t
     }
 }
 
+// Work of one pair launch: tiles (x = k block, y = l block in the group's
+// columns, z = table) times node splits, walked by a persistent grid.
 template <typename T>
 struct PairArgs {
-    const uint2 *tiles;
+    const uint4 *tiles;
     uint32_t n_tiles;
+    uint32_t n_splits;
+    const TableDesc *tables;
     const T *U;       // embedding, or presence words for the bit kernels
     const T *C;       // raw counts (variance adjusted)
-    const T *len;     // embedded lengths
+    const T *len;     // embedded lengths (table z at len + z * len_stride)
+    uint64_t len_stride;
     const T *tot;     // per-sample totals in T (variance adjusted)
     const T *W;       // per-sample weighted sums (weighted normalized)
     const unsigned long long *P;  // presence words (unweighted)
-    const T *lut;                 // 8-bit length tables (unweighted)
+    const T *lut;                 // 8-bit length tables (unweighted), table z at lut + z * lut_stride
+    uint64_t lut_stride;
     uint32_t E;       // embedded rows (or words for the bit kernel)
     uint64_t ld;
-    uint32_t n;
     uint32_t rows_per_split;
     T alpha;
     OutSpec out;
@@ -256,17 +290,23 @@ struct OpWeighted {
     __device__ static T value(const T *acc, T wk, T wl) { return NORMALIZED ? acc[0] / (wk + wl) : acc[0]; }
 };
 
-// (u+v)^alpha with the exact special cases: alpha 1 and 0 are exact in C's
-// pow, and a correctly rounded pow(x, 0.5) is the correctly rounded sqrt.
-template <typename T, int AK>
+// (u+v)^alpha for the general alpha kind.
+template <typename T>
 __device__ __forceinline__ T pow_alpha(T s, T alpha) {
-    if (AK == 1) return sqrt(s);
-    if (AK == 2) return s;
-    if (AK == 3) return T(1);
     return pow(s, alpha);
 }
 
-// src/unifrac_task_impl.hpp:924-1040
+// 1/sqrt(x): one rsqrt instead of a sqrt and a division.  Every term below is
+// rewritten with it in a mathematically identical form (a few ulp per term).
+template <typename T>
+__device__ __forceinline__ T inv_sqrt(T x) {
+    return rsqrt(x);
+}
+
+// src/unifrac_task_impl.hpp:924-1040: per node, with s = u + v and
+// sp = s^alpha L, num += sp |u - v| / s and den += sp (nodes with s = 0 add
+// nothing).  Alpha kinds: 1 (0.5) num += L |u-v| / sqrt(s), den += L sqrt(s);
+// 2 (1) num += L |u-v|, den += L s; 3 (0) num += L |u-v| / s, den += L.
 template <typename T, int AK>
 struct OpGeneralized {
     static constexpr int NACC = 2;
@@ -274,59 +314,88 @@ struct OpGeneralized {
     __device__ static void term(T *acc, T a, T b, T, T, T, T L, T alpha) {
         const T s = a + b;
         if (s != T(0)) {
-            const T sp = pow_alpha<T, AK>(s, alpha) * L;
-            acc[0] = fma(sp, tabs(a - b) / s, acc[0]);
-            acc[1] += sp;
+            if (AK == 2) {
+                acc[0] = fma(L, tabs(a - b), acc[0]);
+                acc[1] = fma(L, s, acc[1]);
+            } else if (AK == 1) {
+                const T t = L * inv_sqrt(s);
+                acc[0] = fma(t, tabs(a - b), acc[0]);
+                acc[1] = fma(t, s, acc[1]);
+            } else if (AK == 3) {
+                acc[0] = fma(L, tabs(a - b) / s, acc[0]);
+                acc[1] += L;
+            } else {
+                const T sp = pow_alpha<T>(s, alpha) * L;
+                acc[0] = fma(sp, tabs(a - b) / s, acc[0]);
+                acc[1] += sp;
+            }
         }
     }
     __device__ static T value(const T *acc, T, T) { return acc[0] / acc[1]; }
 };
 
-// src/unifrac_task_impl.hpp:435-502, 848-922
+// src/unifrac_task_impl.hpp:435-502, 848-922: with vaw = sqrt(mi (m - mi)),
+// num += |u - v| L / vaw and den += (u + v) L / vaw where vaw > 0.
 template <typename T, bool NORMALIZED>
 struct OpVawWeighted {
     static constexpr int NACC = NORMALIZED ? 2 : 1;
     static constexpr bool COUNTS = true;
     __device__ static void term(T *acc, T a, T b, T ca, T cb, T m, T L, T) {
         const T mi = ca + cb;
-        const T vaw = sqrt(mi * (m - mi));
-        if (vaw > T(0)) {
-            acc[0] += (tabs(a - b) * L) / vaw;
-            if (NORMALIZED) acc[1] += ((a + b) * L) / vaw;
+        const T x = mi * (m - mi);
+        if (x > T(0)) {
+            const T t = L * inv_sqrt(x);
+            acc[0] = fma(t, tabs(a - b), acc[0]);
+            if (NORMALIZED) acc[1] = fma(t, a + b, acc[1]);
         }
     }
     __device__ static T value(const T *acc, T, T) { return NORMALIZED ? acc[0] / acc[NACC - 1] : acc[0]; }
 };
 
-// src/unifrac_task_impl.hpp:1042-1119
+// src/unifrac_task_impl.hpp:1042-1119: s1 = (u + v) / vaw, d1 = |u - v| / vaw,
+// sp = s1^alpha L; num += sp d1 / s1, den += sp.
 template <typename T, int AK>
 struct OpVawGeneralized {
     static constexpr int NACC = 2;
     static constexpr bool COUNTS = true;
     __device__ static void term(T *acc, T a, T b, T ca, T cb, T m, T L, T alpha) {
         const T mi = ca + cb;
-        const T vaw = sqrt(mi * (m - mi));
-        if (vaw > T(0)) {
-            const T s1 = (a + b) / vaw;
-            const T d1 = tabs(a - b) / vaw;
-            const T sp = pow_alpha<T, AK>(s1, alpha) * L;
-            acc[0] = fma(sp, d1 / s1, acc[0]);
-            acc[1] += sp;
+        const T x = mi * (m - mi);
+        if (x > T(0)) {
+            const T r = inv_sqrt(x);
+            const T s1 = (a + b) * r;
+            const T d1 = tabs(a - b) * r;
+            if (AK == 1) {
+                const T t = L * inv_sqrt(s1);
+                acc[0] = fma(t, d1, acc[0]);
+                acc[1] = fma(t, s1, acc[1]);
+            } else if (AK == 2) {
+                acc[0] = fma(L, d1, acc[0]);
+                acc[1] = fma(L, s1, acc[1]);
+            } else if (AK == 3) {
+                acc[0] = fma(L, d1 / s1, acc[0]);
+                acc[1] += L;
+            } else {
+                const T sp = pow_alpha<T>(s1, alpha) * L;
+                acc[0] = fma(sp, d1 / s1, acc[0]);
+                acc[1] += sp;
+            }
         }
     }
     __device__ static T value(const T *acc, T, T) { return acc[0] / acc[1]; }
 };
 
-// src/unifrac_task_impl.hpp:1755-1932
+// src/unifrac_task_impl.hpp:1755-1932: L / vaw where exactly one side is
+// present (num) and where either is (den).
 template <typename T, bool NORMALIZED>
 struct OpVawUnweighted {
     static constexpr int NACC = NORMALIZED ? 2 : 1;
     static constexpr bool COUNTS = true;
     __device__ static void term(T *acc, T a, T b, T ca, T cb, T m, T L, T) {
         const T mi = ca + cb;
-        const T vaw = sqrt(mi * (m - mi));
-        if (vaw > T(0)) {
-            const T lv = L / vaw;
+        const T x = mi * (m - mi);
+        if (x > T(0)) {
+            const T lv = L * inv_sqrt(x);
             const bool pa = a > T(0), pb = b > T(0);
             if (pa != pb) acc[0] += lv;
             if (NORMALIZED && (pa || pb)) acc[1] += lv;
@@ -341,6 +410,14 @@ struct OpUnweightedBits {
     static constexpr int NACC = NORMALIZED ? 2 : 1;
     __device__ static T value(const T *acc, T, T) { return NORMALIZED ? acc[0] / acc[NACC - 1] : acc[0]; }
 };
+
+// Single-precision sums over every embedded node run in two levels: each
+// pipeline chunk (32 rows, or 4 presence words) is summed on its own and
+// then added to the running total, so no fp32 sum grows over more than a few
+// hundred terms in a row (the reference's GPU tasks likewise add one
+// 112-node batch at a time into their stripes).
+template <typename T>
+constexpr bool kTwoLevel = sizeof(T) == 4;
 
 // ---- tile geometry -------------------------------------------------------
 // A thread owns TM rows (k) and TN columns (l) of the BM x BN tile, split in
@@ -364,30 +441,39 @@ __device__ __forceinline__ void load_half(T *dst, const T *src) {
     }
 }
 
-// Shared epilogue: per (i, j) owned by the thread, finish the value and emit it.
+// Shared epilogue: per (i, j) owned by the thread, finish the value and emit
+// it into the tile's table (W is indexed by group column, the output by the
+// table's own sample index).
 template <typename T, class Op, int BM, int BN, int TM, int TN>
-__device__ __forceinline__ void pair_epilogue(const PairArgs<T> &a, uint32_t k0, uint32_t l0, int tx, int ty,
+__device__ __forceinline__ void pair_epilogue(const PairArgs<T> &a, const uint4 tile, int tx, int ty,
                                               const T (&acc)[TM][TN][Op::NACC]) {
+    const TableDesc td = a.tables[tile.z];
+    const uint32_t k0 = tile.x * BM, l0 = tile.y * BN;
+    OutSpec o = a.out;
+    if (o.mode == 0) o.ptr = static_cast<T *>(o.ptr) + td.out_off;
 #pragma unroll
     for (int i = 0; i < TM; i++) {
-        const uint32_t k = k0 + tile_row<BM, TM>(ty, i);
-        const T wk = (a.W && k < a.n) ? a.W[k] : T(0);
+        const uint32_t kc = k0 + tile_row<BM, TM>(ty, i);
+        const uint32_t k = kc - td.base;
+        const T wk = (a.W && k < td.n) ? a.W[kc] : T(0);
 #pragma unroll
         for (int j = 0; j < TN; j++) {
-            const uint32_t l = l0 + tile_row<BN, TN>(tx, j);
-            if (k < l && l < a.n) {
-                const T wl = a.W ? a.W[l] : T(0);
-                emit_pair<T>(a.out, a.n, k, l, Op::value(acc[i][j], wk, wl));
+            const uint32_t lc = l0 + tile_row<BN, TN>(tx, j);
+            const uint32_t l = lc - td.base;
+            if (k < l && l < td.n) {
+                const T wl = a.W ? a.W[lc] : T(0);
+                emit_pair<T>(o, td.n, k, l, Op::value(acc[i][j], wk, wl));
             }
         }
     }
 }
 
 template <typename T, class Op, int BM, int BN, int TM, int TN>
-__device__ __forceinline__ void store_partial(const PairArgs<T> &a, const T (&acc)[TM][TN][Op::NACC]) {
+__device__ __forceinline__ void store_partial(const PairArgs<T> &a, uint32_t split, uint32_t tile,
+                                              const T (&acc)[TM][TN][Op::NACC]) {
     constexpr int NT = (BM / TM) * (BN / TN);
     constexpr int NV = TM * TN * Op::NACC;
-    T *base = a.partial + (static_cast<uint64_t>(blockIdx.y) * a.n_tiles + blockIdx.x) * NV * NT;
+    T *base = a.partial + (static_cast<uint64_t>(split) * a.n_tiles + tile) * NV * NT;
 #pragma unroll
     for (int i = 0; i < TM; i++)
 #pragma unroll
@@ -422,14 +508,14 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN))
                 for (int c = 0; c < Op::NACC; c++)
                     acc[i][j][c] += base[static_cast<uint64_t>((i * TN + j) * Op::NACC + c) * NT + threadIdx.x];
     }
-    const uint2 tile = a.tiles[blockIdx.x];
-    pair_epilogue<T, Op, BM, BN, TM, TN>(a, tile.x * BM, tile.y * BN, tx, ty, acc);
+    pair_epilogue<T, Op, BM, BN, TM, TN>(a, a.tiles[blockIdx.x], tx, ty, acc);
 }
 
 // ---- value pair kernel (weighted, generalized, variance adjusted) ---------
 //
-// Grid: x = tile, y = node split.  Each CTA streams its node rows through a
-// two-stage cp.async pipeline of KC rows: BM values of the k block and BN
+// Persistent grid over work items w = split * n_tiles + tile (split-major,
+// so CTAs running together read the same node rows).  Each item streams its
+// node rows through a two-stage cp.async pipeline of KC rows: BM values of the k block and BN
 // of the l block per row (plus raw counts for variance adjustment) and the
 // KC lengths.
 template <typename T, class Op, int BM, int BN, int TM, int TN, int KC>
@@ -447,94 +533,121 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) pair_values_kernel(c
     T *Bcs = Acs + (CNT ? 2 * KC * BM : 0);   // [2][KC][BN] counts
     T *Ls = Bcs + (CNT ? 2 * KC * BN : 0);    // [2][KC]
 
-    const uint2 tile = a.tiles[blockIdx.x];
-    const uint32_t k0 = tile.x * BM, l0 = tile.y * BN;
-    const uint32_t e_begin = blockIdx.y * a.rows_per_split;
-    const uint32_t e_end = min(a.E, e_begin + a.rows_per_split);
     const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+    const uint32_t n_work = a.n_tiles * a.n_splits;
+    for (uint32_t w = blockIdx.x; w < n_work; w += gridDim.x) {
+        const uint32_t split = w / a.n_tiles, ti = w - split * a.n_tiles;
+        const uint4 tile = a.tiles[ti];
+        const uint32_t k0 = tile.x * BM, l0 = tile.y * BN;
+        const uint32_t e_begin = split * a.rows_per_split;
+        const uint32_t e_end = min(a.E, e_begin + a.rows_per_split);
+        const T *lenp = a.len + tile.z * a.len_stride;
 
-    T acc[TM][TN][Op::NACC];
+        T acc[TM][TN][Op::NACC];
 #pragma unroll
-    for (int i = 0; i < TM; i++)
+        for (int i = 0; i < TM; i++)
 #pragma unroll
-        for (int j = 0; j < TN; j++)
+            for (int j = 0; j < TN; j++)
 #pragma unroll
-            for (int c = 0; c < Op::NACC; c++) acc[i][j][c] = T(0);
+                for (int c = 0; c < Op::NACC; c++) acc[i][j][c] = T(0);
 
-    T tk[TM], tl[TN];
-    if (CNT) {
+        T tk[TM], tl[TN];
+        if (CNT) {
 #pragma unroll
-        for (int i = 0; i < TM; i++) tk[i] = a.tot[k0 + tile_row<BM, TM>(ty, i)];
+            for (int i = 0; i < TM; i++) tk[i] = a.tot[k0 + tile_row<BM, TM>(ty, i)];
 #pragma unroll
-        for (int j = 0; j < TN; j++) tl[j] = a.tot[l0 + tile_row<BN, TN>(tx, j)];
-    }
-
-    auto load_stage = [&](int st, uint32_t e0) {
-        for (int c = tid; c < KC * CPR_A; c += NT) {
-            const int r = c / CPR_A, q = c % CPR_A;
-            const uint32_t e = e0 + r;
-            const bool ok = e < e_end;
-            const uint64_t off = static_cast<uint64_t>(ok ? e : 0) * a.ld + k0 + q * VEC;
-            cp_async16(As + (st * KC + r) * BM + q * VEC, a.U + off, ok ? 16 : 0);
-            if (CNT) cp_async16(Acs + (st * KC + r) * BM + q * VEC, a.C + off, ok ? 16 : 0);
+            for (int j = 0; j < TN; j++) tl[j] = a.tot[l0 + tile_row<BN, TN>(tx, j)];
         }
-        for (int c = tid; c < KC * CPR_B; c += NT) {
-            const int r = c / CPR_B, q = c % CPR_B;
-            const uint32_t e = e0 + r;
-            const bool ok = e < e_end;
-            const uint64_t off = static_cast<uint64_t>(ok ? e : 0) * a.ld + l0 + q * VEC;
-            cp_async16(Bs + (st * KC + r) * BN + q * VEC, a.U + off, ok ? 16 : 0);
-            if (CNT) cp_async16(Bcs + (st * KC + r) * BN + q * VEC, a.C + off, ok ? 16 : 0);
-        }
-        for (int c = tid; c < KC; c += NT) {
-            const uint32_t e = e0 + c;
-            const bool ok = e < e_end;
-            cp_async_small<sizeof(T)>(Ls + st * KC + c, a.len + (ok ? e : 0), ok ? (int)sizeof(T) : 0);
-        }
-    };
 
-    const uint32_t n_chunks = e_end > e_begin ? (e_end - e_begin + KC - 1) / KC : 0;
-    if (n_chunks > 0) load_stage(0, e_begin);
-    cp_async_commit();
-    for (uint32_t ch = 0; ch < n_chunks; ch++) {
-        const int st = ch & 1;
-        if (ch + 1 < n_chunks) load_stage(st ^ 1, e_begin + (ch + 1) * KC);
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
-        const T *as = As + st * KC * BM;
-        const T *bs = Bs + st * KC * BN;
-        const T *acs = Acs + st * KC * BM;
-        const T *bcs = Bcs + st * KC * BN;
-#pragma unroll 2
-        for (int c = 0; c < KC; c++) {
-            T av[TM], bv[TN], ac[TM], bc[TN];
-            load_half<T, TM / 2>(av, as + c * BM + ty * (TM / 2));
-            load_half<T, TM / 2>(av + TM / 2, as + c * BM + BM / 2 + ty * (TM / 2));
-            load_half<T, TN / 2>(bv, bs + c * BN + tx * (TN / 2));
-            load_half<T, TN / 2>(bv + TN / 2, bs + c * BN + BN / 2 + tx * (TN / 2));
-            if (CNT) {
-                load_half<T, TM / 2>(ac, acs + c * BM + ty * (TM / 2));
-                load_half<T, TM / 2>(ac + TM / 2, acs + c * BM + BM / 2 + ty * (TM / 2));
-                load_half<T, TN / 2>(bc, bcs + c * BN + tx * (TN / 2));
-                load_half<T, TN / 2>(bc + TN / 2, bcs + c * BN + BN / 2 + tx * (TN / 2));
+        auto load_stage = [&](int st, uint32_t e0) {
+            for (int c = tid; c < KC * CPR_A; c += NT) {
+                const int r = c / CPR_A, q = c % CPR_A;
+                const uint32_t e = e0 + r;
+                const bool ok = e < e_end;
+                const uint64_t off = static_cast<uint64_t>(ok ? e : 0) * a.ld + k0 + q * VEC;
+                cp_async16(As + (st * KC + r) * BM + q * VEC, a.U + off, ok ? 16 : 0);
+                if (CNT) cp_async16(Acs + (st * KC + r) * BM + q * VEC, a.C + off, ok ? 16 : 0);
             }
-            const T L = Ls[st * KC + c];
-#pragma unroll
-            for (int i = 0; i < TM; i++)
-#pragma unroll
-                for (int j = 0; j < TN; j++)
-                    Op::term(acc[i][j], av[i], bv[j], CNT ? ac[i] : T(0), CNT ? bc[j] : T(0),
-                             CNT ? tk[i] + tl[j] : T(0), L, a.alpha);
-        }
-        __syncthreads();
-    }
-    cp_async_wait<0>();
+            for (int c = tid; c < KC * CPR_B; c += NT) {
+                const int r = c / CPR_B, q = c % CPR_B;
+                const uint32_t e = e0 + r;
+                const bool ok = e < e_end;
+                const uint64_t off = static_cast<uint64_t>(ok ? e : 0) * a.ld + l0 + q * VEC;
+                cp_async16(Bs + (st * KC + r) * BN + q * VEC, a.U + off, ok ? 16 : 0);
+                if (CNT) cp_async16(Bcs + (st * KC + r) * BN + q * VEC, a.C + off, ok ? 16 : 0);
+            }
+            for (int c = tid; c < KC; c += NT) {
+                const uint32_t e = e0 + c;
+                const bool ok = e < e_end;
+                cp_async_small<sizeof(T)>(Ls + st * KC + c, lenp + (ok ? e : 0), ok ? (int)sizeof(T) : 0);
+            }
+        };
 
-    if (a.partial)
-        store_partial<T, Op, BM, BN, TM, TN>(a, acc);
-    else
-        pair_epilogue<T, Op, BM, BN, TM, TN>(a, k0, l0, tx, ty, acc);
+        const uint32_t n_chunks = e_end > e_begin ? (e_end - e_begin + KC - 1) / KC : 0;
+        if (n_chunks > 0) load_stage(0, e_begin);
+        cp_async_commit();
+        for (uint32_t ch = 0; ch < n_chunks; ch++) {
+            const int st = ch & 1;
+            if (ch + 1 < n_chunks) load_stage(st ^ 1, e_begin + (ch + 1) * KC);
+            cp_async_commit();
+            cp_async_wait<1>();
+            __syncthreads();
+            const T *as = As + st * KC * BM;
+            const T *bs = Bs + st * KC * BN;
+            const T *acs = Acs + st * KC * BM;
+            const T *bcs = Bcs + st * KC * BN;
+            auto chunk = [&](T (&dst)[TM][TN][Op::NACC]) {
+#pragma unroll 2
+                for (int c = 0; c < KC; c++) {
+                    T av[TM], bv[TN], ac[TM], bc[TN];
+                    load_half<T, TM / 2>(av, as + c * BM + ty * (TM / 2));
+                    load_half<T, TM / 2>(av + TM / 2, as + c * BM + BM / 2 + ty * (TM / 2));
+                    load_half<T, TN / 2>(bv, bs + c * BN + tx * (TN / 2));
+                    load_half<T, TN / 2>(bv + TN / 2, bs + c * BN + BN / 2 + tx * (TN / 2));
+                    if (CNT) {
+                        load_half<T, TM / 2>(ac, acs + c * BM + ty * (TM / 2));
+                        load_half<T, TM / 2>(ac + TM / 2, acs + c * BM + BM / 2 + ty * (TM / 2));
+                        load_half<T, TN / 2>(bc, bcs + c * BN + tx * (TN / 2));
+                        load_half<T, TN / 2>(bc + TN / 2, bcs + c * BN + BN / 2 + tx * (TN / 2));
+                    }
+                    const T L = Ls[st * KC + c];
+#pragma unroll
+                    for (int i = 0; i < TM; i++)
+#pragma unroll
+                        for (int j = 0; j < TN; j++)
+                            Op::term(dst[i][j], av[i], bv[j], CNT ? ac[i] : T(0), CNT ? bc[j] : T(0),
+                                     CNT ? tk[i] + tl[j] : T(0), L, a.alpha);
+                }
+            };
+            if constexpr (kTwoLevel<T>) {
+                // single precision: sum the chunk on its own, then fold it in
+                T part[TM][TN][Op::NACC];
+#pragma unroll
+                for (int i = 0; i < TM; i++)
+#pragma unroll
+                    for (int j = 0; j < TN; j++)
+#pragma unroll
+                        for (int q = 0; q < Op::NACC; q++) part[i][j][q] = T(0);
+                chunk(part);
+#pragma unroll
+                for (int i = 0; i < TM; i++)
+#pragma unroll
+                    for (int j = 0; j < TN; j++)
+#pragma unroll
+                        for (int q = 0; q < Op::NACC; q++) acc[i][j][q] += part[i][j][q];
+            } else {
+                chunk(acc);
+            }
+            __syncthreads();
+        }
+        cp_async_wait<0>();
+
+        if (a.partial)
+            store_partial<T, Op, BM, BN, TM, TN>(a, split, ti, acc);
+        else
+            pair_epilogue<T, Op, BM, BN, TM, TN>(a, tile, tx, ty, acc);
+        __syncthreads();  // shared memory is reused by the next work item
+    }
 }
 
 template <typename T, class Op, int BM, int BN, int KC>
@@ -561,94 +674,116 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) pair_bits_kernel(con
     u64 *As = reinterpret_cast<u64 *>(Ls + 2 * KW * LUTW);  // [2][KW][BM]
     u64 *Bs = As + 2 * KW * BM;                             // [2][KW][BN]
 
-    const uint2 tile = a.tiles[blockIdx.x];
-    const uint32_t k0 = tile.x * BM, l0 = tile.y * BN;
-    const uint32_t w_begin = blockIdx.y * a.rows_per_split;
-    const uint32_t w_end = min(a.E, w_begin + a.rows_per_split);
     const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+    const uint32_t n_work = a.n_tiles * a.n_splits;
+    for (uint32_t wi = blockIdx.x; wi < n_work; wi += gridDim.x) {
+        const uint32_t split = wi / a.n_tiles, ti = wi - split * a.n_tiles;
+        const uint4 tile = a.tiles[ti];
+        const uint32_t k0 = tile.x * BM, l0 = tile.y * BN;
+        const uint32_t w_begin = split * a.rows_per_split;
+        const uint32_t w_end = min(a.E, w_begin + a.rows_per_split);
+        const T *lutp = a.lut + tile.z * a.lut_stride;
 
-    T acc[TM][TN][Op::NACC];
+        T acc[TM][TN][Op::NACC];
 #pragma unroll
-    for (int i = 0; i < TM; i++)
+        for (int i = 0; i < TM; i++)
 #pragma unroll
-        for (int j = 0; j < TN; j++)
+            for (int j = 0; j < TN; j++)
 #pragma unroll
-            for (int c = 0; c < Op::NACC; c++) acc[i][j][c] = T(0);
+                for (int c = 0; c < Op::NACC; c++) acc[i][j][c] = T(0);
 
-    auto load_stage = [&](int st, uint32_t w0) {
-        for (int c = tid; c < KW * LUT_CHUNKS; c += NT) {
-            const int r = c / LUT_CHUNKS, q = c % LUT_CHUNKS;
-            const uint32_t w = w0 + r;
-            const bool ok = w < w_end;
-            cp_async16(reinterpret_cast<unsigned char *>(Ls + (st * KW + r) * LUTW) + q * 16,
-                       reinterpret_cast<const unsigned char *>(a.lut + static_cast<uint64_t>(ok ? w : 0) * LUTW) +
-                           q * 16,
-                       ok ? 16 : 0);
-        }
-        for (int c = tid; c < KW * (BM / 2); c += NT) {
-            const int r = c / (BM / 2), q = c % (BM / 2);
-            const uint32_t w = w0 + r;
-            const bool ok = w < w_end;
-            cp_async16(As + (st * KW + r) * BM + q * 2, a.P + static_cast<uint64_t>(ok ? w : 0) * a.ld + k0 + q * 2,
-                       ok ? 16 : 0);
-        }
-        for (int c = tid; c < KW * (BN / 2); c += NT) {
-            const int r = c / (BN / 2), q = c % (BN / 2);
-            const uint32_t w = w0 + r;
-            const bool ok = w < w_end;
-            cp_async16(Bs + (st * KW + r) * BN + q * 2, a.P + static_cast<uint64_t>(ok ? w : 0) * a.ld + l0 + q * 2,
-                       ok ? 16 : 0);
-        }
-    };
+        auto load_stage = [&](int st, uint32_t w0) {
+            for (int c = tid; c < KW * LUT_CHUNKS; c += NT) {
+                const int r = c / LUT_CHUNKS, q = c % LUT_CHUNKS;
+                const uint32_t w = w0 + r;
+                const bool ok = w < w_end;
+                cp_async16(reinterpret_cast<unsigned char *>(Ls + (st * KW + r) * LUTW) + q * 16,
+                           reinterpret_cast<const unsigned char *>(lutp + static_cast<uint64_t>(ok ? w : 0) * LUTW) +
+                               q * 16,
+                           ok ? 16 : 0);
+            }
+            for (int c = tid; c < KW * (BM / 2); c += NT) {
+                const int r = c / (BM / 2), q = c % (BM / 2);
+                const uint32_t w = w0 + r;
+                const bool ok = w < w_end;
+                cp_async16(As + (st * KW + r) * BM + q * 2, a.P + static_cast<uint64_t>(ok ? w : 0) * a.ld + k0 + q * 2,
+                           ok ? 16 : 0);
+            }
+            for (int c = tid; c < KW * (BN / 2); c += NT) {
+                const int r = c / (BN / 2), q = c % (BN / 2);
+                const uint32_t w = w0 + r;
+                const bool ok = w < w_end;
+                cp_async16(Bs + (st * KW + r) * BN + q * 2, a.P + static_cast<uint64_t>(ok ? w : 0) * a.ld + l0 + q * 2,
+                           ok ? 16 : 0);
+            }
+        };
 
-    const uint32_t n_chunks = w_end > w_begin ? (w_end - w_begin + KW - 1) / KW : 0;
-    if (n_chunks > 0) load_stage(0, w_begin);
-    cp_async_commit();
-    for (uint32_t ch = 0; ch < n_chunks; ch++) {
-        const int st = ch & 1;
-        if (ch + 1 < n_chunks) load_stage(st ^ 1, w_begin + (ch + 1) * KW);
+        const uint32_t n_chunks = w_end > w_begin ? (w_end - w_begin + KW - 1) / KW : 0;
+        if (n_chunks > 0) load_stage(0, w_begin);
         cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
-        for (int r = 0; r < KW; r++) {
-            const T *lut = Ls + (st * KW + r) * LUTW;
-            const u64 *as = As + (st * KW + r) * BM;
-            const u64 *bs = Bs + (st * KW + r) * BN;
-            u64 av[TM], bv[TN];
+        for (uint32_t ch = 0; ch < n_chunks; ch++) {
+            const int st = ch & 1;
+            if (ch + 1 < n_chunks) load_stage(st ^ 1, w_begin + (ch + 1) * KW);
+            cp_async_commit();
+            cp_async_wait<1>();
+            __syncthreads();
+            T part[TM][TN][Op::NACC];
 #pragma unroll
-            for (int i = 0; i < TM; i++) av[i] = as[tile_row<BM, TM>(ty, i)];
+            for (int i = 0; i < TM; i++)
 #pragma unroll
-            for (int j = 0; j < TN; j++) bv[j] = bs[tile_row<BN, TN>(tx, j)];
+                for (int j = 0; j < TN; j++)
 #pragma unroll
-            for (int i = 0; i < TM; i++) {
+                    for (int q = 0; q < Op::NACC; q++) part[i][j][q] = T(0);
+            T(&dst)[TM][TN][Op::NACC] = kTwoLevel<T> ? part : acc;
+            for (int r = 0; r < KW; r++) {
+                const T *lut = Ls + (st * KW + r) * LUTW;
+                const u64 *as = As + (st * KW + r) * BM;
+                const u64 *bs = Bs + (st * KW + r) * BN;
+                u64 av[TM], bv[TN];
 #pragma unroll
-                for (int j = 0; j < TN; j++) {
-                    const u64 o = av[i] | bv[j];
-                    if (o == 0ull) continue;
-                    const u64 x = av[i] ^ bv[j];
-                    const uint32_t xl = static_cast<uint32_t>(x), xh = static_cast<uint32_t>(x >> 32);
-                    acc[i][j][0] += lut[xl & 255u] + lut[256 + ((xl >> 8) & 255u)] + lut[512 + ((xl >> 16) & 255u)] +
-                                    lut[768 + (xl >> 24)] + lut[1024 + (xh & 255u)] +
-                                    lut[1280 + ((xh >> 8) & 255u)] + lut[1536 + ((xh >> 16) & 255u)] +
-                                    lut[1792 + (xh >> 24)];
-                    if (NORMALIZED) {
-                        const uint32_t ol = static_cast<uint32_t>(o), oh = static_cast<uint32_t>(o >> 32);
-                        acc[i][j][1] += lut[ol & 255u] + lut[256 + ((ol >> 8) & 255u)] +
-                                        lut[512 + ((ol >> 16) & 255u)] + lut[768 + (ol >> 24)] +
-                                        lut[1024 + (oh & 255u)] + lut[1280 + ((oh >> 8) & 255u)] +
-                                        lut[1536 + ((oh >> 16) & 255u)] + lut[1792 + (oh >> 24)];
+                for (int i = 0; i < TM; i++) av[i] = as[tile_row<BM, TM>(ty, i)];
+#pragma unroll
+                for (int j = 0; j < TN; j++) bv[j] = bs[tile_row<BN, TN>(tx, j)];
+#pragma unroll
+                for (int i = 0; i < TM; i++) {
+#pragma unroll
+                    for (int j = 0; j < TN; j++) {
+                        const u64 o = av[i] | bv[j];
+                        if (o == 0ull) continue;
+                        const u64 x = av[i] ^ bv[j];
+                        const uint32_t xl = static_cast<uint32_t>(x), xh = static_cast<uint32_t>(x >> 32);
+                        dst[i][j][0] += lut[xl & 255u] + lut[256 + ((xl >> 8) & 255u)] + lut[512 + ((xl >> 16) & 255u)] +
+                                        lut[768 + (xl >> 24)] + lut[1024 + (xh & 255u)] +
+                                        lut[1280 + ((xh >> 8) & 255u)] + lut[1536 + ((xh >> 16) & 255u)] +
+                                        lut[1792 + (xh >> 24)];
+                        if (NORMALIZED) {
+                            const uint32_t ol = static_cast<uint32_t>(o), oh = static_cast<uint32_t>(o >> 32);
+                            dst[i][j][1] += lut[ol & 255u] + lut[256 + ((ol >> 8) & 255u)] +
+                                            lut[512 + ((ol >> 16) & 255u)] + lut[768 + (ol >> 24)] +
+                                            lut[1024 + (oh & 255u)] + lut[1280 + ((oh >> 8) & 255u)] +
+                                            lut[1536 + ((oh >> 16) & 255u)] + lut[1792 + (oh >> 24)];
+                        }
                     }
                 }
             }
+            if constexpr (kTwoLevel<T>) {
+#pragma unroll
+                for (int i = 0; i < TM; i++)
+#pragma unroll
+                    for (int j = 0; j < TN; j++)
+#pragma unroll
+                        for (int q = 0; q < Op::NACC; q++) acc[i][j][q] += part[i][j][q];
+            }
+            __syncthreads();
         }
-        __syncthreads();
-    }
-    cp_async_wait<0>();
+        cp_async_wait<0>();
 
-    if (a.partial)
-        store_partial<T, Op, BM, BN, TM, TN>(a, acc);
-    else
-        pair_epilogue<T, Op, BM, BN, TM, TN>(a, k0, l0, tx, ty, acc);
+        if (a.partial)
+            store_partial<T, Op, BM, BN, TM, TN>(a, split, ti, acc);
+        else
+            pair_epilogue<T, Op, BM, BN, TM, TN>(a, tile, tx, ty, acc);
+        __syncthreads();  // shared memory is reused by the next work item
+    }
 }
 
 template <typename T, int BM, int BN, int KW>

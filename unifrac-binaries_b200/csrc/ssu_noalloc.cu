@@ -96,21 +96,25 @@ template <bool NORM>
 int run(const DeviceSetup &ds, const double *U, const double *len, uint32_t E, uint32_t n, uint64_t ld,
         double *out, cudaStream_t stream) {
     using Op = WeightedOp<NORM>;
-    // tile list: every (kb, lb) holding a pair k < l
-    std::vector<uint2> tiles;
+    // tile list: every (kb, lb) holding a pair k < l, all of table 0
+    std::vector<uint4> tiles;
     const uint32_t nbk = (n + BM - 1) / BM, nbl = (n + BN - 1) / BN;
     for (uint32_t kb = 0; kb < nbk; kb++)
         for (uint32_t lb = 0; lb < nbl; lb++)
             if (static_cast<uint64_t>(kb) * BM < std::min<uint64_t>(n, static_cast<uint64_t>(lb + 1) * BN) - 1)
-                tiles.push_back(make_uint2(kb, lb));
+                tiles.push_back(make_uint4(kb, lb, 0, 0));
     const uint32_t n_tiles = static_cast<uint32_t>(tiles.size());
+    ssu::dev::TableDesc table{};
+    table.n = n;
 
-    // scratch layout: [tiles][W][W partials][split partials], 256-byte aligned
+    // scratch layout: [table][tiles][W][W partials][split partials], 256-byte aligned
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     unsigned char *base = static_cast<unsigned char *>(ds.scratch);
     size_t off = 0;
-    uint2 *d_tiles = reinterpret_cast<uint2 *>(base + off);
-    off = align(off + sizeof(uint2) * std::max<uint32_t>(n_tiles, 1));
+    ssu::dev::TableDesc *d_table = reinterpret_cast<ssu::dev::TableDesc *>(base + off);
+    off = align(off + sizeof(ssu::dev::TableDesc));
+    uint4 *d_tiles = reinterpret_cast<uint4 *>(base + off);
+    off = align(off + sizeof(uint4) * std::max<uint32_t>(n_tiles, 1));
     double *d_W = nullptr, *d_part = nullptr;
     uint32_t n_parts = 0, chunk = kWChunk;
     if (NORM) {
@@ -154,38 +158,45 @@ int run(const DeviceSetup &ds, const double *U, const double *len, uint32_t E, u
     if (splits == 0) splits = 1;
     double *d_split = splits > 1 ? reinterpret_cast<double *>(base + off) : nullptr;
 
-    cudaError_t e = cudaMemcpyAsync(d_tiles, tiles.data(), sizeof(uint2) * n_tiles, cudaMemcpyHostToDevice, stream);
+    cudaError_t e = cudaMemcpyAsync(d_tiles, tiles.data(), sizeof(uint4) * n_tiles, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_table, &table, sizeof(table), cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) {
         note(cudaGetErrorString(e));
         return output_error;
     }
     if (NORM) {
         dim3 grid(static_cast<uint32_t>((ld + 255) / 256), n_parts);
-        ssu::dev::weighted_sums_partial_kernel<double><<<grid, 256, 0, stream>>>(U, len, E, ld, chunk, d_part);
+        ssu::dev::weighted_sums_partial_kernel<double><<<grid, 256, 0, stream>>>(U, len, E, ld, chunk, d_part,
+                                                                                nullptr, 0);
         ssu::dev::reduce_partials_kernel<double><<<static_cast<uint32_t>((ld + 255) / 256), 256, 0, stream>>>(
             d_part, n_parts, ld, d_W);
     }
     ssu::dev::PairArgs<double> a{};
     a.tiles = d_tiles;
     a.n_tiles = n_tiles;
+    a.n_splits = splits;
+    a.tables = d_table;
     a.U = U;
     a.len = len;
     a.W = d_W;
     a.E = E;
     a.ld = ld;
-    a.n = n;
     a.rows_per_split = splits > 1 ? rows : E;
     a.out = ssu::dev::OutSpec{0, out, 0, 0};
     a.partial = d_split;
     const size_t smem = ssu::dev::pair_values_smem<double, Op, BM, BN, KC>();
     if (n_tiles) {
+        const uint64_t work = static_cast<uint64_t>(n_tiles) * splits;
+        const uint32_t ctas =
+            static_cast<uint32_t>(std::min<uint64_t>(work, static_cast<uint64_t>(ds.n_sms) * ds.blocks_per_sm));
         ssu::dev::pair_values_kernel<double, Op, BM, BN, TM, TN, KC>
-            <<<dim3(n_tiles, splits), (BM / TM) * (BN / TN), smem, stream>>>(a);
+            <<<ctas, (BM / TM) * (BN / TN), smem, stream>>>(a);
         if (splits > 1)
             ssu::dev::split_finalize_kernel<double, Op, BM, BN, TM, TN>
                 <<<n_tiles, (BM / TM) * (BN / TN), 0, stream>>>(a, splits);
     }
-    ssu::dev::zero_diagonal_kernel<<<(n + 255) / 256, 256, 0, stream>>>(out, n, 1);
+    ssu::dev::zero_diagonal_kernel<<<dim3((n + 255) / 256, 1), 256, 0, stream>>>(out, d_table, 1);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         note(cudaGetErrorString(e));

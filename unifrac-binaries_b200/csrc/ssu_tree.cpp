@@ -371,4 +371,32 @@ FlatTree flatten(const BPTree &t, bool bypass_tips) {
     return flatten_impl(t, bypass_tips, [&](uint32_t o) -> int32_t { return t.tag.empty() ? -1 : t.tag[o]; });
 }
 
+uint32_t table_embedded(const FlatTree &f, const std::vector<int32_t> &obs_row, bool bypass_tips,
+                        std::vector<uint8_t> *active) {
+    std::vector<uint32_t> tips(f.n_nodes, 0);  // kept tips below each row
+    uint32_t count = 0;
+    if (active) active->assign(f.n_embedded, 0);
+    for (uint32_t k = 0; k < f.n_nodes; k++) {
+        const uint32_t row = f.postorder_row[k];
+        if (f.child_ptr[row] == f.child_ptr[row + 1]) {
+            const int32_t o = f.leaf_obs[row];
+            const bool kept = o >= 0 && static_cast<size_t>(o) < obs_row.size() && obs_row[o] >= 0;
+            tips[row] = kept ? 1 : 0;
+            if (kept && !bypass_tips) count++;
+            if (active && row < f.n_embedded) (*active)[row] = kept ? 1 : 0;
+            continue;
+        }
+        uint32_t below = 0, kids = 0;
+        for (uint32_t q = f.child_ptr[row]; q < f.child_ptr[row + 1]; q++) {
+            const uint32_t c = f.child_rows[q];
+            below += tips[c];
+            kids += tips[c] > 0;
+        }
+        tips[row] = below;
+        if (kids >= 2) count++;
+        if (active && row < f.n_embedded) (*active)[row] = below >= (bypass_tips ? 2u : 1u);
+    }
+    return count;
+}
+
 }  // namespace ssu

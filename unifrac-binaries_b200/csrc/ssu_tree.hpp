@@ -89,4 +89,14 @@ FlatTree flatten(const BPTree &tree, const NameIndex &obs_index, bool bypass_tip
 // Flatten a tree whose tips carry table rows in `tag` (from shear_to).
 FlatTree flatten(const BPTree &tree, bool bypass_tips);
 
+// Embedded node count of the tree sheared to the observations o with
+// obs_row[o] >= 0 and then collapsed, computed on a flattened tree of a
+// superset of those observations: kept tips (unless bypassed) plus the
+// non-root internal nodes with at least two kept children.  With `active`,
+// also which embedded rows of `tree` carry length into that table's sums:
+// rows above at least one kept tip, or at least two with bypassed tips
+// (a chain above a single tip merges into the tip).
+uint32_t table_embedded(const FlatTree &tree, const std::vector<int32_t> &obs_row, bool bypass_tips,
+                        std::vector<uint8_t> *active);
+
 }  // namespace ssu

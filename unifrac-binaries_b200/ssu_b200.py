@@ -139,6 +139,26 @@ def lib():
         L.ssu_b200_plan_pair_kernel.argtypes = [C.c_void_p]
         L.ssu_b200_plan_pair_kernel.restype = C.c_char_p
         L.ssu_b200_version.restype = C.c_char_p
+        batch_common = [P(P(SupportBiom)), C.c_uint, P(SupportBPTree), C.c_char_p, C.c_bool, C.c_double, C.c_bool,
+                        C.c_bool]
+        L.ssu_b200_one_off_batch_inmem_v3.argtypes = batch_common + [P(P(MatFull64))]
+        L.ssu_b200_one_off_batch_inmem_fp32_v3.argtypes = batch_common + [P(P(MatFull32))]
+        sub_common = [P(SupportBiom), P(SupportBPTree), C.c_char_p, C.c_bool, C.c_double, C.c_bool, C.c_bool,
+                      C.c_uint, C.c_uint, C.c_bool]
+        L.ssu_b200_subsample_batch_inmem_v3.argtypes = sub_common + [P(P(MatFull64))]
+        L.ssu_b200_subsample_batch_inmem_fp32_v3.argtypes = sub_common + [P(P(MatFull32))]
+        L.ssu_b200_batch_plan_create.argtypes = batch_common + [C.c_uint64, C.c_int, P(C.c_void_p)]
+        for name, res in [("ssu_b200_plan_n_tables", C.c_uint32), ("ssu_b200_plan_n_groups", C.c_uint32)]:
+            getattr(L, name).argtypes = [C.c_void_p]
+            getattr(L, name).restype = res
+        for name, res in [("ssu_b200_plan_table_samples", C.c_uint32), ("ssu_b200_plan_table_offset", C.c_uint64),
+                          ("ssu_b200_plan_table_embedded", C.c_uint64)]:
+            getattr(L, name).argtypes = [C.c_void_p, C.c_uint32]
+            getattr(L, name).restype = res
+        L.ssu_b200_plan_set_graph.argtypes = [C.c_void_p, C.c_int]
+        L.ssu_b200_plan_set_graph.restype = None
+        L.ssu_b200_plan_tuning.argtypes = [C.c_void_p]
+        L.ssu_b200_plan_tuning.restype = C.c_char_p
         _lib = L
     return _lib
 
@@ -168,11 +188,10 @@ def _strarr(strings):
     return arr
 
 
-class Inputs:
-    """support_biom_t + support_bptree_t views of a (tree, table) pair; keeps
-    the backing numpy arrays alive while the call runs."""
+class TableInputs:
+    """support_biom_t view of a table; keeps the backing arrays alive."""
 
-    def __init__(self, tree, table):
+    def __init__(self, table):
         self.indptr = np.ascontiguousarray(table.indptr, dtype=np.uint32)
         self.indices = np.ascontiguousarray(table.indices, dtype=np.uint32)
         self.data = np.ascontiguousarray(table.data, dtype=np.float64)
@@ -182,12 +201,40 @@ class Inputs:
                                 self.indptr.ctypes.data_as(C.POINTER(C.c_uint32)),
                                 self.data.ctypes.data_as(C.POINTER(C.c_double)), len(table.obs_ids),
                                 len(table.sample_ids), int(self.indptr[-1]) if len(self.indptr) else 0)
+
+
+class TreeInputs:
+    """support_bptree_t view of a tree; keeps the backing arrays alive."""
+
+    def __init__(self, tree):
         self.structure = np.ascontiguousarray(tree.structure, dtype=np.bool_)
         self.lengths = np.ascontiguousarray(tree.lengths, dtype=np.float64)
         self.names = _strarr(tree.names)
         self.tree = SupportBPTree(self.structure.ctypes.data_as(C.POINTER(C.c_bool)),
                                   self.lengths.ctypes.data_as(C.POINTER(C.c_double)), self.names,
                                   len(tree.names))
+
+
+class Inputs:
+    """support_biom_t + support_bptree_t views of a (tree, table) pair; keeps
+    the backing numpy arrays alive while the call runs."""
+
+    def __init__(self, tree, table):
+        self._table = TableInputs(table)
+        self._tree = TreeInputs(tree)
+        self.biom = self._table.biom
+        self.tree = self._tree.tree
+
+
+class BatchInputs:
+    """support_biom_t* array over several tables plus one tree."""
+
+    def __init__(self, tree, tables):
+        self._tables = [TableInputs(t) for t in tables]
+        self._tree = TreeInputs(tree)
+        self.tree = self._tree.tree
+        self.n = len(tables)
+        self.array = (C.POINTER(SupportBiom) * max(self.n, 1))(*[C.pointer(t.biom) for t in self._tables])
 
 
 def _ids(ptr, n):
@@ -250,6 +297,57 @@ def one_off_matrix(tree, table, method, variance_adjust=False, alpha=1.0, bypass
         out = np.ctypeslib.as_array(res.contents.matrix, shape=(n, n)).copy()
         L.destroy_mat_full_fp32(C.byref(res))
     return out, ids
+
+
+def _take_results(res, n_tables, destroy, ctype, copy):
+    out = []
+    for t in range(n_tables):
+        r = res[t]
+        n = r.contents.n_samples
+        ids = _ids(r.contents.sample_ids, n)
+        if copy:
+            m = np.ctypeslib.as_array(r.contents.matrix, shape=(n, n)).copy() if n else np.zeros((0, 0))
+            destroy(C.byref(r))
+        else:
+            m = _owned_view(r, destroy, ctype, n)
+        out.append((m, ids))
+    return out
+
+
+def one_off_batch(tree, tables, method, variance_adjust=False, alpha=1.0, bypass_tips=False, normalize=True,
+                  copy=True):
+    """Full matrices of several tables sharing `tree`, as one batch
+    (ssu_b200_one_off_batch_inmem_v3 / _fp32_v3).  Returns [(matrix, ids)]."""
+    L = lib()
+    x = BatchInputs(tree, tables)
+    fp64 = is_fp64(method)
+    typ = MatFull64 if fp64 else MatFull32
+    res = (C.POINTER(typ) * max(len(tables), 1))()
+    fn = L.ssu_b200_one_off_batch_inmem_v3 if fp64 else L.ssu_b200_one_off_batch_inmem_fp32_v3
+    st = fn(x.array, len(tables), C.byref(x.tree), method.encode(), variance_adjust, alpha, bypass_tips, normalize,
+            res)
+    if st != 0:
+        raise SSUError(st, fn.__name__)
+    return _take_results(res, len(tables), L.destroy_mat_full_fp64 if fp64 else L.destroy_mat_full_fp32,
+                         C.c_double if fp64 else C.c_float, copy)
+
+
+def subsample_batch(tree, table, method, n_subsamples, depth, with_replacement=False, variance_adjust=False,
+                    alpha=1.0, bypass_tips=False, normalize=True, copy=True):
+    """Rarefied replicates of `table` as one batch
+    (ssu_b200_subsample_batch_inmem_v3 / _fp32_v3).  Returns [(matrix, ids)]."""
+    L = lib()
+    x = Inputs(tree, table)
+    fp64 = is_fp64(method)
+    typ = MatFull64 if fp64 else MatFull32
+    res = (C.POINTER(typ) * max(n_subsamples, 1))()
+    fn = L.ssu_b200_subsample_batch_inmem_v3 if fp64 else L.ssu_b200_subsample_batch_inmem_fp32_v3
+    st = fn(C.byref(x.biom), C.byref(x.tree), method.encode(), variance_adjust, alpha, bypass_tips, normalize,
+            n_subsamples, depth, with_replacement, res)
+    if st != 0:
+        raise SSUError(st, fn.__name__)
+    return _take_results(res, n_subsamples, L.destroy_mat_full_fp64 if fp64 else L.destroy_mat_full_fp32,
+                         C.c_double if fp64 else C.c_float, copy)
 
 
 def status_of_matrix_call(tree, table, method, fp32_entry=False, **kw):
@@ -445,6 +543,12 @@ class Plan:
     def pair_kernel(self):
         return lib().ssu_b200_plan_pair_kernel(self.ptr).decode()
 
+    def tuning(self):
+        return lib().ssu_b200_plan_tuning(self.ptr).decode()
+
+    def set_graph(self, on=True):
+        lib().ssu_b200_plan_set_graph(self.ptr, 1 if on else 0)
+
     def set_timing(self, on=True):
         lib().ssu_b200_plan_set_timing(self.ptr, 1 if on else 0)
 
@@ -463,3 +567,39 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+class BatchPlan(Plan):
+    """Device-resident batch plan over several tables sharing one tree."""
+
+    def __init__(self, tree, tables, method, variance_adjust=False, alpha=1.0, bypass_tips=False, normalize=True,
+                 group_bytes=0, autotune=-1):
+        L = lib()
+        self._x = BatchInputs(tree, tables)
+        self.ptr = C.c_void_p()
+        st = L.ssu_b200_batch_plan_create(self._x.array, len(tables), C.byref(self._x.tree), method.encode(),
+                                          variance_adjust, alpha, bypass_tips, normalize, group_bytes, autotune,
+                                          C.byref(self.ptr))
+        if st != 0:
+            raise SSUError(st, "ssu_b200_batch_plan_create")
+        self.method = method
+        self.n = L.ssu_b200_plan_n_samples(self.ptr)
+        self.n_tables = L.ssu_b200_plan_n_tables(self.ptr)
+        self.sizes = [L.ssu_b200_plan_table_samples(self.ptr, t) for t in range(self.n_tables)]
+        self.offsets = [int(L.ssu_b200_plan_table_offset(self.ptr, t)) for t in range(self.n_tables)]
+
+    def n_groups(self):
+        return int(lib().ssu_b200_plan_n_groups(self.ptr))
+
+    def table_embedded(self, t):
+        return int(lib().ssu_b200_plan_table_embedded(self.ptr, t))
+
+    def results(self, stream=None):
+        dt = np.float64 if is_fp64(self.method) else np.float32
+        total = sum(n * n for n in self.sizes)
+        flat = np.empty(max(total, 1), dtype=dt)
+        st = lib().ssu_b200_plan_copy_result(self.ptr, flat.ctypes.data_as(C.c_void_p),
+                                             C.c_void_p(stream) if stream else None)
+        if st != 0:
+            raise SSUError(st, "ssu_b200_plan_copy_result")
+        return [flat[o:o + n * n].reshape(n, n) for o, n in zip(self.offsets, self.sizes)]

@@ -253,23 +253,53 @@ def presence_table(obs_ids, n_samples, rich_lo, rich_hi, seed) -> Table:
 def rarefy(table: Table, depth: int, seed: int) -> Table:
     """Subsample every sample to `depth` counts without replacement; samples
     below `depth` are dropped and features left empty are removed, as the
-    reference's rarefaction does (src/biom_subsampled.cpp:287-353).  The random
-    stream is this generator's own: both engines are fed the same output."""
+    reference's rarefaction does (src/biom_subsampled.cpp:287-353).  Each
+    sample's draw is a multivariate hypergeometric taken feature by feature
+    (univariate hypergeometric of the feature's count against the rest),
+    vectorised across samples.  The random stream is this generator's own:
+    both engines are fed the same output."""
     rng = np.random.default_rng(seed)
-    dense = table.dense()
-    totals = dense.sum(axis=0)
+    n_obs, n = table.n_obs, table.n_samples
+    indptr = np.asarray(table.indptr, dtype=np.int64)
+    obs = np.repeat(np.arange(n_obs), np.diff(indptr))
+    samp = np.asarray(table.indices, dtype=np.int64)
+    vals = np.asarray(table.data, dtype=np.float64).astype(np.int64)
+    totals = np.bincount(samp, weights=vals, minlength=n).astype(np.int64)
     keep = np.flatnonzero(totals >= depth)
-    sub = np.zeros((table.n_obs, keep.shape[0]), dtype=np.float64)
-    for jj, j in enumerate(keep):
-        col = dense[:, j].astype(np.int64)
-        nz = np.flatnonzero(col)
-        sub[nz, jj] = rng.multivariate_hypergeometric(col[nz], depth)
-    rows = np.flatnonzero(sub.sum(axis=1) > 0)
-    sub = sub[rows]
-    flat = np.flatnonzero(sub.ravel() > 0)
-    vals = sub.ravel()[flat]
-    obs_ids = [table.obs_ids[i] for i in rows]
-    t = make_table(obs_ids, keep.shape[0], flat, vals)
+    new_col = np.full(n, -1, dtype=np.int64)
+    new_col[keep] = np.arange(keep.shape[0])
+    sel = new_col[samp] >= 0
+    obs, samp, vals = obs[sel], new_col[samp[sel]], vals[sel]
+    order = np.lexsort((obs, samp))  # sample-major, features in order
+    obs, samp, vals = obs[order], samp[order], vals[order]
+    m = keep.shape[0]
+    counts = np.bincount(samp, minlength=m)
+    start = np.zeros(m + 1, dtype=np.int64)
+    np.cumsum(counts, out=start[1:])
+    rank = np.arange(obs.shape[0]) - start[samp]
+    width = int(counts.max()) if m else 0
+    grid = np.zeros((m, max(width, 1)), dtype=np.int64)
+    grid[samp, rank] = vals
+    left = grid.sum(axis=1)
+    need = np.full(m, depth, dtype=np.int64)
+    drawn = np.zeros_like(grid)
+    for k in range(width):
+        good = grid[:, k]
+        bad = left - good
+        x = rng.hypergeometric(np.maximum(good, 0), np.maximum(bad, 0), need) if m else good
+        x = np.where(good > 0, x, 0)
+        drawn[:, k] = x
+        need -= x
+        left -= good
+    d = drawn[samp, rank].astype(np.float64)
+    pos = d > 0
+    obs, samp, d = obs[pos], samp[pos], d[pos]
+    rows = np.unique(obs)
+    row_new = np.full(n_obs, -1, dtype=np.int64)
+    row_new[rows] = np.arange(rows.shape[0])
+    flat = row_new[obs] * m + samp
+    order = np.argsort(flat)
+    t = make_table([table.obs_ids[i] for i in rows], m, flat[order], d[order])
     t.sample_ids = [table.sample_ids[j] for j in keep]
     return t
 
