@@ -63,13 +63,16 @@ def test_batch_fp64_matches_oracle_per_table(ssu, oracle_mod, method, vaw, bypas
 
 
 @pytest.mark.parametrize("method", METHODS)
-def test_batch_fp32_within_reference_fp32_error(ssu, oracle_mod, method):
+@pytest.mark.parametrize("bypass", [False, True])
+def test_batch_fp32_within_reference_fp32_error(ssu, oracle_mod, method, bypass):
+    """fp32 unweighted batches run on the tensor cores (with bypassed tips,
+    on the presence-word stripe kernel)."""
     tree, tables = _uneven_batch(12)
-    out = ssu.one_off_batch(tree, tables, method + "_fp32", alpha=0.5)
+    out = ssu.one_off_batch(tree, tables, method + "_fp32", alpha=0.5, bypass_tips=bypass)
     for (gpu, _), t in zip(out, tables):
         assert gpu.dtype == np.float32
-        o64 = oracle_mod.oracle_one_off(tree, t, method + "_fp64", alpha=0.5)["matrix"]
-        o32 = oracle_mod.oracle_one_off(tree, t, method + "_fp32", alpha=0.5)["matrix"]
+        o64 = oracle_mod.oracle_one_off(tree, t, method + "_fp64", alpha=0.5, bypass_tips=bypass)["matrix"]
+        o32 = oracle_mod.oracle_one_off(tree, t, method + "_fp32", alpha=0.5, bypass_tips=bypass)["matrix"]
         ref_err, ref_zero = rel_err(o32, o64)
         ours, ours_zero = rel_err(gpu, o64)
         assert ours <= max(4 * ref_err, 1e-6), (ours, ref_err)
@@ -135,6 +138,24 @@ def test_subsample_batch_replicates_match_single_calls(ssu):
         assert ids == sids
         check_fp64(m, single)
     lib.ssu_set_random_seed(5489)
+
+
+def test_unweighted_fp32_defaults_to_tensor_cores(ssu, monkeypatch):
+    tree, tables = _uneven_batch(19, sizes=(70, 150))
+    plan = ssu.BatchPlan(tree, tables, "unweighted_fp32")
+    assert plan.pair_kernel() == "unweighted_tc_kernel"
+    plan.close()
+    single = ssu.Plan(tree, tables[0], "unweighted_fp32")
+    assert single.pair_kernel() == "unweighted_tc_kernel"
+    single.close()
+    monkeypatch.setenv("UNIFRAC_B200_UNWEIGHTED_MODE", "stripe")
+    single = ssu.Plan(tree, tables[0], "unweighted_fp32")
+    assert single.pair_kernel().startswith("pair_bits")
+    single.close()
+    plan = ssu.BatchPlan(tree, tables, "unweighted_fp32", bypass_tips=True)
+    monkeypatch.delenv("UNIFRAC_B200_UNWEIGHTED_MODE")
+    assert plan.pair_kernel().startswith("pair_bits")
+    plan.close()
 
 
 def test_batch_fp32_subsample_and_status_codes(ssu):

@@ -144,6 +144,17 @@ ssu::FlatTree sync_tree(const ssu::Table &table, const ssu::BPTree &tree, bool b
     return ssu::flatten(sheared, bypass_tips);
 }
 
+// UNIFRAC_B200_UNWEIGHTED_MODE: "gemm" runs unweighted methods on the
+// tensor-core contraction for fp64 results too (max relative error ~1e-7
+// instead of the stripe form's bit-level agreement); "stripe" keeps the
+// presence-word stripe kernel for fp32 results as well.
+void unweighted_mode(ssu::MethodSpec &spec) {
+    if (const char *mode = std::getenv("UNIFRAC_B200_UNWEIGHTED_MODE")) {
+        spec.unweighted_gemm = std::string(mode) == "gemm";
+        spec.unweighted_stripe = std::string(mode) == "stripe";
+    }
+}
+
 struct Request {
     const char *method;
     bool vaw;
@@ -160,11 +171,7 @@ ComputeStatus make_plan(const ssu::Table &table, const ssu::BPTree &tree, const 
     spec.alpha = r.alpha;
     spec.bypass_tips = r.bypass;
     spec.normalize = r.normalize;
-    // UNIFRAC_B200_UNWEIGHTED_MODE=gemm selects the tensor-core contraction
-    // for unweighted methods (max relative error ~1e-7 instead of the stripe
-    // form's bit-level agreement)
-    if (const char *mode = std::getenv("UNIFRAC_B200_UNWEIGHTED_MODE"))
-        spec.unweighted_gemm = std::string(mode) == "gemm";
+    unweighted_mode(spec);
     std::string err;
     if (!select_device(err)) {
         report("device", err);
@@ -385,6 +392,7 @@ ComputeStatus batch_plan(const std::vector<const ssu::Table *> &tables, const ss
     spec.alpha = r.alpha;
     spec.bypass_tips = r.bypass;
     spec.normalize = r.normalize;
+    unweighted_mode(spec);
     std::string err;
     if (!select_device(err)) {
         report("device", err);

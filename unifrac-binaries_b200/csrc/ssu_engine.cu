@@ -221,6 +221,9 @@ struct Group {
     std::vector<double> totals;
     uint4 *d_tiles = nullptr;
     uint32_t n_tiles = 0, splits = 1, rows_per_split = 0;
+    // tensor-core path: per operand row, the starting columns of its tips
+    uint32_t *d_sample_ptr = nullptr;
+    int32_t *d_start_col = nullptr;
 };
 
 struct PlanImpl {
@@ -280,14 +283,13 @@ struct PlanImpl {
     uint32_t n_pad = 0, k_pad = 0, n_chunks = 0;
     __half *d_A = nullptr, *d_Bh = nullptr, *d_Bl = nullptr, *d_lhi = nullptr, *d_llo = nullptr;
     double *d_r = nullptr, *d_lsorted = nullptr, *d_chunk_scale = nullptr, *d_G = nullptr;
-    int32_t *d_parent_col = nullptr, *d_start_col = nullptr;
-    uint32_t *d_sample_ptr = nullptr;
-    uint2 *d_gemm_tiles = nullptr;
-    uint32_t n_gemm_tiles = 0;
+    int32_t *d_parent_col = nullptr;
+    std::vector<tc::GemmTable> gtables;
+    tc::GemmTable *d_gtables = nullptr;
     int *d_error = nullptr;
     CUtensorMap map_A{}, map_Bh{}, map_Bl{};
-    int setup_gemm(const Table &table, const FlatTree &tree);
-    int execute_gemm(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t ntiles);
+    int setup_gemm(const TableSet &set, const FlatTree &tree);
+    int execute_gemm(cudaStream_t s, const dev::OutSpec &out);
 
     // CUDA graph of execute()
     bool graph_on = false, capturing = false;
@@ -417,8 +419,14 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
         n_parts = std::max<uint32_t>(1, (E + part_chunk - 1) / part_chunk);
     }
     const bool counts = spec.vaw && !faith;
-    const size_t per_col = el * std::max<uint32_t>(K, 1) * (counts ? 2 : 1) + sizeof(double) + (counts ? el : 0) +
-                           sizeof(unsigned long long) * n_words + (n_parts ? el * (n_parts + 1) : 0);
+    size_t per_col = el * std::max<uint32_t>(K, 1) * (counts ? 2 : 1) + sizeof(double) + (counts ? el : 0) +
+                     sizeof(unsigned long long) * n_words + (n_parts ? el * (n_parts + 1) : 0);
+    if (gemm) {
+        // fp16 operand rows A, B_hi, B_lo over the padded nodes, r, and a row
+        // of the table's fp64 G block
+        const uint64_t kp = (static_cast<uint64_t>(E) + 255) / 256 * 256;
+        per_col = 3 * sizeof(uint16_t) * kp + sizeof(double) + sizeof(double) * ((max_table_n + 127) / 128 * 128);
+    }
     size_t budget = opts.group_bytes;
     if (!budget) {
         if (const char *b = std::getenv("UNIFRAC_B200_GROUP_BYTES")) budget = std::strtoull(b, nullptr, 10);
@@ -833,7 +841,7 @@ int PlanImpl::execute_T(cudaStream_t s, const dev::OutSpec &out) {
 
 int PlanImpl::execute_all(cudaStream_t s) {
     dev::OutSpec o{0, d_full, 0, 0};
-    if (gemm) return execute_gemm(s, o, d_gemm_tiles, n_gemm_tiles);
+    if (gemm) return execute_gemm(s, o);
     return spec.fp64 ? execute_T<double>(s, o) : execute_T<float>(s, o);
 }
 
@@ -841,7 +849,7 @@ int PlanImpl::execute_all(cudaStream_t s) {
 int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop) {
     if (gemm) {
         dev::OutSpec o{mode, d_out, start, stop};
-        return execute_gemm(stream, o, d_gemm_tiles, n_gemm_tiles);
+        return execute_gemm(stream, o);
     }
     const Group &g = groups[0];
     const int BM = spec.fp64 ? kd.BM : kf.BM, BN = spec.fp64 ? kd.BN : kf.BN;
@@ -876,9 +884,8 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
 
 // --------------------------------------------------- tensor-core unweighted
 
-int PlanImpl::setup_gemm(const Table &table, const FlatTree &tree) {
+int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     const uint32_t chunk_nodes = tc::CHUNK_KB * tc::BLOCK_K;
-    n_pad = ((n + tc::BLOCK_M - 1) / tc::BLOCK_M) * tc::BLOCK_M;
     k_pad = std::max<uint32_t>(chunk_nodes, ((E + chunk_nodes - 1) / chunk_nodes) * chunk_nodes);
     n_chunks = k_pad / chunk_nodes;
     // embedded nodes sorted by decreasing length
@@ -912,8 +919,11 @@ int PlanImpl::setup_gemm(const Table &table, const FlatTree &tree) {
         const int32_t p = parent_row[order[c]];
         parent_col[c] = (p >= 0 && static_cast<uint32_t>(p) < E) ? col_of_row[p] : -1;
     }
-    // sample-major list of starting columns (tip, or its parent when tips are bypassed)
-    std::vector<int32_t> start_of_obs(table.n_obs, -1);
+    // starting column of each tree observation: its tip, or the tip's parent
+    // when tips are bypassed
+    uint32_t n_obs_tree = 0;
+    for (uint32_t r : tree.leaf_rows) n_obs_tree = std::max<uint32_t>(n_obs_tree, tree.leaf_obs[r] + 1);
+    std::vector<int32_t> start_of_obs(n_obs_tree, -1);
     for (uint32_t r : tree.leaf_rows) {
         const int32_t obs = tree.leaf_obs[r];
         if (obs < 0) continue;
@@ -921,30 +931,73 @@ int PlanImpl::setup_gemm(const Table &table, const FlatTree &tree) {
         if (r >= E) node = parent_row[r];
         start_of_obs[obs] = (node >= 0 && static_cast<uint32_t>(node) < E) ? col_of_row[node] : -1;
     }
-    std::vector<uint32_t> sample_ptr(n + 1, 0);
-    for (uint32_t i = 0; i < table.n_obs; i++)
-        for (uint32_t q = table.indptr[i]; q < table.indptr[i + 1]; q++)
-            if (table.data[q] > 0.0 && start_of_obs[i] >= 0) sample_ptr[table.indices[q] + 1]++;
-    for (uint32_t j = 0; j < n; j++) sample_ptr[j + 1] += sample_ptr[j];
-    std::vector<int32_t> start_col(std::max<uint32_t>(sample_ptr[n], 1));
-    std::vector<uint32_t> fill(sample_ptr.begin(), sample_ptr.end() - 1);
-    for (uint32_t i = 0; i < table.n_obs; i++)
-        for (uint32_t q = table.indptr[i]; q < table.indptr[i + 1]; q++)
-            if (table.data[q] > 0.0 && start_of_obs[i] >= 0) start_col[fill[table.indices[q]]++] = start_of_obs[i];
+    // per group: operand rows = the group's columns; each row's list of
+    // starting columns (table rows of an observation with a positive count)
+    for (Group &g : groups) {
+        std::vector<uint32_t> sample_ptr(g.ld + 1, 0);
+        std::vector<std::pair<uint32_t, int32_t>> entries;  // (operand row, start column)
+        for (uint32_t t = g.t0; t < g.t1; t++) {
+            const Table &tb = *set.tables[t];
+            const uint32_t base = tdesc[t].base;
+            auto add_row = [&](uint32_t i, int32_t start) {
+                if (start < 0) return;
+                for (uint32_t q = tb.indptr[i]; q < tb.indptr[i + 1]; q++)
+                    if (tb.data[q] > 0.0) entries.emplace_back(base + tb.indices[q], start);
+            };
+            if (set.obs_row.empty()) {
+                for (uint32_t o = 0; o < n_obs_tree; o++)
+                    if (o < tb.n_obs) add_row(o, start_of_obs[o]);
+            } else {
+                const std::vector<int32_t> &m = set.obs_row[t];
+                for (uint32_t o = 0; o < n_obs_tree && o < m.size(); o++)
+                    if (m[o] >= 0) add_row(static_cast<uint32_t>(m[o]), start_of_obs[o]);
+            }
+        }
+        for (const auto &e : entries) sample_ptr[e.first + 1]++;
+        for (uint64_t j = 0; j < g.ld; j++) sample_ptr[j + 1] += sample_ptr[j];
+        std::vector<int32_t> start_col(std::max<size_t>(entries.size(), 1));
+        std::vector<uint32_t> fill(sample_ptr.begin(), sample_ptr.end() - 1);
+        for (const auto &e : entries) start_col[fill[e.first]++] = e.second;
+        SSU_CK(upload(&g.d_sample_ptr, sample_ptr.data(), sizeof(uint32_t) * sample_ptr.size()));
+        SSU_CK(upload(&g.d_start_col, start_col.data(), sizeof(int32_t) * start_col.size()));
+    }
+    // G blocks per table, relative to the group's G buffer; every ordered
+    // tile of each table, grouped 12 x 12 so concurrent CTAs share row
+    // blocks in L2
+    gtables.assign(tdesc.size(), tc::GemmTable{});
+    uint64_t g_max = 0;
+    for (Group &g : groups) {
+        uint64_t off = 0;
+        std::vector<uint4> tiles;
+        for (uint32_t t = g.t0; t < g.t1; t++) {
+            const uint32_t np = (tdesc[t].n + tc::BLOCK_M - 1) / tc::BLOCK_M * tc::BLOCK_M;
+            gtables[t] = tc::GemmTable{off, np, tdesc[t].base};
+            off += static_cast<uint64_t>(np) * np;
+            const uint32_t nb = np / tc::BLOCK_M, b0 = tdesc[t].base / tc::BLOCK_M;
+            for (uint32_t gk = 0; gk < nb; gk += 12)
+                for (uint32_t gl = 0; gl < nb; gl += 12)
+                    for (uint32_t kb = gk; kb < std::min(nb, gk + 12); kb++)
+                        for (uint32_t lb = gl; lb < std::min(nb, gl + 12); lb++)
+                            tiles.push_back(make_uint4(b0 + kb, b0 + lb, t, 0));
+        }
+        g_max = std::max(g_max, off);
+        g.n_tiles = static_cast<uint32_t>(tiles.size());
+        SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * tiles.size()));
+    }
+    SSU_CK(upload(&d_gtables, gtables.data(), sizeof(tc::GemmTable) * std::max<size_t>(gtables.size(), 1)));
 
+    n_pad = static_cast<uint32_t>(ld);
     const size_t op_bytes = sizeof(__half) * static_cast<size_t>(n_pad) * k_pad;
     SSU_CK(alloc(&d_A, op_bytes));
     SSU_CK(alloc(&d_Bh, op_bytes));
     SSU_CK(alloc(&d_Bl, op_bytes));
     SSU_CK(alloc(&d_r, sizeof(double) * n_pad));
-    SSU_CK(alloc(&d_G, sizeof(double) * static_cast<size_t>(n_pad) * n_pad));
+    SSU_CK(alloc(&d_G, sizeof(double) * std::max<uint64_t>(g_max, 1)));
     SSU_CK(upload(&d_lhi, lhi.data(), sizeof(__half) * k_pad));
     SSU_CK(upload(&d_llo, llo.data(), sizeof(__half) * k_pad));
     SSU_CK(upload(&d_lsorted, lsorted.data(), sizeof(double) * k_pad));
     SSU_CK(upload(&d_chunk_scale, scale.data(), sizeof(double) * n_chunks));
     SSU_CK(upload(&d_parent_col, parent_col.data(), sizeof(int32_t) * k_pad));
-    SSU_CK(upload(&d_sample_ptr, sample_ptr.data(), sizeof(uint32_t) * (n + 1)));
-    SSU_CK(upload(&d_start_col, start_col.data(), sizeof(int32_t) * start_col.size()));
     SSU_CK(alloc(&d_error, sizeof(int)));
     SSU_CK(cudaMemsetAsync(d_error, 0, sizeof(int), stream));
     if (!make_fp16_map(&map_A, d_A, n_pad, k_pad) || !make_fp16_map(&map_Bh, d_Bh, n_pad, k_pad) ||
@@ -961,49 +1014,44 @@ int PlanImpl::setup_gemm(const Table &table, const FlatTree &tree) {
     }
     SSU_CK(cudaFuncSetAttribute(tc::presence_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(bits_smem)));
-    // every ordered tile of G, grouped 12 x 12 so concurrent CTAs share row
-    // blocks in L2
-    std::vector<uint2> tiles;
-    const uint32_t nb = n_pad / tc::BLOCK_M;
-    for (uint32_t gk = 0; gk < nb; gk += 12)
-        for (uint32_t gl = 0; gl < nb; gl += 12)
-            for (uint32_t kb = gk; kb < std::min(nb, gk + 12); kb++)
-                for (uint32_t lb = gl; lb < std::min(nb, gl + 12); lb++) tiles.push_back(make_uint2(kb, lb));
-    n_gemm_tiles = static_cast<uint32_t>(tiles.size());
-    SSU_CK(upload(&d_gemm_tiles, tiles.data(), sizeof(uint2) * tiles.size()));
-    gemm = true;
+    SSU_CK(alloc(&d_full, (spec.fp64 ? sizeof(double) : sizeof(float)) * std::max<uint64_t>(full_elems, 1)));
+    tuning = "fixed";
     return 0;
 }
 
-int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out, const uint2 *tiles, uint32_t ntiles) {
+int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
     launches = 0;
     if (timed()) SSU_CK(cudaEventRecord(ev[0], s));
     const size_t bits_smem = sizeof(uint32_t) * (k_pad / 32);
-    tc::presence_rows_kernel<<<n_pad, 256, bits_smem, s>>>(d_sample_ptr, d_start_col, d_parent_col, d_lhi, d_llo,
-                                                           d_lsorted, n, k_pad, d_A, d_Bh, d_Bl, d_r);
-    launches++;
-    if (timed()) SSU_CK(cudaEventRecord(ev[1], s));
-    if (ntiles) {
-        tc::GemmArgs g{};
-        g.tiles = tiles;
-        g.n_tiles = ntiles;
-        g.n = n;
-        g.n_kblocks = k_pad / tc::BLOCK_K;
-        g.chunk_scale = d_chunk_scale;
-        g.G = d_G;
-        g.ldg = n_pad;
-        g.error = d_error;
-        g.wait_cycles = 2000000000LL;  // about one second per wait at B200 clocks
-        tc::unweighted_tc_kernel<<<ntiles, tc::THREADS, tc::SMEM_BYTES, s>>>(map_A, map_Bh, map_Bl, g);
+    for (size_t gi = 0; gi < groups.size(); gi++) {
+        const Group &g = groups[gi];
+        tc::presence_rows_kernel<<<static_cast<uint32_t>(g.ld), 256, bits_smem, s>>>(
+            g.d_sample_ptr, g.d_start_col, d_parent_col, d_lhi, d_llo, d_lsorted, static_cast<uint32_t>(g.ld),
+            k_pad, d_A, d_Bh, d_Bl, d_r);
         launches++;
-    }
-    if (timed()) SSU_CK(cudaEventRecord(ev[2], s));
-    if (n) {
-        const dim3 grid((n + 31) / 32, (n + 31) / 32);
-        tc::finish_unweighted_kernel<<<grid, dim3(32, 8), 0, s>>>(d_G, n_pad, d_r, n,
-                                                                  spec.method == Method::unweighted ? 1 : 0,
-                                                                  spec.fp64 ? 1 : 0, out);
-        launches++;
+        if (gi == 0 && timed()) SSU_CK(cudaEventRecord(ev[1], s));
+        if (g.n_tiles) {
+            tc::GemmArgs a{};
+            a.tiles = g.d_tiles;
+            a.n_tiles = g.n_tiles;
+            a.tables = d_gtables;
+            a.n_kblocks = k_pad / tc::BLOCK_K;
+            a.chunk_scale = d_chunk_scale;
+            a.G = d_G;
+            a.error = d_error;
+            a.wait_cycles = 2000000000LL;  // about one second per wait at B200 clocks
+            tc::unweighted_tc_kernel<<<g.n_tiles, tc::THREADS, tc::SMEM_BYTES, s>>>(map_A, map_Bh, map_Bl, a);
+            launches++;
+        }
+        if (gi + 1 == groups.size() && timed()) SSU_CK(cudaEventRecord(ev[2], s));
+        const uint32_t nb = (max_table_n + 31) / 32;
+        if (nb) {
+            const dim3 grid(nb, nb, g.t1 - g.t0);
+            tc::finish_unweighted_kernel<<<grid, dim3(32, 8), 0, s>>>(
+                d_G, d_gtables + g.t0, d_tdesc + g.t0, d_r, spec.method == Method::unweighted ? 1 : 0,
+                spec.fp64 ? 1 : 0, out);
+            launches++;
+        }
     }
     if (out.mode == 0) zero_diagonal(s, out.ptr);
     if (timed()) SSU_CK(cudaEventRecord(ev[3], s));
@@ -1022,6 +1070,27 @@ int resolve_autotune(int requested, bool batch) {
 
 }  // namespace
 
+namespace {
+
+// Unweighted methods (not variance adjusted) on the tensor-core contraction:
+// by default for fp32 results (its ~2.5e-7 relative error is inside the
+// fp32 stripe form's own), on request for fp64.  Presence is "proportion >
+// 0", the OR of the tips below a node, so it needs counts that are not
+// negative.  A batch with bypassed tips keeps the stripe form (its tables'
+// trees differ in which rows carry length).
+bool use_tensor_cores(const MethodSpec &spec, const TableSet &set, bool batch) {
+    if (spec.vaw || !(spec.method == Method::unweighted || spec.method == Method::unweighted_unnormalized))
+        return false;
+    bool want = spec.unweighted_gemm || (!spec.fp64 && !spec.unweighted_stripe);
+    if (batch && spec.bypass_tips) want = false;
+    for (const Table *t : set.tables)
+        for (uint64_t q = 0; want && q < t->nnz(); q++)
+            if (!(t->data[q] >= 0.0)) want = false;
+    return want;
+}
+
+}  // namespace
+
 int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spec, void *stream, Plan **out,
                  std::string &err) {
     Plan *p = new Plan();
@@ -1033,23 +1102,9 @@ int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spe
     TableSet set;
     set.tables.push_back(&table);
     set.embedded.push_back(tree.n_embedded);
+    m.gemm = use_tensor_cores(spec, set, false);
     int rc = m.setup(set, tree, BatchOptions{});
-    bool want_gemm = spec.unweighted_gemm && !spec.vaw &&
-                     (spec.method == Method::unweighted || spec.method == Method::unweighted_unnormalized);
-    // presence is "proportion > 0": with no negative count it is the OR of
-    // the tips below a node; other inputs keep the stripe kernel
-    for (uint64_t q = 0; want_gemm && q < table.nnz(); q++)
-        if (!(table.data[q] >= 0.0)) want_gemm = false;
-    if (!rc && want_gemm) {
-        rc = m.setup_gemm(table, tree);
-        if (!rc && m.alloc(&m.d_full, (spec.fp64 ? sizeof(double) : sizeof(float)) * std::max<uint64_t>(m.full_elems, 1)) !=
-                       cudaSuccess) {
-            m.last_error = "device allocation failed";
-            rc = kOutputError;
-        }
-    } else if (!rc) {
-        rc = spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
-    }
+    if (!rc) rc = m.gemm ? m.setup_gemm(set, tree) : spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
     if (rc) {
         err = m.last_error;
         delete p;
@@ -1071,12 +1126,12 @@ int Plan::create_batch(const TableSet &set, const FlatTree &tree, const MethodSp
     p->impl_ = new PlanImpl();
     PlanImpl &m = *p->impl_;
     m.spec = spec;
-    m.spec.unweighted_gemm = false;
     m.batch = true;
     m.stream = static_cast<cudaStream_t>(stream);
     m.autotune = resolve_autotune(opts.autotune, true);
+    m.gemm = use_tensor_cores(spec, set, true);
     int rc = m.setup(set, tree, opts);
-    if (!rc) rc = spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
+    if (!rc) rc = m.gemm ? m.setup_gemm(set, tree) : spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
     if (rc) {
         err = m.last_error;
         delete p;

@@ -27,9 +27,11 @@ struct MethodSpec {
     double alpha = 1.0;
     bool bypass_tips = false;
     bool normalize = true;
-    // unweighted (non variance-adjusted) only: run the tcgen05 contraction
-    // instead of the presence-word stripe kernel
+    // unweighted (non variance-adjusted) only: the tcgen05 contraction is
+    // the default for fp32 results; unweighted_gemm asks for it with fp64
+    // results too, unweighted_stripe keeps the presence-word stripe kernel
     bool unweighted_gemm = false;
+    bool unweighted_stripe = false;
 };
 
 // Method-name table of the reference (src/api.cpp:55-88): bare names are fp32.

@@ -56,14 +56,21 @@ constexpr size_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 enum : int { ERR_NONE = 0, ERR_FULL_WAIT = 1, ERR_EMPTY_WAIT = 2, ERR_ACC_FULL_WAIT = 3, ERR_ACC_EMPTY_WAIT = 4,
              ERR_DONE_WAIT = 5, ERR_DRAIN_WAIT = 6 };
 
+// G block of one table: table t's rows are operand rows [base, base + ldg)
+// and its G is ldg x ldg (row major) at G + g_off.
+struct GemmTable {
+    uint64_t g_off;
+    uint32_t ldg;   // the table's samples rounded up to BLOCK_M
+    uint32_t base;  // first operand row of the table
+};
+
 struct GemmArgs {
-    const uint2 *tiles;
+    const uint4 *tiles;   // x = row block of k, y = row block of l, z = table
     uint32_t n_tiles;
-    uint32_t n;           // samples
+    const GemmTable *tables;
     uint32_t n_kblocks;   // padded nodes / BLOCK_K, a multiple of CHUNK_KB
     const double *chunk_scale;  // 2^-s_c per chunk
-    double *G;            // n_pad x n_pad, row major
-    uint32_t ldg;         // n_pad
+    double *G;
     int *error;           // first error code of any CTA
     long long wait_cycles;  // budget of one mbarrier wait
 };
@@ -171,8 +178,9 @@ __global__ void __launch_bounds__(THREADS, 1)
     int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const uint2 tile = args.tiles[blockIdx.x];
+    const uint4 tile = args.tiles[blockIdx.x];
     const int m0 = static_cast<int>(tile.x) * BLOCK_M, n0 = static_cast<int>(tile.y) * BLOCK_N;
+    const GemmTable gt = args.tables[tile.z];
     const uint32_t nkb = args.n_kblocks;
     const uint32_t nchunks = nkb / CHUNK_KB;
     const long long budget = args.wait_cycles;
@@ -298,7 +306,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             if (lane == 0) mbar_arrive(acce + buf);
         }
         if (ok && !*vabort) {
-            double *g = args.G + static_cast<uint64_t>(m0 + row) * args.ldg + n0 + half * (BLOCK_N / 2);
+            double *g = args.G + gt.g_off + static_cast<uint64_t>(m0 - gt.base + row) * gt.ldg + (n0 - gt.base) +
+                        half * (BLOCK_N / 2);
 #pragma unroll
             for (int i = 0; i < BLOCK_N / 2; i += 2)
                 *reinterpret_cast<double2 *>(g + i) = make_double2(acc[i], acc[i + 1]);
@@ -369,26 +378,34 @@ __global__ void presence_rows_kernel(const uint32_t *__restrict__ sample_ptr, co
 }
 
 // num = G[k][l] + G[l][k], den = r[k] + G[l][k] for k < l, then the output
-// layout of the other pair kernels.
-__global__ void finish_unweighted_kernel(const double *__restrict__ G, uint32_t ldg, const double *__restrict__ r,
-                                         uint32_t n, int normalized, int out_fp64, dev::OutSpec out) {
+// layout of the other pair kernels; grid.z = table of the group.
+__global__ void finish_unweighted_kernel(const double *__restrict__ G, const GemmTable *__restrict__ gtables,
+                                         const dev::TableDesc *__restrict__ tables, const double *__restrict__ r,
+                                         int normalized, int out_fp64, dev::OutSpec out) {
     // 32 x 32 block of pairs per CTA; both G tiles through shared memory
     __shared__ double gt[32][33];
+    const GemmTable g = gtables[blockIdx.z];
+    const dev::TableDesc td = tables[blockIdx.z];
+    const uint32_t n = td.n;
     const uint32_t k0 = blockIdx.y * 32, l0 = blockIdx.x * 32;
-    if (k0 > l0 + 31) return;
+    if (k0 > l0 + 31 || k0 >= n || l0 >= n) return;
+    const double *Gt = G + g.g_off;
+    const uint32_t ldg = g.ldg;
+    const double *rt = r + g.base;
+    if (out.mode == 0) out.ptr = static_cast<char *>(out.ptr) + td.out_off * (out_fp64 ? sizeof(double) : sizeof(float));
     const uint32_t tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
     for (uint32_t i = ty; i < 32; i += 8) {
         const uint32_t l = l0 + i, k = k0 + tx;
-        gt[i][tx] = (l < n && k < n) ? G[static_cast<uint64_t>(l) * ldg + k] : 0.0;  // G[l][k]
+        gt[i][tx] = (l < n && k < n) ? Gt[static_cast<uint64_t>(l) * ldg + k] : 0.0;  // G[l][k]
     }
     __syncthreads();
     for (uint32_t i = ty; i < 32; i += 8) {
         const uint32_t k = k0 + i, l = l0 + tx;
         if (k < l && l < n) {
-            const double gkl = G[static_cast<uint64_t>(k) * ldg + l];
+            const double gkl = Gt[static_cast<uint64_t>(k) * ldg + l];
             const double glk = gt[tx][i];
             const double num = gkl + glk;
-            const double v = normalized ? num / (r[k] + glk) : num;
+            const double v = normalized ? num / (rt[k] + glk) : num;
             if (out.mode == 0 && !out_fp64)
                 dev::emit_pair<float>(out, n, k, l, static_cast<float>(v));
             else
