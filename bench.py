@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--replicates", type=int, default=100)
     p.add_argument("--tables5", type=int, default=64)
+    p.add_argument("--tips5", type=int, default=50000)
     p.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
                    help="config3: unweighted fp64, tensor-core contraction vs the plain stripe form")
     p.add_argument("--samples3", type=int, default=25000)
@@ -385,7 +386,7 @@ def run_config4(args):
     tree, base, reps = ssu_synth.config4(n_replicates=args.replicates)
     gen_s = time.perf_counter() - t0
     methods = ["unweighted_fp32", "weighted_normalized_fp32"]
-    per, total_units, total_ms, launches = {}, 0, 0.0, 0
+    per, total_units, total_ms, launches, e2e = {}, 0, 0.0, 0, {}
     clocks = ClockSampler(0)
     for m in methods:
         t0 = time.perf_counter()
@@ -399,17 +400,26 @@ def run_config4(args):
         total_units += units
         total_ms += ms
         r0 = plan.results()[0]
+        info = {"groups": plan.n_groups(), "tuning": plan.tuning(), "kernel": plan.pair_kernel(),
+                "launches_per_step": plan.launches()}
+        plan.close()
+        # end to end through the batch C API: host tables in, host matrices out
+        if args.e2e_steps > 0:
+            t0 = time.perf_counter()
+            out = ssu_b200.one_off_batch(tree, reps, m, copy=False)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            e2e[m] = {"seconds": dt, "value": units / dt}
+            del out
         per_table_ms = _unbatched_ms(torch, ssu_b200, tree, reps, m, stream)
         single = ssu_b200.Plan(tree, reps[0], m)
         single.execute()
         s0 = single.result()
         single.close()
-        per[m] = {"ms_per_step": ms, "value": units / (ms / 1e3), "units": units, "groups": plan.n_groups(),
-                  "tuning": plan.tuning(), "kernel": plan.pair_kernel(), "launches_per_step": plan.launches(),
+        per[m] = {"ms_per_step": ms, "value": units / (ms / 1e3), "units": units, **info,
                   "plan_create_s": create_s, "clocks": clk, "one_plan_per_replicate_ms": per_table_ms,
                   "batched_speedup": per_table_ms / ms,
                   "replicate0_vs_one_table_plan_max_rel": _rel_err(r0, s0)[0]}
-        plan.close()
         # parity of replicate 0 with the reference's own CPU build (fp32 and fp64)
         if oracle_py.ref_available():
             ref64 = oracle_py.ref_one_off(tree, reps[0], m.replace("_fp32", "_fp64"), with_timing=True)
@@ -422,16 +432,6 @@ def run_config4(args):
             per[m]["cpu_reference_replicate0"] = {"seconds": ref32["seconds"][0],
                                                   "value": n0 * (n0 - 1) / 2 * e / ref32["seconds"][0],
                                                   "cores": os.cpu_count()}
-    # end to end through the batch C API: host tables in, host matrices out
-    e2e = {}
-    if args.e2e_steps > 0:
-        for m in methods:
-            t0 = time.perf_counter()
-            out = ssu_b200.one_off_batch(tree, reps, m, copy=False)
-            torch.cuda.synchronize()
-            dt = time.perf_counter() - t0
-            e2e[m] = {"seconds": dt, "value": per[m]["units"] / dt}
-            del out
     h2d = sum(int(t.indptr.nbytes + t.indices.nbytes + t.data.nbytes) for t in reps)
     d2h = sum(4 * t.n_samples ** 2 for t in reps)
     line = {
@@ -462,7 +462,7 @@ def run_config5(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
     t0 = time.perf_counter()
-    tree, tables = ssu_synth.config5(n_tables=args.tables5)
+    tree, tables = ssu_synth.config5(n_tables=args.tables5, n_tips=args.tips5)
     gen_s = time.perf_counter() - t0
     runs = [("generalized_fp64", False), ("unweighted_fp64", True), ("weighted_normalized_fp64", True),
             ("weighted_unnormalized_fp64", True), ("generalized_fp64", True)]
@@ -501,7 +501,7 @@ def run_config5(args):
         "warmup": args.warmup, "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-5 generator)",
         "config": {"workload": f"{len(tables)} tables, sample counts log-uniform in [64, 4096] "
-                               f"(total {sum(t.n_samples for t in tables)}), 50k-tip tree, 1% non-zero; "
+                               f"(total {sum(t.n_samples for t in tables)}), {args.tips5}-tip tree, 1% non-zero; "
                                "generalized a=0.5 and VAW unweighted / weighted_normalized / "
                                "weighted_unnormalized / generalized a=0.5, fp64, full matrices",
                    "l2": "flushed between steps; embedding > L2", "generation_s": gen_s},
@@ -582,6 +582,7 @@ def main():
         m, _ = ssu_b200.one_off_matrix(tree, table, args.method, copy=False)
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) * 1e3
+        del m  # the caller is done with the result: destroy_mat_full_fp64
         if i > 0:
             e2e_ms.append(dt)
     h2d = int(table.indptr.nbytes + table.indices.nbytes + table.data.nbytes + tree.structure.nbytes +

@@ -251,3 +251,67 @@ def test_zero_copy_result_view_outlives_its_parent(ssu):
     np.testing.assert_array_equal(row, ref[3])
     v32, _ = ssu.one_off_matrix(tree, table, "weighted_normalized_fp32", copy=False)
     assert v32.dtype == np.float32 and v32.shape == (64, 64)
+
+
+def test_marshalled_inputs_follow_replaced_arrays(ssu):
+    tree, table = _case(58, n_samples=40)
+    other = ssu_synth.geometric_table(table.obs_ids, 40, 0.12, 10.0, 991)
+    first, _ = ssu.one_off_matrix(tree, table, "weighted_unnormalized_fp64")
+    again, _ = ssu.one_off_matrix(tree, table, "weighted_unnormalized_fp64")
+    np.testing.assert_array_equal(first, again)
+    table.indptr, table.indices, table.data = other.indptr, other.indices, other.data
+    swapped, _ = ssu.one_off_matrix(tree, table, "weighted_unnormalized_fp64")
+    ref, _ = ssu.one_off_matrix(tree, other, "weighted_unnormalized_fp64")
+    np.testing.assert_array_equal(swapped, ref)
+    table.data = other.data.copy()
+    plain, _ = ssu.one_off_matrix(tree, table, "weighted_unnormalized_fp64", normalize=False)
+    table.data *= 3.0  # in place: the marshalled view shares the array
+    tripled, _ = ssu.one_off_matrix(tree, table, "weighted_unnormalized_fp64", normalize=False)
+    np.testing.assert_allclose(tripled, 3.0 * plain, rtol=1e-12)
+
+
+def _near_duplicates(seed, n_tips=150, n_base=12, copies=4):
+    """Samples in clusters of near-duplicates: copies of a base sample with
+    one count nudged by a relative 1e-7 (or not at all), so the weighted
+    distances inside a cluster are tiny or exactly zero."""
+    tree = ssu_synth.random_binary_tree(n_tips, 0.1, seed)
+    base = ssu_synth.geometric_table(tree.tip_names(), n_base, 0.1, 10.0, seed + 1).dense()
+    base[0, :] += 1.0  # no empty sample
+    rng = np.random.default_rng(seed + 2)
+    cols = []
+    for j in range(n_base):
+        for c in range(copies):
+            col = base[:, j].copy()
+            if c:
+                nz = np.flatnonzero(col)
+                col[nz[rng.integers(0, nz.size)]] *= 1.0 + 1e-7 * c
+            cols.append(col)
+    dense = np.stack(cols, axis=1)
+    flat = np.flatnonzero(dense.ravel() > 0)
+    table = ssu_synth.make_table(tree.tip_names(), dense.shape[1], flat, dense.ravel()[flat])
+    return tree, table
+
+
+@pytest.mark.parametrize("method", ["weighted_normalized_fp64", "weighted_unnormalized_fp64"])
+def test_weighted_close_pairs_are_exact(ssu, oracle_mod, method):
+    """Pairs whose sparse-form subtraction could lose digits are recomputed
+    in the exact |u - v| form: near-duplicate samples still meet 1e-12."""
+    tree, table = _near_duplicates(61)
+    gpu, _ = ssu.one_off_matrix(tree, table, method)
+    ref = oracle_mod.oracle_one_off(tree, table, method)["matrix"]
+    check_fp64(gpu, ref)
+    small = (ref > 0) & (ref < 1e-5)
+    assert small.any()
+
+
+@pytest.mark.parametrize("method", ["weighted_normalized", "weighted_unnormalized"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_weighted_sparse_and_dense_forms_agree(ssu, monkeypatch, method, prec):
+    tree, table = _case(62, n_tips=300, n_samples=300, density=0.03)
+    hybrid, _ = ssu.one_off_matrix(tree, table, f"{method}_{prec}")
+    monkeypatch.setenv("UNIFRAC_B200_WEIGHTED_MODE", "dense")
+    dense, _ = ssu.one_off_matrix(tree, table, f"{method}_{prec}")
+    if prec == "fp64":
+        check_fp64(hybrid, dense)
+    else:
+        np.testing.assert_allclose(hybrid, dense, rtol=5e-6, atol=1e-7)

@@ -17,8 +17,11 @@
 #include <sstream>
 #include <string>
 #include <sys/mman.h>
+#include <map>
+#include <mutex>
 #include <thread>
 #include <unistd.h>
+#include <unordered_map>
 #include <unordered_set>
 #include <vector>
 
@@ -32,6 +35,7 @@ namespace {
 
 constexpr uint32_t kMmapFdMask = 0x0fff;  // src/api.cpp:27-28
 constexpr uint32_t kMmapFlag = 0x1000;
+constexpr uint32_t kPinnedFlag = 0x2000;  // matrix from the page-locked result pool
 constexpr size_t kHugeAlign = size_t(2) << 20;
 
 std::atomic<uint64_t> g_seed{5489u};
@@ -190,6 +194,66 @@ ComputeStatus make_plan(const ssu::Table &table, const ssu::BPTree &tree, const 
     return okay;
 }
 
+// Page-locked host memory for full results: the copy-out then runs at the
+// link's rate with no per-call page registration.  Blocks released through
+// destroy_mat_full_* are kept for later results (best fit, up to twice the
+// request) while the pool holds at most UNIFRAC_B200_PINNED_BYTES (default
+// 4 GiB) live and cached together; beyond that results use pageable memory.
+class PinnedPool {
+  public:
+    static PinnedPool &get() {
+        static PinnedPool p;
+        return p;
+    }
+    void *take(size_t bytes) {
+        std::lock_guard<std::mutex> lock(mu_);
+        auto it = free_.lower_bound(bytes);
+        if (it != free_.end() && it->first <= 2 * bytes) {
+            void *p = it->second;
+            cached_ -= it->first;
+            live_[p] = it->first;
+            free_.erase(it);
+            return p;
+        }
+        while (held() + bytes > limit_ && !free_.empty()) {  // make room from the cache
+            auto big = std::prev(free_.end());
+            cudaFreeHost(big->second);
+            cached_ -= big->first;
+            free_.erase(big);
+        }
+        if (held() + bytes > limit_) return nullptr;
+        void *p = nullptr;
+        if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        live_[p] = bytes;
+        live_bytes_ += bytes;
+        return p;
+    }
+    void give(void *p) {
+        std::lock_guard<std::mutex> lock(mu_);
+        auto it = live_.find(p);
+        if (it == live_.end()) return;
+        const size_t cap = it->second;
+        live_.erase(it);
+        live_bytes_ -= cap;
+        free_.emplace(cap, p);
+        cached_ += cap;
+    }
+
+  private:
+    PinnedPool() {
+        if (const char *v = std::getenv("UNIFRAC_B200_PINNED_BYTES")) limit_ = std::strtoull(v, nullptr, 10);
+    }
+    size_t held() const { return live_bytes_ + cached_; }
+    std::mutex mu_;
+    std::multimap<size_t, void *> free_;
+    std::unordered_map<void *, size_t> live_;
+    size_t live_bytes_ = 0, cached_ = 0;
+    size_t limit_ = size_t(4) << 30;
+};
+
 template <class TReal, class TMat>
 bool alloc_full(TMat *&result, const std::vector<std::string_view> &ids, const char *mmap_dir) {
     result = static_cast<TMat *>(std::malloc(sizeof(TMat)));
@@ -214,9 +278,14 @@ bool alloc_full(TMat *&result, const std::vector<std::string_view> &ids, const c
             if (!result->matrix) close(fd);
         }
     } else if (bytes >= kHugeAlign) {
+        void *p = PinnedPool::get().take(bytes);
+        if (p) {
+            result->matrix = static_cast<TReal *>(p);
+            result->flags = kPinnedFlag;
+            return true;
+        }
         // 2 MiB-aligned with transparent huge pages: ~500x fewer page faults
         // when the result is written; still released with free()
-        void *p = nullptr;
         if (posix_memalign(&p, kHugeAlign, bytes) == 0) {
             madvise(p, bytes, MADV_HUGEPAGE);
             result->matrix = static_cast<TReal *>(p);
@@ -251,7 +320,9 @@ void destroy_full(TMat **result) {
     for (uint32_t i = 0; i < r->n_samples; i++) std::free(r->sample_ids[i]);
     std::free(r->sample_ids);
     if (r->matrix) {
-        if ((r->flags & kMmapFlag) == 0) {
+        if (r->flags & kPinnedFlag) {
+            PinnedPool::get().give(r->matrix);
+        } else if ((r->flags & kMmapFlag) == 0) {
             std::free(r->matrix);
         } else {
             const uint64_t n = r->n_samples;
@@ -288,9 +359,11 @@ ComputeStatus full_matrix(const ssu::Table &table, const ssu::BPTree &tree, cons
     std::string err;
     int rc = plan->execute(nullptr);
     if (rc == 0) {
+        // a fresh pageable result is faulted in while the device computes and
+        // page-locked for the copy; a pooled one is page-locked already
         const bool fresh = allocated && (*result)->flags == 0;
         const size_t bytes = sizeof(TReal) * static_cast<size_t>(table.n_samples) * table.n_samples;
-        if (fresh && bytes >= kHugeAlign) prefault((*result)->matrix, bytes);  // overlaps the device work
+        if (fresh && bytes >= kHugeAlign) prefault((*result)->matrix, bytes);
         rc = plan->download_full((*result)->matrix, fresh, err);
     } else {
         err = "launch failed";
@@ -438,12 +511,12 @@ ComputeStatus batch_matrices(const std::vector<const ssu::Table *> &tables, cons
     if (rc == 0) {
         for (size_t t = 0; t < T; t++) {  // overlaps the device work
             const size_t bytes = sizeof(TReal) * static_cast<size_t>(tables[t]->n_samples) * tables[t]->n_samples;
-            if (bytes >= kHugeAlign) prefault(results[t]->matrix, bytes);
+            if (results[t]->flags == 0 && bytes >= kHugeAlign) prefault(results[t]->matrix, bytes);
         }
         for (size_t t = 0; t < T && rc == 0; t++) {
             const uint64_t n = tables[t]->n_samples;
-            rc = plan->download_range(plan->table_offset(static_cast<uint32_t>(t)), n * n, results[t]->matrix, true,
-                                      err);
+            rc = plan->download_range(plan->table_offset(static_cast<uint32_t>(t)), n * n, results[t]->matrix,
+                                      results[t]->flags == 0, err);
         }
     } else {
         err = "launch failed";

@@ -17,6 +17,7 @@
 #include "ssu_gemm.cuh"
 #include "ssu_kernels.cuh"
 #include "ssu_pairs.cuh"
+#include "ssu_sparse.cuh"
 
 namespace ssu {
 
@@ -270,6 +271,21 @@ struct PlanImpl {
     void *d_full = nullptr;
     uint64_t full_elems = 0;
 
+    // weighted methods over the sparse embedding (dense rows in registers,
+    // sparse rows on their intersections, flagged tiles recomputed exactly)
+    bool hybrid = false;
+    bool nonneg_data = true;  // no negative count in any table
+    unsigned long long *d_masks = nullptr;
+    uint32_t *d_counts = nullptr, *d_dense_rows = nullptr, *d_sparse_rows = nullptr, *d_nrows = nullptr;
+    double *d_Ws = nullptr, *d_ws_part = nullptr, *d_hpartial = nullptr;
+    int *d_flags = nullptr;
+    size_t hpartial_bytes = 0;
+    template <typename T>
+    int setup_hybrid();
+    template <typename T>
+    int hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &out, const uint4 *tiles, uint32_t ntiles,
+                     uint32_t splits, bool last);
+
     // pair stage
     PairKernel<double> kd;
     PairKernel<float> kf;
@@ -379,6 +395,8 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
     full_elems = 0;
     for (uint32_t t = 0; t < n_tables; t++) {
         const Table &tb = *set.tables[t];
+        for (uint64_t q = 0; q < tb.nnz() && nonneg_data; q++)
+            if (!(tb.data[q] >= 0.0)) nonneg_data = false;
         dev::TableDesc &d = tdesc[t];
         d.n = tb.n_samples;
         d.out_off = full_elems;
@@ -598,12 +616,22 @@ int PlanImpl::setup_method() {
     SSU_CK(alloc(&d_full, sizeof(T) * std::max<uint64_t>(full_elems, 1)));
 
     size_t chosen = 0;
-    if (cands.size() > 1 && autotune == 1) {
+    // min(a, b) = 0 off the intersection of the supports needs u >= 0
+    hybrid = !spec.vaw && len_stride == 0 && nonneg_data &&
+             (spec.method == Method::weighted_normalized || spec.method == Method::weighted_unnormalized);
+    if (const char *m = std::getenv("UNIFRAC_B200_WEIGHTED_MODE"))
+        if (std::string(m) == "dense") hybrid = false;
+    if (hybrid) {
+        // the exact recomputation of flagged tiles runs the 128 x 128 shape
+        chosen = 0;
+        tuning = "sparse hybrid";
+    } else if (cands.size() > 1 && autotune == 1) {
         const int rc = tune<T>(cands, chosen);
         if (rc) return rc;
     }
     kern<T>() = cands[chosen];
     const PairKernel<T> &k = kern<T>();
+    if (hybrid) return setup_hybrid<T>();
 
     partial_bytes = 0;
     for (Group &g : groups) {
@@ -616,6 +644,142 @@ int PlanImpl::setup_method() {
             partial_bytes = std::max(partial_bytes, sizeof(T) * k.partial_per_tile * g.n_tiles * g.splits);
     }
     if (partial_bytes) SSU_CK(alloc(&d_partial, partial_bytes));
+    return 0;
+}
+
+template <typename T>
+int PlanImpl::setup_hybrid() {
+    const uint64_t words = ld / 64;
+    SSU_CK(alloc(&d_masks, sizeof(unsigned long long) * std::max<uint64_t>(static_cast<uint64_t>(E) * words, 1)));
+    SSU_CK(alloc(&d_counts, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
+    SSU_CK(alloc(&d_dense_rows, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
+    SSU_CK(alloc(&d_sparse_rows, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
+    SSU_CK(alloc(&d_nrows, sizeof(uint32_t) * 2));
+    SSU_CK(alloc(&d_Ws, sizeof(double) * ld));
+    part_chunk = part_chunk ? part_chunk : 512;
+    n_parts = std::max<uint32_t>(1, (E + part_chunk - 1) / part_chunk);
+    SSU_CK(alloc(&d_ws_part, sizeof(double) * ld * n_parts));
+    auto kfn = dev::pair_hybrid_kernel<T, true>;
+    auto kfu = dev::pair_hybrid_kernel<T, false>;
+    const int smem = static_cast<int>(dev::hybrid_smem<T>());
+    SSU_CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SSU_CK(cudaFuncSetAttribute(kfu, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    uint32_t max_tiles = 0;
+    hpartial_bytes = 0;
+    for (Group &g : groups) {
+        std::vector<uint4> tiles;
+        for (uint32_t t = g.t0; t < g.t1; t++) append_tiles(tiles, t, tdesc[t].base, tdesc[t].n, dev::HB, dev::HB, false, 0, 0);
+        g.n_tiles = static_cast<uint32_t>(tiles.size());
+        SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * tiles.size()));
+        // node splits so the tiles fill the SMs (one CTA per SM)
+        uint32_t best_s = 1;
+        double best = 1e300;
+        const uint32_t max_s = std::max<uint32_t>(1, std::min<uint32_t>(16, E / 2048));
+        for (uint32_t sp = 1; sp <= max_s; sp++) {
+            const double cost = std::ceil(static_cast<double>(g.n_tiles) * sp / n_sms) / sp * (1.0 + 0.02 * (sp - 1));
+            if (cost < best - 1e-12) {
+                best = cost;
+                best_s = sp;
+            }
+        }
+        g.splits = best_s;
+        max_tiles = std::max(max_tiles, g.n_tiles);
+        if (g.splits > 1)
+            hpartial_bytes = std::max(hpartial_bytes, sizeof(double) * dev::HB * dev::HB * g.n_tiles * g.splits);
+    }
+    SSU_CK(alloc(&d_flags, sizeof(int) * std::max<uint32_t>(max_tiles, 1)));
+    if (hpartial_bytes) SSU_CK(alloc(&d_hpartial, hpartial_bytes));
+    return 0;
+}
+
+// Hybrid weighted pair stage of one group (its embedding and W ready):
+// masks and counts, dense / sparse row lists, sparse one-sided sums, the
+// hybrid tile kernel (+ split finalize), then the exact dense kernel on the
+// tiles it flagged.
+template <typename T>
+int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &out, const uint4 *tiles,
+                           uint32_t ntiles, uint32_t splits, bool last) {
+    const T *U = static_cast<const T *>(d_U);
+    const uint64_t words = g.ld / 64;
+    SSU_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * std::max<uint32_t>(E, 1), s));
+    if (E) {
+        const uint64_t items = static_cast<uint64_t>(E) * words;
+        const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((items + 7) / 8, 1u << 20));
+        dev::row_masks_kernel<T><<<grid, 256, 0, s>>>(U, E, g.ld, d_masks, d_counts);
+        launches++;
+    }
+    dev::classify_rows_kernel<<<1, 1024, 0, s>>>(d_counts, E, static_cast<uint32_t>(g.ld / 4), d_dense_rows,
+                                                 d_sparse_rows, d_nrows);
+    launches++;
+    {
+        dim3 grid(static_cast<uint32_t>((g.ld + 255) / 256), n_parts);
+        dev::sparse_sums_partial_kernel<T><<<grid, 256, 0, s>>>(U, static_cast<const T *>(d_len), d_sparse_rows,
+                                                                d_nrows, g.ld, part_chunk, d_ws_part);
+        dev::reduce_partials_kernel<double><<<static_cast<uint32_t>((g.ld + 255) / 256), 256, 0, s>>>(
+            d_ws_part, n_parts, g.ld, d_Ws);
+        launches += 2;
+    }
+    if (ntiles == 0) return 0;
+    SSU_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * ntiles, s));
+    dev::HybridArgs<T> h{};
+    h.tiles = tiles;
+    h.n_tiles = ntiles;
+    h.n_splits = std::max<uint32_t>(splits, 1);
+    h.tables = d_tdesc;
+    h.U = U;
+    h.len = static_cast<const T *>(d_len);
+    h.masks = d_masks;
+    h.words = words;
+    h.ld = g.ld;
+    h.dense_rows = d_dense_rows;
+    h.sparse_rows = d_sparse_rows;
+    h.n_rows = d_nrows;
+    h.W = static_cast<const T *>(d_W);
+    h.Ws = d_Ws;
+    h.tau = 0.02;
+    h.tile_flags = d_flags;
+    h.partial = h.n_splits > 1 ? d_hpartial : nullptr;
+    if (h.n_splits > 1 && sizeof(double) * dev::HB * dev::HB * ntiles * h.n_splits > hpartial_bytes) {
+        h.n_splits = 1;
+        h.partial = nullptr;
+    }
+    h.out = out;
+    const bool norm = spec.method == Method::weighted_normalized;
+    const uint32_t ctas = static_cast<uint32_t>(
+        std::min<uint64_t>(static_cast<uint64_t>(ntiles) * h.n_splits, static_cast<uint64_t>(n_sms)));
+    const size_t smem = dev::hybrid_smem<T>();
+    if (norm)
+        dev::pair_hybrid_kernel<T, true><<<ctas, dev::HTHREADS, smem, s>>>(h);
+    else
+        dev::pair_hybrid_kernel<T, false><<<ctas, dev::HTHREADS, smem, s>>>(h);
+    launches++;
+    if (h.partial) {
+        if (norm)
+            dev::hybrid_finalize_kernel<T, true><<<ntiles, dev::HTHREADS, 0, s>>>(h);
+        else
+            dev::hybrid_finalize_kernel<T, false><<<ntiles, dev::HTHREADS, 0, s>>>(h);
+        launches++;
+    }
+    if (last && timed()) SSU_CK(cudaEventRecord(ev[2], s));
+    // exact |a - b| recomputation of the flagged tiles (all nodes)
+    const PairKernel<T> &k = kern<T>();
+    dev::PairArgs<T> a{};
+    a.tiles = tiles;
+    a.n_tiles = ntiles;
+    a.n_splits = 1;
+    a.tables = d_tdesc;
+    a.U = U;
+    a.len = static_cast<const T *>(d_len);
+    a.W = static_cast<const T *>(d_W);
+    a.E = E;
+    a.ld = g.ld;
+    a.rows_per_split = E;
+    a.out = out;
+    a.tile_flags = d_flags;
+    k.launch(a, static_cast<uint32_t>(std::min<uint64_t>(ntiles, static_cast<uint64_t>(n_sms) * k.blocks_per_sm)),
+             k.smem, s);
+    launches++;
+    SSU_CK(cudaGetLastError());
     return 0;
 }
 
@@ -829,7 +993,9 @@ int PlanImpl::execute_T(cudaStream_t s, const dev::OutSpec &out) {
         if (!rc) rc = prepare<T>(s, g);
         if (rc) return rc;
         if (gi == 0 && timed()) SSU_CK(cudaEventRecord(ev[1], s));
-        rc = pair_stage<T>(s, g, out, g.d_tiles, g.n_tiles, g.splits, g.rows_per_split, gi + 1 == groups.size());
+        rc = hybrid ? hybrid_stage<T>(s, g, out, g.d_tiles, g.n_tiles, g.splits, gi + 1 == groups.size())
+                    : pair_stage<T>(s, g, out, g.d_tiles, g.n_tiles, g.splits, g.rows_per_split,
+                                    gi + 1 == groups.size());
         if (rc) return rc;
         if (gi + 1 == groups.size() && g.n_tiles == 0 && timed()) SSU_CK(cudaEventRecord(ev[2], s));
     }
@@ -857,6 +1023,22 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
     append_tiles(tiles, 0, 0, tdesc[0].n, BM, BN, mode == 1, start, stop);
     uint4 *d_t = nullptr;
     SSU_CK(upload(&d_t, tiles.data(), sizeof(uint4) * tiles.size()));
+    if (hybrid) {
+        dev::OutSpec o{mode, d_out, start, stop};
+        launches = 0;
+        const uint32_t nt = static_cast<uint32_t>(tiles.size());
+        int rc = 0;
+        if (spec.fp64) {
+            rc = embed<double>(stream, g);
+            if (!rc) rc = prepare<double>(stream, g);
+            if (!rc) rc = hybrid_stage<double>(stream, g, o, d_t, nt, 1, true);
+        } else {
+            rc = embed<float>(stream, g);
+            if (!rc) rc = prepare<float>(stream, g);
+            if (!rc) rc = hybrid_stage<float>(stream, g, o, d_t, nt, 1, true);
+        }
+        return rc;
+    }
     uint32_t s = 1, rows = 0;
     if (spec.fp64)
         choose_splits<double>(kd, static_cast<uint32_t>(tiles.size()), s, rows);

@@ -275,6 +275,7 @@ struct PairArgs {
     T alpha;
     OutSpec out;
     T *partial;       // per-split raw accumulators; nullptr when not split
+    const int *tile_flags;  // when set, only tiles with a non-zero flag are computed
 };
 
 // ---- per-term operators (one (k, l) pair, one embedded node) -------------
@@ -537,6 +538,7 @@ __global__ void __launch_bounds__((BM / TM) * (BN / TN), 1) pair_values_kernel(c
     const uint32_t n_work = a.n_tiles * a.n_splits;
     for (uint32_t w = blockIdx.x; w < n_work; w += gridDim.x) {
         const uint32_t split = w / a.n_tiles, ti = w - split * a.n_tiles;
+        if (a.tile_flags && !a.tile_flags[ti]) continue;  // uniform over the CTA
         const uint4 tile = a.tiles[ti];
         const uint32_t k0 = tile.x * BM, l0 = tile.y * BN;
         const uint32_t e_begin = split * a.rows_per_split;

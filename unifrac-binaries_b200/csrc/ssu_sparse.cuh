@@ -1,0 +1,400 @@
+// Weighted UniFrac over a sparse embedding (sm_100a).
+//
+// Most embedded nodes are zero for most samples: with 1% of the features
+// present per sample, a node is non-zero for ~5% of the samples on average.
+// For a node with u = a in sample k and b in sample l,
+//     |a - b| = a + b - 2 min(a, b),
+// and min(a, b) = 0 unless both are non-zero.  So over a set S of "sparse"
+// nodes
+//     sum_S L |a - b| = Ws_k + Ws_l - 2 sum_{S, a>0, b>0} L min(a, b),
+// Ws_j = sum_S L u(j) being one number per sample.  Nodes are split per call:
+//   dense rows  (non-zero in more than a quarter of the columns): summed as
+//               L |a - b| in registers, exactly as the dense pair kernel;
+//   sparse rows (the rest, all-zero rows dropped): only the pairs where both
+//               samples are non-zero are touched, -2 L min(a, b) accumulated
+//               in an fp64 tile in shared memory, rows in order, one lane per
+//               element (deterministic).
+// d = D + (M + Ws_k + Ws_l) subtracts; where d < tau (Ws_k + Ws_l) the
+// rounding of that subtraction could reach 1e-13 relative, so the tile is
+// flagged and recomputed exactly (all nodes, |a - b| form) by the dense pair
+// kernel afterwards.
+//
+// Presence masks: bit i of masks[e * words + w] is U[e][64 w + i] > 0.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ssu_kernels.cuh"
+
+namespace ssu {
+namespace dev {
+
+// Presence masks and non-zero counts of the embedded rows; one warp per
+// (row, 64-column word).  counts must start at zero.
+template <typename T>
+__global__ void row_masks_kernel(const T *__restrict__ U, uint32_t E, uint64_t ld,
+                                 unsigned long long *__restrict__ masks, uint32_t *__restrict__ counts) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t words = ld / 64;
+    const uint64_t total = static_cast<uint64_t>(E) * words;
+    const uint64_t nwarps = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
+    for (uint64_t item = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / 32; item < total;
+         item += nwarps) {
+        const uint64_t e = item / words, w = item % words;
+        const T *u = U + e * ld + w * 64;
+        const uint32_t b0 = __ballot_sync(0xffffffffu, u[lane] > T(0));
+        const uint32_t b1 = __ballot_sync(0xffffffffu, u[lane + 32] > T(0));
+        if (lane == 0) {
+            masks[item] = static_cast<unsigned long long>(b0) | (static_cast<unsigned long long>(b1) << 32);
+            const uint32_t c = __popc(b0) + __popc(b1);
+            if (c) atomicAdd(counts + e, c);
+        }
+    }
+}
+
+// Rows in order into dense (count > threshold) and sparse (0 < count <=
+// threshold) lists; one CTA of 1024 threads.  n_out = {dense, sparse}.
+static __global__ void __launch_bounds__(1024) classify_rows_kernel(const uint32_t *__restrict__ counts, uint32_t E,
+                                                                    uint32_t threshold, uint32_t *__restrict__ dense,
+                                                                    uint32_t *__restrict__ sparse,
+                                                                    uint32_t *__restrict__ n_out) {
+    __shared__ uint32_t warp_base[32][2];
+    __shared__ uint32_t run[2];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x < 2) run[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < E; c0 += blockDim.x) {
+        const uint32_t e = c0 + threadIdx.x;
+        const uint32_t cnt = e < E ? counts[e] : 0;
+        const bool is_dense = cnt > threshold;
+        const bool is_sparse = cnt > 0 && !is_dense;
+        const uint32_t bd = __ballot_sync(0xffffffffu, is_dense);
+        const uint32_t bs = __ballot_sync(0xffffffffu, is_sparse);
+        if (lane == 0) {
+            warp_base[warp][0] = __popc(bd);
+            warp_base[warp][1] = __popc(bs);
+        }
+        __syncthreads();
+        if (threadIdx.x < 2) {
+            uint32_t r = run[threadIdx.x];
+            for (uint32_t w = 0; w < nw; w++) {
+                const uint32_t t = warp_base[w][threadIdx.x];
+                warp_base[w][threadIdx.x] = r;
+                r += t;
+            }
+            run[threadIdx.x] = r;
+        }
+        __syncthreads();
+        const uint32_t below = (1u << lane) - 1u;
+        if (is_dense) dense[warp_base[warp][0] + __popc(bd & below)] = e;
+        if (is_sparse) sparse[warp_base[warp][1] + __popc(bs & below)] = e;
+        __syncthreads();
+    }
+    if (threadIdx.x < 2) n_out[threadIdx.x] = run[threadIdx.x];
+}
+
+// Ws[j] = sum over the sparse rows (in order, in fixed chunks) of L u[j],
+// in fp64; partial sums per chunk, then reduce_partials_kernel<double>.
+template <typename T>
+__global__ void sparse_sums_partial_kernel(const T *__restrict__ U, const T *__restrict__ len,
+                                           const uint32_t *__restrict__ rows, const uint32_t *__restrict__ n_rows,
+                                           uint64_t ld, uint32_t chunk, double *__restrict__ partial) {
+    const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= ld) return;
+    const uint32_t n = n_rows[1];
+    const uint32_t i0 = blockIdx.y * chunk;
+    const uint32_t i1 = min(n, i0 + chunk);
+    double s = 0.0;
+    for (uint32_t i = i0; i < i1; i++) {
+        const uint32_t e = rows[i];
+        s = fma(static_cast<double>(U[static_cast<uint64_t>(e) * ld + j]), static_cast<double>(len[e]), s);
+    }
+    partial[static_cast<uint64_t>(blockIdx.y) * ld + j] = s;
+}
+
+template <typename T>
+struct HybridArgs {
+    const uint4 *tiles;  // 128 x 128 tiles: x, y blocks of 128 columns, z table
+    uint32_t n_tiles, n_splits;
+    const TableDesc *tables;
+    const T *U;
+    const T *len;        // per embedded row
+    const unsigned long long *masks;
+    uint64_t words;      // ld / 64
+    uint64_t ld;
+    const uint32_t *dense_rows, *sparse_rows;
+    const uint32_t *n_rows;  // {dense, sparse}
+    const T *W;          // full one-sided sums (normalized)
+    const double *Ws;    // one-sided sums over the sparse rows
+    double tau;
+    int *tile_flags;     // tiles that need the exact recomputation
+    double *partial;     // per (split, tile) 128 x 128 fp64 raw sums; nullptr: no splits
+    OutSpec out;
+};
+
+constexpr int HB = 128;     // tile edge
+constexpr int HKC = 8;      // rows per pipeline stage (one per warp when loading)
+constexpr int HSTAGES = 5;  // stages in the ring
+constexpr int HTHREADS = 256;
+
+template <typename T>
+constexpr size_t hybrid_smem() {
+    return sizeof(double) * HB * HB + HSTAGES * (sizeof(T) * HKC * 2 * HB + 8 * 4 * HKC + sizeof(T) * HKC) + 64;
+}
+
+// Epilogue of one element: value from the raw sum x = D - 2 M.
+template <typename T, bool NORM>
+__device__ __forceinline__ void hybrid_emit(const HybridArgs<T> &a, const TableDesc &td, OutSpec o, uint32_t ti,
+                                            uint32_t kc, uint32_t lc, double x) {
+    const uint32_t k = kc - td.base, l = lc - td.base;
+    if (!(k < l && l < td.n)) return;
+    const double ws = a.Ws[kc] + a.Ws[lc];
+    const double d = x + ws;
+    if (d < a.tau * ws) atomicOr(a.tile_flags + ti, 1);
+    const T v = NORM ? static_cast<T>(d) / (a.W[kc] + a.W[lc]) : static_cast<T>(d);
+    emit_pair<T>(o, td.n, k, l, v);
+}
+
+template <typename T, bool NORM>
+__global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridArgs<T> a) {
+    constexpr int TX = 16;         // dense phase: 16 x 16 threads, 8 x 8 pairs each
+    constexpr int VEC = 16 / sizeof(T);
+    constexpr int CPR = 2 * HB / VEC;  // 16-byte pieces per staged row (k block then l block)
+    constexpr int PPT = CPR / 32;      // pieces per thread: warp w loads row w of a chunk
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *Mt = reinterpret_cast<double *>(smem_raw);                                      // [128][128]
+    T *Vs = reinterpret_cast<T *>(Mt + HB * HB);                                            // [S][HKC][256]
+    unsigned long long *Ms = reinterpret_cast<unsigned long long *>(Vs + HSTAGES * HKC * 2 * HB);  // [S][HKC][4]
+    T *Ls = reinterpret_cast<T *>(Ms + HSTAGES * HKC * 4);                                   // [S][HKC]
+
+    const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+    const int lane = tid & 31, warp = tid >> 5;
+    const uint32_t n_dense = a.n_rows[0], n_sparse = a.n_rows[1];
+    const uint32_t n_work = a.n_tiles * a.n_splits;
+    for (uint32_t w = blockIdx.x; w < n_work; w += gridDim.x) {
+        const uint32_t split = w / a.n_tiles, ti = w - split * a.n_tiles;
+        const uint4 tile = a.tiles[ti];
+        const uint32_t k0 = tile.x * HB, l0 = tile.y * HB;
+        const uint32_t dr = (n_dense + a.n_splits - 1) / a.n_splits;
+        const uint32_t sr = (n_sparse + a.n_splits - 1) / a.n_splits;
+        const uint32_t d_begin = min(n_dense, split * dr), d_end = min(n_dense, d_begin + dr);
+        const uint32_t s_begin = min(n_sparse, split * sr), s_end = min(n_sparse, s_begin + sr);
+
+        // Data of row `warp` of a chunk, issued by that warp: both value
+        // blocks (PPT 16-byte pieces per lane), the four mask words of the two
+        // blocks and the length.  `e` is the row id, `ok` whether it exists.
+        auto load_row = [&](int st, uint32_t e, bool ok, bool with_masks) {
+            T *dst = Vs + (st * HKC + warp) * 2 * HB;
+            const T *src = a.U + static_cast<uint64_t>(e) * a.ld;
+#pragma unroll
+            for (int m = 0; m < PPT; m++) {
+                const int q = lane + 32 * m;
+                const uint32_t col = q < CPR / 2 ? k0 + q * VEC : l0 + (q - CPR / 2) * VEC;
+                cp_async16(dst + q * VEC, src + col, ok ? 16 : 0);
+            }
+            if (with_masks && lane < 4) {
+                const uint64_t word = (lane < 2 ? k0 / 64 : l0 / 64) + (lane & 1);
+                cp_async_small<8>(Ms + (st * HKC + warp) * 4 + lane, a.masks + static_cast<uint64_t>(e) * a.words + word,
+                                  ok ? 8 : 0);
+            }
+            if (lane == 4) cp_async_small<sizeof(T)>(Ls + st * HKC + warp, a.len + e, ok ? (int)sizeof(T) : 0);
+        };
+        // Ring of HSTAGES chunks over rows [begin, end) of `rows`: chunk c is
+        // issued HSTAGES - 1 iterations before it is consumed; each warp keeps
+        // the row ids of its next two chunks in registers.
+        auto stream_rows = [&](const uint32_t *rows, uint32_t begin, uint32_t end, bool with_masks, auto consume) {
+            const uint32_t n_chunks = end > begin ? (end - begin + HKC - 1) / HKC : 0;
+            if (n_chunks == 0) return;
+            auto id_of = [&](uint32_t chunk) -> uint32_t {
+                const uint32_t i = begin + chunk * HKC + warp;
+                return (chunk < n_chunks && i < end) ? rows[i] : 0u;
+            };
+            auto ok_of = [&](uint32_t chunk) { return chunk < n_chunks && begin + chunk * HKC + warp < end; };
+            for (uint32_t c = 0; c + 1 < HSTAGES; c++) {
+                if (c < n_chunks) load_row(static_cast<int>(c), id_of(c), ok_of(c), with_masks);
+                cp_async_commit();
+            }
+            uint32_t id1 = id_of(HSTAGES - 1), id2 = id_of(HSTAGES);
+            for (uint32_t ch = 0; ch < n_chunks; ch++) {
+                const uint32_t nxt = ch + HSTAGES - 1;
+                if (nxt < n_chunks) load_row(static_cast<int>(nxt % HSTAGES), id1, ok_of(nxt), with_masks);
+                cp_async_commit();
+                id1 = id2;
+                id2 = id_of(ch + HSTAGES + 1);
+                cp_async_wait<HSTAGES - 1>();
+                __syncthreads();
+                consume(static_cast<int>(ch % HSTAGES));
+                __syncthreads();
+            }
+            cp_async_wait<0>();
+        };
+
+        // ---- dense rows: L |a - b| in registers, 8 x 8 pairs per thread
+        double acc[8][8];
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
+        stream_rows(a.dense_rows, d_begin, d_end, false, [&](int st) {
+            const T *vs = Vs + st * HKC * 2 * HB;
+#pragma unroll 2
+            for (int c = 0; c < HKC; c++) {
+                T av[8], bv[8];
+                load_half<T, 4>(av, vs + c * 2 * HB + ty * 4);
+                load_half<T, 4>(av + 4, vs + c * 2 * HB + HB / 2 + ty * 4);
+                load_half<T, 4>(bv, vs + c * 2 * HB + HB + tx * 4);
+                load_half<T, 4>(bv + 4, vs + c * 2 * HB + HB + HB / 2 + tx * 4);
+                const double L = static_cast<double>(Ls[st * HKC + c]);
+#pragma unroll
+                for (int i = 0; i < 8; i++)
+#pragma unroll
+                    for (int j = 0; j < 8; j++)
+                        acc[i][j] =
+                            fma(fabs(static_cast<double>(av[i]) - static_cast<double>(bv[j])), L, acc[i][j]);
+            }
+        });
+        // the dense sums seed the shared tile
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                Mt[tile_row<HB, 8>(ty, i) * HB + tile_row<HB, 8>(tx, j)] = acc[i][j];
+        __syncthreads();
+
+        // ---- sparse rows: -2 L min(a, b) where both are non-zero.  Each warp
+        // walks the sparse rows on its own (no block barrier), owning tile
+        // rows 16 warp .. 16 warp + 15.  Per batch of 32 rows, lane i holds
+        // row i's id, mask words and length (fetched one batch ahead, the ids
+        // two); one ballot finds the rows with a non-zero in both the warp's
+        // rows and the l block; their values are gathered eight rows at a
+        // time (lane r < 16: row value r, lane j: columns j + 32 m) and the
+        // updates of row r use its value from lane r by shuffle.
+        {
+            const uint64_t kwd = k0 / 64 + (warp >> 2), lwd = l0 / 64;
+            const int kshift = 16 * (warp & 3);
+            double *Mw = Mt + 16 * warp * HB;
+            const uint32_t n_batches = s_end > s_begin ? (s_end - s_begin + 31) / 32 : 0;
+            auto row_id = [&](uint32_t batch) -> uint32_t {
+                const uint32_t i = s_begin + batch * 32 + lane;
+                return (batch < n_batches && i < s_end) ? a.sparse_rows[i] : 0u;
+            };
+            uint32_t e_cur = row_id(0), e_next = row_id(1);
+            bool ok_cur = s_begin + lane < s_end;
+            unsigned long long km_cur = 0, m0_cur = 0, m1_cur = 0;
+            double L_cur = 0.0;
+            if (ok_cur) {
+                const unsigned long long *mp = a.masks + static_cast<uint64_t>(e_cur) * a.words;
+                km_cur = mp[kwd];
+                m0_cur = mp[lwd];
+                m1_cur = mp[lwd + 1];
+                L_cur = static_cast<double>(a.len[e_cur]);
+            }
+            for (uint32_t b = 0; b < n_batches; b++) {
+                // fetch the next batch (masks through the ids already held)
+                const bool ok_next = b + 1 < n_batches && s_begin + (b + 1) * 32 + lane < s_end;
+                unsigned long long km_next = 0, m0_next = 0, m1_next = 0;
+                double L_next = 0.0;
+                if (ok_next) {
+                    const unsigned long long *mp = a.masks + static_cast<uint64_t>(e_next) * a.words;
+                    km_next = mp[kwd];
+                    m0_next = mp[lwd];
+                    m1_next = mp[lwd + 1];
+                    L_next = static_cast<double>(a.len[e_next]);
+                }
+                const uint32_t e_after = row_id(b + 2);
+
+                const uint32_t mk_l = static_cast<uint32_t>(km_cur >> kshift) & 0xFFFFu;
+                uint32_t active = __ballot_sync(0xffffffffu, ok_cur && mk_l != 0 && (m0_cur | m1_cur) != 0ull);
+                while (active) {
+                    int slot_lane[8];
+                    int cnt = 0;
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        slot_lane[j] = active ? __ffs(active) - 1 : 0;
+                        cnt += active ? 1 : 0;
+                        active &= active ? active - 1 : 0u;
+                    }
+                    double va[8], vb[8][4];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        const int c = slot_lane[j];
+                        const uint32_t e = __shfl_sync(0xffffffffu, e_cur, c);
+                        const uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
+                        const unsigned long long m0 = __shfl_sync(0xffffffffu, m0_cur, c);
+                        const unsigned long long m1 = __shfl_sync(0xffffffffu, m1_cur, c);
+                        const T *row = a.U + static_cast<uint64_t>(e) * a.ld;
+                        const bool live = j < cnt;
+                        va[j] = (live && lane < 16 && ((mk >> lane) & 1u))
+                                    ? static_cast<double>(row[k0 + 16 * warp + lane]) : 0.0;
+#pragma unroll
+                        for (int m = 0; m < 4; m++) {
+                            const unsigned long long wv = m < 2 ? m0 : m1;
+                            const bool on = live && ((wv >> (32 * (m & 1) + lane)) & 1ull);
+                            vb[j][m] = on ? static_cast<double>(row[l0 + 32 * m + lane]) : -1.0;
+                        }
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        if (j < cnt) {
+                            const int c = slot_lane[j];
+                            uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
+                            const double L2 = -2.0 * __shfl_sync(0xffffffffu, L_cur, c);
+                            while (mk) {
+                                const int r = __ffs(mk) - 1;
+                                mk &= mk - 1;
+                                const double av = __shfl_sync(0xffffffffu, va[j], r);
+#pragma unroll
+                                for (int m = 0; m < 4; m++) {
+                                    if (vb[j][m] >= 0.0) {
+                                        double *p = Mw + r * HB + 32 * m + lane;
+                                        *p = fma(L2, fmin(av, vb[j][m]), *p);
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+                e_cur = e_next;
+                e_next = e_after;
+                ok_cur = ok_next;
+                km_cur = km_next;
+                m0_cur = m0_next;
+                m1_cur = m1_next;
+                L_cur = L_next;
+            }
+        }
+        __syncthreads();
+
+        // ---- epilogue: raw sums to the split buffer, or finished values
+        if (a.partial) {
+            double *dst = a.partial + (static_cast<uint64_t>(split) * a.n_tiles + ti) * HB * HB;
+            for (int e = tid; e < HB * HB; e += HTHREADS) dst[e] = Mt[e];
+        } else {
+            const TableDesc td = a.tables[tile.z];
+            OutSpec o = a.out;
+            if (o.mode == 0) o.ptr = static_cast<T *>(o.ptr) + td.out_off;
+            for (int e = tid; e < HB * HB; e += HTHREADS)
+                hybrid_emit<T, NORM>(a, td, o, ti, k0 + e / HB, l0 + e % HB, Mt[e]);
+        }
+        __syncthreads();  // the shared tile is reused by the next work item
+    }
+}
+
+// Split partials of each tile summed in split order, then the epilogue.
+template <typename T, bool NORM>
+__global__ void __launch_bounds__(HTHREADS) hybrid_finalize_kernel(const HybridArgs<T> a) {
+    const uint32_t ti = blockIdx.x;
+    const uint4 tile = a.tiles[ti];
+    const TableDesc td = a.tables[tile.z];
+    OutSpec o = a.out;
+    if (o.mode == 0) o.ptr = static_cast<T *>(o.ptr) + td.out_off;
+    for (int e = threadIdx.x; e < HB * HB; e += HTHREADS) {
+        double x = 0.0;
+        for (uint32_t s = 0; s < a.n_splits; s++) x += a.partial[(static_cast<uint64_t>(s) * a.n_tiles + ti) * HB * HB + e];
+        hybrid_emit<T, NORM>(a, td, o, ti, tile.x * HB + e / HB, tile.y * HB + e % HB, x);
+    }
+}
+
+}  // namespace dev
+}  // namespace ssu

@@ -201,6 +201,7 @@ class TableInputs:
                                 self.indptr.ctypes.data_as(C.POINTER(C.c_uint32)),
                                 self.data.ctypes.data_as(C.POINTER(C.c_double)), len(table.obs_ids),
                                 len(table.sample_ids), int(self.indptr[-1]) if len(self.indptr) else 0)
+        self.arrays = (self.indptr, self.indices, self.data)
 
 
 class TreeInputs:
@@ -213,6 +214,30 @@ class TreeInputs:
         self.tree = SupportBPTree(self.structure.ctypes.data_as(C.POINTER(C.c_bool)),
                                   self.lengths.ctypes.data_as(C.POINTER(C.c_double)), self.names,
                                   len(tree.names))
+        self.arrays = (self.structure, self.lengths)
+
+
+_MARSHALLED = {}
+
+
+def _marshalled(obj, make, arrays, names):
+    """The C view of a table or tree, reused while the object, its arrays and
+    its name lists are the same objects (name lists are not expected to be
+    edited in place between calls)."""
+    key = tuple(id(a) for a in arrays) + tuple((id(n), len(n)) for n in names)
+    hit = _MARSHALLED.get(id(obj))
+    if hit is not None and hit[0]() is obj and hit[1] == key:
+        return hit[2]
+    view = make(obj)
+    # only views that share the caller's arrays (no dtype or layout copy)
+    shared = all(np.ascontiguousarray(a, dtype=b.dtype) is a for a, b in zip(arrays, view.arrays))
+    if shared:
+        try:
+            ref = weakref.ref(obj, lambda _, i=id(obj): _MARSHALLED.pop(i, None))
+            _MARSHALLED[id(obj)] = (ref, key, view)
+        except TypeError:
+            pass
+    return view
 
 
 class Inputs:
@@ -220,8 +245,9 @@ class Inputs:
     the backing numpy arrays alive while the call runs."""
 
     def __init__(self, tree, table):
-        self._table = TableInputs(table)
-        self._tree = TreeInputs(tree)
+        self._table = _marshalled(table, TableInputs, (table.indptr, table.indices, table.data),
+                                  (table.obs_ids, table.sample_ids))
+        self._tree = _marshalled(tree, TreeInputs, (tree.structure, tree.lengths), (tree.names,))
         self.biom = self._table.biom
         self.tree = self._tree.tree
 
