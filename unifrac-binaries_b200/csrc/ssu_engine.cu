@@ -274,6 +274,7 @@ struct PlanImpl {
     // weighted methods over the sparse embedding (dense rows in registers,
     // sparse rows on their intersections, flagged tiles recomputed exactly)
     bool hybrid = false;
+    uint32_t hybrid_div = 8;  // rows non-zero in more than ld / hybrid_div columns are dense
     bool nonneg_data = true;  // no negative count in any table
     unsigned long long *d_masks = nullptr;
     uint32_t *d_counts = nullptr, *d_dense_rows = nullptr, *d_sparse_rows = nullptr, *d_nrows = nullptr;
@@ -616,8 +617,11 @@ int PlanImpl::setup_method() {
     SSU_CK(alloc(&d_full, sizeof(T) * std::max<uint64_t>(full_elems, 1)));
 
     size_t chosen = 0;
-    // min(a, b) = 0 off the intersection of the supports needs u >= 0
-    hybrid = !spec.vaw && len_stride == 0 && nonneg_data &&
+    // min(a, b) = 0 off the intersection of the supports needs u >= 0.  In
+    // single precision the dense pair kernel (fp32 pipe) is faster than the
+    // hybrid's fp64 tile (measured: 7.4 vs 8.7 ms on 2,048 samples x 40k
+    // nodes), so the hybrid serves the fp64 methods.
+    hybrid = sizeof(T) == 8 && !spec.vaw && len_stride == 0 && nonneg_data &&
              (spec.method == Method::weighted_normalized || spec.method == Method::weighted_unnormalized);
     if (const char *m = std::getenv("UNIFRAC_B200_WEIGHTED_MODE"))
         if (std::string(m) == "dense") hybrid = false;
@@ -649,6 +653,7 @@ int PlanImpl::setup_method() {
 
 template <typename T>
 int PlanImpl::setup_hybrid() {
+    hybrid_div = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_HYBRID_DIV", 8)));
     const uint64_t words = ld / 64;
     SSU_CK(alloc(&d_masks, sizeof(unsigned long long) * std::max<uint64_t>(static_cast<uint64_t>(E) * words, 1)));
     SSU_CK(alloc(&d_counts, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
@@ -708,8 +713,8 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
         dev::row_masks_kernel<T><<<grid, 256, 0, s>>>(U, E, g.ld, d_masks, d_counts);
         launches++;
     }
-    dev::classify_rows_kernel<<<1, 1024, 0, s>>>(d_counts, E, static_cast<uint32_t>(g.ld / 4), d_dense_rows,
-                                                 d_sparse_rows, d_nrows);
+    dev::classify_rows_kernel<<<1, 1024, 0, s>>>(d_counts, E, static_cast<uint32_t>(g.ld / hybrid_div),
+                                                 d_dense_rows, d_sparse_rows, d_nrows);
     launches++;
     {
         dim3 grid(static_cast<uint32_t>((g.ld + 255) / 256), n_parts);
@@ -1590,6 +1595,9 @@ uint64_t Plan::work_units() const {
 uint32_t Plan::launches() const { return impl_->launches; }
 const char *Plan::pair_kernel_name() const {
     if (impl_->gemm) return "unweighted_tc_kernel";
+    if (impl_->hybrid)
+        return impl_->spec.method == Method::weighted_normalized ? "pair_hybrid<weighted_normalized>"
+                                                                 : "pair_hybrid<weighted_unnormalized>";
     return impl_->spec.fp64 ? impl_->kd.name : impl_->kf.name;
 }
 const char *Plan::tuning() const {

@@ -8,7 +8,7 @@
 // nodes
 //     sum_S L |a - b| = Ws_k + Ws_l - 2 sum_{S, a>0, b>0} L min(a, b),
 // Ws_j = sum_S L u(j) being one number per sample.  Nodes are split per call:
-//   dense rows  (non-zero in more than a quarter of the columns): summed as
+//   dense rows  (non-zero in more than an eighth of the columns): summed as
 //               L |a - b| in registers, exactly as the dense pair kernel;
 //   sparse rows (the rest, all-zero rows dropped): only the pairs where both
 //               samples are non-zero are touched, -2 L min(a, b) accumulated
