@@ -51,7 +51,7 @@ def parse():
     p.add_argument("--replicates", type=int, default=100)
     p.add_argument("--tables5", type=int, default=64)
     p.add_argument("--tips5", type=int, default=50000)
-    p.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "config5"],
+    p.add_argument("--workload", default="config2", choices=["config1", "config2", "config3", "config4", "config5"],
                    help="config3: unweighted fp64, tensor-core contraction vs the plain stripe form")
     p.add_argument("--samples3", type=int, default=25000)
     p.add_argument("--tips3", type=int, default=100000)
@@ -373,6 +373,61 @@ def _batch_setup():
     return torch, stream, flush
 
 
+def run_config1(args):
+    """1,000-tip tree, 1,000 x 128 table: unweighted and weighted-normalized
+    fp64, condensed 128 x 128 form through the C API.  Too small for a
+    roofline (launch- and latency-bound): times only, next to the reference's
+    CPU build on the same input."""
+    torch, stream, flush = _batch_setup()
+    import ssu_b200
+    import ssu_synth
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    tree, table = ssu_synth.config1()
+    out = {}
+    total_units, total_e2e, total_dev = 0, 0.0, 0.0
+    for m in ("unweighted_fp64", "weighted_normalized_fp64"):
+        plan = ssu_b200.Plan(tree, table, m)
+        units = plan.work_units()
+        for _ in range(args.warmup):
+            plan.execute(stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.execute(stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        dev_ms = e0.elapsed_time(e1) / args.steps
+        kernel = plan.pair_kernel()
+        plan.close()
+        for _ in range(args.warmup):
+            ssu_b200.one_off(tree, table, m)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            cf, _, _ = ssu_b200.one_off(tree, table, m)
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+        entry = {"device_ms": dev_ms, "e2e_ms": e2e_ms, "units": units, "kernel": kernel}
+        if oracle_py.ref_available():
+            ref = oracle_py.ref_one_off(tree, table, m, with_timing=True)
+            n = table.n_samples
+            iu = __import__("numpy").triu_indices(n, 1)
+            entry["reference_cpu_ms"] = 1e3 * sum(ref["seconds"])
+            entry["max_rel_vs_reference"] = _rel_err(cf, ref["matrix"][iu])[0]
+        out[m] = entry
+        total_units += units
+        total_e2e += e2e_ms
+        total_dev += dev_ms
+    line = {"metric": METRIC, "value": total_units / (total_dev / 1e3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_dev, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-1 generator)",
+            "config": {"workload": "unweighted_fp64 + weighted_normalized_fp64, 1k-tip tree, 1k features x 128 "
+                                   "samples, condensed form"},
+            "methods": out,
+            "e2e": {"value": total_units / (total_e2e / 1e3), "unit": UNIT, "ms_per_step": total_e2e}}
+    print(json.dumps(line), flush=True)
+
+
 def run_config4(args):
     """100 rarefied replicates (depth 1,000) of a 10,000-feature x 5,000-sample
     table on a 10,000-tip tree, unweighted and weighted-normalized fp32, every
@@ -519,6 +574,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "config1":
+        return run_config1(args)
     if args.workload == "config3":
         return run_config3(args)
     if args.workload == "config4":

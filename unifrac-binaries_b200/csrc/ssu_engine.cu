@@ -679,7 +679,7 @@ int PlanImpl::setup_hybrid() {
         // node splits so the tiles fill the SMs (one CTA per SM)
         uint32_t best_s = 1;
         double best = 1e300;
-        const uint32_t max_s = std::max<uint32_t>(1, std::min<uint32_t>(16, E / 2048));
+        const uint32_t max_s = std::max<uint32_t>(1, std::min<uint32_t>(64, E / 128));
         for (uint32_t sp = 1; sp <= max_s; sp++) {
             const double cost = std::ceil(static_cast<double>(g.n_tiles) * sp / n_sms) / sp * (1.0 + 0.02 * (sp - 1));
             if (cost < best - 1e-12) {
