@@ -133,10 +133,13 @@ struct HybridArgs {
     OutSpec out;
 };
 
-constexpr int HB = 128;     // tile edge
-constexpr int HKC = 8;      // rows per pipeline stage (one per warp when loading)
-constexpr int HSTAGES = 5;  // stages in the ring
-constexpr int HTHREADS = 256;
+constexpr int HB = 128;      // tile edge
+constexpr int HKC = 8;       // rows per pipeline stage (warps 0..7 load one each)
+constexpr int HSTAGES = 5;   // stages in the ring
+constexpr int HTHREADS = 512;
+constexpr int HWARPS = HTHREADS / 32;
+constexpr int HROWS = HB / HWARPS;  // tile rows owned by a warp in the sparse phase
+constexpr int HSLOTS = 4;           // active rows gathered together per warp
 
 template <typename T>
 constexpr size_t hybrid_smem() {
@@ -158,7 +161,8 @@ __device__ __forceinline__ void hybrid_emit(const HybridArgs<T> &a, const TableD
 
 template <typename T, bool NORM>
 __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridArgs<T> a) {
-    constexpr int TX = 16;         // dense phase: 16 x 16 threads, 8 x 8 pairs each
+    constexpr int TX = 16;         // dense phase: 16 (l) x 32 (k) threads, 4 x 8 pairs each
+    constexpr int TM = 4, TN = 8;
     constexpr int VEC = 16 / sizeof(T);
     constexpr int CPR = 2 * HB / VEC;  // 16-byte pieces per staged row (k block then l block)
     constexpr int PPT = CPR / 32;      // pieces per thread: warp w loads row w of a chunk
@@ -185,6 +189,7 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
         // blocks (PPT 16-byte pieces per lane), the four mask words of the two
         // blocks and the length.  `e` is the row id, `ok` whether it exists.
         auto load_row = [&](int st, uint32_t e, bool ok, bool with_masks) {
+            if (warp >= HKC) return;
             T *dst = Vs + (st * HKC + warp) * 2 * HB;
             const T *src = a.U + static_cast<uint64_t>(e) * a.ld;
 #pragma unroll
@@ -208,9 +213,11 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
             if (n_chunks == 0) return;
             auto id_of = [&](uint32_t chunk) -> uint32_t {
                 const uint32_t i = begin + chunk * HKC + warp;
-                return (chunk < n_chunks && i < end) ? rows[i] : 0u;
+                return (warp < HKC && chunk < n_chunks && i < end) ? rows[i] : 0u;
             };
-            auto ok_of = [&](uint32_t chunk) { return chunk < n_chunks && begin + chunk * HKC + warp < end; };
+            auto ok_of = [&](uint32_t chunk) {
+                return warp < HKC && chunk < n_chunks && begin + chunk * HKC + warp < end;
+            };
             for (uint32_t c = 0; c + 1 < HSTAGES; c++) {
                 if (c < n_chunks) load_row(static_cast<int>(c), id_of(c), ok_of(c), with_masks);
                 cp_async_commit();
@@ -230,50 +237,52 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
             cp_async_wait<0>();
         };
 
-        // ---- dense rows: L |a - b| in registers, 8 x 8 pairs per thread
-        double acc[8][8];
+        // ---- dense rows: L |a - b| in registers, 4 x 8 pairs per thread
+        double acc[TM][TN];
 #pragma unroll
-        for (int i = 0; i < 8; i++)
+        for (int i = 0; i < TM; i++)
 #pragma unroll
-            for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
+            for (int j = 0; j < TN; j++) acc[i][j] = 0.0;
         stream_rows(a.dense_rows, d_begin, d_end, false, [&](int st) {
             const T *vs = Vs + st * HKC * 2 * HB;
 #pragma unroll 2
             for (int c = 0; c < HKC; c++) {
-                T av[8], bv[8];
-                load_half<T, 4>(av, vs + c * 2 * HB + ty * 4);
-                load_half<T, 4>(av + 4, vs + c * 2 * HB + HB / 2 + ty * 4);
-                load_half<T, 4>(bv, vs + c * 2 * HB + HB + tx * 4);
-                load_half<T, 4>(bv + 4, vs + c * 2 * HB + HB + HB / 2 + tx * 4);
+                T av[TM], bv[TN];
+                load_half<T, TM / 2>(av, vs + c * 2 * HB + ty * (TM / 2));
+                load_half<T, TM / 2>(av + TM / 2, vs + c * 2 * HB + HB / 2 + ty * (TM / 2));
+                load_half<T, TN / 2>(bv, vs + c * 2 * HB + HB + tx * (TN / 2));
+                load_half<T, TN / 2>(bv + TN / 2, vs + c * 2 * HB + HB + HB / 2 + tx * (TN / 2));
                 const double L = static_cast<double>(Ls[st * HKC + c]);
 #pragma unroll
-                for (int i = 0; i < 8; i++)
+                for (int i = 0; i < TM; i++)
 #pragma unroll
-                    for (int j = 0; j < 8; j++)
+                    for (int j = 0; j < TN; j++)
                         acc[i][j] =
                             fma(fabs(static_cast<double>(av[i]) - static_cast<double>(bv[j])), L, acc[i][j]);
             }
         });
         // the dense sums seed the shared tile
 #pragma unroll
-        for (int i = 0; i < 8; i++)
+        for (int i = 0; i < TM; i++)
 #pragma unroll
-            for (int j = 0; j < 8; j++)
-                Mt[tile_row<HB, 8>(ty, i) * HB + tile_row<HB, 8>(tx, j)] = acc[i][j];
+            for (int j = 0; j < TN; j++)
+                Mt[tile_row<HB, TM>(ty, i) * HB + tile_row<HB, TN>(tx, j)] = acc[i][j];
         __syncthreads();
 
         // ---- sparse rows: -2 L min(a, b) where both are non-zero.  Each warp
         // walks the sparse rows on its own (no block barrier), owning tile
-        // rows 16 warp .. 16 warp + 15.  Per batch of 32 rows, lane i holds
-        // row i's id, mask words and length (fetched one batch ahead, the ids
-        // two); one ballot finds the rows with a non-zero in both the warp's
-        // rows and the l block; their values are gathered eight rows at a
-        // time (lane r < 16: row value r, lane j: columns j + 32 m) and the
-        // updates of row r use its value from lane r by shuffle.
+        // rows HROWS warp .. HROWS warp + HROWS - 1.  Per batch of 32 rows,
+        // lane i holds row i's id, mask words and length (fetched one batch
+        // ahead, the ids two); one ballot finds the rows with a non-zero in
+        // both the warp's rows and the l block; their values are gathered
+        // HSLOTS rows at a time (lane r < HROWS: row value r, lane j: columns
+        // j + 32 m) and the updates of row r take its value from lane r by
+        // shuffle.
         {
-            const uint64_t kwd = k0 / 64 + (warp >> 2), lwd = l0 / 64;
-            const int kshift = 16 * (warp & 3);
-            double *Mw = Mt + 16 * warp * HB;
+            const uint64_t kwd = k0 / 64 + (warp * HROWS) / 64, lwd = l0 / 64;
+            const int kshift = (warp * HROWS) % 64;
+            constexpr uint32_t kmask = (1u << HROWS) - 1u;
+            double *Mw = Mt + HROWS * warp * HB;
             const uint32_t n_batches = s_end > s_begin ? (s_end - s_begin + 31) / 32 : 0;
             auto row_id = [&](uint32_t batch) -> uint32_t {
                 const uint32_t i = s_begin + batch * 32 + lane;
@@ -304,20 +313,20 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                 }
                 const uint32_t e_after = row_id(b + 2);
 
-                const uint32_t mk_l = static_cast<uint32_t>(km_cur >> kshift) & 0xFFFFu;
+                const uint32_t mk_l = static_cast<uint32_t>(km_cur >> kshift) & kmask;
                 uint32_t active = __ballot_sync(0xffffffffu, ok_cur && mk_l != 0 && (m0_cur | m1_cur) != 0ull);
                 while (active) {
-                    int slot_lane[8];
+                    int slot_lane[HSLOTS];
                     int cnt = 0;
 #pragma unroll
-                    for (int j = 0; j < 8; j++) {
+                    for (int j = 0; j < HSLOTS; j++) {
                         slot_lane[j] = active ? __ffs(active) - 1 : 0;
                         cnt += active ? 1 : 0;
                         active &= active ? active - 1 : 0u;
                     }
-                    double va[8], vb[8][4];
+                    double va[HSLOTS], vb[HSLOTS][4];
 #pragma unroll
-                    for (int j = 0; j < 8; j++) {
+                    for (int j = 0; j < HSLOTS; j++) {
                         const int c = slot_lane[j];
                         const uint32_t e = __shfl_sync(0xffffffffu, e_cur, c);
                         const uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
@@ -325,8 +334,8 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                         const unsigned long long m1 = __shfl_sync(0xffffffffu, m1_cur, c);
                         const T *row = a.U + static_cast<uint64_t>(e) * a.ld;
                         const bool live = j < cnt;
-                        va[j] = (live && lane < 16 && ((mk >> lane) & 1u))
-                                    ? static_cast<double>(row[k0 + 16 * warp + lane]) : 0.0;
+                        va[j] = (live && lane < HROWS && ((mk >> lane) & 1u))
+                                    ? static_cast<double>(row[k0 + HROWS * warp + lane]) : 0.0;
 #pragma unroll
                         for (int m = 0; m < 4; m++) {
                             const unsigned long long wv = m < 2 ? m0 : m1;
@@ -335,7 +344,7 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                         }
                     }
 #pragma unroll
-                    for (int j = 0; j < 8; j++) {
+                    for (int j = 0; j < HSLOTS; j++) {
                         if (j < cnt) {
                             const int c = slot_lane[j];
                             uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
