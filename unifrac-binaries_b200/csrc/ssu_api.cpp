@@ -121,30 +121,45 @@ ssu::BPTree tree_from(const support_bptree_t *t, bool copy_names = false) {
 }
 
 // Observation name -> row (the last row wins for a repeated name, as the
-// reference's obs_id_index map); *distinct gets the number of distinct names.
-ssu::NameMap obs_map(const ssu::Table &table, uint32_t *distinct) {
-    ssu::NameMap m(table.n_obs);
-    for (uint32_t i = 0; i < table.n_obs; i++) m.set(table.obs_ids[i], i);
-    uint32_t d = 0;
-    for (uint32_t i = 0; i < table.n_obs; i++) d += m.find(table.obs_ids[i]) == static_cast<int64_t>(i);
-    *distinct = d;
-    return m;
+// reference's obs_id_index map), built once per table and call; the table
+// keeps it with its number of distinct names.
+const ssu::NameMap &obs_map(const ssu::Table &table) {
+    if (!table.names) {
+        auto m = std::make_shared<ssu::NameMap>(table.n_obs);
+        uint32_t d = 0;
+        for (uint32_t i = 0; i < table.n_obs; i++) d += m->set(table.obs_ids[i], i) ? 1u : 0u;
+        table.distinct_names = d;
+        table.names = std::move(m);
+    }
+    return *table.names;
+}
+
+// The table's tips matched against `tree`, computed once per call.
+const ssu::TipMatch &tip_match(const ssu::Table &table, const ssu::BPTree &tree) {
+    if (!table.tip_match || table.tip_match->tree_id != tree.open.data() ||
+        table.tip_match->tree_size != tree.size())
+        table.tip_match = std::make_shared<ssu::TipMatch>(tree.match_tips(obs_map(table), table.n_obs));
+    return *table.tip_match;
 }
 
 // VALIDATE_TREE_TABLE (src/api.cpp:94-100): every table id is a tip name.
 ComputeStatus validate(const ssu::Table &table, const ssu::BPTree &tree) {
     if (table.n_samples == 0 || table.n_obs == 0) return table_empty;
-    uint32_t distinct = 0;
-    const ssu::NameMap obs = obs_map(table, &distinct);
-    return tree.count_matched(obs, table.n_obs) == distinct ? okay : table_and_tree_do_not_overlap;
+    const ssu::TipMatch &m = tip_match(table, tree);
+    return m.rows_matched == table.distinct_names ? okay : table_and_tree_do_not_overlap;
 }
 
-// SYNC_TREE_TABLE (src/api.cpp:90-92) + flattening for the device; the
-// shear tags the kept tips with their table rows.
+// SYNC_TREE_TABLE (src/api.cpp:90-92) + flattening for the device.  The kept
+// tips carry their table rows; when every tip is in the table the shear is
+// the tree itself, and a tree without single-child nodes collapses to itself.
 ssu::FlatTree sync_tree(const ssu::Table &table, const ssu::BPTree &tree, bool bypass_tips) {
-    uint32_t distinct = 0;
-    const ssu::NameMap obs = obs_map(table, &distinct);
-    const ssu::BPTree sheared = tree.shear_to(obs, table.n_obs, nullptr).collapse();
+    const ssu::TipMatch &m = tip_match(table, tree);
+    if (m.all_tips) {
+        if (!tree.has_single_child()) return ssu::flatten(tree, bypass_tips, &m.tags);
+        return ssu::flatten(tree.collapse(&m.tags), bypass_tips);
+    }
+    ssu::BPTree sheared = tree.shear_matched(m);
+    if (sheared.has_single_child()) sheared = sheared.collapse();
     return ssu::flatten(sheared, bypass_tips);
 }
 

@@ -20,12 +20,14 @@ class NameMap {
     }
 
     // Insert or overwrite (the last index for a repeated name wins, as a
-    // std::unordered_map assignment would).
-    void set(std::string_view key, uint32_t value) {
+    // std::unordered_map assignment would); true when the key is new.
+    bool set(std::string_view key, uint32_t value) {
         size_t i = hash(key) & mask_;
         while (vals_[i] != kEmpty && keys_[i] != key) i = (i + 1) & mask_;
+        const bool fresh = vals_[i] == kEmpty;
         keys_[i] = key;
         vals_[i] = value;
+        return fresh;
     }
 
     // Index of `key`, or -1.

@@ -4,12 +4,16 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <string_view>
 #include <unordered_map>
 #include <vector>
 
 namespace ssu {
+
+struct TipMatch;
+class NameMap;
 
 struct Table {
     Table() = default;
@@ -27,6 +31,12 @@ struct Table {
     std::vector<std::string_view> obs_ids;
     std::vector<std::string_view> sample_ids;
     std::vector<double> totals;  // per-sample sum, accumulated in observation order
+
+    // Name matching of this table against the call's tree, made once by the
+    // validation and reused by the shear (host-side cache of one call).
+    mutable std::shared_ptr<const NameMap> names;
+    mutable uint32_t distinct_names = 0;
+    mutable std::shared_ptr<const TipMatch> tip_match;
 
     // storage when the table owns its arrays
     std::vector<uint32_t> own_indptr, own_indices;

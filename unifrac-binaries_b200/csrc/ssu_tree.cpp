@@ -188,6 +188,62 @@ BPTree BPTree::masked(const std::vector<uint8_t> &keep, const std::vector<double
     return r;
 }
 
+TipMatch BPTree::match_tips(const NameMap &obs, uint32_t n_obs) const {
+    TipMatch m;
+    const uint32_t n = size();
+    m.tags.assign(n, -1);
+    m.tree_id = open.data();
+    m.tree_size = n;
+    std::vector<uint8_t> seen(n_obs, 0);
+    bool all = true;
+    for (uint32_t i = 0; i + 1 < n; i++) {
+        if (!leaf(i)) continue;
+        const int64_t row = obs.find(name[i]);
+        if (row < 0) {
+            all = false;
+            continue;
+        }
+        m.tags[i] = static_cast<int32_t>(row);
+        if (!seen[row]) {
+            seen[row] = 1;
+            m.rows_matched++;
+        }
+    }
+    m.all_tips = all;
+    return m;
+}
+
+BPTree BPTree::shear_matched(const TipMatch &m) const {
+    const uint32_t n = size();
+    std::vector<uint8_t> mask(n, 0);
+    std::vector<uint32_t> parent(n, UINT32_MAX);
+    std::vector<uint32_t> stack;
+    stack.reserve(64);
+    for (uint32_t i = 0; i < n; i++) {
+        if (open[i]) {
+            parent[i] = stack.empty() ? UINT32_MAX : stack.back();
+            stack.push_back(i);
+        } else if (!stack.empty()) {
+            stack.pop_back();
+        }
+    }
+    for (uint32_t i = 0; i + 1 < n; i++) {
+        if (m.tags[i] < 0) continue;
+        mask[i] = mask[i + 1] = 1;
+        for (uint32_t p = parent[i]; p != UINT32_MAX && !mask[p]; p = parent[p]) mask[p] = mask[match[p]] = 1;
+    }
+    return masked(mask, length, &m.tags);
+}
+
+bool BPTree::has_single_child() const {
+    const uint32_t n = size();
+    for (uint32_t cur = 1; cur < n; cur++) {
+        if (!open[cur] || leaf(cur)) continue;
+        if (cur + 1 == match[match[cur] - 1]) return true;  // first child is also the last
+    }
+    return false;
+}
+
 BPTree BPTree::shear_to(const NameMap &obs, uint32_t n_obs, uint32_t *n_rows_matched) const {
     const uint32_t n = size();
     std::vector<uint8_t> mask(n, 0);
@@ -241,7 +297,7 @@ BPTree BPTree::shear(const NameSet &keep) const {
     return masked(mask, length);
 }
 
-BPTree BPTree::collapse() const {
+BPTree BPTree::collapse(const std::vector<int32_t> *tags) const {
     const uint32_t n = size();
     std::vector<uint8_t> mask(n, 0);
     std::vector<double> len(length);
@@ -258,7 +314,7 @@ BPTree BPTree::collapse() const {
         else
             mask[cur] = mask[match[cur]] = 1;
     }
-    return masked(mask, len);
+    return masked(mask, len, tags);
 }
 
 NameSet BPTree::tip_names() const {
@@ -367,8 +423,9 @@ FlatTree flatten(const BPTree &t, const NameIndex &obs_index, bool bypass_tips) 
     });
 }
 
-FlatTree flatten(const BPTree &t, bool bypass_tips) {
-    return flatten_impl(t, bypass_tips, [&](uint32_t o) -> int32_t { return t.tag.empty() ? -1 : t.tag[o]; });
+FlatTree flatten(const BPTree &t, bool bypass_tips, const std::vector<int32_t> *tags) {
+    const std::vector<int32_t> &tg = tags ? *tags : t.tag;
+    return flatten_impl(t, bypass_tips, [&](uint32_t o) -> int32_t { return tg.empty() ? -1 : tg[o]; });
 }
 
 uint32_t table_embedded(const FlatTree &f, const std::vector<int32_t> &obs_row, bool bypass_tips,

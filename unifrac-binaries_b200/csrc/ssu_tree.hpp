@@ -19,6 +19,19 @@ namespace ssu {
 using NameSet = std::unordered_set<std::string_view>;
 using NameIndex = std::unordered_map<std::string_view, uint32_t>;
 
+struct BPTree;
+
+// The tips of a tree matched against a table's observation names, computed
+// once per call and shared by validation and the shear: tags[i] = table row of
+// the tip opening at i (-1 for unmatched tips and internal nodes).
+struct TipMatch {
+    std::vector<int32_t> tags;
+    uint32_t rows_matched = 0;  // distinct table rows some tip carries
+    bool all_tips = false;      // every tip matched: the shear keeps the whole tree
+    const uint8_t *tree_id = nullptr;  // the tree it was computed for
+    uint32_t tree_size = 0;
+};
+
 // A rooted tree in balanced-parentheses form.  open[i] is true for '(' and
 // the length and name of a node live at its opening index, as the
 // reference's BPTree (src/tree.hpp:21-153).  match[i] pairs every
@@ -54,9 +67,16 @@ struct BPTree {
     // to its row): kept tips are tagged with their row.  *n_rows_matched, when
     // given, receives how many distinct rows some tip carries.
     BPTree shear_to(const NameMap &obs, uint32_t n_obs, uint32_t *n_rows_matched) const;
+    // Tips against a table's names (obs: name -> row).
+    TipMatch match_tips(const NameMap &obs, uint32_t n_obs) const;
+    // shear_to with the tips already matched; `m` must not be all_tips.
+    BPTree shear_matched(const TipMatch &m) const;
     // Remove non-root nodes with a single child, adding their length to the
-    // child, in preorder (src/tree.cpp:165-191).
-    BPTree collapse() const;
+    // child, in preorder (src/tree.cpp:165-191).  `tags` (default: the
+    // tree's own) are carried to the result.
+    BPTree collapse(const std::vector<int32_t> *tags = nullptr) const;
+    // Whether collapse() would change the tree.
+    bool has_single_child() const;
     // The parentheses flagged in `keep`, with `lengths` (and `tags`, or this
     // tree's own tags) carried along.
     BPTree masked(const std::vector<uint8_t> &keep, const std::vector<double> &lengths,
@@ -86,8 +106,9 @@ struct FlatTree {
 };
 
 FlatTree flatten(const BPTree &tree, const NameIndex &obs_index, bool bypass_tips);
-// Flatten a tree whose tips carry table rows in `tag` (from shear_to).
-FlatTree flatten(const BPTree &tree, bool bypass_tips);
+// Flatten a tree whose tips carry table rows in `tag` (from shear_to), or in
+// `tags` when given.
+FlatTree flatten(const BPTree &tree, bool bypass_tips, const std::vector<int32_t> *tags = nullptr);
 
 // Embedded node count of the tree sheared to the observations o with
 // obs_row[o] >= 0 and then collapsed, computed on a flattened tree of a
