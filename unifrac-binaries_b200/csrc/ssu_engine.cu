@@ -278,6 +278,7 @@ struct PlanImpl {
     bool nonneg_data = true;  // no negative count in any table
     unsigned long long *d_masks = nullptr;
     uint32_t *d_counts = nullptr, *d_dense_rows = nullptr, *d_sparse_rows = nullptr, *d_nrows = nullptr;
+    uint8_t *d_row_class = nullptr;
     double *d_Ws = nullptr, *d_ws_part = nullptr, *d_hpartial = nullptr;
     int *d_flags = nullptr;
     size_t hpartial_bytes = 0;
@@ -657,6 +658,7 @@ int PlanImpl::setup_hybrid() {
     const uint64_t words = ld / 64;
     SSU_CK(alloc(&d_masks, sizeof(unsigned long long) * std::max<uint64_t>(static_cast<uint64_t>(E) * words, 1)));
     SSU_CK(alloc(&d_counts, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
+    SSU_CK(alloc(&d_row_class, std::max<uint32_t>(E, 1)));
     SSU_CK(alloc(&d_dense_rows, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
     SSU_CK(alloc(&d_sparse_rows, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
     SSU_CK(alloc(&d_nrows, sizeof(uint32_t) * 2));
@@ -714,7 +716,7 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
         launches++;
     }
     dev::classify_rows_kernel<<<1, 1024, 0, s>>>(d_counts, E, static_cast<uint32_t>(g.ld / hybrid_div),
-                                                 d_dense_rows, d_sparse_rows, d_nrows);
+                                                 d_dense_rows, d_sparse_rows, d_row_class, d_nrows);
     launches++;
     {
         dim3 grid(static_cast<uint32_t>((g.ld + 255) / 256), n_parts);
@@ -734,7 +736,8 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
     h.U = U;
     h.len = static_cast<const T *>(d_len);
     h.masks = d_masks;
-    h.words = words;
+    h.row_class = d_row_class;
+    h.E = E;
     h.ld = g.ld;
     h.dense_rows = d_dense_rows;
     h.sparse_rows = d_sparse_rows;

@@ -19,7 +19,8 @@
 // flagged and recomputed exactly (all nodes, |a - b| form) by the dense pair
 // kernel afterwards.
 //
-// Presence masks: bit i of masks[e * words + w] is U[e][64 w + i] > 0.
+// Presence masks, word-major: bit i of masks[w * E + e] is U[e][64 w + i] > 0,
+// so the masks of consecutive rows for one 64-column word are contiguous.
 #pragma once
 
 #include <cstdint>
@@ -30,8 +31,8 @@
 namespace ssu {
 namespace dev {
 
-// Presence masks and non-zero counts of the embedded rows; one warp per
-// (row, 64-column word).  counts must start at zero.
+// Presence masks (word-major) and non-zero counts of the embedded rows; one
+// warp per (row, 64-column word).  counts must start at zero.
 template <typename T>
 __global__ void row_masks_kernel(const T *__restrict__ U, uint32_t E, uint64_t ld,
                                  unsigned long long *__restrict__ masks, uint32_t *__restrict__ counts) {
@@ -46,7 +47,7 @@ __global__ void row_masks_kernel(const T *__restrict__ U, uint32_t E, uint64_t l
         const uint32_t b0 = __ballot_sync(0xffffffffu, u[lane] > T(0));
         const uint32_t b1 = __ballot_sync(0xffffffffu, u[lane + 32] > T(0));
         if (lane == 0) {
-            masks[item] = static_cast<unsigned long long>(b0) | (static_cast<unsigned long long>(b1) << 32);
+            masks[w * E + e] = static_cast<unsigned long long>(b0) | (static_cast<unsigned long long>(b1) << 32);
             const uint32_t c = __popc(b0) + __popc(b1);
             if (c) atomicAdd(counts + e, c);
         }
@@ -54,10 +55,12 @@ __global__ void row_masks_kernel(const T *__restrict__ U, uint32_t E, uint64_t l
 }
 
 // Rows in order into dense (count > threshold) and sparse (0 < count <=
-// threshold) lists; one CTA of 1024 threads.  n_out = {dense, sparse}.
+// threshold) lists, and each row's class (0 all zero, 1 sparse, 2 dense);
+// one CTA of 1024 threads.  n_out = {dense, sparse}.
 static __global__ void __launch_bounds__(1024) classify_rows_kernel(const uint32_t *__restrict__ counts, uint32_t E,
                                                                     uint32_t threshold, uint32_t *__restrict__ dense,
                                                                     uint32_t *__restrict__ sparse,
+                                                                    uint8_t *__restrict__ row_class,
                                                                     uint32_t *__restrict__ n_out) {
     __shared__ uint32_t warp_base[32][2];
     __shared__ uint32_t run[2];
@@ -69,6 +72,7 @@ static __global__ void __launch_bounds__(1024) classify_rows_kernel(const uint32
         const uint32_t cnt = e < E ? counts[e] : 0;
         const bool is_dense = cnt > threshold;
         const bool is_sparse = cnt > 0 && !is_dense;
+        if (e < E) row_class[e] = is_dense ? 2 : (is_sparse ? 1 : 0);
         const uint32_t bd = __ballot_sync(0xffffffffu, is_dense);
         const uint32_t bs = __ballot_sync(0xffffffffu, is_sparse);
         if (lane == 0) {
@@ -120,8 +124,9 @@ struct HybridArgs {
     const TableDesc *tables;
     const T *U;
     const T *len;        // per embedded row
-    const unsigned long long *masks;
-    uint64_t words;      // ld / 64
+    const unsigned long long *masks;  // word-major, E rows per word
+    const uint8_t *row_class;         // 0 zero, 1 sparse, 2 dense
+    uint32_t E;          // embedded rows
     uint64_t ld;
     const uint32_t *dense_rows, *sparse_rows;
     const uint32_t *n_rows;  // {dense, sparse}
@@ -174,16 +179,14 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
 
     const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
     const int lane = tid & 31, warp = tid >> 5;
-    const uint32_t n_dense = a.n_rows[0], n_sparse = a.n_rows[1];
+    const uint32_t n_dense = a.n_rows[0];
     const uint32_t n_work = a.n_tiles * a.n_splits;
     for (uint32_t w = blockIdx.x; w < n_work; w += gridDim.x) {
         const uint32_t split = w / a.n_tiles, ti = w - split * a.n_tiles;
         const uint4 tile = a.tiles[ti];
         const uint32_t k0 = tile.x * HB, l0 = tile.y * HB;
         const uint32_t dr = (n_dense + a.n_splits - 1) / a.n_splits;
-        const uint32_t sr = (n_sparse + a.n_splits - 1) / a.n_splits;
         const uint32_t d_begin = min(n_dense, split * dr), d_end = min(n_dense, d_begin + dr);
-        const uint32_t s_begin = min(n_sparse, split * sr), s_end = min(n_sparse, s_begin + sr);
 
         // Data of row `warp` of a chunk, issued by that warp: both value
         // blocks (PPT 16-byte pieces per lane), the four mask words of the two
@@ -197,11 +200,6 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                 const int q = lane + 32 * m;
                 const uint32_t col = q < CPR / 2 ? k0 + q * VEC : l0 + (q - CPR / 2) * VEC;
                 cp_async16(dst + q * VEC, src + col, ok ? 16 : 0);
-            }
-            if (with_masks && lane < 4) {
-                const uint64_t word = (lane < 2 ? k0 / 64 : l0 / 64) + (lane & 1);
-                cp_async_small<8>(Ms + (st * HKC + warp) * 4 + lane, a.masks + static_cast<uint64_t>(e) * a.words + word,
-                                  ok ? 8 : 0);
             }
             if (lane == 4) cp_async_small<sizeof(T)>(Ls + st * HKC + warp, a.len + e, ok ? (int)sizeof(T) : 0);
         };
@@ -270,51 +268,49 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
         __syncthreads();
 
         // ---- sparse rows: -2 L min(a, b) where both are non-zero.  Each warp
-        // walks the sparse rows on its own (no block barrier), owning tile
-        // rows HROWS warp .. HROWS warp + HROWS - 1.  Per batch of 32 rows,
-        // lane i holds row i's id, mask words and length (fetched one batch
-        // ahead, the ids two); one ballot finds the rows with a non-zero in
-        // both the warp's rows and the l block; their values are gathered
-        // HSLOTS rows at a time (lane r < HROWS: row value r, lane j: columns
-        // j + 32 m) and the updates of row r take its value from lane r by
-        // shuffle.
+        // walks the embedded rows on its own (no block barrier) in batches of
+        // 32 consecutive rows, owning tile rows HROWS warp .. HROWS warp +
+        // HROWS - 1.  Lane i holds row i's class, mask words (its rows' word
+        // and the two words of the l block, coalesced over the batch) and
+        // length, fetched two batches ahead.  One ballot finds the sparse rows
+        // with a non-zero in both the warp's rows and the l block; their values
+        // are gathered HSLOTS rows at a time (lane r < HROWS: row value r,
+        // lane j: columns j + 32 m) and the updates of row r take its value
+        // from lane r by shuffle.
         {
             const uint64_t kwd = k0 / 64 + (warp * HROWS) / 64, lwd = l0 / 64;
             const int kshift = (warp * HROWS) % 64;
             constexpr uint32_t kmask = (1u << HROWS) - 1u;
             double *Mw = Mt + HROWS * warp * HB;
-            const uint32_t n_batches = s_end > s_begin ? (s_end - s_begin + 31) / 32 : 0;
-            auto row_id = [&](uint32_t batch) -> uint32_t {
-                const uint32_t i = s_begin + batch * 32 + lane;
-                return (batch < n_batches && i < s_end) ? a.sparse_rows[i] : 0u;
+            const uint32_t er = (a.E + a.n_splits - 1) / a.n_splits;
+            const uint32_t r_begin = min(a.E, split * er), r_end = min(a.E, r_begin + er);
+            const uint32_t n_batches = r_end > r_begin ? (r_end - r_begin + 31) / 32 : 0;
+            const unsigned long long *mk_base = a.masks + kwd * a.E;
+            const unsigned long long *m0_base = a.masks + lwd * a.E;
+            const unsigned long long *m1_base = a.masks + (lwd + 1) * a.E;
+            struct Fetch {
+                unsigned long long km, m0, m1;
+                double L;
+                bool ok;
             };
-            uint32_t e_cur = row_id(0), e_next = row_id(1);
-            bool ok_cur = s_begin + lane < s_end;
-            unsigned long long km_cur = 0, m0_cur = 0, m1_cur = 0;
-            double L_cur = 0.0;
-            if (ok_cur) {
-                const unsigned long long *mp = a.masks + static_cast<uint64_t>(e_cur) * a.words;
-                km_cur = mp[kwd];
-                m0_cur = mp[lwd];
-                m1_cur = mp[lwd + 1];
-                L_cur = static_cast<double>(a.len[e_cur]);
-            }
-            for (uint32_t b = 0; b < n_batches; b++) {
-                // fetch the next batch (masks through the ids already held)
-                const bool ok_next = b + 1 < n_batches && s_begin + (b + 1) * 32 + lane < s_end;
-                unsigned long long km_next = 0, m0_next = 0, m1_next = 0;
-                double L_next = 0.0;
-                if (ok_next) {
-                    const unsigned long long *mp = a.masks + static_cast<uint64_t>(e_next) * a.words;
-                    km_next = mp[kwd];
-                    m0_next = mp[lwd];
-                    m1_next = mp[lwd + 1];
-                    L_next = static_cast<double>(a.len[e_next]);
+            auto fetch = [&](uint32_t batch) {
+                Fetch f{0ull, 0ull, 0ull, 0.0, false};
+                const uint32_t e = r_begin + batch * 32 + lane;
+                if (batch < n_batches && e < r_end && a.row_class[e] == 1) {
+                    f.km = mk_base[e];
+                    f.m0 = m0_base[e];
+                    f.m1 = m1_base[e];
+                    f.L = static_cast<double>(a.len[e]);
+                    f.ok = true;
                 }
-                const uint32_t e_after = row_id(b + 2);
-
-                const uint32_t mk_l = static_cast<uint32_t>(km_cur >> kshift) & kmask;
-                uint32_t active = __ballot_sync(0xffffffffu, ok_cur && mk_l != 0 && (m0_cur | m1_cur) != 0ull);
+                return f;
+            };
+            Fetch cur = fetch(0), nxt = fetch(1);
+            for (uint32_t b = 0; b < n_batches; b++) {
+                const Fetch after = fetch(b + 2);
+                const uint32_t e_cur = r_begin + b * 32 + lane;
+                const uint32_t mk_l = static_cast<uint32_t>(cur.km >> kshift) & kmask;
+                uint32_t active = __ballot_sync(0xffffffffu, cur.ok && mk_l != 0 && (cur.m0 | cur.m1) != 0ull);
                 while (active) {
                     int slot_lane[HSLOTS];
                     int cnt = 0;
@@ -330,8 +326,8 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                         const int c = slot_lane[j];
                         const uint32_t e = __shfl_sync(0xffffffffu, e_cur, c);
                         const uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
-                        const unsigned long long m0 = __shfl_sync(0xffffffffu, m0_cur, c);
-                        const unsigned long long m1 = __shfl_sync(0xffffffffu, m1_cur, c);
+                        const unsigned long long m0 = __shfl_sync(0xffffffffu, cur.m0, c);
+                        const unsigned long long m1 = __shfl_sync(0xffffffffu, cur.m1, c);
                         const T *row = a.U + static_cast<uint64_t>(e) * a.ld;
                         const bool live = j < cnt;
                         va[j] = (live && lane < HROWS && ((mk >> lane) & 1u))
@@ -348,7 +344,7 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                         if (j < cnt) {
                             const int c = slot_lane[j];
                             uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
-                            const double L2 = -2.0 * __shfl_sync(0xffffffffu, L_cur, c);
+                            const double L2 = -2.0 * __shfl_sync(0xffffffffu, cur.L, c);
                             while (mk) {
                                 const int r = __ffs(mk) - 1;
                                 mk &= mk - 1;
@@ -364,13 +360,8 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                         }
                     }
                 }
-                e_cur = e_next;
-                e_next = e_after;
-                ok_cur = ok_next;
-                km_cur = km_next;
-                m0_cur = m0_next;
-                m1_cur = m1_next;
-                L_cur = L_next;
+                cur = nxt;
+                nxt = after;
             }
         }
         __syncthreads();
