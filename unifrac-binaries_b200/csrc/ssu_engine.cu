@@ -744,7 +744,6 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
     h.E = E;
     h.ld = g.ld;
     h.dense_rows = d_dense_rows;
-    h.sparse_rows = d_sparse_rows;
     h.n_rows = d_nrows;
     h.W = static_cast<const T *>(d_W);
     h.Ws = d_Ws;

@@ -128,7 +128,7 @@ struct HybridArgs {
     const uint8_t *row_class;         // 0 zero, 1 sparse, 2 dense
     uint32_t E;          // embedded rows
     uint64_t ld;
-    const uint32_t *dense_rows, *sparse_rows;
+    const uint32_t *dense_rows;
     const uint32_t *n_rows;  // {dense, sparse}
     const T *W;          // full one-sided sums (normalized)
     const double *Ws;    // one-sided sums over the sparse rows
@@ -148,7 +148,7 @@ constexpr int HSLOTS = 4;           // active rows gathered together per warp
 
 template <typename T>
 constexpr size_t hybrid_smem() {
-    return sizeof(double) * HB * HB + HSTAGES * (sizeof(T) * HKC * 2 * HB + 8 * 4 * HKC + sizeof(T) * HKC) + 64;
+    return sizeof(double) * HB * HB + HSTAGES * (sizeof(T) * HKC * 2 * HB + sizeof(T) * HKC) + 64;
 }
 
 // Epilogue of one element: value from the raw sum x = D - 2 M.
@@ -174,8 +174,7 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *Mt = reinterpret_cast<double *>(smem_raw);                                      // [128][128]
     T *Vs = reinterpret_cast<T *>(Mt + HB * HB);                                            // [S][HKC][256]
-    unsigned long long *Ms = reinterpret_cast<unsigned long long *>(Vs + HSTAGES * HKC * 2 * HB);  // [S][HKC][4]
-    T *Ls = reinterpret_cast<T *>(Ms + HSTAGES * HKC * 4);                                   // [S][HKC]
+    T *Ls = Vs + HSTAGES * HKC * 2 * HB;                                                    // [S][HKC]
 
     const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
     const int lane = tid & 31, warp = tid >> 5;
@@ -189,9 +188,9 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
         const uint32_t d_begin = min(n_dense, split * dr), d_end = min(n_dense, d_begin + dr);
 
         // Data of row `warp` of a chunk, issued by that warp: both value
-        // blocks (PPT 16-byte pieces per lane), the four mask words of the two
-        // blocks and the length.  `e` is the row id, `ok` whether it exists.
-        auto load_row = [&](int st, uint32_t e, bool ok, bool with_masks) {
+        // blocks (PPT 16-byte pieces per lane) and the length.  `e` is the row
+        // id, `ok` whether it exists.
+        auto load_row = [&](int st, uint32_t e, bool ok) {
             if (warp >= HKC) return;
             T *dst = Vs + (st * HKC + warp) * 2 * HB;
             const T *src = a.U + static_cast<uint64_t>(e) * a.ld;
@@ -206,7 +205,7 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
         // Ring of HSTAGES chunks over rows [begin, end) of `rows`: chunk c is
         // issued HSTAGES - 1 iterations before it is consumed; each warp keeps
         // the row ids of its next two chunks in registers.
-        auto stream_rows = [&](const uint32_t *rows, uint32_t begin, uint32_t end, bool with_masks, auto consume) {
+        auto stream_rows = [&](const uint32_t *rows, uint32_t begin, uint32_t end, auto consume) {
             const uint32_t n_chunks = end > begin ? (end - begin + HKC - 1) / HKC : 0;
             if (n_chunks == 0) return;
             auto id_of = [&](uint32_t chunk) -> uint32_t {
@@ -217,13 +216,13 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                 return warp < HKC && chunk < n_chunks && begin + chunk * HKC + warp < end;
             };
             for (uint32_t c = 0; c + 1 < HSTAGES; c++) {
-                if (c < n_chunks) load_row(static_cast<int>(c), id_of(c), ok_of(c), with_masks);
+                if (c < n_chunks) load_row(static_cast<int>(c), id_of(c), ok_of(c));
                 cp_async_commit();
             }
             uint32_t id1 = id_of(HSTAGES - 1), id2 = id_of(HSTAGES);
             for (uint32_t ch = 0; ch < n_chunks; ch++) {
                 const uint32_t nxt = ch + HSTAGES - 1;
-                if (nxt < n_chunks) load_row(static_cast<int>(nxt % HSTAGES), id1, ok_of(nxt), with_masks);
+                if (nxt < n_chunks) load_row(static_cast<int>(nxt % HSTAGES), id1, ok_of(nxt));
                 cp_async_commit();
                 id1 = id2;
                 id2 = id_of(ch + HSTAGES + 1);
@@ -241,7 +240,7 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
         for (int i = 0; i < TM; i++)
 #pragma unroll
             for (int j = 0; j < TN; j++) acc[i][j] = 0.0;
-        stream_rows(a.dense_rows, d_begin, d_end, false, [&](int st) {
+        stream_rows(a.dense_rows, d_begin, d_end, [&](int st) {
             const T *vs = Vs + st * HKC * 2 * HB;
 #pragma unroll 2
             for (int c = 0; c < HKC; c++) {

@@ -325,20 +325,6 @@ NameSet BPTree::tip_names() const {
     return out;
 }
 
-uint32_t BPTree::count_matched(const NameMap &obs, uint32_t n_obs) const {
-    std::vector<uint8_t> seen(n_obs, 0);
-    uint32_t matched = 0;
-    for (uint32_t i = 0; i + 1 < size(); i++) {
-        if (!leaf(i)) continue;
-        const int64_t row = obs.find(name[i]);
-        if (row >= 0 && !seen[row]) {
-            seen[row] = 1;
-            matched++;
-        }
-    }
-    return matched;
-}
-
 uint32_t BPTree::n_tips() const {
     uint32_t c = 0;
     for (uint32_t i = 0; i + 1 < size(); i++) c += leaf(i);

@@ -83,8 +83,6 @@ struct BPTree {
                   const std::vector<int32_t> *tags = nullptr) const;
 
     NameSet tip_names() const;
-    // Distinct rows of `obs` that some tip's name maps to.
-    uint32_t count_matched(const NameMap &obs, uint32_t n_obs) const;
     uint32_t n_tips() const;
 };
 
