@@ -315,3 +315,44 @@ def test_weighted_sparse_and_dense_forms_agree(ssu, monkeypatch, method, prec):
         check_fp64(hybrid, dense)
     else:
         np.testing.assert_allclose(hybrid, dense, rtol=5e-6, atol=1e-7)
+
+
+UNION_RUNS = [("generalized", False, 0.5), ("generalized", False, 0.0), ("generalized", False, 1.0),
+              ("generalized", False, 0.25), ("unweighted", True, 1.0), ("unweighted_unnormalized", True, 1.0),
+              ("weighted_normalized", True, 1.0), ("weighted_unnormalized", True, 1.0),
+              ("generalized", True, 0.5), ("generalized", True, 0.25)]
+
+
+@pytest.mark.parametrize("method,vaw,alpha", UNION_RUNS)
+def test_union_and_dense_forms_agree(ssu, oracle_mod, monkeypatch, method, vaw, alpha):
+    """Generalized and variance-adjusted fp64 pairs summed over the union of
+    the two supports (sparse rows) equal the dense form and the oracle; the
+    small table splits the node range (split partials + finalize)."""
+    tree, table = _case(63, n_tips=400, n_samples=260, density=0.03)
+    kw = dict(variance_adjust=vaw, alpha=alpha)
+    plan = ssu.Plan(tree, table, method + "_fp64", **kw)
+    assert plan.pair_kernel().startswith("pair_union")
+    plan.close()
+    union, _ = ssu.one_off_matrix(tree, table, method + "_fp64", **kw)
+    monkeypatch.setenv("UNIFRAC_B200_UNION_MODE", "dense")
+    plan = ssu.Plan(tree, table, method + "_fp64", **kw)
+    assert plan.pair_kernel().startswith("pair_values")
+    plan.close()
+    dense, _ = ssu.one_off_matrix(tree, table, method + "_fp64", **kw)
+    check_fp64(union, dense)
+    check_fp64(union, oracle_mod.oracle_one_off(tree, table, method + "_fp64", **kw)["matrix"])
+
+
+@pytest.mark.parametrize("div", ["1", "4", "1000000"])
+def test_union_row_classes_do_not_change_results(ssu, oracle_mod, monkeypatch, div):
+    """All rows dense, the default split, and all rows sparse give the same
+    matrix; stripe windows go through the same kernel."""
+    tree, table = _case(64, n_tips=300, n_samples=150, density=0.05)
+    monkeypatch.setenv("UNIFRAC_B200_UNION_DIV", div)
+    kw = dict(variance_adjust=True, alpha=0.5)
+    ref = oracle_mod.oracle_one_off(tree, table, "generalized_fp64", **kw)["matrix"]
+    gpu, _ = ssu.one_off_matrix(tree, table, "generalized_fp64", **kw)
+    check_fp64(gpu, ref)
+    stripes, _ = ssu.partial(tree, table, "generalized_fp64", 10, 40, **kw)
+    check_fp64(stripes, oracle_mod.oracle_one_off(tree, table, "generalized_fp64", stripe_start=10, stripe_stop=40,
+                                                  **kw)["stripes"])

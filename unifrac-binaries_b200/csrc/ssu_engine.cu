@@ -18,6 +18,7 @@
 #include "ssu_kernels.cuh"
 #include "ssu_pairs.cuh"
 #include "ssu_sparse.cuh"
+#include "ssu_union.cuh"
 
 namespace ssu {
 
@@ -287,6 +288,20 @@ struct PlanImpl {
     template <typename T>
     int hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &out, const uint4 *tiles, uint32_t ntiles,
                      uint32_t splits, bool last);
+    // generalized and variance-adjusted methods over the union of the two
+    // samples' supports (same masks and row classes as the hybrid)
+    bool union_mode = false;
+    uint32_t union_div = 4;  // rows non-zero in more than ld / union_div columns are dense
+    double *d_upartial = nullptr;
+    size_t upartial_bytes = 0;
+    int sparse_prep_alloc();
+    template <typename T>
+    int sparse_prep(cudaStream_t s, const Group &g, uint32_t div);
+    template <typename T>
+    int setup_union();
+    template <typename T>
+    int union_stage(cudaStream_t s, const Group &g, const dev::OutSpec &out, const uint4 *tiles, uint32_t ntiles,
+                    uint32_t splits, bool last);
 
     // pair stage
     PairKernel<double> kd;
@@ -451,7 +466,7 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
     if (!budget) {
         if (const char *b = std::getenv("UNIFRAC_B200_GROUP_BYTES")) budget = std::strtoull(b, nullptr, 10);
     }
-    if (!budget) {
+    if (!budget && n_tables > 1) {  // one table is one group whatever the budget
         size_t free_b = 0, total_b = 0;
         SSU_CK(cudaMemGetInfo(&free_b, &total_b));
         const size_t fixed = el * full_elems + 12 * nnz_total;
@@ -465,7 +480,15 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
              (spec.method == Method::weighted_normalized || spec.method == Method::weighted_unnormalized);
     if (const char *m = std::getenv("UNIFRAC_B200_WEIGHTED_MODE"))
         if (std::string(m) == "dense") hybrid = false;
-    if (hybrid) max_cols = std::min<uint64_t>(max_cols, std::max<uint64_t>(8192, (max_table_n + 127) / 128 * 128));
+    // generalized and variance-adjusted methods in fp64: only the union of
+    // the two samples' supports adds to a pair (needs u >= 0 so presence is
+    // u > 0).  In fp32 the dense kernels' single-precision terms are faster.
+    union_mode = spec.fp64 && !faith && !gemm && nonneg_data && set.row_active.empty() &&
+                 (spec.vaw || spec.method == Method::generalized);
+    if (const char *m = std::getenv("UNIFRAC_B200_UNION_MODE"))
+        if (std::string(m) == "dense") union_mode = false;
+    if (hybrid || union_mode)
+        max_cols = std::min<uint64_t>(max_cols, std::max<uint64_t>(8192, (max_table_n + 127) / 128 * 128));
     groups.clear();
     uint64_t cols = 0;
     for (uint32_t t = 0; t < n_tables; t++) {
@@ -634,6 +657,8 @@ int PlanImpl::setup_method() {
         // the exact recomputation of flagged tiles runs the 128 x 128 shape
         chosen = 0;
         tuning = "sparse hybrid";
+    } else if (union_mode) {
+        tuning = "sparse union";
     } else if (cands.size() > 1 && autotune == 1) {
         const int rc = tune<T>(cands, chosen);
         if (rc) return rc;
@@ -641,6 +666,7 @@ int PlanImpl::setup_method() {
     kern<T>() = cands[chosen];
     const PairKernel<T> &k = kern<T>();
     if (hybrid) return setup_hybrid<T>();
+    if (union_mode) return setup_union<T>();
 
     partial_bytes = 0;
     for (Group &g : groups) {
@@ -659,13 +685,7 @@ int PlanImpl::setup_method() {
 template <typename T>
 int PlanImpl::setup_hybrid() {
     hybrid_div = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_HYBRID_DIV", 8)));
-    const uint64_t words = ld / 64;
-    SSU_CK(alloc(&d_masks, sizeof(unsigned long long) * std::max<uint64_t>(static_cast<uint64_t>(E) * words, 1)));
-    SSU_CK(alloc(&d_counts, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
-    SSU_CK(alloc(&d_row_class, std::max<uint32_t>(E, 1)));
-    SSU_CK(alloc(&d_dense_rows, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
-    SSU_CK(alloc(&d_sparse_rows, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
-    SSU_CK(alloc(&d_nrows, sizeof(uint32_t) * 2));
+    if (const int rc = sparse_prep_alloc()) return rc;
     SSU_CK(alloc(&d_Ws, sizeof(double) * ld));
     part_chunk = part_chunk ? part_chunk : 512;
     n_parts = std::max<uint32_t>(1, (E + part_chunk - 1) / part_chunk);
@@ -711,17 +731,7 @@ template <typename T>
 int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &out, const uint4 *tiles,
                            uint32_t ntiles, uint32_t splits, bool last) {
     const T *U = static_cast<const T *>(d_U);
-    const uint64_t words = g.ld / 64;
-    SSU_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * std::max<uint32_t>(E, 1), s));
-    if (E) {
-        const uint64_t items = static_cast<uint64_t>(E) * words;
-        const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((items + 7) / 8, 1u << 20));
-        dev::row_masks_kernel<T><<<grid, 256, 0, s>>>(U, E, g.ld, d_masks, d_counts);
-        launches++;
-    }
-    dev::classify_rows_kernel<<<1, 1024, 0, s>>>(d_counts, E, static_cast<uint32_t>(g.ld / hybrid_div),
-                                                 d_dense_rows, d_sparse_rows, d_row_class, d_nrows);
-    launches++;
+    if (const int rc = sparse_prep<T>(s, g, hybrid_div)) return rc;
     {
         dim3 grid(static_cast<uint32_t>((g.ld + 255) / 256), n_parts);
         dev::sparse_sums_partial_kernel<T><<<grid, 256, 0, s>>>(U, static_cast<const T *>(d_len), d_sparse_rows,
@@ -791,6 +801,107 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
              k.smem, s);
     launches++;
     SSU_CK(cudaGetLastError());
+    return 0;
+}
+
+// Buffers of the per-call row classification shared by the hybrid and union
+// paths: word-major presence masks, non-zero counts, classes, row lists.
+int PlanImpl::sparse_prep_alloc() {
+    const uint64_t words = ld / 64;
+    SSU_CK(alloc(&d_masks, sizeof(unsigned long long) * std::max<uint64_t>(static_cast<uint64_t>(E) * words, 1)));
+    SSU_CK(alloc(&d_counts, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
+    SSU_CK(alloc(&d_row_class, std::max<uint32_t>(E, 1)));
+    SSU_CK(alloc(&d_dense_rows, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
+    SSU_CK(alloc(&d_sparse_rows, sizeof(uint32_t) * std::max<uint32_t>(E, 1)));
+    SSU_CK(alloc(&d_nrows, sizeof(uint32_t) * 2));
+    return 0;
+}
+
+// Masks and counts of the group's embedding, then the row classes (dense:
+// non-zero in more than ld / div columns).
+template <typename T>
+int PlanImpl::sparse_prep(cudaStream_t s, const Group &g, uint32_t div) {
+    const T *U = static_cast<const T *>(d_U);
+    const uint64_t words = g.ld / 64;
+    SSU_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * std::max<uint32_t>(E, 1), s));
+    if (E) {
+        const uint64_t items = static_cast<uint64_t>(E) * words;
+        const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((items + 7) / 8, 1u << 20));
+        dev::row_masks_kernel<T><<<grid, 256, 0, s>>>(U, E, g.ld, d_masks, d_counts);
+        launches++;
+    }
+    dev::classify_rows_kernel<<<1, 1024, 0, s>>>(d_counts, E, static_cast<uint32_t>(g.ld / div), d_dense_rows,
+                                                 d_sparse_rows, d_row_class, d_nrows);
+    launches++;
+    SSU_CK(cudaGetLastError());
+    return 0;
+}
+
+template <typename T>
+int PlanImpl::setup_union() {
+    union_div = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_UNION_DIV", 4)));
+    if (const int rc = sparse_prep_alloc()) return rc;
+    size_t smem = 0;
+    SSU_CK(dev::union_configure<T>(spec, &smem));
+    upartial_bytes = 0;
+    for (Group &g : groups) {
+        std::vector<uint4> tiles;
+        for (uint32_t t = g.t0; t < g.t1; t++)
+            append_tiles(tiles, t, tdesc[t].base, tdesc[t].n, dev::UK, dev::UL, false, 0, 0);
+        g.n_tiles = static_cast<uint32_t>(tiles.size());
+        SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * tiles.size()));
+        // node splits so the tiles fill the SMs (one CTA per SM)
+        uint32_t best_s = 1;
+        double best = 1e300;
+        const uint32_t max_s = std::max<uint32_t>(1, std::min<uint32_t>(64, E / 128));
+        for (uint32_t sp = 1; sp <= max_s; sp++) {
+            const double cost = std::ceil(static_cast<double>(g.n_tiles) * sp / n_sms) / sp * (1.0 + 0.02 * (sp - 1));
+            if (cost < best - 1e-12) {
+                best = cost;
+                best_s = sp;
+            }
+        }
+        g.splits = best_s;
+        if (g.splits > 1)
+            upartial_bytes =
+                std::max(upartial_bytes, sizeof(double) * 2 * dev::UK * dev::UL * g.n_tiles * g.splits);
+    }
+    if (upartial_bytes) SSU_CK(alloc(&d_upartial, upartial_bytes));
+    return 0;
+}
+
+// Union pair stage of one group (its embedding ready): row classes, then the
+// union tile kernel (+ split finalize).
+template <typename T>
+int PlanImpl::union_stage(cudaStream_t s, const Group &g, const dev::OutSpec &out, const uint4 *tiles,
+                          uint32_t ntiles, uint32_t splits, bool last) {
+    if (const int rc = sparse_prep<T>(s, g, union_div)) return rc;
+    if (ntiles == 0) return 0;
+    dev::UnionArgs<T> u{};
+    u.tiles = tiles;
+    u.n_tiles = ntiles;
+    u.n_splits = std::max<uint32_t>(splits, 1);
+    if (u.n_splits > 1 && sizeof(double) * 2 * dev::UK * dev::UL * ntiles * u.n_splits > upartial_bytes)
+        u.n_splits = 1;
+    u.tables = d_tdesc;
+    u.U = static_cast<const T *>(d_U);
+    u.C = static_cast<const T *>(d_C);
+    u.tot = static_cast<const T *>(g.d_tot);
+    u.len = static_cast<const T *>(d_len);
+    u.masks = d_masks;
+    u.row_class = d_row_class;
+    u.E = E;
+    u.ld = g.ld;
+    u.dense_rows = d_dense_rows;
+    u.n_rows = d_nrows;
+    u.alpha = spec.alpha;
+    u.partial = u.n_splits > 1 ? d_upartial : nullptr;
+    u.out = out;
+    const uint32_t ctas = static_cast<uint32_t>(
+        std::min<uint64_t>(static_cast<uint64_t>(ntiles) * u.n_splits, static_cast<uint64_t>(n_sms)));
+    SSU_CK(dev::union_launch<T>(spec, u, ctas, s));
+    launches += u.partial ? 2 : 1;
+    if (last && timed()) SSU_CK(cudaEventRecord(ev[2], s));
     return 0;
 }
 
@@ -1004,7 +1115,8 @@ int PlanImpl::execute_T(cudaStream_t s, const dev::OutSpec &out) {
         if (!rc) rc = prepare<T>(s, g);
         if (rc) return rc;
         if (gi == 0 && timed()) SSU_CK(cudaEventRecord(ev[1], s));
-        rc = hybrid ? hybrid_stage<T>(s, g, out, g.d_tiles, g.n_tiles, g.splits, gi + 1 == groups.size())
+        rc = union_mode ? union_stage<T>(s, g, out, g.d_tiles, g.n_tiles, g.splits, gi + 1 == groups.size())
+             : hybrid ? hybrid_stage<T>(s, g, out, g.d_tiles, g.n_tiles, g.splits, gi + 1 == groups.size())
                     : pair_stage<T>(s, g, out, g.d_tiles, g.n_tiles, g.splits, g.rows_per_split,
                                     gi + 1 == groups.size());
         if (rc) return rc;
@@ -1029,11 +1141,26 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
         return execute_gemm(stream, o);
     }
     const Group &g = groups[0];
-    const int BM = spec.fp64 ? kd.BM : kf.BM, BN = spec.fp64 ? kd.BN : kf.BN;
+    const int BM = union_mode ? dev::UK : spec.fp64 ? kd.BM : kf.BM;
+    const int BN = union_mode ? dev::UL : spec.fp64 ? kd.BN : kf.BN;
     std::vector<uint4> tiles;
     append_tiles(tiles, 0, 0, tdesc[0].n, BM, BN, mode == 1, start, stop);
     uint4 *d_t = nullptr;
     SSU_CK(upload(&d_t, tiles.data(), sizeof(uint4) * tiles.size()));
+    if (union_mode) {
+        dev::OutSpec o{mode, d_out, start, stop};
+        launches = 0;
+        const uint32_t nt = static_cast<uint32_t>(tiles.size());
+        int rc = 0;
+        if (spec.fp64) {
+            rc = embed<double>(stream, g);
+            if (!rc) rc = union_stage<double>(stream, g, o, d_t, nt, 1, true);
+        } else {
+            rc = embed<float>(stream, g);
+            if (!rc) rc = union_stage<float>(stream, g, o, d_t, nt, 1, true);
+        }
+        return rc;
+    }
     if (hybrid) {
         dev::OutSpec o{mode, d_out, start, stop};
         launches = 0;
@@ -1601,6 +1728,7 @@ uint64_t Plan::work_units() const {
 uint32_t Plan::launches() const { return impl_->launches; }
 const char *Plan::pair_kernel_name() const {
     if (impl_->gemm) return "unweighted_tc_kernel";
+    if (impl_->union_mode) return impl_->spec.vaw ? "pair_union<variance_adjusted>" : "pair_union<generalized>";
     if (impl_->hybrid)
         return impl_->spec.method == Method::weighted_normalized ? "pair_hybrid<weighted_normalized>"
                                                                  : "pair_hybrid<weighted_unnormalized>";
