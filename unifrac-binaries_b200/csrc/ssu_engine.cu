@@ -893,6 +893,7 @@ int PlanImpl::union_stage(cudaStream_t s, const Group &g, const dev::OutSpec &ou
     u.E = E;
     u.ld = g.ld;
     u.dense_rows = d_dense_rows;
+    u.sparse_rows = d_sparse_rows;
     u.n_rows = d_nrows;
     u.alpha = spec.alpha;
     u.partial = u.n_splits > 1 ? d_upartial : nullptr;

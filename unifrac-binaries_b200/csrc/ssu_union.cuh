@@ -3,16 +3,20 @@
 // A node adds nothing to a pair where neither sample has it: the VAW weight
 // mi (m - mi) is 0 there (mi = counts of both samples), and so is the
 // generalized u + v.  Per node, only the pairs with the row sample present
-// (row pass: all 64 columns of the tile) or the column sample present (column
-// pass: the rows without it) are evaluated, each with the method's own term -
-// no rearrangement, so the result matches the dense form up to the order of
-// the summation (no cancellation, nothing to recompute).  Rows non-zero in
-// more than ld / div columns run the dense loop in registers first.
+// (row pass: all 64 columns of the tile) or only the column sample present
+// (column pass: the rows without it) are evaluated, each with the method's
+// own term - no rearrangement, so the result matches the dense form up to
+// the order of the summation (no cancellation, nothing to recompute).  Rows
+// non-zero in more than ld / div columns run the dense loop in registers
+// first.
 //
-// Tile: 128 (k) x 64 (l) pairs, 512 threads; fp64 numerator and denominator
-// tiles in shared memory; warp w owns tile rows 8w .. 8w + 7 and updates them
-// in row order, one lane per element (deterministic).  Uses the presence masks
-// and row classes of ssu_sparse.cuh.
+// Tile: 128 (k) x 64 (l) pairs, 512 threads.  Sparse rows stream through a
+// cp.async ring 16 at a time (one row per warp).  Row pass: warp w owns tile
+// rows 8w .. 8w + 7 (fp64 numerator / denominator tiles in shared memory,
+// lanes over columns).  Column pass: warp w owns columns 4w .. 4w + 3 over
+// all 128 rows (registers, lanes over rows).  Every element has one owner
+// per pass, so the sums are deterministic.  Uses the presence masks and row
+// classes of ssu_sparse.cuh.
 #pragma once
 
 #include <cstdint>
@@ -35,7 +39,7 @@ struct UnionArgs {
     const uint8_t *row_class;         // 0 zero, 1 sparse, 2 dense
     uint32_t E;
     uint64_t ld;
-    const uint32_t *dense_rows;
+    const uint32_t *dense_rows, *sparse_rows;
     const uint32_t *n_rows;  // {dense, sparse}
     double alpha;
     double *partial;     // per (split, tile) 2 x 128 x 64 fp64; nullptr: no splits
@@ -46,13 +50,33 @@ constexpr int UK = 128, UL = 64;             // tile: k rows x l columns
 constexpr int UKC = 8;                       // rows per dense pipeline stage
 constexpr int USTAGES = 3;
 constexpr int UTHREADS = 512;
-constexpr int UROWS = UK / (UTHREADS / 32);  // 8 tile rows per warp
-constexpr int USLOTS = 4;                    // active rows gathered together per warp
+constexpr int UWARPS = UTHREADS / 32;
+constexpr int UROWS = UK / UWARPS;           // 8 tile rows per warp (row pass)
+constexpr int UCOLS = UL / UWARPS;           // 4 tile columns per warp (column pass)
+constexpr int USK = UWARPS;                  // sparse rows per stage, one per warp
+
+template <bool CNT>
+__host__ __device__ constexpr int union_sparse_stages() {
+    return CNT ? 2 : 3;
+}
+
+// staged sparse row: k block, l block, 16 bytes of padding (bank spread)
+template <typename T>
+__host__ __device__ constexpr int union_row_pitch() {
+    return UK + UL + 16 / static_cast<int>(sizeof(T));
+}
 
 template <typename T, bool CNT>
-constexpr size_t union_smem() {
-    return 2 * sizeof(double) * UK * UL + USTAGES * (sizeof(T) * UKC * (UK + UL) * (CNT ? 2 : 1) + sizeof(T) * UKC) +
-           64;
+__host__ __device__ constexpr size_t union_stage_bytes() {
+    constexpr size_t dense = USTAGES * (sizeof(T) * UKC * (UK + UL) * (CNT ? 2 : 1) + sizeof(T) * UKC);
+    constexpr size_t sparse = union_sparse_stages<CNT>() *
+                              (sizeof(T) * USK * union_row_pitch<T>() * (CNT ? 2 : 1) + sizeof(T) * USK);
+    return ((dense > sparse ? dense : sparse) + 15) / 16 * 16;
+}
+
+template <typename T, bool CNT>
+__host__ __device__ constexpr size_t union_smem() {
+    return 2 * sizeof(double) * UK * UL + union_stage_bytes<T, CNT>() + (CNT ? sizeof(double) * (UK + UL) : 0);
 }
 
 template <typename T, class Op>
@@ -70,18 +94,27 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
     constexpr bool CNT = Op::COUNTS;
     constexpr int TX = UL / 4, TM = 4, TN = 4;  // dense phase: 16 (l) x 32 (k) threads, 4 x 4 pairs
     constexpr int VEC = 16 / sizeof(T);
-    constexpr int ROW = UK + UL;                // staged values per row: k block then l block
+    constexpr int ROW = UK + UL;                // dense staged values per row: k block then l block
     constexpr int CPR = ROW / VEC;              // 16-byte pieces per staged row
+    constexpr int PITCH = union_row_pitch<T>();
+    constexpr int SST = union_sparse_stages<CNT>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *Mn = reinterpret_cast<double *>(smem_raw);  // [128][64] numerator
     double *Md = Mn + UK * UL;                          // [128][64] denominator
-    T *Vs = reinterpret_cast<T *>(Md + UK * UL);        // [S][UKC][ROW] values
+    unsigned char *stage = reinterpret_cast<unsigned char *>(Md + UK * UL);
+    double *Ts = reinterpret_cast<double *>(stage + union_stage_bytes<T, CNT>());  // [192] column totals
+    // dense phase staging
+    T *Vs = reinterpret_cast<T *>(stage);               // [S][UKC][ROW] values
     T *Cs = Vs + USTAGES * UKC * ROW;                   // [S][UKC][ROW] counts (variance adjusted)
     T *Ls = Cs + (CNT ? USTAGES * UKC * ROW : 0);       // [S][UKC]
+    // sparse phase staging (same bytes)
+    T *Sv = reinterpret_cast<T *>(stage);               // [SST][USK][PITCH] values
+    T *Sc = Sv + SST * USK * PITCH;                     // [SST][USK][PITCH] counts
+    T *Sl = Sc + (CNT ? SST * USK * PITCH : 0);         // [SST][USK]
 
     const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
     const int lane = tid & 31, warp = tid >> 5;
-    const uint32_t n_dense = a.n_rows[0];
+    const uint32_t n_dense = a.n_rows[0], n_sparse = a.n_rows[1];
     const uint32_t n_work = a.n_tiles * a.n_splits;
     for (uint32_t w = blockIdx.x; w < n_work; w += gridDim.x) {
         const uint32_t split = w / a.n_tiles, ti = w - split * a.n_tiles;
@@ -89,6 +122,10 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
         const uint32_t k0 = tile.x * UK, l0 = tile.y * UL;
         const uint32_t dr = (n_dense + a.n_splits - 1) / a.n_splits;
         const uint32_t d_begin = min(n_dense, split * dr), d_end = min(n_dense, d_begin + dr);
+        if (CNT)
+            for (int c = tid; c < UK + UL; c += UTHREADS)
+                Ts[c] = static_cast<double>(a.tot[c < UK ? k0 + c : l0 + (c - UK)]);
+        __syncthreads();
 
         // ---- dense rows, 4 x 4 pairs per thread in registers
         double acc[TM][TN][2];
@@ -98,9 +135,9 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
             for (int j = 0; j < TN; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
         double tkd[TM], tld[TN];
 #pragma unroll
-        for (int i = 0; i < TM; i++) tkd[i] = CNT ? static_cast<double>(a.tot[k0 + tile_row<UK, TM>(ty, i)]) : 0.0;
+        for (int i = 0; i < TM; i++) tkd[i] = CNT ? Ts[tile_row<UK, TM>(ty, i)] : 0.0;
 #pragma unroll
-        for (int j = 0; j < TN; j++) tld[j] = CNT ? static_cast<double>(a.tot[l0 + tile_row<UL, TN>(tx, j)]) : 0.0;
+        for (int j = 0; j < TN; j++) tld[j] = CNT ? Ts[UK + tile_row<UL, TN>(tx, j)] : 0.0;
         {
             // warp r < UKC stages row r of a chunk
             auto load_row = [&](int st, uint32_t e, bool ok) {
@@ -172,136 +209,118 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
             }
         __syncthreads();
 
-        // ---- sparse rows, walked in order by each warp on its own in batches
-        // of 32; lane i holds row i's class, mask words (the warp's rows, the
-        // l block) and length, fetched two batches ahead
+        // ---- sparse rows, 16 per stage
         {
-            const int r0 = UROWS * warp;
-            const uint64_t kwd = k0 / 64 + r0 / 64, lwd = l0 / 64;
-            const int kshift = r0 % 64;
-            constexpr uint32_t kmask = (1u << UROWS) - 1u;
-            double *Wn = Mn + r0 * UL, *Wd = Md + r0 * UL;
-            const double tl0 = CNT ? static_cast<double>(a.tot[l0 + lane]) : 0.0;
-            const double tl1 = CNT ? static_cast<double>(a.tot[l0 + lane + 32]) : 0.0;
-            const double tk_lane = (CNT && lane < UROWS) ? static_cast<double>(a.tot[k0 + r0 + lane]) : 0.0;
-            const uint32_t er = (a.E + a.n_splits - 1) / a.n_splits;
-            const uint32_t e_begin = min(a.E, split * er), e_end = min(a.E, e_begin + er);
-            const uint32_t n_batches = e_end > e_begin ? (e_end - e_begin + 31) / 32 : 0;
-            const unsigned long long *mk_base = a.masks + kwd * a.E;
-            const unsigned long long *ml_base = a.masks + lwd * a.E;
-            struct Fetch {
-                unsigned long long km, ml;
-                double L;
-                bool ok;
-            };
-            auto fetch = [&](uint32_t batch) {
-                Fetch f{0ull, 0ull, 0.0, false};
-                const uint32_t e = e_begin + batch * 32 + lane;
-                if (batch < n_batches && e < e_end && a.row_class[e] == 1) {
-                    f.km = mk_base[e];
-                    f.ml = ml_base[e];
-                    f.L = static_cast<double>(a.len[e]);
-                    f.ok = true;
+            const int r0 = UROWS * warp, c0 = UCOLS * warp;
+            const uint32_t sr = (n_sparse + a.n_splits - 1) / a.n_splits;
+            const uint32_t s_begin = min(n_sparse, split * sr), s_end = min(n_sparse, s_begin + sr);
+            const uint32_t n_chunks = s_end > s_begin ? (s_end - s_begin + USK - 1) / USK : 0;
+            // warp w stages row w of a chunk
+            auto load = [&](uint32_t chunk) {
+                const int st = static_cast<int>(chunk % SST);
+                const uint32_t i = s_begin + chunk * USK + warp;
+                const bool ok = i < s_end;
+                const uint32_t e = ok ? a.sparse_rows[i] : 0u;
+                const uint64_t base = static_cast<uint64_t>(e) * a.ld;
+                T *dv = Sv + (st * USK + warp) * PITCH;
+                T *dc = Sc + (st * USK + warp) * PITCH;
+                for (int q = lane; q < CPR; q += 32) {
+                    const uint32_t col = q < UK / VEC ? k0 + q * VEC : l0 + (q - UK / VEC) * VEC;
+                    cp_async16(dv + q * VEC, a.U + base + col, ok ? 16 : 0);
+                    if (CNT) cp_async16(dc + q * VEC, a.C + base + col, ok ? 16 : 0);
                 }
-                return f;
+                if (lane == 0) cp_async_small<sizeof(T)>(Sl + st * USK + warp, a.len + e, ok ? (int)sizeof(T) : 0);
             };
-            Fetch cur = fetch(0), nxt = fetch(1);
-            for (uint32_t b = 0; b < n_batches; b++) {
-                const Fetch after = fetch(b + 2);
-                const uint32_t e_cur = e_begin + b * 32 + lane;
-                const uint32_t mk_l = static_cast<uint32_t>(cur.km >> kshift) & kmask;
-                uint32_t active = __ballot_sync(0xffffffffu, cur.ok && (mk_l != 0 || cur.ml != 0ull));
-                while (active) {
-                    int slot_lane[USLOTS];
-                    int cnt = 0;
+            // column pass accumulators: rows lane + 32 j of columns c0 + cc
+            double bacc[UCOLS][4][2];
 #pragma unroll
-                    for (int j = 0; j < USLOTS; j++) {
-                        slot_lane[j] = active ? __ffs(active) - 1 : 0;
-                        cnt += active ? 1 : 0;
-                        active &= active ? active - 1 : 0u;
-                    }
-                    // gather: lanes r < 8 the row values present, every lane its
-                    // two columns when present
-                    double va[USLOTS], vca[USLOTS], vb[USLOTS][2], vcb[USLOTS][2];
+            for (int cc = 0; cc < UCOLS; cc++)
 #pragma unroll
-                    for (int j = 0; j < USLOTS; j++) {
-                        const int c = slot_lane[j];
-                        const uint32_t e = __shfl_sync(0xffffffffu, e_cur, c);
-                        const uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
-                        const unsigned long long ml = __shfl_sync(0xffffffffu, cur.ml, c);
-                        const uint64_t base = static_cast<uint64_t>(e) * a.ld;
-                        const bool live = j < cnt;
-                        const bool ron = live && lane < UROWS && ((mk >> lane) & 1u);
-                        va[j] = ron ? static_cast<double>(a.U[base + k0 + r0 + lane]) : 0.0;
-                        vca[j] = (CNT && ron) ? static_cast<double>(a.C[base + k0 + r0 + lane]) : 0.0;
-#pragma unroll
-                        for (int m = 0; m < 2; m++) {
-                            const bool con = live && ((ml >> (lane + 32 * m)) & 1ull);
-                            vb[j][m] = con ? static_cast<double>(a.U[base + l0 + lane + 32 * m]) : 0.0;
-                            vcb[j][m] = (CNT && con) ? static_cast<double>(a.C[base + l0 + lane + 32 * m]) : 0.0;
-                        }
-                    }
-#pragma unroll
-                    for (int j = 0; j < USLOTS; j++) {
-                        if (j < cnt) {  // uniform
-                            const int c = slot_lane[j];
-                            const uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
-                            const unsigned long long ml = __shfl_sync(0xffffffffu, cur.ml, c);
-                            const double L = __shfl_sync(0xffffffffu, cur.L, c);
-                            // row pass: the warp's rows present x every column
-                            uint32_t rows = mk;
-                            while (rows) {
-                                const int r = __ffs(rows) - 1;
-                                rows &= rows - 1;
-                                const double av = __shfl_sync(0xffffffffu, va[j], r);
-                                const double cav = __shfl_sync(0xffffffffu, vca[j], r);
-                                const double tk = __shfl_sync(0xffffffffu, tk_lane, r);
-#pragma unroll
-                                for (int m = 0; m < 2; m++) {
-                                    const int at = r * UL + lane + 32 * m;
-                                    double t[2] = {Wn[at], Wd[at]};
-                                    Op::term(t, av, vb[j][m], cav, vcb[j][m], tk + (m ? tl1 : tl0), L, a.alpha);
-                                    Wn[at] = t[0];
-                                    Wd[at] = t[1];
-                                }
-                            }
-                            // column pass: columns present x the warp's rows
-                            // absent, 4 columns x 8 rows per round
-                            const uint32_t absent = ~mk & kmask;
-                            const uint32_t lo = static_cast<uint32_t>(ml), hi = static_cast<uint32_t>(ml >> 32);
-                            const int plo = __popc(lo), ncol = absent ? plo + __popc(hi) : 0;
-                            for (int ib = 0; ib < ncol; ib += 32 / UROWS) {
-                                const int i = ib + lane / UROWS, r = lane % UROWS;
-                                int col = 0;
-                                if (i < ncol)
-                                    col = i < plo ? static_cast<int>(__fns(lo, 0, i + 1))
-                                                  : 32 + static_cast<int>(__fns(hi, 0, i - plo + 1));
-                                const int src = col & 31;
-                                const double b0 = __shfl_sync(0xffffffffu, vb[j][0], src);
-                                const double b1 = __shfl_sync(0xffffffffu, vb[j][1], src);
-                                const double c0 = __shfl_sync(0xffffffffu, vcb[j][0], src);
-                                const double c1 = __shfl_sync(0xffffffffu, vcb[j][1], src);
-                                const double t0 = __shfl_sync(0xffffffffu, tl0, src);
-                                const double t1 = __shfl_sync(0xffffffffu, tl1, src);
-                                const double tk = __shfl_sync(0xffffffffu, tk_lane, r);
-                                if (i < ncol && ((absent >> r) & 1u)) {
-                                    const bool up = col >= 32;
-                                    const int at = r * UL + col;
-                                    double t[2] = {Wn[at], Wd[at]};
-                                    Op::term(t, 0.0, up ? b1 : b0, 0.0, up ? c1 : c0, tk + (up ? t1 : t0), L,
-                                             a.alpha);
-                                    Wn[at] = t[0];
-                                    Wd[at] = t[1];
-                                }
-                            }
-                            // the next row's passes give an element to another lane
-                            __syncwarp();
-                        }
-                    }
-                }
-                cur = nxt;
-                nxt = after;
+                for (int j = 0; j < 4; j++) bacc[cc][j][0] = bacc[cc][j][1] = 0.0;
+            const double tl0 = CNT ? Ts[UK + lane] : 0.0, tl1 = CNT ? Ts[UK + lane + 32] : 0.0;
+            for (uint32_t c = 0; c + 1 < SST; c++) {
+                if (c < n_chunks) load(c);
+                cp_async_commit();
             }
+            for (uint32_t ch = 0; ch < n_chunks; ch++) {
+                if (ch + SST - 1 < n_chunks) load(ch + SST - 1);
+                cp_async_commit();
+                cp_async_wait<SST - 1>();
+                __syncthreads();
+                const int st = static_cast<int>(ch % SST);
+                const T *vs = Sv + st * USK * PITCH;
+                const T *cs = Sc + st * USK * PITCH;
+                const T *ls = Sl + st * USK;
+                const int hn = lane & 15, hq = lane >> 4;
+
+                // row pass: rows r0 + rr present; bit n of word rr: staged row n
+                uint32_t rmask[UROWS / 2];
+#pragma unroll
+                for (int q = 0; q < UROWS / 2; q++)
+                    rmask[q] = __ballot_sync(0xffffffffu, vs[hn * PITCH + r0 + 2 * q + hq] > T(0));
+#pragma unroll
+                for (int rr = 0; rr < UROWS; rr++) {
+                    uint32_t nm = (rmask[rr / 2] >> (16 * (rr % 2))) & 0xffffu;
+                    if (!nm) continue;
+                    const int r = r0 + rr;
+                    double t0[2] = {Mn[r * UL + lane], Md[r * UL + lane]};
+                    double t1[2] = {Mn[r * UL + lane + 32], Md[r * UL + lane + 32]};
+                    const double tk = CNT ? Ts[r] : 0.0;
+                    while (nm) {
+                        const int n = __ffs(nm) - 1;
+                        nm &= nm - 1;
+                        const T *v = vs + n * PITCH;
+                        const T *cv = cs + n * PITCH;
+                        const double L = static_cast<double>(ls[n]);
+                        const double av = static_cast<double>(v[r]);
+                        const double ca = CNT ? static_cast<double>(cv[r]) : 0.0;
+                        Op::term(t0, av, static_cast<double>(v[UK + lane]), ca,
+                                 CNT ? static_cast<double>(cv[UK + lane]) : 0.0, tk + tl0, L, a.alpha);
+                        Op::term(t1, av, static_cast<double>(v[UK + lane + 32]), ca,
+                                 CNT ? static_cast<double>(cv[UK + lane + 32]) : 0.0, tk + tl1, L, a.alpha);
+                    }
+                    Mn[r * UL + lane] = t0[0];
+                    Md[r * UL + lane] = t0[1];
+                    Mn[r * UL + lane + 32] = t1[0];
+                    Md[r * UL + lane + 32] = t1[1];
+                }
+
+                // column pass: columns c0 + cc present, rows without the node
+                uint32_t cmask[UCOLS / 2];
+#pragma unroll
+                for (int q = 0; q < UCOLS / 2; q++)
+                    cmask[q] = __ballot_sync(0xffffffffu, vs[hn * PITCH + UK + c0 + 2 * q + hq] > T(0));
+#pragma unroll
+                for (int cc = 0; cc < UCOLS; cc++) {
+                    uint32_t nm = (cmask[cc / 2] >> (16 * (cc % 2))) & 0xffffu;
+                    const double tl = CNT ? Ts[UK + c0 + cc] : 0.0;
+                    while (nm) {
+                        const int n = __ffs(nm) - 1;
+                        nm &= nm - 1;
+                        const T *v = vs + n * PITCH;
+                        const double L = static_cast<double>(ls[n]);
+                        const double bv = static_cast<double>(v[UK + c0 + cc]);
+                        const double cb = CNT ? static_cast<double>(cs[n * PITCH + UK + c0 + cc]) : 0.0;
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            const int r = lane + 32 * j;
+                            if (v[r] == T(0))
+                                Op::term(bacc[cc][j], 0.0, bv, 0.0, cb, (CNT ? Ts[r] : 0.0) + tl, L, a.alpha);
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            cp_async_wait<0>();
+            // the row pass is complete (barrier above): add the column pass
+#pragma unroll
+            for (int cc = 0; cc < UCOLS; cc++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int at = (lane + 32 * j) * UL + c0 + cc;
+                    Mn[at] += bacc[cc][j][0];
+                    Md[at] += bacc[cc][j][1];
+                }
         }
         __syncthreads();
 
