@@ -291,9 +291,10 @@ struct PlanImpl {
     // generalized and variance-adjusted methods over the union of the two
     // samples' supports (same masks and row classes as the hybrid)
     bool union_mode = false;
-    uint32_t union_div = 4;  // rows non-zero in more than ld / union_div columns are dense
+    uint32_t union_div = 3;  // rows non-zero in more than ld / union_div columns are dense
     double *d_upartial = nullptr;
     size_t upartial_bytes = 0;
+    void *d_slen = nullptr;  // branch length per sparse row, in sparse-row order
     int sparse_prep_alloc();
     template <typename T>
     int sparse_prep(cudaStream_t s, const Group &g, uint32_t div);
@@ -480,10 +481,9 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
              (spec.method == Method::weighted_normalized || spec.method == Method::weighted_unnormalized);
     if (const char *m = std::getenv("UNIFRAC_B200_WEIGHTED_MODE"))
         if (std::string(m) == "dense") hybrid = false;
-    // generalized and variance-adjusted methods in fp64: only the union of
-    // the two samples' supports adds to a pair (needs u >= 0 so presence is
-    // u > 0).  In fp32 the dense kernels' single-precision terms are faster.
-    union_mode = spec.fp64 && !faith && !gemm && nonneg_data && set.row_active.empty() &&
+    // generalized and variance-adjusted methods: only the union of the two
+    // samples' supports adds to a pair (needs u >= 0 so presence is u > 0)
+    union_mode = !faith && !gemm && nonneg_data && set.row_active.empty() &&
                  (spec.vaw || spec.method == Method::generalized);
     if (const char *m = std::getenv("UNIFRAC_B200_UNION_MODE"))
         if (std::string(m) == "dense") union_mode = false;
@@ -839,7 +839,7 @@ int PlanImpl::sparse_prep(cudaStream_t s, const Group &g, uint32_t div) {
 
 template <typename T>
 int PlanImpl::setup_union() {
-    union_div = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_UNION_DIV", 4)));
+    union_div = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_UNION_DIV", 3)));
     if (const int rc = sparse_prep_alloc()) return rc;
     size_t smem = 0;
     SSU_CK(dev::union_configure<T>(spec, &smem));
@@ -847,7 +847,7 @@ int PlanImpl::setup_union() {
     for (Group &g : groups) {
         std::vector<uint4> tiles;
         for (uint32_t t = g.t0; t < g.t1; t++)
-            append_tiles(tiles, t, tdesc[t].base, tdesc[t].n, dev::UK, dev::UL, false, 0, 0);
+            append_tiles(tiles, t, tdesc[t].base, tdesc[t].n, dev::UT, dev::UT, false, 0, 0);
         g.n_tiles = static_cast<uint32_t>(tiles.size());
         SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * tiles.size()));
         // node splits so the tiles fill the SMs (one CTA per SM)
@@ -863,10 +863,14 @@ int PlanImpl::setup_union() {
         }
         g.splits = best_s;
         if (g.splits > 1)
-            upartial_bytes =
-                std::max(upartial_bytes, sizeof(double) * 2 * dev::UK * dev::UL * g.n_tiles * g.splits);
+            upartial_bytes = std::max(upartial_bytes, sizeof(double) * 2 * dev::UT * dev::UT * g.n_tiles * g.splits);
     }
     if (upartial_bytes) SSU_CK(alloc(&d_upartial, upartial_bytes));
+    SSU_CK(alloc(reinterpret_cast<T **>(&d_slen), sizeof(T) * (static_cast<size_t>(E) + dev::URS)));
+    if (!d_error) {
+        SSU_CK(alloc(&d_error, sizeof(int)));
+        SSU_CK(cudaMemsetAsync(d_error, 0, sizeof(int), stream));
+    }
     return 0;
 }
 
@@ -877,19 +881,25 @@ int PlanImpl::union_stage(cudaStream_t s, const Group &g, const dev::OutSpec &ou
                           uint32_t ntiles, uint32_t splits, bool last) {
     if (const int rc = sparse_prep<T>(s, g, union_div)) return rc;
     if (ntiles == 0) return 0;
+    T *slen = static_cast<T *>(d_slen);
+    if (E) {
+        const uint32_t grid = std::min<uint32_t>((E + 255) / 256, 4 * n_sms);
+        dev::gather_sparse_len_kernel<T><<<grid, 256, 0, s>>>(d_sparse_rows, d_nrows, static_cast<const T *>(d_len),
+                                                              E, slen);
+        launches++;
+    }
     dev::UnionArgs<T> u{};
     u.tiles = tiles;
     u.n_tiles = ntiles;
     u.n_splits = std::max<uint32_t>(splits, 1);
-    if (u.n_splits > 1 && sizeof(double) * 2 * dev::UK * dev::UL * ntiles * u.n_splits > upartial_bytes)
+    if (u.n_splits > 1 && sizeof(double) * 2 * dev::UT * dev::UT * ntiles * u.n_splits > upartial_bytes)
         u.n_splits = 1;
     u.tables = d_tdesc;
     u.U = static_cast<const T *>(d_U);
     u.C = static_cast<const T *>(d_C);
     u.tot = static_cast<const T *>(g.d_tot);
     u.len = static_cast<const T *>(d_len);
-    u.masks = d_masks;
-    u.row_class = d_row_class;
+    u.slen = slen;
     u.E = E;
     u.ld = g.ld;
     u.dense_rows = d_dense_rows;
@@ -898,6 +908,8 @@ int PlanImpl::union_stage(cudaStream_t s, const Group &g, const dev::OutSpec &ou
     u.alpha = spec.alpha;
     u.partial = u.n_splits > 1 ? d_upartial : nullptr;
     u.out = out;
+    u.error = d_error;
+    u.wait_cycles = 2000000000LL;  // about one second per wait at B200 clocks
     const uint32_t ctas = static_cast<uint32_t>(
         std::min<uint64_t>(static_cast<uint64_t>(ntiles) * u.n_splits, static_cast<uint64_t>(n_sms)));
     SSU_CK(dev::union_launch<T>(spec, u, ctas, s));
@@ -1142,8 +1154,8 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
         return execute_gemm(stream, o);
     }
     const Group &g = groups[0];
-    const int BM = union_mode ? dev::UK : spec.fp64 ? kd.BM : kf.BM;
-    const int BN = union_mode ? dev::UL : spec.fp64 ? kd.BN : kf.BN;
+    const int BM = union_mode ? dev::UT : spec.fp64 ? kd.BM : kf.BM;
+    const int BN = union_mode ? dev::UT : spec.fp64 ? kd.BN : kf.BN;
     std::vector<uint4> tiles;
     append_tiles(tiles, 0, 0, tdesc[0].n, BM, BN, mode == 1, start, stop);
     uint4 *d_t = nullptr;

@@ -18,7 +18,7 @@ cudaError_t configure_one(size_t *smem) {
 template <typename T, class Op>
 cudaError_t launch_one(const UnionArgs<T> &a, uint32_t ctas, cudaStream_t s) {
     pair_union_kernel<T, Op><<<ctas, UTHREADS, union_smem<T, Op::COUNTS>(), s>>>(a);
-    if (a.partial) union_finalize_kernel<T, Op><<<a.n_tiles, UTHREADS, 0, s>>>(a);
+    if (a.partial) union_finalize_kernel<T, Op><<<a.n_tiles, UFIN_THREADS, 0, s>>>(a);
     return cudaGetLastError();
 }
 
