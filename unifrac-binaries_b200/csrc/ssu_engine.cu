@@ -1750,6 +1750,7 @@ const char *Plan::pair_kernel_name() const {
 const char *Plan::tuning() const {
     if (impl_->gemm) return "fixed";
     static thread_local std::string s;
+    if (impl_->union_mode) return "sparse union 64x64";
     s = impl_->tuning + " " + (impl_->spec.fp64 ? impl_->kd.shape : impl_->kf.shape);
     return s.c_str();
 }
