@@ -154,13 +154,16 @@ ComputeStatus validate(const ssu::Table &table, const ssu::BPTree &tree) {
 // the tree itself, and a tree without single-child nodes collapses to itself.
 ssu::FlatTree sync_tree(const ssu::Table &table, const ssu::BPTree &tree, bool bypass_tips) {
     const ssu::TipMatch &m = tip_match(table, tree);
+    bool single = false;
     if (m.all_tips) {
-        if (!tree.has_single_child()) return ssu::flatten(tree, bypass_tips, &m.tags);
+        ssu::FlatTree f = ssu::flatten(tree, bypass_tips, &m.tags, &single);
+        if (!single) return f;
         return ssu::flatten(tree.collapse(&m.tags), bypass_tips);
     }
-    ssu::BPTree sheared = tree.shear_matched(m);
-    if (sheared.has_single_child()) sheared = sheared.collapse();
-    return ssu::flatten(sheared, bypass_tips);
+    const ssu::BPTree sheared = tree.shear_matched(m);
+    ssu::FlatTree f = ssu::flatten(sheared, bypass_tips, nullptr, &single);
+    if (!single) return f;
+    return ssu::flatten(sheared.collapse(), bypass_tips);
 }
 
 // UNIFRAC_B200_UNWEIGHTED_MODE: "gemm" runs unweighted methods on the
@@ -403,9 +406,12 @@ ComputeStatus full_matrix_v3(const support_biom_t *table_data, const support_bpt
     if (fp64 != want_fp64) return invalid_method;
     if (!table_data || table_data->n_samples <= 0 || table_data->n_obs <= 0) return table_empty;
     if (!tree_data) return tree_missing;
+    StepTimer timer("one_off_matrix_v3");
     ssu::Table table = table_from(table_data);
     const ssu::BPTree tree = tree_from(tree_data);
+    timer.step("read_table_tree");
     st = validate(table, tree);
+    timer.step("validate");
     if (st != okay) return st;
     if (subsample_depth > 0) {
         ssu::Table sub = table.rarefied(subsample_depth, with_replacement, g_seed.load());

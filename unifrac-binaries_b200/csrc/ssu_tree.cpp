@@ -334,68 +334,84 @@ uint32_t BPTree::n_tips() const {
 namespace {
 
 template <class ObsOf>
-FlatTree flatten_impl(const BPTree &t, bool bypass_tips, ObsOf obs_of) {
+FlatTree flatten_impl(const BPTree &t, bool bypass_tips, ObsOf obs_of, bool *single_child) {
     FlatTree f;
     const uint32_t n = t.size();
     const uint32_t total = n / 2;
     f.n_nodes = total > 0 ? total - 1 : 0;
-    // postorder: the k-th closing parenthesis closes the k-th postorder node;
-    // the root closes last and is not a row (src/unifrac_cmp.cpp:97-100)
-    std::vector<uint32_t> post_open;
-    post_open.reserve(f.n_nodes);
-    for (uint32_t i = 0; i < n && post_open.size() < f.n_nodes; i++)
-        if (!t.open[i]) post_open.push_back(t.match[i]);
-    std::vector<uint32_t> row_of_open(n, UINT32_MAX);
-    uint32_t r = 0;
-    for (uint32_t k = 0; k < f.n_nodes; k++)
-        if (!(bypass_tips && t.leaf(post_open[k]))) row_of_open[post_open[k]] = r++;
-    f.n_embedded = r;
-    for (uint32_t k = 0; k < f.n_nodes; k++)
-        if (row_of_open[post_open[k]] == UINT32_MAX) row_of_open[post_open[k]] = r++;
+    const uint32_t N = f.n_nodes;
+    if (single_child) *single_child = false;
+    // Rows: the k-th closing parenthesis closes the k-th postorder node and
+    // the root closes last, without a row (src/unifrac_cmp.cpp:97-100).
+    // Embedded nodes take rows in postorder; with bypassed tips the tips
+    // follow them, in postorder too.
+    uint32_t n_leaves = 0;
+    if (bypass_tips)
+        for (uint32_t i = 0; i + 1 < n; i++) n_leaves += (t.open[i] && !t.open[i + 1]) ? 1u : 0u;
+    f.n_embedded = bypass_tips ? N - std::min(N, n_leaves) : N;
+    f.length.resize(N);
+    f.leaf_obs.assign(N, -1);
+    f.postorder_row.resize(N);
+    f.child_ptr.assign(N + 1, 0);
+    f.child_rows.reserve(N);
+    f.leaf_rows.reserve(bypass_tips ? n_leaves : N / 2 + 1);
+    std::vector<uint32_t> height(N, 0);
 
-    f.length.assign(f.n_nodes, 0.0);
-    f.leaf_obs.assign(f.n_nodes, -1);
-    f.postorder_row.resize(f.n_nodes);
-    std::vector<uint32_t> height(f.n_nodes, 0);
-    std::vector<uint32_t> n_kids(f.n_nodes, 0);
-    uint32_t max_height = 0;
-    for (uint32_t k = 0; k < f.n_nodes; k++) {
-        const uint32_t o = post_open[k];
-        const uint32_t row = row_of_open[o];
-        f.postorder_row[k] = row;
-        f.length[row] = t.length[o];
-        if (t.leaf(o)) {
+    // One walk over the parentheses: an open node keeps its opening index,
+    // the tallest child seen + 1 and where its children start on `pend`,
+    // the stack of rows whose parent has not closed yet (left to right).
+    struct Open {
+        uint32_t o, h, first;
+    };
+    std::vector<Open> stack;
+    stack.reserve(64);
+    std::vector<uint32_t> pend;
+    pend.reserve(64);
+    uint32_t k = 0, emb = 0, tip = 0, max_height = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        if (t.open[i]) {
+            stack.push_back({i, 0, static_cast<uint32_t>(pend.size())});
+            continue;
+        }
+        if (stack.empty()) continue;
+        const Open e = stack.back();
+        stack.pop_back();
+        if (stack.empty() || k >= N) break;  // the root
+        const bool leaf = e.o + 1 == i;
+        const uint32_t row = (bypass_tips && leaf) ? f.n_embedded + tip++ : emb++;
+        f.postorder_row[k++] = row;
+        f.length[row] = t.length[e.o];
+        uint32_t h = 0;
+        if (leaf) {
             f.leaf_rows.push_back(row);
-            f.leaf_obs[row] = obs_of(o);
+            f.leaf_obs[row] = obs_of(e.o);
         } else {
-            uint32_t h = 0, nk = 0;
-            for (uint32_t c = o + 1; c < n && t.open[c]; c = t.match[c] + 1) {
-                h = std::max(h, height[row_of_open[c]] + 1);
-                nk++;
-            }
-            n_kids[row] = nk;
+            // internal rows are numbered in closing order, so their child
+            // lists are appended in row order
+            const uint32_t nk = static_cast<uint32_t>(pend.size()) - e.first;
+            if (nk == 1 && single_child) *single_child = true;
+            f.child_ptr[row] = static_cast<uint32_t>(f.child_rows.size());
+            f.child_rows.insert(f.child_rows.end(), pend.begin() + e.first, pend.end());
+            f.child_ptr[row + 1] = static_cast<uint32_t>(f.child_rows.size());
+            h = e.h;
             height[row] = h;
             max_height = std::max(max_height, h);
         }
+        pend.resize(e.first);
+        pend.push_back(row);
+        stack.back().h = std::max(stack.back().h, h + 1);
     }
-    // children as CSR, left to right
-    f.child_ptr.assign(f.n_nodes + 1, 0);
-    for (uint32_t row = 0; row < f.n_nodes; row++) f.child_ptr[row + 1] = f.child_ptr[row] + n_kids[row];
-    f.child_rows.assign(f.child_ptr[f.n_nodes], 0);
-    for (uint32_t k = 0; k < f.n_nodes; k++) {
-        const uint32_t o = post_open[k];
-        if (t.leaf(o)) continue;
-        uint32_t w = f.child_ptr[row_of_open[o]];
-        for (uint32_t c = o + 1; c < n && t.open[c]; c = t.match[c] + 1) f.child_rows[w++] = row_of_open[c];
-    }
-    // internal rows bucketed by height 1..max_height
+    // rows without children (tips) point at the end of their predecessor's list
+    for (uint32_t row = 0; row < N; row++)
+        if (f.child_ptr[row + 1] < f.child_ptr[row]) f.child_ptr[row + 1] = f.child_ptr[row];
+    // internal rows bucketed by height 1..max_height, rows ascending
     f.level_ptr.assign(max_height + 1, 0);
-    for (uint32_t row = 0; row < f.n_nodes; row++)
+    for (uint32_t row = 0; row < N; row++)
         if (height[row] > 0) f.level_ptr[height[row]]++;
     for (uint32_t h = 1; h <= max_height; h++) f.level_ptr[h] += f.level_ptr[h - 1];
     f.level_rows.assign(f.level_ptr[max_height], 0);
     std::vector<uint32_t> fill(f.level_ptr.begin(), f.level_ptr.end());
-    for (uint32_t row = 0; row < f.n_nodes; row++)
+    for (uint32_t row = 0; row < N; row++)
         if (height[row] > 0) f.level_rows[fill[height[row] - 1]++] = row;
     return f;
 }
@@ -403,15 +419,18 @@ FlatTree flatten_impl(const BPTree &t, bool bypass_tips, ObsOf obs_of) {
 }  // namespace
 
 FlatTree flatten(const BPTree &t, const NameIndex &obs_index, bool bypass_tips) {
-    return flatten_impl(t, bypass_tips, [&](uint32_t o) -> int32_t {
-        auto it = obs_index.find(t.name[o]);
-        return it != obs_index.end() ? static_cast<int32_t>(it->second) : -1;
-    });
+    return flatten_impl(
+        t, bypass_tips,
+        [&](uint32_t o) -> int32_t {
+            auto it = obs_index.find(t.name[o]);
+            return it != obs_index.end() ? static_cast<int32_t>(it->second) : -1;
+        },
+        nullptr);
 }
 
-FlatTree flatten(const BPTree &t, bool bypass_tips, const std::vector<int32_t> *tags) {
+FlatTree flatten(const BPTree &t, bool bypass_tips, const std::vector<int32_t> *tags, bool *single_child) {
     const std::vector<int32_t> &tg = tags ? *tags : t.tag;
-    return flatten_impl(t, bypass_tips, [&](uint32_t o) -> int32_t { return tg.empty() ? -1 : tg[o]; });
+    return flatten_impl(t, bypass_tips, [&](uint32_t o) -> int32_t { return tg.empty() ? -1 : tg[o]; }, single_child);
 }
 
 uint32_t table_embedded(const FlatTree &f, const std::vector<int32_t> &obs_row, bool bypass_tips,

@@ -105,8 +105,11 @@ struct FlatTree {
 
 FlatTree flatten(const BPTree &tree, const NameIndex &obs_index, bool bypass_tips);
 // Flatten a tree whose tips carry table rows in `tag` (from shear_to), or in
-// `tags` when given.
-FlatTree flatten(const BPTree &tree, bool bypass_tips, const std::vector<int32_t> *tags = nullptr);
+// `tags` when given.  `single_child`, when given, reports whether some
+// non-root node has a single child (the tree is then not collapsed: the
+// caller collapses and flattens again).
+FlatTree flatten(const BPTree &tree, bool bypass_tips, const std::vector<int32_t> *tags = nullptr,
+                 bool *single_child = nullptr);
 
 // Embedded node count of the tree sheared to the observations o with
 // obs_row[o] >= 0 and then collapsed, computed on a flattened tree of a
