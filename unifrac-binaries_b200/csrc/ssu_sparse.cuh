@@ -242,20 +242,48 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
             for (int j = 0; j < TN; j++) acc[i][j] = 0.0;
         stream_rows(a.dense_rows, d_begin, d_end, [&](int st) {
             const T *vs = Vs + st * HKC * 2 * HB;
-#pragma unroll 2
-            for (int c = 0; c < HKC; c++) {
-                T av[TM], bv[TN];
-                load_half<T, TM / 2>(av, vs + c * 2 * HB + ty * (TM / 2));
-                load_half<T, TM / 2>(av + TM / 2, vs + c * 2 * HB + HB / 2 + ty * (TM / 2));
-                load_half<T, TN / 2>(bv, vs + c * 2 * HB + HB + tx * (TN / 2));
-                load_half<T, TN / 2>(bv + TN / 2, vs + c * 2 * HB + HB + HB / 2 + tx * (TN / 2));
-                const double L = static_cast<double>(Ls[st * HKC + c]);
+            if constexpr (sizeof(T) == 4) {
+                // single precision: each stage's 8 rows summed in fp32 (the
+                // reference fp32 build's own arithmetic), then folded into the
+                // fp64 totals, so no fp32 sum runs over more than 8 terms
+                float part[TM][TN];
 #pragma unroll
                 for (int i = 0; i < TM; i++)
 #pragma unroll
-                    for (int j = 0; j < TN; j++)
-                        acc[i][j] =
-                            fma(fabs(static_cast<double>(av[i]) - static_cast<double>(bv[j])), L, acc[i][j]);
+                    for (int j = 0; j < TN; j++) part[i][j] = 0.0f;
+#pragma unroll 2
+                for (int c = 0; c < HKC; c++) {
+                    T av[TM], bv[TN];
+                    load_half<T, TM / 2>(av, vs + c * 2 * HB + ty * (TM / 2));
+                    load_half<T, TM / 2>(av + TM / 2, vs + c * 2 * HB + HB / 2 + ty * (TM / 2));
+                    load_half<T, TN / 2>(bv, vs + c * 2 * HB + HB + tx * (TN / 2));
+                    load_half<T, TN / 2>(bv + TN / 2, vs + c * 2 * HB + HB + HB / 2 + tx * (TN / 2));
+                    const float L = static_cast<float>(Ls[st * HKC + c]);
+#pragma unroll
+                    for (int i = 0; i < TM; i++)
+#pragma unroll
+                        for (int j = 0; j < TN; j++) part[i][j] = fmaf(fabsf(av[i] - bv[j]), L, part[i][j]);
+                }
+#pragma unroll
+                for (int i = 0; i < TM; i++)
+#pragma unroll
+                    for (int j = 0; j < TN; j++) acc[i][j] += static_cast<double>(part[i][j]);
+            } else {
+#pragma unroll 2
+                for (int c = 0; c < HKC; c++) {
+                    T av[TM], bv[TN];
+                    load_half<T, TM / 2>(av, vs + c * 2 * HB + ty * (TM / 2));
+                    load_half<T, TM / 2>(av + TM / 2, vs + c * 2 * HB + HB / 2 + ty * (TM / 2));
+                    load_half<T, TN / 2>(bv, vs + c * 2 * HB + HB + tx * (TN / 2));
+                    load_half<T, TN / 2>(bv + TN / 2, vs + c * 2 * HB + HB + HB / 2 + tx * (TN / 2));
+                    const double L = static_cast<double>(Ls[st * HKC + c]);
+#pragma unroll
+                    for (int i = 0; i < TM; i++)
+#pragma unroll
+                        for (int j = 0; j < TN; j++)
+                            acc[i][j] =
+                                fma(fabs(static_cast<double>(av[i]) - static_cast<double>(bv[j])), L, acc[i][j]);
+                }
             }
         });
         // the dense sums seed the shared tile
