@@ -120,6 +120,26 @@ ssu::BPTree tree_from(const support_bptree_t *t, bool copy_names = false) {
     return ssu::BPTree::from_arrays(t->structure, t->lengths, t->names, t->n_parens, copy_names);
 }
 
+const ssu::NameMap &obs_map(const ssu::Table &table);
+
+// The caller's table and tree, read side by side for large trees: the
+// tree's arrays on a helper thread while this thread reads the table (ids,
+// per-sample totals) and builds its name map.  Small trees are read inline,
+// where a thread would cost more than it saves.
+void read_inputs(const support_biom_t *table_data, const support_bptree_t *tree_data, ssu::Table &table,
+                 ssu::BPTree &tree) {
+    constexpr int kThreadedParens = 16384;
+    if (tree_data->n_parens < kThreadedParens) {
+        table = table_from(table_data);
+        tree = tree_from(tree_data);
+        return;
+    }
+    std::thread reader([&tree, tree_data] { tree = tree_from(tree_data); });
+    table = table_from(table_data);
+    obs_map(table);
+    reader.join();
+}
+
 // Observation name -> row (the last row wins for a repeated name, as the
 // reference's obs_id_index map), built once per table and call; the table
 // keeps it with its number of distinct names.
@@ -407,8 +427,9 @@ ComputeStatus full_matrix_v3(const support_biom_t *table_data, const support_bpt
     if (!table_data || table_data->n_samples <= 0 || table_data->n_obs <= 0) return table_empty;
     if (!tree_data) return tree_missing;
     StepTimer timer("one_off_matrix_v3");
-    ssu::Table table = table_from(table_data);
-    const ssu::BPTree tree = tree_from(tree_data);
+    ssu::Table table;
+    ssu::BPTree tree;
+    read_inputs(table_data, tree_data, table, tree);
     timer.step("read_table_tree");
     st = validate(table, tree);
     timer.step("validate");
@@ -584,8 +605,9 @@ ComputeStatus subsample_batch_v3(const support_biom_t *table_data, const support
         !results)
         return table_empty;
     if (!tree_data) return tree_missing;
-    const ssu::Table table = table_from(table_data);
-    const ssu::BPTree tree = tree_from(tree_data);
+    ssu::Table table;
+    ssu::BPTree tree;
+    read_inputs(table_data, tree_data, table, tree);
     st = validate(table, tree);
     if (st != okay) return st;
     std::vector<ssu::Table> reps;
@@ -662,8 +684,7 @@ ComputeStatus inmem_common(const support_biom_t *table_data, const support_bptre
                            ssu::BPTree &tree) {
     if (!table_data || table_data->n_samples <= 0 || table_data->n_obs <= 0) return table_empty;
     if (!tree_data) return tree_missing;
-    table = table_from(table_data);
-    tree = tree_from(tree_data);
+    read_inputs(table_data, tree_data, table, tree);
     return validate(table, tree);
 }
 
