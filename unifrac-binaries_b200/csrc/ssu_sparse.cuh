@@ -12,8 +12,13 @@
 //               L |a - b| in registers, exactly as the dense pair kernel;
 //   sparse rows (the rest, all-zero rows dropped): only the pairs where both
 //               samples are non-zero are touched, -2 L min(a, b) accumulated
-//               in an fp64 tile in shared memory, rows in order, one lane per
-//               element (deterministic).
+//               in an fp64 tile in shared memory.  fp64 plans: each warp owns
+//               8 tile rows and walks every row, in order, one lane per element
+//               (bit-reproducible).  fp32 plans: each row is handled by one
+//               warp, which gathers only the present values and adds the
+//               products with shared-memory atomics (13% faster on config-4
+//               data; the order of these additions, so the last bits of the
+//               fp64 sums, can vary between runs).
 // d = D + (M + Ws_k + Ws_l) subtracts; where d < tau (Ws_k + Ws_l) the
 // rounding of that subtraction could reach 1e-13 relative, so the tile is
 // flagged and recomputed exactly (all nodes, |a - b| form) by the dense pair
@@ -294,101 +299,234 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                 Mt[tile_row<HB, TM>(ty, i) * HB + tile_row<HB, TN>(tx, j)] = acc[i][j];
         __syncthreads();
 
-        // ---- sparse rows: -2 L min(a, b) where both are non-zero.  Each warp
-        // walks the embedded rows on its own (no block barrier) in batches of
-        // 32 consecutive rows, owning tile rows HROWS warp .. HROWS warp +
-        // HROWS - 1.  Lane i holds row i's class, mask words (its rows' word
-        // and the two words of the l block, coalesced over the batch) and
-        // length, fetched two batches ahead.  One ballot finds the sparse rows
-        // with a non-zero in both the warp's rows and the l block; their values
-        // are gathered HSLOTS rows at a time (lane r < HROWS: row value r,
-        // lane j: columns j + 32 m) and the updates of row r take its value
-        // from lane r by shuffle.
-        {
-            const uint64_t kwd = k0 / 64 + (warp * HROWS) / 64, lwd = l0 / 64;
-            const int kshift = (warp * HROWS) % 64;
-            constexpr uint32_t kmask = (1u << HROWS) - 1u;
-            double *Mw = Mt + HROWS * warp * HB;
-            const uint32_t er = (a.E + a.n_splits - 1) / a.n_splits;
-            const uint32_t r_begin = min(a.E, split * er), r_end = min(a.E, r_begin + er);
-            const uint32_t n_batches = r_end > r_begin ? (r_end - r_begin + 31) / 32 : 0;
-            const unsigned long long *mk_base = a.masks + kwd * a.E;
-            const unsigned long long *m0_base = a.masks + lwd * a.E;
-            const unsigned long long *m1_base = a.masks + (lwd + 1) * a.E;
-            struct Fetch {
-                unsigned long long km, m0, m1;
-                double L;
-                bool ok;
-            };
-            auto fetch = [&](uint32_t batch) {
-                Fetch f{0ull, 0ull, 0ull, 0.0, false};
-                const uint32_t e = r_begin + batch * 32 + lane;
-                if (batch < n_batches && e < r_end && a.row_class[e] == 1) {
-                    f.km = mk_base[e];
-                    f.m0 = m0_base[e];
-                    f.m1 = m1_base[e];
-                    f.L = static_cast<double>(a.len[e]);
-                    f.ok = true;
-                }
-                return f;
-            };
-            Fetch cur = fetch(0), nxt = fetch(1);
-            for (uint32_t b = 0; b < n_batches; b++) {
-                const Fetch after = fetch(b + 2);
-                const uint32_t e_cur = r_begin + b * 32 + lane;
-                const uint32_t mk_l = static_cast<uint32_t>(cur.km >> kshift) & kmask;
-                uint32_t active = __ballot_sync(0xffffffffu, cur.ok && mk_l != 0 && (cur.m0 | cur.m1) != 0ull);
-                while (active) {
-                    int slot_lane[HSLOTS];
-                    int cnt = 0;
-#pragma unroll
-                    for (int j = 0; j < HSLOTS; j++) {
-                        slot_lane[j] = active ? __ffs(active) - 1 : 0;
-                        cnt += active ? 1 : 0;
-                        active &= active ? active - 1 : 0u;
+        if constexpr (sizeof(T) == 4) {
+            // ---- sparse rows, fp32 plans: -2 L min(a, b) where both are non-zero.  Warp w
+            // takes batches w, w + 16, ... of 32 consecutive rows (lane i: row i's
+            // class, its k-block and l-block mask words and length, fetched two
+            // batches ahead), so each row is handled once per tile.  For a row
+            // with nk present k columns and nl present l columns, lanes gather
+            // the present values (one lane per present column, HSLOTS rows at a
+            // time so the loads overlap) and the nk x nl products are added into
+            // the shared tile with shared-memory atomics (k by k, lanes over l).
+            {
+                const uint32_t er = (a.E + a.n_splits - 1) / a.n_splits;
+                const uint32_t r_begin = min(a.E, split * er), r_end = min(a.E, r_begin + er);
+                const uint32_t n_batches = r_end > r_begin ? (r_end - r_begin + 31) / 32 : 0;
+                const uint64_t kwd = k0 / 64, lwd = l0 / 64;
+                const unsigned long long *k0_base = a.masks + kwd * a.E;
+                const unsigned long long *k1_base = a.masks + (kwd + 1) * a.E;
+                const unsigned long long *l0_base = a.masks + lwd * a.E;
+                const unsigned long long *l1_base = a.masks + (lwd + 1) * a.E;
+                struct Fetch {
+                    unsigned long long k0, k1, l0, l1;
+                    double L;
+                    bool ok;
+                };
+                auto fetch = [&](uint32_t batch) {
+                    Fetch f{0ull, 0ull, 0ull, 0ull, 0.0, false};
+                    const uint32_t e = r_begin + batch * 32 + lane;
+                    if (batch < n_batches && e < r_end && a.row_class[e] == 1) {
+                        f.k0 = k0_base[e];
+                        f.k1 = k1_base[e];
+                        f.l0 = l0_base[e];
+                        f.l1 = l1_base[e];
+                        f.L = static_cast<double>(a.len[e]);
+                        f.ok = true;
                     }
-                    double va[HSLOTS], vb[HSLOTS][4];
-#pragma unroll
-                    for (int j = 0; j < HSLOTS; j++) {
-                        const int c = slot_lane[j];
-                        const uint32_t e = __shfl_sync(0xffffffffu, e_cur, c);
-                        const uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
-                        const unsigned long long m0 = __shfl_sync(0xffffffffu, cur.m0, c);
-                        const unsigned long long m1 = __shfl_sync(0xffffffffu, cur.m1, c);
-                        const T *row = a.U + static_cast<uint64_t>(e) * a.ld;
-                        const bool live = j < cnt;
-                        va[j] = (live && lane < HROWS && ((mk >> lane) & 1u))
-                                    ? static_cast<double>(row[k0 + HROWS * warp + lane]) : 0.0;
-#pragma unroll
-                        for (int m = 0; m < 4; m++) {
-                            const unsigned long long wv = m < 2 ? m0 : m1;
-                            const bool on = live && ((wv >> (32 * (m & 1) + lane)) & 1ull);
-                            vb[j][m] = on ? static_cast<double>(row[l0 + 32 * m + lane]) : -1.0;
+                    return f;
+                };
+                // the col-th set bit (0-based) of the 128-bit word pair (w0, w1)
+                auto nth_bit = [](unsigned long long w0, unsigned long long w1, int col) -> int {
+                    const int c0 = __popcll(w0);
+                    const unsigned long long w = col < c0 ? w0 : w1;
+                    int r = col < c0 ? col : col - c0;
+                    const uint32_t lo = static_cast<uint32_t>(w), hi = static_cast<uint32_t>(w >> 32);
+                    const int pl = __popc(lo);
+                    const int bit = r < pl ? static_cast<int>(__fns(lo, 0, r + 1))
+                                           : 32 + static_cast<int>(__fns(hi, 0, r - pl + 1));
+                    return (col < c0 ? 0 : 64) + bit;
+                };
+                uint32_t b = warp;
+                Fetch cur = fetch(b), nxt = fetch(b + HWARPS);
+                for (; b < n_batches; b += HWARPS) {
+                    const Fetch after = fetch(b + 2 * HWARPS);
+                    const uint32_t e_cur = r_begin + b * 32 + lane;
+                    const int nk_l = __popcll(cur.k0) + __popcll(cur.k1);
+                    const int nl_l = __popcll(cur.l0) + __popcll(cur.l1);
+                    uint32_t active = __ballot_sync(0xffffffffu, cur.ok && nk_l > 0 && nl_l > 0);
+                    // rows with more than 32 present k or l columns take the
+                    // chunked path one at a time
+                    uint32_t wide = __ballot_sync(0xffffffffu, cur.ok && nk_l > 0 && nl_l > 0 &&
+                                                                  (nk_l > 32 || nl_l > 32));
+                    uint32_t narrow = active & ~wide;
+                    while (narrow) {
+                        int src[HSLOTS];
+                        int cnt = 0;
+    #pragma unroll
+                        for (int j = 0; j < HSLOTS; j++) {
+                            src[j] = narrow ? __ffs(narrow) - 1 : 0;
+                            cnt += narrow ? 1 : 0;
+                            narrow &= narrow ? narrow - 1 : 0u;
+                        }
+                        double va[HSLOTS], vb[HSLOTS];
+                        int kid[HSLOTS], lid[HSLOTS], nk[HSLOTS], nl[HSLOTS];
+    #pragma unroll
+                        for (int j = 0; j < HSLOTS; j++) {
+                            const int c = src[j];
+                            const uint32_t e = __shfl_sync(0xffffffffu, e_cur, c);
+                            const unsigned long long w0 = __shfl_sync(0xffffffffu, cur.k0, c);
+                            const unsigned long long w1 = __shfl_sync(0xffffffffu, cur.k1, c);
+                            const unsigned long long v0 = __shfl_sync(0xffffffffu, cur.l0, c);
+                            const unsigned long long v1 = __shfl_sync(0xffffffffu, cur.l1, c);
+                            nk[j] = j < cnt ? __popcll(w0) + __popcll(w1) : 0;
+                            nl[j] = j < cnt ? __popcll(v0) + __popcll(v1) : 0;
+                            const T *row = a.U + static_cast<uint64_t>(e) * a.ld;
+                            kid[j] = lane < nk[j] ? nth_bit(w0, w1, lane) : 0;
+                            lid[j] = lane < nl[j] ? nth_bit(v0, v1, lane) : 0;
+                            va[j] = lane < nk[j] ? static_cast<double>(row[k0 + kid[j]]) : 0.0;
+                            vb[j] = lane < nl[j] ? static_cast<double>(row[l0 + lid[j]]) : 0.0;
+                        }
+    #pragma unroll
+                        for (int j = 0; j < HSLOTS; j++) {
+                            if (j < cnt) {
+                                const double L2 = -2.0 * __shfl_sync(0xffffffffu, cur.L, src[j]);
+                                for (int kk = 0; kk < nk[j]; kk++) {
+                                    const double av = __shfl_sync(0xffffffffu, va[j], kk);
+                                    const int kr = __shfl_sync(0xffffffffu, kid[j], kk);
+                                    if (lane < nl[j]) atomicAdd(Mt + kr * HB + lid[j], L2 * fmin(av, vb[j]));
+                                }
+                            }
                         }
                     }
-#pragma unroll
-                    for (int j = 0; j < HSLOTS; j++) {
-                        if (j < cnt) {
+                    while (wide) {
+                        const int c = __ffs(wide) - 1;
+                        wide &= wide - 1;
+                        const uint32_t e = __shfl_sync(0xffffffffu, e_cur, c);
+                        const unsigned long long w0 = __shfl_sync(0xffffffffu, cur.k0, c);
+                        const unsigned long long w1 = __shfl_sync(0xffffffffu, cur.k1, c);
+                        const unsigned long long v0 = __shfl_sync(0xffffffffu, cur.l0, c);
+                        const unsigned long long v1 = __shfl_sync(0xffffffffu, cur.l1, c);
+                        const double L2 = -2.0 * __shfl_sync(0xffffffffu, cur.L, c);
+                        const int nkw = __popcll(w0) + __popcll(w1), nlw = __popcll(v0) + __popcll(v1);
+                        const T *row = a.U + static_cast<uint64_t>(e) * a.ld;
+                        for (int kc = 0; kc < nkw; kc += 32) {
+                            const int kq = kc + lane;
+                            const int kr_l = kq < nkw ? nth_bit(w0, w1, kq) : 0;
+                            const double a_l = kq < nkw ? static_cast<double>(row[k0 + kr_l]) : 0.0;
+                            for (int lc = 0; lc < nlw; lc += 32) {
+                                const int lq = lc + lane;
+                                const int lr = lq < nlw ? nth_bit(v0, v1, lq) : 0;
+                                const double b_l = lq < nlw ? static_cast<double>(row[l0 + lr]) : 0.0;
+                                const int kn = min(32, nkw - kc);
+                                for (int kk = 0; kk < kn; kk++) {
+                                    const double av = __shfl_sync(0xffffffffu, a_l, kk);
+                                    const int kr = __shfl_sync(0xffffffffu, kr_l, kk);
+                                    if (lq < nlw) atomicAdd(Mt + kr * HB + lr, L2 * fmin(av, b_l));
+                                }
+                            }
+                        }
+                    }
+                    cur = nxt;
+                    nxt = after;
+                }
+            }
+        } else {
+            // ---- sparse rows: -2 L min(a, b) where both are non-zero.  Each warp
+            // walks the embedded rows on its own (no block barrier) in batches of
+            // 32 consecutive rows, owning tile rows HROWS warp .. HROWS warp +
+            // HROWS - 1.  Lane i holds row i's class, mask words (its rows' word
+            // and the two words of the l block, coalesced over the batch) and
+            // length, fetched two batches ahead.  One ballot finds the sparse rows
+            // with a non-zero in both the warp's rows and the l block; their values
+            // are gathered HSLOTS rows at a time (lane r < HROWS: row value r,
+            // lane j: columns j + 32 m) and the updates of row r take its value
+            // from lane r by shuffle.
+            {
+                const uint64_t kwd = k0 / 64 + (warp * HROWS) / 64, lwd = l0 / 64;
+                const int kshift = (warp * HROWS) % 64;
+                constexpr uint32_t kmask = (1u << HROWS) - 1u;
+                double *Mw = Mt + HROWS * warp * HB;
+                const uint32_t er = (a.E + a.n_splits - 1) / a.n_splits;
+                const uint32_t r_begin = min(a.E, split * er), r_end = min(a.E, r_begin + er);
+                const uint32_t n_batches = r_end > r_begin ? (r_end - r_begin + 31) / 32 : 0;
+                const unsigned long long *mk_base = a.masks + kwd * a.E;
+                const unsigned long long *m0_base = a.masks + lwd * a.E;
+                const unsigned long long *m1_base = a.masks + (lwd + 1) * a.E;
+                struct Fetch {
+                    unsigned long long km, m0, m1;
+                    double L;
+                    bool ok;
+                };
+                auto fetch = [&](uint32_t batch) {
+                    Fetch f{0ull, 0ull, 0ull, 0.0, false};
+                    const uint32_t e = r_begin + batch * 32 + lane;
+                    if (batch < n_batches && e < r_end && a.row_class[e] == 1) {
+                        f.km = mk_base[e];
+                        f.m0 = m0_base[e];
+                        f.m1 = m1_base[e];
+                        f.L = static_cast<double>(a.len[e]);
+                        f.ok = true;
+                    }
+                    return f;
+                };
+                Fetch cur = fetch(0), nxt = fetch(1);
+                for (uint32_t b = 0; b < n_batches; b++) {
+                    const Fetch after = fetch(b + 2);
+                    const uint32_t e_cur = r_begin + b * 32 + lane;
+                    const uint32_t mk_l = static_cast<uint32_t>(cur.km >> kshift) & kmask;
+                    uint32_t active = __ballot_sync(0xffffffffu, cur.ok && mk_l != 0 && (cur.m0 | cur.m1) != 0ull);
+                    while (active) {
+                        int slot_lane[HSLOTS];
+                        int cnt = 0;
+    #pragma unroll
+                        for (int j = 0; j < HSLOTS; j++) {
+                            slot_lane[j] = active ? __ffs(active) - 1 : 0;
+                            cnt += active ? 1 : 0;
+                            active &= active ? active - 1 : 0u;
+                        }
+                        double va[HSLOTS], vb[HSLOTS][4];
+    #pragma unroll
+                        for (int j = 0; j < HSLOTS; j++) {
                             const int c = slot_lane[j];
-                            uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
-                            const double L2 = -2.0 * __shfl_sync(0xffffffffu, cur.L, c);
-                            while (mk) {
-                                const int r = __ffs(mk) - 1;
-                                mk &= mk - 1;
-                                const double av = __shfl_sync(0xffffffffu, va[j], r);
-#pragma unroll
-                                for (int m = 0; m < 4; m++) {
-                                    if (vb[j][m] >= 0.0) {
-                                        double *p = Mw + r * HB + 32 * m + lane;
-                                        *p = fma(L2, fmin(av, vb[j][m]), *p);
+                            const uint32_t e = __shfl_sync(0xffffffffu, e_cur, c);
+                            const uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
+                            const unsigned long long m0 = __shfl_sync(0xffffffffu, cur.m0, c);
+                            const unsigned long long m1 = __shfl_sync(0xffffffffu, cur.m1, c);
+                            const T *row = a.U + static_cast<uint64_t>(e) * a.ld;
+                            const bool live = j < cnt;
+                            va[j] = (live && lane < HROWS && ((mk >> lane) & 1u))
+                                        ? static_cast<double>(row[k0 + HROWS * warp + lane]) : 0.0;
+    #pragma unroll
+                            for (int m = 0; m < 4; m++) {
+                                const unsigned long long wv = m < 2 ? m0 : m1;
+                                const bool on = live && ((wv >> (32 * (m & 1) + lane)) & 1ull);
+                                vb[j][m] = on ? static_cast<double>(row[l0 + 32 * m + lane]) : -1.0;
+                            }
+                        }
+    #pragma unroll
+                        for (int j = 0; j < HSLOTS; j++) {
+                            if (j < cnt) {
+                                const int c = slot_lane[j];
+                                uint32_t mk = __shfl_sync(0xffffffffu, mk_l, c);
+                                const double L2 = -2.0 * __shfl_sync(0xffffffffu, cur.L, c);
+                                while (mk) {
+                                    const int r = __ffs(mk) - 1;
+                                    mk &= mk - 1;
+                                    const double av = __shfl_sync(0xffffffffu, va[j], r);
+    #pragma unroll
+                                    for (int m = 0; m < 4; m++) {
+                                        if (vb[j][m] >= 0.0) {
+                                            double *p = Mw + r * HB + 32 * m + lane;
+                                            *p = fma(L2, fmin(av, vb[j][m]), *p);
+                                        }
                                     }
                                 }
                             }
                         }
                     }
+                    cur = nxt;
+                    nxt = after;
                 }
-                cur = nxt;
-                nxt = after;
             }
         }
         __syncthreads();
