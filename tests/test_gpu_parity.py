@@ -370,3 +370,29 @@ def test_union_fp32_within_reference_fp32_error(ssu, oracle_mod, method, vaw):
     gpu, _ = ssu.one_off_matrix(tree, table, method + "_fp32", **kw)
     assert gpu.dtype == np.float32
     check_fp32(gpu, oracle_mod, tree, table, method, **kw)
+
+
+@pytest.mark.parametrize("method", ["unweighted", "weighted_normalized", "weighted_unnormalized", "generalized"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_negative_counts_take_the_dense_kernels(ssu, oracle_mod, method, prec):
+    """Negative entries (the reference accepts them): presence is u > 0, the
+    sparse forms need u >= 0, so weighted and generalized plans run the dense
+    kernels; results match the oracle (which matches the reference on this
+    input)."""
+    tree, base = _case(66, n_tips=120, n_samples=70, density=0.15)
+    rng = np.random.default_rng(166)
+    data = base.data.copy()
+    flip = rng.random(data.size) < 0.05
+    data[flip] = -0.5 * data[flip]
+    table = ssu_synth.Table(base.obs_ids, base.sample_ids, base.indptr, base.indices, data)
+    plan = ssu.Plan(tree, table, f"{method}_{prec}", alpha=1.0)
+    kernel = plan.pair_kernel()
+    plan.close()
+    assert "hybrid" not in kernel and "union" not in kernel and "tc" not in kernel
+    gpu, _ = ssu.one_off_matrix(tree, table, f"{method}_{prec}", alpha=1.0)
+    if prec == "fp64":
+        ref = oracle_mod.oracle_one_off(tree, table, method + "_fp64", alpha=1.0)["matrix"]
+        assert np.array_equal(np.isnan(gpu), np.isnan(ref))
+        check_fp64(gpu, ref)
+    else:
+        check_fp32(gpu, oracle_mod, tree, table, method, alpha=1.0)

@@ -77,3 +77,25 @@ def test_oracle_unnormalized_counts(ref):
         b = ref.oracle_one_off(tree, table, m, normalize=False)["matrix"]
         r, _ = rel_err(b, a)
         assert r <= 1e-13
+
+
+def _negative_case(seed):
+    """A table with about 5% of its entries negated (every sample keeps a
+    positive total)."""
+    tree, table = _small_case(seed)
+    rng = np.random.default_rng(seed + 99)
+    data = table.data.copy()
+    flip = rng.random(data.size) < 0.05
+    data[flip] = -0.5 * data[flip]
+    return tree, ssu_synth.Table(table.obs_ids, table.sample_ids, table.indptr, table.indices, data)
+
+
+@pytest.mark.parametrize("method,alpha", [("unweighted", 1.0), ("weighted_normalized", 1.0),
+                                          ("weighted_unnormalized", 1.0), ("generalized", 1.0)])
+def test_oracle_with_negative_counts_equals_reference(ref, method, alpha):
+    tree, table = _negative_case(15)
+    a = ref.ref_one_off(tree, table, method + "_fp64", alpha=alpha)["matrix"]
+    b = ref.oracle_one_off(tree, table, method + "_fp64", alpha=alpha)["matrix"]
+    assert np.array_equal(np.isnan(a), np.isnan(b))
+    r, z = rel_err(b, a)
+    assert r <= 1e-13 and z <= 1e-13
