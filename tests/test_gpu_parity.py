@@ -396,3 +396,24 @@ def test_negative_counts_take_the_dense_kernels(ssu, oracle_mod, method, prec):
         check_fp64(gpu, ref)
     else:
         check_fp32(gpu, oracle_mod, tree, table, method, alpha=1.0)
+
+
+def test_union_wait_that_runs_out_is_an_error_and_the_device_stays_usable(ssu, oracle_mod, monkeypatch):
+    """Failure injection without a fault: with UNIFRAC_B200_TEST_STALL the
+    union kernel's producer issues no copy, so every consumer's bounded wait
+    (here ~1 ms) runs out; the call returns output_error instead of hanging,
+    and the next call in the same process is correct."""
+    tree, table = _case(67, n_tips=200, n_samples=80, density=0.05)
+    kw = dict(variance_adjust=True, alpha=0.5)
+    monkeypatch.setenv("UNIFRAC_B200_TEST_STALL", "1")
+    monkeypatch.setenv("UNIFRAC_B200_WAIT_CYCLES", "2000000")
+    plan = ssu.Plan(tree, table, "generalized_fp64", **kw)
+    assert plan.pair_kernel().startswith("pair_union")
+    plan.close()
+    with pytest.raises(ssu.SSUError) as e:
+        ssu.one_off_matrix(tree, table, "generalized_fp64", **kw)
+    assert e.value.status == 6  # output_error
+    monkeypatch.delenv("UNIFRAC_B200_TEST_STALL")
+    monkeypatch.delenv("UNIFRAC_B200_WAIT_CYCLES")
+    gpu, _ = ssu.one_off_matrix(tree, table, "generalized_fp64", **kw)
+    check_fp64(gpu, oracle_mod.oracle_one_off(tree, table, "generalized_fp64", **kw)["matrix"])

@@ -295,6 +295,12 @@ struct PlanImpl {
     double *d_upartial = nullptr;
     size_t upartial_bytes = 0;
     void *d_slen = nullptr;  // branch length per sparse row, in sparse-row order
+    // budget of one mbarrier wait in the union kernel (UNIFRAC_B200_WAIT_CYCLES,
+    // default about one second), and its test switch UNIFRAC_B200_TEST_STALL=1
+    // (the kernel's producer issues nothing, so its waits run out and the call
+    // returns output_error: host-side failure injection, no fault)
+    long long union_wait_cycles = 2000000000LL;
+    int union_stall = 0;
     int sparse_prep_alloc();
     template <typename T>
     int sparse_prep(cudaStream_t s, const Group &g, uint32_t div);
@@ -840,6 +846,8 @@ int PlanImpl::sparse_prep(cudaStream_t s, const Group &g, uint32_t div) {
 template <typename T>
 int PlanImpl::setup_union() {
     union_div = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_UNION_DIV", 3)));
+    if (const char *w = std::getenv("UNIFRAC_B200_WAIT_CYCLES")) union_wait_cycles = std::max(0LL, std::atoll(w));
+    union_stall = env_int("UNIFRAC_B200_TEST_STALL", 0) ? 1 : 0;
     if (const int rc = sparse_prep_alloc()) return rc;
     size_t smem = 0;
     SSU_CK(dev::union_configure<T>(spec, &smem));
@@ -909,7 +917,8 @@ int PlanImpl::union_stage(cudaStream_t s, const Group &g, const dev::OutSpec &ou
     u.partial = u.n_splits > 1 ? d_upartial : nullptr;
     u.out = out;
     u.error = d_error;
-    u.wait_cycles = 2000000000LL;  // about one second per wait at B200 clocks
+    u.wait_cycles = union_wait_cycles;
+    u.stall = union_stall;
     const uint32_t ctas = static_cast<uint32_t>(
         std::min<uint64_t>(static_cast<uint64_t>(ntiles) * u.n_splits, static_cast<uint64_t>(n_sms)));
     SSU_CK(dev::union_launch<T>(spec, u, ctas, s));

@@ -47,9 +47,12 @@ struct UnionArgs {
     OutSpec out;
     int *error;          // first error code of any block
     long long wait_cycles;
+    int stall;           // test switch: the producer issues nothing, so every
+                         // consumer wait runs out (off in normal use)
 };
 
 enum : int { UNION_ERR_FULL_WAIT = 11, UNION_ERR_EMPTY_WAIT = 12, UNION_ERR_DRAIN_WAIT = 13 };
+constexpr long long kDrainCycles = 2000000000LL;  // about one second at B200 clocks
 
 constexpr int UT = 64;                    // tile: 64 (k) x 64 (l)
 constexpr int UCW = 16;                   // consumer warps
@@ -184,7 +187,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
             };
             uint32_t e1 = id_of(0), e2 = id_of(1);
             uint32_t issued = 0;
-            for (uint32_t c = 0; c < n_chunks; c++) {
+            for (uint32_t c = 0; c < (a.stall ? 0u : n_chunks); c++) {
                 const uint32_t e = e1;
                 e1 = e2;
                 e2 = id_of(c + 2);
@@ -223,9 +226,11 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
                 issued = c + 1;
             }
             // never leave with copies in flight: each stage's last fill lands
+            // (at least about a second per wait, whatever the wait budget)
+            const long long drain_budget = budget > kDrainCycles ? budget : kDrainCycles;
             if (lane == 0)
                 for (uint32_t c = issued > static_cast<uint32_t>(NS) ? issued - NS : 0; c < issued; c++)
-                    if (!mbar_wait(full + (g + c) % NS, ((g + c) / NS) & 1, budget))
+                    if (!mbar_wait(full + (g + c) % NS, ((g + c) / NS) & 1, drain_budget))
                         union_fail(abort_flag, a.error, UNION_ERR_DRAIN_WAIT);
             __syncwarp();
         } else {
