@@ -174,3 +174,26 @@ def test_header_is_plain_c(tmp_path):
     subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", inc, str(src), "-o", str(exe), "-L", libdir,
                     "-lssu_b200", f"-Wl,-rpath,{libdir}"], check=True)
     assert subprocess.run([str(exe)]).returncode == 0
+
+
+def test_malformed_csr_is_rejected_before_device_work(ssu, test_tree, test_table):
+    """A borrowed CSR whose offsets or sample positions are out of range would
+    be read and scattered out of bounds; it is reported as table_missing
+    (the reference has no check and reads out of bounds)."""
+    t = test_table
+
+    def with_arrays(indptr, indices):
+        return ssu_synth.Table(t.obs_ids, t.sample_ids, indptr, indices, t.data)
+
+    bad_index = t.indices.copy()
+    bad_index[len(bad_index) // 2] = t.n_samples
+    assert ssu.status_of_matrix_call(test_tree, with_arrays(t.indptr, bad_index), "unweighted_fp64") == 2
+    shifted = t.indptr.copy()
+    shifted[0] = 1
+    assert ssu.status_of_matrix_call(test_tree, with_arrays(shifted, t.indices), "unweighted_fp64") == 2
+    decreasing = t.indptr.copy()
+    decreasing[2] = decreasing[1] - 1 if decreasing[1] > 0 else decreasing[3] + 1
+    assert ssu.status_of_matrix_call(test_tree, with_arrays(decreasing, t.indices), "weighted_normalized_fp64") == 2
+    # the well-formed table passes this check (without a GPU it stops later,
+    # at the device)
+    assert ssu.status_of_matrix_call(test_tree, t, "unweighted_fp64") != 2

@@ -165,6 +165,10 @@ const ssu::TipMatch &tip_match(const ssu::Table &table, const ssu::BPTree &tree)
 // VALIDATE_TREE_TABLE (src/api.cpp:94-100): every table id is a tip name.
 ComputeStatus validate(const ssu::Table &table, const ssu::BPTree &tree) {
     if (table.n_samples == 0 || table.n_obs == 0) return table_empty;
+    if (table.malformed) {
+        report("table", "malformed CSR (offsets or sample positions out of range)");
+        return table_missing;
+    }
     const ssu::TipMatch &m = tip_match(table, tree);
     return m.rows_matched == table.distinct_names ? okay : table_and_tree_do_not_overlap;
 }
@@ -458,6 +462,10 @@ ComputeStatus batch_prepare(const std::vector<const ssu::Table *> &tables, const
     size_t total_obs = 0;
     for (const ssu::Table *t : tables) {
         if (t->n_samples == 0 || t->n_obs == 0) return table_empty;
+        if (t->malformed) {
+            report("table", "malformed CSR (offsets or sample positions out of range)");
+            return table_missing;
+        }
         total_obs += t->n_obs;
     }
     ssu::NameMap uni(total_obs);

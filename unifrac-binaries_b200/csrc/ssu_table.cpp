@@ -13,8 +13,20 @@ void Table::adopt_owned() {
 
 void Table::compute_totals() {
     totals.assign(n_samples, 0.0);
-    for (uint32_t i = 0; i < n_obs; i++)
-        for (uint32_t q = indptr[i]; q < indptr[i + 1]; q++) totals[indices[q]] += data[q];
+    if (n_obs && indptr[0] != 0) malformed = true;
+    for (uint32_t i = 0; i < n_obs; i++) {
+        if (indptr[i + 1] < indptr[i]) {
+            malformed = true;
+            continue;
+        }
+        for (uint32_t q = indptr[i]; q < indptr[i + 1]; q++) {
+            const uint32_t j = indices[q];
+            if (j < n_samples)
+                totals[j] += data[q];
+            else
+                malformed = true;
+        }
+    }
 }
 
 Table Table::borrow(uint32_t n_obs, uint32_t n_samples, const uint32_t *indptr, const uint32_t *indices,

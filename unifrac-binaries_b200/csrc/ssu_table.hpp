@@ -31,6 +31,10 @@ struct Table {
     std::vector<std::string_view> obs_ids;
     std::vector<std::string_view> sample_ids;
     std::vector<double> totals;  // per-sample sum, accumulated in observation order
+    // a borrowed CSR that cannot be indexed safely: offsets not starting at 0
+    // or decreasing, or a sample position >= n_samples (such entries are left
+    // out of the totals; validation rejects the table before device work)
+    bool malformed = false;
 
     // Name matching of this table against the call's tree, made once by the
     // validation and reused by the shear (host-side cache of one call).
