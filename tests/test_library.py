@@ -197,3 +197,14 @@ def test_malformed_csr_is_rejected_before_device_work(ssu, test_tree, test_table
     # the well-formed table passes this check (without a GPU it stops later,
     # at the device)
     assert ssu.status_of_matrix_call(test_tree, t, "unweighted_fp64") != 2
+
+
+def test_unbalanced_tree_is_rejected_before_device_work(ssu, test_tree, test_table):
+    """Parentheses that do not pair up are reported as tree_missing."""
+    t = test_tree
+    open_end = np.array(t.structure, dtype=bool).copy()
+    open_end[-1] = True  # the root never closes
+    tree = ssu_synth.BPTree(open_end, t.lengths, t.names)
+    assert ssu.status_of_matrix_call(tree, test_table, "unweighted_fp64") == 1
+    odd = ssu_synth.BPTree(np.array(t.structure, dtype=bool)[:-1], t.lengths[:-1], t.names[:-1])
+    assert ssu.status_of_matrix_call(odd, test_table, "weighted_normalized_fp64") == 1

@@ -169,6 +169,10 @@ ComputeStatus validate(const ssu::Table &table, const ssu::BPTree &tree) {
         report("table", "malformed CSR (offsets or sample positions out of range)");
         return table_missing;
     }
+    if (tree.malformed) {
+        report("tree", "parentheses do not pair up");
+        return tree_missing;
+    }
     const ssu::TipMatch &m = tip_match(table, tree);
     return m.rows_matched == table.distinct_names ? okay : table_and_tree_do_not_overlap;
 }
@@ -459,6 +463,10 @@ struct BatchHost {
 ComputeStatus batch_prepare(const std::vector<const ssu::Table *> &tables, const ssu::BPTree &tree, bool bypass,
                             BatchHost &bh) {
     if (tables.empty() || tables.size() > 65535) return table_empty;
+    if (tree.malformed) {
+        report("tree", "parentheses do not pair up");
+        return tree_missing;
+    }
     size_t total_obs = 0;
     for (const ssu::Table *t : tables) {
         if (t->n_samples == 0 || t->n_obs == 0) return table_empty;

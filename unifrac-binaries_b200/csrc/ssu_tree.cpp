@@ -8,8 +8,9 @@ namespace ssu {
 
 void BPTree::pair_parentheses() {
     match.assign(open.size(), 0);
-    std::vector<uint32_t> stack(open.size() / 2 + 1);
+    std::vector<uint32_t> stack(open.size() + 1);
     size_t top = 0;
+    malformed = open.size() % 2 != 0;
     for (uint32_t i = 0; i < open.size(); i++) {
         if (open[i]) {
             stack[top++] = i;
@@ -17,8 +18,11 @@ void BPTree::pair_parentheses() {
             const uint32_t o = stack[--top];
             match[o] = i;
             match[i] = o;
+        } else {
+            malformed = true;
         }
     }
+    if (top != 0) malformed = true;
 }
 
 BPTree BPTree::from_arrays(const bool *structure, const double *lengths, const char *const *names, int n,

@@ -46,6 +46,9 @@ struct BPTree {
     // optional per-parenthesis tag carried through shear/collapse: the table
     // row of each kept tip (-1 elsewhere)
     std::vector<int32_t> tag;
+    // parentheses that do not pair up (odd count, a close without an open, or
+    // opens left at the end): validation rejects the tree before device work
+    bool malformed = false;
 
     uint32_t size() const { return static_cast<uint32_t>(open.size()); }
     bool leaf(uint32_t i) const { return open[i] && i + 1 < open.size() && !open[i + 1]; }
