@@ -419,8 +419,7 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
     full_elems = 0;
     for (uint32_t t = 0; t < n_tables; t++) {
         const Table &tb = *set.tables[t];
-        for (uint64_t q = 0; q < tb.nnz() && nonneg_data; q++)
-            if (!(tb.data[q] >= 0.0)) nonneg_data = false;
+        if (!tb.nonneg) nonneg_data = false;
         dev::TableDesc &d = tdesc[t];
         d.n = tb.n_samples;
         d.out_off = full_elems;

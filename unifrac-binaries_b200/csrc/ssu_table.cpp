@@ -13,6 +13,8 @@ void Table::adopt_owned() {
 
 void Table::compute_totals() {
     totals.assign(n_samples, 0.0);
+    nonneg = true;
+    malformed = false;
     if (n_obs && indptr[0] != 0) malformed = true;
     for (uint32_t i = 0; i < n_obs; i++) {
         if (indptr[i + 1] < indptr[i]) {
@@ -21,6 +23,7 @@ void Table::compute_totals() {
         }
         for (uint32_t q = indptr[i]; q < indptr[i + 1]; q++) {
             const uint32_t j = indices[q];
+            if (!(data[q] >= 0.0)) nonneg = false;
             if (j < n_samples)
                 totals[j] += data[q];
             else
@@ -79,6 +82,7 @@ Table Table::filtered(double min_total) const {
             if (new_idx[indices[q]] == UINT32_MAX) continue;
             t.own_indices.push_back(new_idx[indices[q]]);
             t.own_data.push_back(data[q]);
+            if (!(data[q] >= 0.0)) t.nonneg = false;
         }
         if (t.own_indices.size() > before) {
             t.obs_ids.push_back(obs_ids[i]);

@@ -35,6 +35,8 @@ struct Table {
     // or decreasing, or a sample position >= n_samples (such entries are left
     // out of the totals; validation rejects the table before device work)
     bool malformed = false;
+    // no entry below zero (found while the totals are summed)
+    bool nonneg = true;
 
     // Name matching of this table against the call's tree, made once by the
     // validation and reused by the shear (host-side cache of one call).
