@@ -417,3 +417,23 @@ def test_union_wait_that_runs_out_is_an_error_and_the_device_stays_usable(ssu, o
     monkeypatch.delenv("UNIFRAC_B200_WAIT_CYCLES")
     gpu, _ = ssu.one_off_matrix(tree, table, "generalized_fp64", **kw)
     check_fp64(gpu, oracle_mod.oracle_one_off(tree, table, "generalized_fp64", **kw)["matrix"])
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_hybrid_with_every_row_sparse_matches_dense_form(ssu, monkeypatch, prec):
+    """UNIFRAC_B200_HYBRID_DIV=1 sends every row, however dense, through the
+    sparse-row path: rows with more than 32 present columns in a 128-column
+    block take its chunked branch (fp32) or long walks (fp64)."""
+    tree, table = _case(68, n_tips=200, n_samples=300, density=0.3)
+    monkeypatch.setenv("UNIFRAC_B200_WEIGHTED_MODE", "dense")
+    dense, _ = ssu.one_off_matrix(tree, table, f"weighted_normalized_{prec}")
+    monkeypatch.delenv("UNIFRAC_B200_WEIGHTED_MODE")
+    monkeypatch.setenv("UNIFRAC_B200_HYBRID_DIV", "1")
+    plan = ssu.Plan(tree, table, f"weighted_normalized_{prec}")
+    assert plan.pair_kernel().startswith("pair_hybrid")
+    plan.close()
+    sparse, _ = ssu.one_off_matrix(tree, table, f"weighted_normalized_{prec}")
+    if prec == "fp64":
+        check_fp64(sparse, dense)
+    else:
+        np.testing.assert_allclose(sparse, dense, rtol=5e-6, atol=1e-7)
