@@ -672,8 +672,9 @@ def main():
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": algo_bytes,
                          "note": "reference-form bytes (2 fp64 accumulators RMW per 112-node batch) over the "
-                                 "pair stage (row masks, dense/sparse row lists, one-sided sums, hybrid tile "
-                                 "kernel); traffic is the hybrid kernel's measured DRAM bytes per launch",
+                                 "pair stage (dense/sparse row lists, one-sided sums, hybrid tile kernel; the "
+                                 "presence masks are written by the embedding, outside the stage); traffic is "
+                                 "the hybrid kernel's measured DRAM bytes per launch",
                          "fp64_dense_equivalent": {"achieved_tflops": fp64_achieved,
                                                    "peak_tflops_at_clock": fp64_peak,
                                                    "frac": fp64_achieved / fp64_peak}},

@@ -822,19 +822,11 @@ int PlanImpl::sparse_prep_alloc() {
     return 0;
 }
 
-// Masks and counts of the group's embedding, then the row classes (dense:
-// non-zero in more than ld / div columns).
+// Row classes of the group's embedding (dense: non-zero in more than ld / div
+// columns), from the counts the embedding wrote with the masks.
 template <typename T>
 int PlanImpl::sparse_prep(cudaStream_t s, const Group &g, uint32_t div) {
-    const T *U = static_cast<const T *>(d_U);
-    const uint64_t words = g.ld / 64;
-    SSU_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * std::max<uint32_t>(E, 1), s));
-    if (E) {
-        const uint64_t items = static_cast<uint64_t>(E) * words;
-        const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>((items + 7) / 8, 1u << 20));
-        dev::row_masks_kernel<T><<<grid, 256, 0, s>>>(U, E, g.ld, d_masks, d_counts);
-        launches++;
-    }
+    if (!E) SSU_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t), s));
     dev::classify_rows_kernel<<<1, 1024, 0, s>>>(d_counts, E, static_cast<uint32_t>(g.ld / div), d_dense_rows,
                                                  d_sparse_rows, d_row_class, d_nrows);
     launches++;
@@ -1019,16 +1011,25 @@ int PlanImpl::embed(cudaStream_t s, const Group &g) {
     T *C = static_cast<T *>(d_C);
     const bool normalize = faith ? true : spec.normalize;
     const uint32_t tg = g.t1 - g.t0;
+    // the sparse pair kernels' presence masks and counts, filled as rows are
+    // embedded (no separate pass over U)
+    dev::MaskOut mo{nullptr, nullptr, E};
+    if ((hybrid || union_mode) && d_masks && E) {
+        SSU_CK(cudaMemsetAsync(d_masks, 0, sizeof(unsigned long long) * E * (g.ld / 64), s));
+        SSU_CK(cudaMemsetAsync(d_counts, 0, sizeof(uint32_t) * E, s));
+        mo.masks = d_masks;
+        mo.counts = d_counts;
+    }
     if (n_tips) {
         const uint32_t grid = std::min<uint32_t>(n_tips, 65535u * 8);
         if (counts)
             dev::embed_tips_kernel<T, true><<<grid, 256, 0, s>>>(d_tip_rows, g.d_tip_obs, n_tips, tg, d_tdesc + g.t0,
                                                                  d_indptr, d_indices, d_data, g.d_totals, normalize,
-                                                                 U, C, g.ld);
+                                                                 U, C, g.ld, mo);
         else
             dev::embed_tips_kernel<T, false><<<grid, 256, 0, s>>>(d_tip_rows, g.d_tip_obs, n_tips, tg,
                                                                   d_tdesc + g.t0, d_indptr, d_indices, d_data,
-                                                                  g.d_totals, normalize, U, C, g.ld);
+                                                                  g.d_totals, normalize, U, C, g.ld, mo);
         launches++;
     }
     const uint64_t nvec = g.ld / dev::Vec16<T>::n;
@@ -1041,10 +1042,10 @@ int PlanImpl::embed(cudaStream_t s, const Group &g) {
         const uint32_t grid = static_cast<uint32_t>(std::min<uint64_t>(blocks, 1u << 20));
         if (counts)
             dev::embed_level_kernel<T, true><<<grid, threads, 0, s>>>(d_level_rows + a, b - a, d_child_ptr,
-                                                                      d_child_rows, U, C, g.ld, col_blocks);
+                                                                      d_child_rows, U, C, g.ld, col_blocks, mo);
         else
             dev::embed_level_kernel<T, false><<<grid, threads, 0, s>>>(d_level_rows + a, b - a, d_child_ptr,
-                                                                       d_child_rows, U, C, g.ld, col_blocks);
+                                                                       d_child_rows, U, C, g.ld, col_blocks, mo);
         launches++;
     }
     SSU_CK(cudaGetLastError());

@@ -96,12 +96,40 @@ struct TableDesc {
 // observation from every table of the group; proportions are data / total in
 // fp64 and then rounded to T (src/biom_inmem.cpp:473-497).
 // tip_obs[t * n_tables + i] = row of tip t's observation in table i, or -1.
+// Presence masks written by the embedding (the sparse pair kernels' input):
+// bit i of masks[w * E + row] is U[row][64 w + i] > 0, counts[row] the row's
+// set bits; both zeroed before the embedding.  masks == nullptr: none.
+struct MaskOut {
+    unsigned long long *masks;
+    uint32_t *counts;
+    uint32_t E;
+};
+
+// bit i of x -> bit 2i, and bit i of the low 16 bits -> bit 4i
+__device__ __forceinline__ unsigned long long spread2(uint32_t v) {
+    unsigned long long x = v;
+    x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
+    x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x << 2)) & 0x3333333333333333ull;
+    x = (x | (x << 1)) & 0x5555555555555555ull;
+    return x;
+}
+__device__ __forceinline__ unsigned long long spread4(uint32_t v) {
+    unsigned long long x = v & 0xFFFFu;
+    x = (x | (x << 24)) & 0x000000FF000000FFull;
+    x = (x | (x << 12)) & 0x000F000F000F000Full;
+    x = (x | (x << 6)) & 0x0303030303030303ull;
+    x = (x | (x << 3)) & 0x1111111111111111ull;
+    return x;
+}
+
 template <typename T, bool COUNTS>
 __global__ void embed_tips_kernel(const uint32_t *__restrict__ tip_rows, const int32_t *__restrict__ tip_obs,
                                   uint32_t n_tips, uint32_t n_tables, const TableDesc *__restrict__ tables,
                                   const uint32_t *__restrict__ indptr, const uint32_t *__restrict__ indices,
                                   const double *__restrict__ data, const double *__restrict__ totals, bool normalize,
-                                  T *__restrict__ U, T *__restrict__ C, uint64_t ld) {
+                                  T *__restrict__ U, T *__restrict__ C, uint64_t ld, MaskOut mo) {
     for (uint32_t t = blockIdx.x; t < n_tips; t += gridDim.x) {
         const uint64_t row = tip_rows[t];
         T *u = U + row * ld;
@@ -120,8 +148,13 @@ __global__ void embed_tips_kernel(const uint32_t *__restrict__ tip_rows, const i
                 const uint64_t qa = td.nnz_off + q;
                 const uint32_t j = td.base + indices[qa];
                 const double v = data[qa];
-                u[j] = normalize ? static_cast<T>(v / totals[j]) : static_cast<T>(v);
+                const T uv = normalize ? static_cast<T>(v / totals[j]) : static_cast<T>(v);
+                u[j] = uv;
                 if (COUNTS) c[j] = static_cast<T>(v);
+                if (mo.masks && row < mo.E && uv > T(0)) {
+                    atomicOr(mo.masks + (j >> 6) * mo.E + row, 1ull << (j & 63));
+                    atomicAdd(mo.counts + row, 1u);
+                }
             }
         }
         __syncthreads();
@@ -147,23 +180,56 @@ template <> struct Vec16<float> {
 template <typename T, bool COUNTS>
 __global__ void embed_level_kernel(const uint32_t *__restrict__ rows, uint32_t n_rows,
                                    const uint32_t *__restrict__ child_ptr, const uint32_t *__restrict__ child_rows,
-                                   T *__restrict__ U, T *__restrict__ C, uint64_t ld, uint32_t col_blocks) {
+                                   T *__restrict__ U, T *__restrict__ C, uint64_t ld, uint32_t col_blocks, MaskOut mo) {
     using V = typename Vec16<T>::type;
     const uint64_t nvec = ld / Vec16<T>::n;
     const uint64_t total = static_cast<uint64_t>(n_rows) * col_blocks;
+    const uint32_t lane = threadIdx.x & 31;
     for (uint64_t b = blockIdx.x; b < total; b += gridDim.x) {
         const uint32_t row = rows[b / col_blocks];
         const uint64_t v = (b % col_blocks) * blockDim.x + threadIdx.x;
-        if (v >= nvec) continue;
+        const bool ok = v < nvec;
         V s = Vec16<T>::zero();
         V sc = Vec16<T>::zero();
-        for (uint32_t c = child_ptr[row]; c < child_ptr[row + 1]; c++) {
-            const uint64_t cr = child_rows[c];
-            s = Vec16<T>::add(s, reinterpret_cast<const V *>(U + cr * ld)[v]);
-            if (COUNTS) sc = Vec16<T>::add(sc, reinterpret_cast<const V *>(C + cr * ld)[v]);
+        if (ok) {
+            for (uint32_t c = child_ptr[row]; c < child_ptr[row + 1]; c++) {
+                const uint64_t cr = child_rows[c];
+                s = Vec16<T>::add(s, reinterpret_cast<const V *>(U + cr * ld)[v]);
+                if (COUNTS) sc = Vec16<T>::add(sc, reinterpret_cast<const V *>(C + cr * ld)[v]);
+            }
+            reinterpret_cast<V *>(U + static_cast<uint64_t>(row) * ld)[v] = s;
+            if (COUNTS) reinterpret_cast<V *>(C + static_cast<uint64_t>(row) * ld)[v] = sc;
         }
-        reinterpret_cast<V *>(U + static_cast<uint64_t>(row) * ld)[v] = s;
-        if (COUNTS) reinterpret_cast<V *>(C + static_cast<uint64_t>(row) * ld)[v] = sc;
+        if (mo.masks) {
+            // the warp's 32 vectors are 64 (fp64) or 128 (fp32) consecutive
+            // columns starting on a 64-column word
+            const uint64_t w0 = (v - lane) * Vec16<T>::n / 64;
+            if constexpr (sizeof(T) == 8) {
+                const uint32_t bx = __ballot_sync(0xffffffffu, ok && s.x > T(0));
+                const uint32_t by = __ballot_sync(0xffffffffu, ok && s.y > T(0));
+                if (lane == 0 && row < mo.E) {
+                    const unsigned long long word = spread2(bx) | (spread2(by) << 1);
+                    if (word) {
+                        mo.masks[w0 * mo.E + row] = word;
+                        atomicAdd(mo.counts + row, static_cast<uint32_t>(__popcll(word)));
+                    }
+                }
+            } else {
+                const uint32_t b0 = __ballot_sync(0xffffffffu, ok && s.x > T(0));
+                const uint32_t b1 = __ballot_sync(0xffffffffu, ok && s.y > T(0));
+                const uint32_t b2 = __ballot_sync(0xffffffffu, ok && s.z > T(0));
+                const uint32_t b3 = __ballot_sync(0xffffffffu, ok && s.w > T(0));
+                if (lane < 2 && row < mo.E) {
+                    const uint32_t sh = 16 * lane;
+                    const unsigned long long word = spread4(b0 >> sh) | (spread4(b1 >> sh) << 1) |
+                                                    (spread4(b2 >> sh) << 2) | (spread4(b3 >> sh) << 3);
+                    if (word && (w0 + lane) * 64 < ld) {
+                        mo.masks[(w0 + lane) * mo.E + row] = word;
+                        atomicAdd(mo.counts + row, static_cast<uint32_t>(__popcll(word)));
+                    }
+                }
+            }
+        }
     }
 }
 

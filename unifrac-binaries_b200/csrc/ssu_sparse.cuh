@@ -25,7 +25,8 @@
 // kernel afterwards.
 //
 // Presence masks, word-major: bit i of masks[w * E + e] is U[e][64 w + i] > 0,
-// so the masks of consecutive rows for one 64-column word are contiguous.
+// so the masks of consecutive rows for one 64-column word are contiguous; the
+// embedding kernels write them (and the per-row counts) as they fill U.
 #pragma once
 
 #include <cstdint>
@@ -35,29 +36,6 @@
 
 namespace ssu {
 namespace dev {
-
-// Presence masks (word-major) and non-zero counts of the embedded rows; one
-// warp per (row, 64-column word).  counts must start at zero.
-template <typename T>
-__global__ void row_masks_kernel(const T *__restrict__ U, uint32_t E, uint64_t ld,
-                                 unsigned long long *__restrict__ masks, uint32_t *__restrict__ counts) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t words = ld / 64;
-    const uint64_t total = static_cast<uint64_t>(E) * words;
-    const uint64_t nwarps = static_cast<uint64_t>(gridDim.x) * (blockDim.x / 32);
-    for (uint64_t item = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / 32; item < total;
-         item += nwarps) {
-        const uint64_t e = item / words, w = item % words;
-        const T *u = U + e * ld + w * 64;
-        const uint32_t b0 = __ballot_sync(0xffffffffu, u[lane] > T(0));
-        const uint32_t b1 = __ballot_sync(0xffffffffu, u[lane + 32] > T(0));
-        if (lane == 0) {
-            masks[w * E + e] = static_cast<unsigned long long>(b0) | (static_cast<unsigned long long>(b1) << 32);
-            const uint32_t c = __popc(b0) + __popc(b1);
-            if (c) atomicAdd(counts + e, c);
-        }
-    }
-}
 
 // Rows in order into dense (count > threshold) and sparse (0 < count <=
 // threshold) lists, and each row's class (0 all zero, 1 sparse, 2 dense);
