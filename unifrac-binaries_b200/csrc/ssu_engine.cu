@@ -737,14 +737,24 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
                            uint32_t ntiles, uint32_t splits, bool last) {
     const T *U = static_cast<const T *>(d_U);
     if (const int rc = sparse_prep<T>(s, g, hybrid_div)) return rc;
-    {
+    if (d_W) {
+        // weighted normalized: W and Ws in one pass over the embedding
+        dim3 grid(static_cast<uint32_t>((g.ld + 127) / 128), n_parts);
+        dev::hybrid_sums_partial_kernel<T><<<grid, 128, 0, s>>>(U, static_cast<const T *>(d_len), d_row_class, E,
+                                                                g.ld, part_chunk, static_cast<T *>(d_part), d_ws_part);
+        dev::reduce_partials_kernel<T><<<static_cast<uint32_t>((g.ld + 255) / 256), 256, 0, s>>>(
+            static_cast<const T *>(d_part), n_parts, g.ld, static_cast<T *>(d_W));
+        launches += 2;
+    } else {
+        // weighted unnormalized: Ws only, reading the sparse rows alone
         dim3 grid(static_cast<uint32_t>((g.ld + 255) / 256), n_parts);
         dev::sparse_sums_partial_kernel<T><<<grid, 256, 0, s>>>(U, static_cast<const T *>(d_len), d_sparse_rows,
                                                                 d_nrows, g.ld, part_chunk, d_ws_part);
-        dev::reduce_partials_kernel<double><<<static_cast<uint32_t>((g.ld + 255) / 256), 256, 0, s>>>(
-            d_ws_part, n_parts, g.ld, d_Ws);
-        launches += 2;
+        launches++;
     }
+    dev::reduce_partials_kernel<double><<<static_cast<uint32_t>((g.ld + 255) / 256), 256, 0, s>>>(
+        d_ws_part, n_parts, g.ld, d_Ws);
+    launches++;
     if (ntiles == 0) return 0;
     SSU_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * ntiles, s));
     dev::HybridArgs<T> h{};
@@ -1056,7 +1066,7 @@ template <typename T>
 int PlanImpl::prepare(cudaStream_t s, const Group &g) {
     const T *U = static_cast<const T *>(d_U);
     const T *len = static_cast<const T *>(d_len);
-    if (d_W) {
+    if (d_W && !hybrid) {  // the hybrid sums W with its Ws (hybrid_stage)
         dim3 grid(static_cast<uint32_t>((g.ld + 127) / 128), n_parts);
         dev::weighted_sums_partial_kernel<T><<<grid, 128, 0, s>>>(U, len, E, g.ld, part_chunk,
                                                                  static_cast<T *>(d_part),

@@ -83,6 +83,7 @@ static __global__ void __launch_bounds__(1024) classify_rows_kernel(const uint32
 
 // Ws[j] = sum over the sparse rows (in order, in fixed chunks) of L u[j],
 // in fp64; partial sums per chunk, then reduce_partials_kernel<double>.
+// (weighted unnormalized: no W is needed, so only the sparse rows are read)
 template <typename T>
 __global__ void sparse_sums_partial_kernel(const T *__restrict__ U, const T *__restrict__ len,
                                            const uint32_t *__restrict__ rows, const uint32_t *__restrict__ n_rows,
@@ -98,6 +99,31 @@ __global__ void sparse_sums_partial_kernel(const T *__restrict__ U, const T *__r
         s = fma(static_cast<double>(U[static_cast<uint64_t>(e) * ld + j]), static_cast<double>(len[e]), s);
     }
     partial[static_cast<uint64_t>(blockIdx.y) * ld + j] = s;
+}
+
+// One pass over the embedding for both one-sided sums of the hybrid, per
+// column j and chunk of `chunk` rows (weighted normalized): W[j] = sum of
+// L u[j] over every row, in T as the dense kernels'
+// weighted_sums_partial_kernel, and Ws[j] = the same over the sparse rows
+// (row_class 1), in fp64; partial sums per chunk, then reduce_partials_kernel.
+template <typename T>
+__global__ void hybrid_sums_partial_kernel(const T *__restrict__ U, const T *__restrict__ len,
+                                           const uint8_t *__restrict__ row_class, uint32_t E, uint64_t ld,
+                                           uint32_t chunk, T *__restrict__ w_part, double *__restrict__ ws_part) {
+    const uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= ld) return;
+    const uint32_t e0 = blockIdx.y * chunk;
+    const uint32_t e1 = min(E, e0 + chunk);
+    T s = T(0);
+    double ss = 0.0;
+    for (uint32_t e = e0; e < e1; e++) {
+        const T u = U[static_cast<uint64_t>(e) * ld + j];
+        const T L = len[e];
+        s = fma(u, L, s);
+        if (row_class[e] == 1) ss = fma(static_cast<double>(u), static_cast<double>(L), ss);
+    }
+    w_part[static_cast<uint64_t>(blockIdx.y) * ld + j] = s;
+    ws_part[static_cast<uint64_t>(blockIdx.y) * ld + j] = ss;
 }
 
 template <typename T>
