@@ -22,29 +22,29 @@ cudaError_t launch_one(const UnionArgs<T> &a, uint32_t ctas, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// Calls f.template operator()<Op>() for the method's double-precision operator.
-template <class F>
+// Calls f.template operator()<Op>() for the method's operator in precision R.
+template <typename R, class F>
 cudaError_t with_op(const MethodSpec &spec, F &&f) {
     const int ak = alpha_kind(spec.alpha);
     if (!spec.vaw) {
         switch (ak) {
-        case 1: return f.template operator()<OpGeneralized<double, 1>>();
-        case 2: return f.template operator()<OpGeneralized<double, 2>>();
-        case 3: return f.template operator()<OpGeneralized<double, 3>>();
-        default: return f.template operator()<OpGeneralized<double, 0>>();
+        case 1: return f.template operator()<OpGeneralized<R, 1>>();
+        case 2: return f.template operator()<OpGeneralized<R, 2>>();
+        case 3: return f.template operator()<OpGeneralized<R, 3>>();
+        default: return f.template operator()<OpGeneralized<R, 0>>();
         }
     }
     switch (spec.method) {
-    case Method::unweighted: return f.template operator()<OpVawUnweighted<double, true>>();
-    case Method::unweighted_unnormalized: return f.template operator()<OpVawUnweighted<double, false>>();
-    case Method::weighted_normalized: return f.template operator()<OpVawWeighted<double, true>>();
-    case Method::weighted_unnormalized: return f.template operator()<OpVawWeighted<double, false>>();
+    case Method::unweighted: return f.template operator()<OpVawUnweighted<R, true>>();
+    case Method::unweighted_unnormalized: return f.template operator()<OpVawUnweighted<R, false>>();
+    case Method::weighted_normalized: return f.template operator()<OpVawWeighted<R, true>>();
+    case Method::weighted_unnormalized: return f.template operator()<OpVawWeighted<R, false>>();
     case Method::generalized:
         switch (ak) {
-        case 1: return f.template operator()<OpVawGeneralized<double, 1>>();
-        case 2: return f.template operator()<OpVawGeneralized<double, 2>>();
-        case 3: return f.template operator()<OpVawGeneralized<double, 3>>();
-        default: return f.template operator()<OpVawGeneralized<double, 0>>();
+        case 1: return f.template operator()<OpVawGeneralized<R, 1>>();
+        case 2: return f.template operator()<OpVawGeneralized<R, 2>>();
+        case 3: return f.template operator()<OpVawGeneralized<R, 3>>();
+        default: return f.template operator()<OpVawGeneralized<R, 0>>();
         }
     }
     return cudaErrorInvalidValue;
@@ -74,12 +74,12 @@ struct Launch {
 
 template <typename T>
 cudaError_t union_configure(const MethodSpec &spec, size_t *smem) {
-    return with_op(spec, Configure<T>{smem});
+    return with_op<T>(spec, Configure<T>{smem});
 }
 
 template <typename T>
 cudaError_t union_launch(const MethodSpec &spec, const UnionArgs<T> &a, uint32_t ctas, cudaStream_t s) {
-    return with_op(spec, Launch<T>{a, ctas, s});
+    return with_op<T>(spec, Launch<T>{a, ctas, s});
 }
 
 template cudaError_t union_configure<double>(const MethodSpec &, size_t *);

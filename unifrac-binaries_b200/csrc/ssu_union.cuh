@@ -108,16 +108,42 @@ __device__ __forceinline__ void union_fail(int *abort_flag, int *error, int code
 
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(UCT) : "memory"); }
 
+// The scalar type an operator computes its terms in.
+template <class Op> struct op_real;
+template <typename R, int AK> struct op_real<OpGeneralized<R, AK>> { using type = R; };
+template <typename R, int AK> struct op_real<OpVawGeneralized<R, AK>> { using type = R; };
+template <typename R, bool N> struct op_real<OpVawWeighted<R, N>> { using type = R; };
+template <typename R, bool N> struct op_real<OpVawUnweighted<R, N>> { using type = R; };
+
+// One term of the method added to fp64 sums: fp64 operators accumulate
+// directly; fp32 operators (fp32 plans, as the reference fp32 build's terms)
+// compute the term in single precision and add it in fp64.
+template <class Op>
+__device__ __forceinline__ void union_term(double *acc, double a, double b, double ca, double cb, double m, double L,
+                                           double alpha) {
+    using R = typename op_real<Op>::type;
+    if constexpr (sizeof(R) == 8) {
+        Op::term(acc, a, b, ca, cb, m, L, alpha);
+    } else {
+        R t[2] = {R(0), R(0)};
+        Op::term(t, static_cast<R>(a), static_cast<R>(b), static_cast<R>(ca), static_cast<R>(cb), static_cast<R>(m),
+                 static_cast<R>(L), static_cast<R>(alpha));
+        acc[0] += static_cast<double>(t[0]);
+        if (Op::NACC > 1) acc[1] += static_cast<double>(t[1]);
+    }
+}
+
+// The distance from the fp64 sums: num / den for the two-sum operators, num
+// for the one-sum (unnormalized variance-adjusted) ones.
 template <typename T, class Op>
 __device__ __forceinline__ void union_emit(const TableDesc &td, OutSpec o, uint32_t kc, uint32_t lc, double num,
                                            double den) {
     const uint32_t k = kc - td.base, l = lc - td.base;
     if (!(k < l && l < td.n)) return;
-    const double acc[2] = {num, den};
-    emit_pair<T>(o, td.n, k, l, static_cast<T>(Op::value(acc, 0.0, 0.0)));
+    emit_pair<T>(o, td.n, k, l, static_cast<T>(Op::NACC > 1 ? num / den : num));
 }
 
-// Op: the method's operator in double precision (its term and value).
+// Op: the method's operator, in the plan's precision (its term).
 template <typename T, class Op>
 __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs<T> a) {
     constexpr bool CNT = Op::COUNTS;
@@ -274,9 +300,9 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
                         const double L = static_cast<double>(ls[n]);
                         const double av = static_cast<double>(v[r]);
                         const double ca = CNT ? static_cast<double>(cv[r]) : 0.0;
-                        Op::term(A[rr][0], av, static_cast<double>(v[UT + lane]), ca,
+                        union_term<Op>(A[rr][0], av, static_cast<double>(v[UT + lane]), ca,
                                  CNT ? static_cast<double>(cv[UT + lane]) : 0.0, tk + tl0, L, a.alpha);
-                        Op::term(A[rr][1], av, static_cast<double>(v[UT + lane + 32]), ca,
+                        union_term<Op>(A[rr][1], av, static_cast<double>(v[UT + lane + 32]), ca,
                                  CNT ? static_cast<double>(cv[UT + lane + 32]) : 0.0, tk + tl1, L, a.alpha);
                     }
                 }
@@ -293,8 +319,8 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
                         const double L = static_cast<double>(ls[n]);
                         const double bv = static_cast<double>(v[col]);
                         const double cb = CNT ? static_cast<double>(cs[n * P + col]) : 0.0;
-                        if (v[lane] == T(0)) Op::term(B[cc][0], 0.0, bv, 0.0, cb, tk0 + tl, L, a.alpha);
-                        if (v[lane + 32] == T(0)) Op::term(B[cc][1], 0.0, bv, 0.0, cb, tk1 + tl, L, a.alpha);
+                        if (v[lane] == T(0)) union_term<Op>(B[cc][0], 0.0, bv, 0.0, cb, tk0 + tl, L, a.alpha);
+                        if (v[lane + 32] == T(0)) union_term<Op>(B[cc][1], 0.0, bv, 0.0, cb, tk1 + tl, L, a.alpha);
                     }
                 }
                 __syncwarp();
@@ -388,7 +414,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
                             const double bc = CNT ? static_cast<double>(cs[c * 2 * UT + UT + tx + 32 * j]) : 0.0;
 #pragma unroll
                             for (int i = 0; i < TM; i++)
-                                Op::term(acc[i][j], static_cast<double>(av[i]), bv,
+                                union_term<Op>(acc[i][j], static_cast<double>(av[i]), bv,
                                          CNT ? static_cast<double>(ac[i]) : 0.0, bc, tkd[i] + tld[j], L, a.alpha);
                         }
                     }
