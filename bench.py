@@ -95,51 +95,110 @@ def make_workload(seed, args):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region.
+
+    Two read-only sources over the same window: `nvidia-smi -lms 200` (the
+    CSV query of clocks and event reasons) and an NVML poll every 10 ms in a
+    thread, so a timed region of a few tens of milliseconds still holds
+    samples.  The GPU is named by its UUID, so the right device is read under
+    CUDA_VISIBLE_DEVICES.  start() returns once the poll has its first
+    sample."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
+        self.uuid = None
+        try:
+            import torch
+            self.uuid = "GPU-" + str(torch.cuda.get_device_properties(gpu_index).uuid)
+        except Exception:
+            self.uuid = None
         self.proc = None
+        self.thread = None
+        self.polled = []
+        self.first = None
+        self.done = None
+
+    def _poll(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+        except Exception:
+            self.first.set()
+            return
+        try:
+            h = nv.nvmlDeviceGetHandleByUUID(self.uuid) if self.uuid else nv.nvmlDeviceGetHandleByIndex(self.gpu)
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            while True:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.polled.append((float(sm), float(mx), [n for n, b in zip(self.NAMES, bits) if mask & b]))
+                self.first.set()
+                if self.done.wait(0.01):
+                    break
+        except Exception:
+            pass
+        finally:
+            self.first.set()
+            try:
+                nv.nvmlShutdown()
+            except Exception:
+                pass
 
     def start(self):
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.uuid or str(self.gpu), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+        self.first, self.done = threading.Event(), threading.Event()
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+        self.thread.start()
+        self.first.wait(2.0)
 
     def stop(self):
-        if not self.proc:
-            return None
-        self.proc.terminate()
-        try:
-            out, _ = self.proc.communicate(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-            out, _ = self.proc.communicate()
         sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
+        smi = 0
+        if self.thread:
+            self.done.set()
+            self.thread.join(5.0)
+            for s, m, r in self.polled:
+                sm.append(s)
+                mx.append(m)
+                reasons.update(r)
+        if self.proc:
+            self.proc.terminate()
             try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
-            except ValueError:
-                continue
-            for name, val in zip(names, f[5:9]):
-                if val.lower() == "active":
-                    reasons.add(name)
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            for line in out.splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    s, m = float(f[1]), float(f[2])
+                except ValueError:
+                    continue
+                sm.append(s)
+                mx.append(m)
+                smi += 1
+                for name, val in zip(self.NAMES, f[5:9]):
+                    if val.lower() == "active":
+                        reasons.add(name)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "sm_min_mhz": min(sm),
+                "reasons": sorted(reasons), "samples": len(sm), "nvidia_smi_samples": smi}
 
 
 def read_traffic():

@@ -81,3 +81,15 @@ def test_stripe_window_covers_every_stripe_once(n, world):
     windows = [bench.stripe_window(n, r, world) for r in range(world)]
     assert windows[0][0] == 0 and windows[-1][1] == total
     assert all(windows[i][1] == windows[i + 1][0] for i in range(world - 1))
+
+
+def test_clock_sampler_returns_promptly_without_a_gpu():
+    import time
+    sys.path.insert(0, ROOT)
+    import bench
+    t0 = time.monotonic()
+    s = bench.ClockSampler(0)
+    s.start()
+    clk = s.stop()
+    assert time.monotonic() - t0 < 10
+    assert clk is None or {"sm_mhz", "sm_max_mhz", "reasons", "samples"} <= set(clk)

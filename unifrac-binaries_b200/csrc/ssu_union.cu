@@ -8,9 +8,17 @@ namespace dev {
 
 namespace {
 
+// The kernel's setmaxnreg split assumes the block launches with exactly
+// UREG_LAUNCH registers per thread: with fewer, the consumers' increase could
+// never be granted.  An instance built otherwise is refused here, before any
+// launch.
 template <typename T, class Op>
 cudaError_t configure_one(size_t *smem) {
     *smem = union_smem<T, Op::COUNTS>();
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, pair_union_kernel<T, Op>);
+    if (e != cudaSuccess) return e;
+    if (fa.numRegs != UREG_LAUNCH || fa.maxThreadsPerBlock < UTHREADS) return cudaErrorInvalidConfiguration;
     return cudaFuncSetAttribute(pair_union_kernel<T, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(*smem));
 }

@@ -8,17 +8,20 @@
 // own term - no rearrangement, so the result matches the dense form up to
 // the order of the summation (no cancellation, nothing to recompute).
 //
-// Tile: 64 (k) x 64 (l) pairs; 16 consumer warps and one producer warp.
-// Sparse rows: the producer streams the tile's k and l blocks of 16 rows at
-// a time (1D bulk copies, no multicast) into a ring of mbarrier-guarded
-// stages; each consumer warp waits only for the stage it reads, so a warp
-// with little work runs ahead instead of idling at a block barrier.  Row
-// pass: warp w owns rows 4w .. 4w + 3 (lanes over the 64 columns); column
-// pass: warp w owns columns 4w .. 4w + 3 (lanes over the 64 rows); both in
-// registers, one owner per element (deterministic sums).  Dense rows (non-zero
-// in more than ld / div columns) then run a register-tiled loop, and the
-// three parts meet in shared memory.  Every mbarrier wait is bounded: on
-// expiry the block records an error, stops, and lets its copies land.
+// Tile: 64 (k) x 64 (l) pairs; 16 consumer warps and a producer warpgroup
+// (one warp issues the copies; the group hands most of its registers to the
+// consumers through setmaxnreg, so accumulators and terms stay in
+// registers).  Sparse rows: the producer streams the tile's k and l blocks
+// of 16 rows at a time (1D bulk copies, no multicast) into a ring of
+// mbarrier-guarded stages; each consumer warp waits only for the stage it
+// reads, so a warp with little work runs ahead instead of idling at a block
+// barrier.  Row pass: warp w owns rows 4w .. 4w + 3 (lanes over the 64
+// columns); column pass: warp w owns columns 4w .. 4w + 3 (lanes over the 64
+// rows); both in registers, one owner per element (deterministic sums).
+// Dense rows (non-zero in more than ld / div columns) then run a
+// register-tiled loop, and the three parts meet in shared memory.  Every
+// mbarrier wait is bounded: on expiry the block records an error, stops, and
+// lets its copies land.
 #pragma once
 
 #include <cstdint>
@@ -55,9 +58,19 @@ enum : int { UNION_ERR_FULL_WAIT = 11, UNION_ERR_EMPTY_WAIT = 12, UNION_ERR_DRAI
 constexpr long long kDrainCycles = 2000000000LL;  // about one second at B200 clocks
 
 constexpr int UT = 64;                    // tile: 64 (k) x 64 (l)
-constexpr int UCW = 16;                   // consumer warps
+constexpr int UCW = 16;                   // consumer warps (four warpgroups)
 constexpr int UCT = 32 * UCW;             // consumer threads
-constexpr int UTHREADS = UCT + 32;        // + the producer warp
+constexpr int UTHREADS = UCT + 128;       // + the producer warpgroup (one warp copies)
+// Register split (setmaxnreg): the block launches with 96 per thread
+// (65,536 / 640, rounded down to a multiple of 8); the producer warpgroup
+// hands back all but 32 and the consumer warpgroups take them, 112 each.
+constexpr int UREG_LAUNCH = 96;
+constexpr int UREG_PRODUCER = 32;
+constexpr int UREG_CONSUMER = 112;
+static_assert(UREG_CONSUMER * UCT + UREG_PRODUCER * 128 <= UREG_LAUNCH * UTHREADS,
+              "the warpgroups' register shares exceed the block's launch registers");
+static_assert(UREG_LAUNCH * UTHREADS <= 65536 && UREG_CONSUMER % 8 == 0 && UREG_PRODUCER % 8 == 0,
+              "setmaxnreg counts are multiples of 8 within the register file");
 constexpr int UR = UT / UCW;              // rows (row pass) / columns (column pass) per warp
 constexpr int URS = 16;                   // sparse rows per ring stage
 constexpr int UKC = 8;                    // dense rows per dense stage
@@ -107,6 +120,15 @@ __device__ __forceinline__ void union_fail(int *abort_flag, int *error, int code
 }
 
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(UCT) : "memory"); }
+
+template <int N>
+__device__ __forceinline__ void regs_release() {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(N));
+}
+template <int N>
+__device__ __forceinline__ void regs_take() {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(N));
+}
 
 // The scalar type an operator computes its terms in.
 template <class Op> struct op_real;
@@ -166,7 +188,6 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
     T *Dl = Dc + (CNT ? UDS * UKC * 2 * UT : 0);    // [UDS][UKC]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool producer = warp == UCW;
     const long long budget = a.wait_cycles;
     if (tid == 0) {
         for (int s = 0; s < NS; s++) {
@@ -184,7 +205,83 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
     // starts on a 16-row boundary (aligned length copies)
     const uint32_t sr = ((n_sparse + a.n_splits - 1) / a.n_splits + URS - 1) / URS * URS;
     const uint32_t n_work = a.n_tiles * a.n_splits;
+    // Each role runs its own loop over the work items; per item both take
+    // the same two block barriers (ring drained; shared tiles free again).
     uint32_t g = 0;  // stages used so far (same count in every warp)
+    if (warp >= UCW) {
+        regs_release<UREG_PRODUCER>();
+        for (uint32_t w = blockIdx.x; w < n_work; w += gridDim.x) {
+            const uint32_t split = w / a.n_tiles, ti = w - split * a.n_tiles;
+            const uint32_t s_begin = min(n_sparse, split * sr), s_end = min(n_sparse, s_begin + sr);
+            const uint32_t n_chunks = (s_end - s_begin + URS - 1) / URS;
+            if (warp == UCW) {
+                const uint4 tile = a.tiles[ti];
+                const uint32_t k0 = tile.x * UT, l0 = tile.y * UT;
+                // ---- producer: lane r < 16 copies row r of each stage, lane 16
+                // the stage's lengths; row ids fetched two stages ahead
+                auto id_of = [&](uint32_t c) -> uint32_t {
+                    const uint32_t i = s_begin + c * URS + static_cast<uint32_t>(lane);
+                    return (lane < URS && c < n_chunks && i < s_end) ? a.sparse_rows[i] : 0u;
+                };
+                uint32_t e1 = id_of(0), e2 = id_of(1);
+                uint32_t issued = 0;
+                for (uint32_t c = 0; c < (a.stall ? 0u : n_chunks); c++) {
+                    const uint32_t e = e1;
+                    e1 = e2;
+                    e2 = id_of(c + 2);
+                    const uint32_t gc = g + c, st = gc % NS, use = gc / NS;
+                    int ok = 1;
+                    if (lane == 0) {
+                        if (*vabort) {
+                            ok = 0;
+                        } else if (use > 0 && !mbar_wait(empty + st, (use - 1) & 1, budget)) {
+                            union_fail(abort_flag, a.error, UNION_ERR_EMPTY_WAIT);
+                            ok = 0;
+                        }
+                    }
+                    if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+                    const uint32_t i0 = s_begin + c * URS;
+                    const uint32_t nv = min(static_cast<uint32_t>(URS), s_end - i0);
+                    unsigned char *sp = ring + st * SB;
+                    if (lane == 0)
+                        mbar_expect_tx(full + st, static_cast<uint32_t>(nv * 2 * UT * sizeof(T) * (CNT ? 2 : 1) +
+                                                                        URS * sizeof(T)));
+                    __syncwarp();
+                    if (static_cast<uint32_t>(lane) < nv) {
+                        const uint64_t base = static_cast<uint64_t>(e) * a.ld;
+                        T *dv = reinterpret_cast<T *>(sp) + lane * P;
+                        bulk_load(dv, a.U + base + k0, UT * sizeof(T), full + st);
+                        bulk_load(dv + UT, a.U + base + l0, UT * sizeof(T), full + st);
+                        if (CNT) {
+                            T *dc = reinterpret_cast<T *>(sp) + URS * P + lane * P;
+                            bulk_load(dc, a.C + base + k0, UT * sizeof(T), full + st);
+                            bulk_load(dc + UT, a.C + base + l0, UT * sizeof(T), full + st);
+                        }
+                    } else if (lane == URS) {
+                        T *dl = reinterpret_cast<T *>(sp) + URS * P * (CNT ? 2 : 1);
+                        bulk_load(dl, a.slen + i0, URS * sizeof(T), full + st);
+                    }
+                    issued = c + 1;
+                }
+                // never leave with copies in flight: each stage's last fill lands
+                // (at least about a second per wait, whatever the wait budget)
+                const long long drain_budget = budget > kDrainCycles ? budget : kDrainCycles;
+                if (lane == 0)
+                    for (uint32_t c = issued > static_cast<uint32_t>(NS) ? issued - NS : 0; c < issued; c++)
+                        if (!mbar_wait(full + (g + c) % NS, ((g + c) / NS) & 1, drain_budget))
+                            union_fail(abort_flag, a.error, UNION_ERR_DRAIN_WAIT);
+                __syncwarp();
+            }
+            g += n_chunks;
+            __syncthreads();  // the ring has drained (every stage's copies landed and were read)
+            const bool failed = *vabort != 0;
+            __syncthreads();  // the consumers' epilogue is done with the shared tiles
+            if (failed) break;
+        }
+        return;
+    }
+
+    regs_take<UREG_CONSUMER>();
     for (uint32_t w = blockIdx.x; w < n_work; w += gridDim.x) {
         const uint32_t split = w / a.n_tiles, ti = w - split * a.n_tiles;
         const uint4 tile = a.tiles[ti];
@@ -192,9 +289,9 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
         const uint32_t s_begin = min(n_sparse, split * sr), s_end = min(n_sparse, s_begin + sr);
         const uint32_t n_chunks = (s_end - s_begin + URS - 1) / URS;
         if (CNT)
-            for (int c = tid; c < 2 * UT; c += UTHREADS)
+            for (int c = tid; c < 2 * UT; c += UCT)
                 Ts[c] = static_cast<double>(a.tot[c < UT ? k0 + c : l0 + (c - UT)]);
-        __syncthreads();
+        consumer_sync();
 
         // row pass: rows r0 + rr x columns lane + 32 j; column pass: rows
         // lane + 32 j x columns c0 + cc
@@ -203,63 +300,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
         for (int i = 0; i < UR; i++)
 #pragma unroll
             for (int j = 0; j < 2; j++) A[i][j][0] = A[i][j][1] = B[i][j][0] = B[i][j][1] = 0.0;
-
-        if (producer) {
-            // ---- producer: lane r < 16 copies row r of each stage, lane 16
-            // the stage's lengths; row ids fetched two stages ahead
-            auto id_of = [&](uint32_t c) -> uint32_t {
-                const uint32_t i = s_begin + c * URS + static_cast<uint32_t>(lane);
-                return (lane < URS && c < n_chunks && i < s_end) ? a.sparse_rows[i] : 0u;
-            };
-            uint32_t e1 = id_of(0), e2 = id_of(1);
-            uint32_t issued = 0;
-            for (uint32_t c = 0; c < (a.stall ? 0u : n_chunks); c++) {
-                const uint32_t e = e1;
-                e1 = e2;
-                e2 = id_of(c + 2);
-                const uint32_t gc = g + c, st = gc % NS, use = gc / NS;
-                int ok = 1;
-                if (lane == 0) {
-                    if (*vabort) {
-                        ok = 0;
-                    } else if (use > 0 && !mbar_wait(empty + st, (use - 1) & 1, budget)) {
-                        union_fail(abort_flag, a.error, UNION_ERR_EMPTY_WAIT);
-                        ok = 0;
-                    }
-                }
-                if (!__shfl_sync(0xffffffffu, ok, 0)) break;
-                const uint32_t i0 = s_begin + c * URS;
-                const uint32_t nv = min(static_cast<uint32_t>(URS), s_end - i0);
-                unsigned char *sp = ring + st * SB;
-                if (lane == 0)
-                    mbar_expect_tx(full + st, static_cast<uint32_t>(nv * 2 * UT * sizeof(T) * (CNT ? 2 : 1) +
-                                                                    URS * sizeof(T)));
-                __syncwarp();
-                if (static_cast<uint32_t>(lane) < nv) {
-                    const uint64_t base = static_cast<uint64_t>(e) * a.ld;
-                    T *dv = reinterpret_cast<T *>(sp) + lane * P;
-                    bulk_load(dv, a.U + base + k0, UT * sizeof(T), full + st);
-                    bulk_load(dv + UT, a.U + base + l0, UT * sizeof(T), full + st);
-                    if (CNT) {
-                        T *dc = reinterpret_cast<T *>(sp) + URS * P + lane * P;
-                        bulk_load(dc, a.C + base + k0, UT * sizeof(T), full + st);
-                        bulk_load(dc + UT, a.C + base + l0, UT * sizeof(T), full + st);
-                    }
-                } else if (lane == URS) {
-                    T *dl = reinterpret_cast<T *>(sp) + URS * P * (CNT ? 2 : 1);
-                    bulk_load(dl, a.slen + i0, URS * sizeof(T), full + st);
-                }
-                issued = c + 1;
-            }
-            // never leave with copies in flight: each stage's last fill lands
-            // (at least about a second per wait, whatever the wait budget)
-            const long long drain_budget = budget > kDrainCycles ? budget : kDrainCycles;
-            if (lane == 0)
-                for (uint32_t c = issued > static_cast<uint32_t>(NS) ? issued - NS : 0; c < issued; c++)
-                    if (!mbar_wait(full + (g + c) % NS, ((g + c) / NS) & 1, drain_budget))
-                        union_fail(abort_flag, a.error, UNION_ERR_DRAIN_WAIT);
-            __syncwarp();
-        } else {
+        {
             // ---- consumers
             const int r0 = UR * warp, c0 = UR * warp;
             const int hn = lane & 15, hq = lane >> 4;
@@ -331,7 +372,7 @@ __global__ void __launch_bounds__(UTHREADS, 1) pair_union_kernel(const UnionArgs
         __syncthreads();  // the ring has drained (every stage's copies landed and were read)
         const bool failed = *vabort != 0;
 
-        if (!producer && !failed) {
+        if (!failed) {
             const int ctid = tid;
             const int r0 = UR * warp, c0 = UR * warp;
 #pragma unroll
