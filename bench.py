@@ -159,6 +159,7 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+        self.polled = []
         self.first, self.done = threading.Event(), threading.Event()
         self.thread = threading.Thread(target=self._poll, daemon=True)
         self.thread.start()

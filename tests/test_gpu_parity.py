@@ -343,13 +343,17 @@ def test_union_and_dense_forms_agree(ssu, oracle_mod, monkeypatch, method, vaw, 
     check_fp64(union, oracle_mod.oracle_one_off(tree, table, method + "_fp64", **kw)["matrix"])
 
 
-@pytest.mark.parametrize("div", ["1", "3", "1000000"])
-def test_union_row_classes_do_not_change_results(ssu, oracle_mod, monkeypatch, div):
-    """All rows dense, the default split, and all rows sparse give the same
-    matrix; stripe windows go through the same kernel."""
-    tree, table = _case(64, n_tips=300, n_samples=150, density=0.05)
-    monkeypatch.setenv("UNIFRAC_B200_UNION_DIV", div)
+@pytest.mark.parametrize("n_tips", [5, 9, 40, 301])
+def test_union_rows_stream_in_whole_and_partial_stages(ssu, oracle_mod, n_tips):
+    """The union kernel streams the embedded rows 16 at a time: trees whose
+    row count is below one stage or not a multiple of 16 (the last stage
+    partly past the rows, read as zero) give the oracle's matrix; stripe
+    windows go through the same kernel."""
+    tree, table = _case(64, n_tips=n_tips, n_samples=150, density=0.3 if n_tips < 40 else 0.05, drop=1)
     kw = dict(variance_adjust=True, alpha=0.5)
+    plan = ssu.Plan(tree, table, "generalized_fp64", **kw)
+    assert plan.pair_kernel().startswith("pair_union")
+    plan.close()
     ref = oracle_mod.oracle_one_off(tree, table, "generalized_fp64", **kw)["matrix"]
     gpu, _ = ssu.one_off_matrix(tree, table, "generalized_fp64", **kw)
     check_fp64(gpu, ref)

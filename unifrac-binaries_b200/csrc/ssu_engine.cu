@@ -123,6 +123,23 @@ bool make_fp16_map(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols) {
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// 2-D tensor map over the first `rows` rows of a row-major [.][cols] matrix of
+// T (fp64 or fp32), box 64 columns x 16 rows, no swizzle; rows past `rows`
+// read as zero.  cols * sizeof(T) must be a multiple of 16.
+template <typename T>
+bool make_rows_map(CUtensorMap *map, const void *base, uint64_t rows, uint64_t cols) {
+    EncodeTiledFn f = encode_tiled();
+    if (!f) return false;
+    const cuuint64_t dims[2] = {cols, std::max<uint64_t>(rows, 1)};
+    const cuuint64_t strides[1] = {cols * sizeof(T)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(dev::UT), static_cast<cuuint32_t>(dev::URS)};
+    const cuuint32_t estr[2] = {1, 1};
+    return f(map, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+             const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Tiles of one table (columns [base, base + n) of its group) holding at
 // least one pair k < l; with a stripe window only those whose pairs reach a
 // stripe in [start, stop).  x and y are block indices in the group's
@@ -291,10 +308,9 @@ struct PlanImpl {
     // generalized and variance-adjusted methods over the union of the two
     // samples' supports (same masks and row classes as the hybrid)
     bool union_mode = false;
-    uint32_t union_div = 3;  // rows non-zero in more than ld / union_div columns are dense
     double *d_upartial = nullptr;
     size_t upartial_bytes = 0;
-    void *d_slen = nullptr;  // branch length per sparse row, in sparse-row order
+    void *d_slen = nullptr;  // union kernel: branch lengths in T, zero-padded to whole 16-row stages
     // budget of one mbarrier wait in the union kernel (UNIFRAC_B200_WAIT_CYCLES,
     // default about one second), and its test switch UNIFRAC_B200_TEST_STALL=1
     // (the kernel's producer issues nothing, so its waits run out and the call
@@ -846,7 +862,6 @@ int PlanImpl::sparse_prep(cudaStream_t s, const Group &g, uint32_t div) {
 
 template <typename T>
 int PlanImpl::setup_union() {
-    union_div = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_UNION_DIV", 3)));
     if (const char *w = std::getenv("UNIFRAC_B200_WAIT_CYCLES")) union_wait_cycles = std::max(0LL, std::atoll(w));
     union_stall = env_int("UNIFRAC_B200_TEST_STALL", 0) ? 1 : 0;
     if (const int rc = sparse_prep_alloc()) return rc;
@@ -875,7 +890,10 @@ int PlanImpl::setup_union() {
             upartial_bytes = std::max(upartial_bytes, sizeof(double) * 2 * dev::UT * dev::UT * g.n_tiles * g.splits);
     }
     if (upartial_bytes) SSU_CK(alloc(&d_upartial, upartial_bytes));
-    SSU_CK(alloc(reinterpret_cast<T **>(&d_slen), sizeof(T) * (static_cast<size_t>(E) + dev::URS)));
+    // branch lengths in T, zero-padded to whole stages (a stage copies 16)
+    std::vector<T> lens((static_cast<size_t>(E) + dev::URS - 1) / dev::URS * dev::URS + dev::URS, T(0));
+    for (uint32_t e = 0; e < E; e++) lens[e] = static_cast<T>(host_len[e]);
+    SSU_CK(upload(reinterpret_cast<T **>(&d_slen), lens.data(), sizeof(T) * lens.size()));
     if (!d_error) {
         SSU_CK(alloc(&d_error, sizeof(int)));
         SSU_CK(cudaMemsetAsync(d_error, 0, sizeof(int), stream));
@@ -883,19 +901,17 @@ int PlanImpl::setup_union() {
     return 0;
 }
 
-// Union pair stage of one group (its embedding ready): row classes, then the
-// union tile kernel (+ split finalize).
+// Union pair stage of one group (its embedding and presence words ready):
+// the union tile kernel (+ split finalize) over 2-D maps of the group's
+// proportions and counts.
 template <typename T>
 int PlanImpl::union_stage(cudaStream_t s, const Group &g, const dev::OutSpec &out, const uint4 *tiles,
                           uint32_t ntiles, uint32_t splits, bool last) {
-    if (const int rc = sparse_prep<T>(s, g, union_div)) return rc;
     if (ntiles == 0) return 0;
-    T *slen = static_cast<T *>(d_slen);
-    if (E) {
-        const uint32_t grid = std::min<uint32_t>((E + 255) / 256, 4 * n_sms);
-        dev::gather_sparse_len_kernel<T><<<grid, 256, 0, s>>>(d_sparse_rows, d_nrows, static_cast<const T *>(d_len),
-                                                              E, slen);
-        launches++;
+    CUtensorMap tmU{}, tmC{};
+    if (!make_rows_map<T>(&tmU, d_U, E, g.ld) || (spec.vaw && !make_rows_map<T>(&tmC, d_C, E, g.ld))) {
+        last_error = "cuTensorMapEncodeTiled failed";
+        return kOutputError;
     }
     dev::UnionArgs<T> u{};
     u.tiles = tiles;
@@ -904,16 +920,11 @@ int PlanImpl::union_stage(cudaStream_t s, const Group &g, const dev::OutSpec &ou
     if (u.n_splits > 1 && sizeof(double) * 2 * dev::UT * dev::UT * ntiles * u.n_splits > upartial_bytes)
         u.n_splits = 1;
     u.tables = d_tdesc;
-    u.U = static_cast<const T *>(d_U);
-    u.C = static_cast<const T *>(d_C);
     u.tot = static_cast<const T *>(g.d_tot);
-    u.len = static_cast<const T *>(d_len);
-    u.slen = slen;
+    u.len = static_cast<const T *>(d_slen);
+    u.masks = d_masks;
     u.E = E;
     u.ld = g.ld;
-    u.dense_rows = d_dense_rows;
-    u.sparse_rows = d_sparse_rows;
-    u.n_rows = d_nrows;
     u.alpha = spec.alpha;
     u.partial = u.n_splits > 1 ? d_upartial : nullptr;
     u.out = out;
@@ -922,7 +933,7 @@ int PlanImpl::union_stage(cudaStream_t s, const Group &g, const dev::OutSpec &ou
     u.stall = union_stall;
     const uint32_t ctas = static_cast<uint32_t>(
         std::min<uint64_t>(static_cast<uint64_t>(ntiles) * u.n_splits, static_cast<uint64_t>(n_sms)));
-    SSU_CK(dev::union_launch<T>(spec, u, ctas, s));
+    SSU_CK(dev::union_launch<T>(spec, tmU, spec.vaw ? tmC : tmU, u, ctas, s));
     launches += u.partial ? 2 : 1;
     if (last && timed()) SSU_CK(cudaEventRecord(ev[2], s));
     return 0;

@@ -82,12 +82,7 @@ using dev::mbar_try_wait;
 using dev::mbar_wait;
 using dev::smem_u32;
 
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
-        : "memory");
-}
+using dev::tma_load_2d;
 
 // K-major operand tile in shared memory with 128-byte swizzle: rows of 128
 // bytes, 8-row groups 1024 bytes apart (SBO), LBO unused (1), descriptor

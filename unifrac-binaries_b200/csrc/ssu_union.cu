@@ -24,8 +24,9 @@ cudaError_t configure_one(size_t *smem) {
 }
 
 template <typename T, class Op>
-cudaError_t launch_one(const UnionArgs<T> &a, uint32_t ctas, cudaStream_t s) {
-    pair_union_kernel<T, Op><<<ctas, UTHREADS, union_smem<T, Op::COUNTS>(), s>>>(a);
+cudaError_t launch_one(const CUtensorMap &tmU, const CUtensorMap &tmC, const UnionArgs<T> &a, uint32_t ctas,
+                       cudaStream_t s) {
+    pair_union_kernel<T, Op><<<ctas, UTHREADS, union_smem<T, Op::COUNTS>(), s>>>(tmU, tmC, a);
     if (a.partial) union_finalize_kernel<T, Op><<<a.n_tiles, UFIN_THREADS, 0, s>>>(a);
     return cudaGetLastError();
 }
@@ -71,12 +72,13 @@ struct Configure {
 
 template <typename T>
 struct Launch {
+    const CUtensorMap &tmU, &tmC;
     const UnionArgs<T> &a;
     uint32_t ctas;
     cudaStream_t s;
     template <class Op>
     cudaError_t operator()() const {
-        return launch_one<T, Op>(a, ctas, s);
+        return launch_one<T, Op>(tmU, tmC, a, ctas, s);
     }
 };
 
@@ -86,14 +88,17 @@ cudaError_t union_configure(const MethodSpec &spec, size_t *smem) {
 }
 
 template <typename T>
-cudaError_t union_launch(const MethodSpec &spec, const UnionArgs<T> &a, uint32_t ctas, cudaStream_t s) {
-    return with_op<T>(spec, Launch<T>{a, ctas, s});
+cudaError_t union_launch(const MethodSpec &spec, const CUtensorMap &tmU, const CUtensorMap &tmC,
+                         const UnionArgs<T> &a, uint32_t ctas, cudaStream_t s) {
+    return with_op<T>(spec, Launch<T>{tmU, tmC, a, ctas, s});
 }
 
 template cudaError_t union_configure<double>(const MethodSpec &, size_t *);
 template cudaError_t union_configure<float>(const MethodSpec &, size_t *);
-template cudaError_t union_launch<double>(const MethodSpec &, const UnionArgs<double> &, uint32_t, cudaStream_t);
-template cudaError_t union_launch<float>(const MethodSpec &, const UnionArgs<float> &, uint32_t, cudaStream_t);
+template cudaError_t union_launch<double>(const MethodSpec &, const CUtensorMap &, const CUtensorMap &,
+                                          const UnionArgs<double> &, uint32_t, cudaStream_t);
+template cudaError_t union_launch<float>(const MethodSpec &, const CUtensorMap &, const CUtensorMap &,
+                                         const UnionArgs<float> &, uint32_t, cudaStream_t);
 
 }  // namespace dev
 }  // namespace ssu
