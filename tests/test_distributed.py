@@ -93,3 +93,30 @@ def test_clock_sampler_returns_promptly_without_a_gpu():
     clk = s.stop()
     assert time.monotonic() - t0 < 10
     assert clk is None or {"sm_mhz", "sm_max_mhz", "reasons", "samples"} <= set(clk)
+
+
+def _reference_arm(env_extra):
+    import json
+    import subprocess
+    env = dict(os.environ)
+    env.update(env_extra)
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0", "--samples", "96", "--tips", "600"],
+                         capture_output=True, text=True, env=env, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    return [json.loads(x) for x in out.stdout.splitlines() if x.startswith("{")]
+
+
+def test_reference_arm_prints_one_contract_line_on_rank_0():
+    lines = _reference_arm({"RANK": "0", "WORLD_SIZE": "1"})
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference" and d["metric"] == "pair-branch updates/s" and d["unit"] == "updates/s"
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 1 and d["warmup"] == 0
+    assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
+    assert d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    assert _reference_arm({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []
