@@ -372,7 +372,8 @@ void destroy_full(TMat **result) {
             std::free(r->matrix);
         } else {
             const uint64_t n = r->n_samples;
-            munmap(r->matrix, sizeof(TReal) * n * n ? sizeof(TReal) * n * n : 1);
+            const size_t bytes = sizeof(TReal) * n * n;
+            munmap(r->matrix, bytes ? bytes : 1);
             close(static_cast<int>(r->flags & kMmapFdMask));
         }
         r->matrix = nullptr;
