@@ -22,9 +22,9 @@
 // pass: warp w owns rows 4w .. 4w + 3 (lanes over the 64 columns); column
 // pass: warp w owns columns 4w .. 4w + 3 (lanes over the 64 rows); both in
 // registers, one owner per element (deterministic sums); the two parts meet
-// in shared memory for the epilogue.  A staged row with more than half of
-// the tile's 128 samples present is evaluated for every pair of the warp's
-// rows instead (eight independent terms per thread, no item search).  Every mbarrier wait is bounded: on
+// in shared memory for the epilogue.  A staged row with more than 40 of the
+// tile's 128 samples present is evaluated for every pair of the warp's rows
+// instead (eight independent terms per thread, no item search).  Every mbarrier wait is bounded: on
 // expiry the block records an error, stops, and lets its copies land.
 #pragma once
 
@@ -75,6 +75,11 @@ static_assert(UREG_LAUNCH * UTHREADS <= 65536 && UREG_CONSUMER % 8 == 0 && UREG_
               "setmaxnreg counts are multiples of 8 within the register file");
 constexpr int UR = UT / UCW;              // rows (row pass) / columns (column pass) per warp
 constexpr int URS = 16;                   // embedded rows per ring stage (the box height)
+// A staged row with more than this many of the tile's 128 samples present
+// (about 31%) is evaluated for every pair of the warp's rows: past it the
+// item path issues more term slots (about 16 p per lane at presence p,
+// masked lanes included) than the eight of the all-pairs path.
+constexpr int UDENSE_BITS = 40;
 constexpr int UFIN_THREADS = 256;
 
 // one staged box: 16 rows x 64 columns, densely packed
@@ -310,13 +315,13 @@ __global__ void __launch_bounds__(UTHREADS, 1)
                 const T *ls = vk + URS * UT * (CNT ? 4 : 2);                // [16] lengths
                 // bit n: staged row n has row r0 + rr (row pass) / column
                 // c0 + cc (column pass)
-                // staged rows dense in this tile (more than half of its 128
-                // samples present): every pair of the warp's rows, below
+                // staged rows dense in this tile (more than UDENSE_BITS of its
+                // 128 samples present): every pair of the warp's rows, below
                 uint32_t dm = 0;
                 if constexpr (op_dense_rows<Op>::value) {
                     const int pc = __popcll(word);
                     const int both = pc + __shfl_xor_sync(0xffffffffu, pc, 16);
-                    dm = __ballot_sync(0xffffffffu, lane < 16 && both > UT) & 0xffffu;
+                    dm = __ballot_sync(0xffffffffu, lane < 16 && both > UDENSE_BITS) & 0xffffu;
                 }
                 uint32_t rm[UR], cm[UR];
 #pragma unroll
