@@ -30,11 +30,21 @@ METRIC = "pair-branch updates/s"
 UNIT = "updates/s"
 WORKLOAD = "weighted_normalized_fp64 UniFrac, 20k-tip tree, 20k features x 2048 samples, full matrix"
 METHOD = "weighted_normalized_fp64"
+# --workload choices: each names the data it runs
+WORKLOADS = {
+    "20k-tips-2048-samples": "weighted_normalized_fp64, 20,000-tip tree, 20,000 x 2,048 table (the default line)",
+    "1k-tips-128-samples": "unweighted + weighted_normalized fp64, 1,000-tip tree, 1,000 x 128 table, condensed form",
+    "100k-tips-25k-presence": "unweighted fp64, 100,000-tip tree, 25,000 presence samples: tensor-core contraction "
+                              "vs the plain stripe form",
+    "100-replicates-5k-samples": "unweighted + weighted_normalized fp32, 100 rarefied replicates of a 10,000 x 5,000 "
+                                 "table, 10,000-tip tree",
+    "64-uneven-tables": "generalized + four VAW methods fp64, 64 tables of 64-4,096 samples, 50,000-tip tree",
+}
 # reference-form algorithmic bytes per pair-branch update of this method
 # (accumulator read-modify-write of two fp64 stripes per 112-node batch:
 # 2 * 2 * 8 / 112)
 ALGO_BYTES_PER_UPDATE = 2 * 2 * 8 / 112.0
-PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "pair_hybrid_weighted_normalized_fp64_config2.md")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "pair_hybrid_weighted_normalized_fp64_20k_tips_2048_samples.md")
 
 
 def parse():
@@ -49,12 +59,12 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--replicates", type=int, default=100)
-    p.add_argument("--tables5", type=int, default=64)
-    p.add_argument("--tips5", type=int, default=50000)
-    p.add_argument("--workload", default="config2", choices=["config1", "config2", "config3", "config4", "config5"],
-                   help="config3: unweighted fp64, tensor-core contraction vs the plain stripe form")
-    p.add_argument("--samples3", type=int, default=25000)
-    p.add_argument("--tips3", type=int, default=100000)
+    p.add_argument("--uneven-tables", type=int, default=64)
+    p.add_argument("--uneven-tips", type=int, default=50000)
+    p.add_argument("--workload", default="20k-tips-2048-samples", choices=list(WORKLOADS),
+                   help="; ".join(f"{k}: {v}" for k, v in WORKLOADS.items()))
+    p.add_argument("--presence-samples", type=int, default=25000)
+    p.add_argument("--presence-tips", type=int, default=100000)
     return p.parse_args()
 
 
@@ -91,7 +101,7 @@ def combine_ranks(values, world, device):
 
 def make_workload(seed, args):
     import ssu_synth
-    return ssu_synth.config2(seed=seed, n_samples=args.samples, n_tips=args.tips)
+    return ssu_synth.lognormal_20k_tips_2048_samples(seed=seed, n_samples=args.samples, n_tips=args.tips)
 
 
 class ClockSampler:
@@ -270,7 +280,7 @@ def run_reference(args):
     cb["value"] = value
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-2 generator)",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator lognormal_20k_tips_2048_samples)",
             "config": {"workload": WORKLOAD + " (CPU: stripe sub-range sample)", "method": args.method,
                        "n_samples": args.samples, "n_tips": args.tips},
             "impl": "reference", "cpu_baseline": cb,
@@ -308,7 +318,7 @@ def _timed_steps(torch, plan, stream, steps, warmup, flush):
     return total / steps, kern / steps
 
 
-def run_config3(args):
+def run_presence(args):
     """Unweighted fp64 on the 100,000-tip / 25,000-sample presence table:
     the tcgen05 contraction against the plain stripe (presence-word) form."""
     import torch
@@ -318,7 +328,7 @@ def run_config3(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    tree, table = ssu_synth.config3(seed=3, n_samples=args.samples3, n_tips=args.tips3)
+    tree, table = ssu_synth.presence_100k_tips_25k_samples(seed=3, n_samples=args.presence_samples, n_tips=args.presence_tips)
     method = "unweighted_fp64"
     os.environ["UNIFRAC_B200_UNWEIGHTED_MODE"] = "gemm"
     gp = ssu_b200.Plan(tree, table, method)
@@ -363,8 +373,8 @@ def run_config3(args):
         "metric": METRIC, "value": units / (g_step / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": g_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f16 operands, f32 accumulate per 256 nodes, f64 across chunks and ratio",
-        "data": "synthetic (seeded config-3 generator)",
-        "config": {"workload": f"unweighted_fp64 UniFrac, {args.tips3}-tip tree, {n} samples (presence, "
+        "data": "synthetic (seeded generator presence_100k_tips_25k_samples)",
+        "config": {"workload": f"unweighted_fp64 UniFrac, {args.presence_tips}-tip tree, {n} samples (presence, "
                                f"log-uniform richness 50-2000), full matrix", "embedded_branches": gp_units_e(units, n),
                    "tc_kernel_ms": g_kern, "launches_per_step": g_launches},
         "stripe_form": {"kernel": s_name, "ms_per_step": s_step, "kernel_ms": s_kern,
@@ -433,7 +443,7 @@ def _batch_setup():
     return torch, stream, flush
 
 
-def run_config1(args):
+def run_small(args):
     """1,000-tip tree, 1,000 x 128 table: unweighted and weighted-normalized
     fp64, condensed 128 x 128 form through the C API.  Too small for a
     roofline (launch- and latency-bound): times only, next to the reference's
@@ -443,7 +453,7 @@ def run_config1(args):
     import ssu_synth
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
-    tree, table = ssu_synth.config1()
+    tree, table = ssu_synth.geometric_1k_tips_128_samples()
     out = {}
     total_units, total_e2e, total_dev = 0, 0.0, 0.0
     for m in ("unweighted_fp64", "weighted_normalized_fp64"):
@@ -480,7 +490,7 @@ def run_config1(args):
         total_dev += dev_ms
     line = {"metric": METRIC, "value": total_units / (total_dev / 1e3), "unit": UNIT, "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_dev, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-1 generator)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator geometric_1k_tips_128_samples)",
             "config": {"workload": "unweighted_fp64 + weighted_normalized_fp64, 1k-tip tree, 1k features x 128 "
                                    "samples, condensed form"},
             "methods": out,
@@ -488,7 +498,7 @@ def run_config1(args):
     print(json.dumps(line), flush=True)
 
 
-def run_config4(args):
+def run_replicates(args):
     """100 rarefied replicates (depth 1,000) of a 10,000-feature x 5,000-sample
     table on a 10,000-tip tree, unweighted and weighted-normalized fp32, every
     replicate of a method in one batch plan replayed as one CUDA graph."""
@@ -498,7 +508,7 @@ def run_config4(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
     t0 = time.perf_counter()
-    tree, base, reps = ssu_synth.config4(n_replicates=args.replicates)
+    tree, base, reps = ssu_synth.rarefied_replicates_10k_tips_5k_samples(n_replicates=args.replicates)
     gen_s = time.perf_counter() - t0
     methods = ["unweighted_fp32", "weighted_normalized_fp32"]
     per, total_units, total_ms, launches, e2e = {}, 0, 0.0, 0, {}
@@ -552,7 +562,7 @@ def run_config4(args):
     line = {
         "metric": METRIC, "value": total_units / (total_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded config-4 generator; replicates rarefied "
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator rarefied_replicates_10k_tips_5k_samples; replicates rarefied "
                                                     "on the host, the same tables fed to both engines)",
         "config": {"workload": f"{args.replicates} rarefied replicates (depth 1000) of 10k features x 5000 samples, "
                                "10k-tip tree; unweighted_fp32 + weighted_normalized_fp32; full matrices",
@@ -566,7 +576,7 @@ def run_config4(args):
     print(json.dumps(line), flush=True)
 
 
-def run_config5(args):
+def run_uneven_tables(args):
     """64 tables of log-uniform sample counts in [64, 4096] on one 50,000-tip
     tree, generalized (alpha 0.5) and the four variance-adjusted methods in
     fp64, each method one batch plan replayed as one CUDA graph; per-table
@@ -577,7 +587,7 @@ def run_config5(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
     t0 = time.perf_counter()
-    tree, tables = ssu_synth.config5(n_tables=args.tables5, n_tips=args.tips5)
+    tree, tables = ssu_synth.uneven_tables_50k_tips(n_tables=args.uneven_tables, n_tips=args.uneven_tips)
     gen_s = time.perf_counter() - t0
     runs = [("generalized_fp64", False), ("unweighted_fp64", True), ("weighted_normalized_fp64", True),
             ("weighted_unnormalized_fp64", True), ("generalized_fp64", True)]
@@ -614,9 +624,9 @@ def run_config5(args):
     line = {
         "metric": METRIC, "value": total_units / (total_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-5 generator)",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator uneven_tables_50k_tips)",
         "config": {"workload": f"{len(tables)} tables, sample counts log-uniform in [64, 4096] "
-                               f"(total {sum(t.n_samples for t in tables)}), {args.tips5}-tip tree, 1% non-zero; "
+                               f"(total {sum(t.n_samples for t in tables)}), {args.uneven_tips}-tip tree, 1% non-zero; "
                                "generalized a=0.5 and VAW unweighted / weighted_normalized / "
                                "weighted_unnormalized / generalized a=0.5, fp64, full matrices",
                    "l2": "flushed between steps; embedding > L2", "generation_s": gen_s},
@@ -634,14 +644,14 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload == "config1":
-        return run_config1(args)
-    if args.workload == "config3":
-        return run_config3(args)
-    if args.workload == "config4":
-        return run_config4(args)
-    if args.workload == "config5":
-        return run_config5(args)
+    if args.workload == "1k-tips-128-samples":
+        return run_small(args)
+    if args.workload == "100k-tips-25k-presence":
+        return run_presence(args)
+    if args.workload == "100-replicates-5k-samples":
+        return run_replicates(args)
+    if args.workload == "64-uneven-tables":
+        return run_uneven_tables(args)
     import torch
     import torch.distributed as dist
     world, rank, local = dist_init()
@@ -723,7 +733,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-2 generator)",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator lognormal_20k_tips_2048_samples)",
             "config": {"workload": WORKLOAD, "method": args.method, "n_samples": args.samples, "n_tips": args.tips,
                        "embedded_branches": plan.n_embedded(), "pair_kernel": plan.pair_kernel(),
                        "l2": "flushed between steps (256 MiB write outside the step events); embedding 655 MB > L2",

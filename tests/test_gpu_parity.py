@@ -218,10 +218,10 @@ def test_rarefaction_keeps_deep_samples(ssu):
     assert np.all(np.isfinite(m))
 
 
-def test_config2_full_size_stripe_windows(ssu, oracle_mod):
-    """Full 20,000-tip x 2,048-sample config-2 input: the GPU matrix against
+def test_20k_tips_2048_samples_full_size_stripe_windows(ssu, oracle_mod):
+    """Full 20,000-tip x 2,048-sample input: the GPU matrix against
     the oracle on the first and last stripes, plus matrix properties."""
-    tree, table = ssu_synth.config2()
+    tree, table = ssu_synth.lognormal_20k_tips_2048_samples()
     n = table.n_samples
     s_total = (n + 1) // 2
     for m in ("weighted_normalized_fp64", "weighted_unnormalized_fp64"):

@@ -16,8 +16,8 @@
 //               8 tile rows and walks every row, in order, one lane per element
 //               (bit-reproducible).  fp32 plans: each row is handled by one
 //               warp, which gathers only the present values and adds the
-//               products with shared-memory atomics (13% faster on config-4
-//               data; the order of these additions, so the last bits of the
+//               products with shared-memory atomics (13% faster on rarefied
+//               replicate tables; the order of these additions, so the last bits of the
 //               fp64 sums, can vary between runs).
 // d = D + (M + Ws_k + Ws_l) subtracts; where d < tau (Ws_k + Ws_l) the
 // rounding of that subtraction could reach 1e-13 relative, so the tile is

@@ -306,14 +306,14 @@ def rarefy(table: Table, depth: int, seed: int) -> Table:
 
 # ---------------------------------------------------------------- workloads
 
-def config1(seed: int = 1):
+def geometric_1k_tips_128_samples(seed: int = 1):
     """1,000-tip tree (Exp mean 0.1); 1,000 x 128 table, 5% non-zero, Geometric(20)+1."""
     tree = random_binary_tree(1000, 0.1, seed)
     table = geometric_table(tree.tip_names(), 128, 0.05, 20.0, seed + 1000)
     return tree, table
 
 
-def config2(seed: int = 2, n_samples: int = 2048, n_tips: int = 20000):
+def lognormal_20k_tips_2048_samples(seed: int = 2, n_samples: int = 2048, n_tips: int = 20000):
     """20,000-tip tree (Exp mean 0.05); 20,000 x 2,048 table, 1% non-zero,
     round(LogNormal(2, 1.5)) + 1."""
     tree = random_binary_tree(n_tips, 0.05, seed)
@@ -321,14 +321,15 @@ def config2(seed: int = 2, n_samples: int = 2048, n_tips: int = 20000):
     return tree, table
 
 
-def config3(seed: int = 3, n_samples: int = 25000, n_tips: int = 100000):
+def presence_100k_tips_25k_samples(seed: int = 3, n_samples: int = 25000, n_tips: int = 100000):
     """100,000-tip tree (Exp mean 0.02); presence table, richness LogUniform[50, 2000]."""
     tree = random_binary_tree(n_tips, 0.02, seed)
     table = presence_table(tree.tip_names(), n_samples, 50, min(2000, n_tips), seed + 1000)
     return tree, table
 
 
-def config4(seed: int = 4, n_replicates: int = 100, n_samples: int = 5000, n_tips: int = 10000, depth: int = 1000):
+def rarefied_replicates_10k_tips_5k_samples(seed: int = 4, n_replicates: int = 100, n_samples: int = 5000,
+                                             n_tips: int = 10000, depth: int = 1000):
     """10,000-tip tree (Exp mean 0.1); base 10,000 x 5,000 table, 2% non-zero,
     NegBinomial(50, 0.5); replicates rarefied to `depth` with seed+r."""
     tree = random_binary_tree(n_tips, 0.1, seed)
@@ -337,7 +338,7 @@ def config4(seed: int = 4, n_replicates: int = 100, n_samples: int = 5000, n_tip
     return tree, base, reps
 
 
-def config5(seed: int = 5, n_tables: int = 64, n_tips: int = 50000, lo: int = 64, hi: int = 4096):
+def uneven_tables_50k_tips(seed: int = 5, n_tables: int = 64, n_tips: int = 50000, lo: int = 64, hi: int = 4096):
     """One 50,000-tip tree (Exp mean 0.03); tables with log-uniform sample
     counts in [lo, hi], 1% non-zero, round(LogNormal(2, 1.5)) + 1."""
     tree = random_binary_tree(n_tips, 0.03, seed)
