@@ -192,24 +192,31 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            for line in out.splitlines():
-                f = [x.strip() for x in line.split(",")]
-                if len(f) < 9:
-                    continue
-                try:
-                    s, m = float(f[1]), float(f[2])
-                except ValueError:
-                    continue
+            for s, m, r in self.parse_smi(out):
                 sm.append(s)
                 mx.append(m)
                 smi += 1
-                for name, val in zip(self.NAMES, f[5:9]):
-                    if val.lower() == "active":
-                        reasons.add(name)
+                reasons.update(r)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "sm_min_mhz": min(sm),
                 "reasons": sorted(reasons), "samples": len(sm), "nvidia_smi_samples": smi}
+
+    @classmethod
+    def parse_smi(cls, text):
+        """(sm MHz, max sm MHz, active throttle reasons) per line of the
+        FIELDS query in csv,noheader,nounits form; other lines are skipped."""
+        rows = []
+        for line in text.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                s, m = float(f[1]), float(f[2])
+            except ValueError:
+                continue
+            rows.append((s, m, [name for name, val in zip(cls.NAMES, f[5:9]) if val.lower() == "active"]))
+        return rows
 
 
 def read_traffic():

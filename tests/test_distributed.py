@@ -120,3 +120,18 @@ def test_reference_arm_prints_one_contract_line_on_rank_0():
 
 def test_reference_arm_other_ranks_exit_without_work():
     assert _reference_arm({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []
+
+
+def test_clock_lines_parse_with_throttle_reasons():
+    sys.path.insert(0, ROOT)
+    import bench
+    text = ("0, 1965, 1965, 512.3, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active\n"
+            "0, 1500, 1965, 998.7, 0x0000000000000004, Not Active, Not Active, Not Active, Active\n"
+            "0, 1200, 1965, 700.0, 0x0000000000000008, Active, Not Active, Active, Not Active\n"
+            "0, [N/A], 1965, 1.0, 0x0, Not Active, Not Active, Not Active, Not Active\n"
+            "garbage\n")
+    rows = bench.ClockSampler.parse_smi(text)
+    assert [r[0] for r in rows] == [1965.0, 1500.0, 1200.0]
+    assert all(r[1] == 1965.0 for r in rows)
+    assert rows[0][2] == [] and rows[1][2] == ["sw_power_cap"]
+    assert rows[2][2] == ["hw_slowdown", "sw_thermal_slowdown"]
