@@ -115,6 +115,19 @@ __host__ __device__ constexpr size_t union_smem() {
     return union_ring_bytes<T, CNT>() + sizeof(double) * 2 * UT + sizeof(uint64_t) * 2 * union_stages<T, CNT>() + 16;
 }
 
+// Layout checks for every instance: whole 128-byte stages (each TMA box
+// lands 128-aligned), a transaction count within the mbarrier's range, and
+// the block's shared memory within the 227 KB a CTA may have.
+template <typename T, bool CNT>
+constexpr bool union_layout_ok() {
+    return union_stage_bytes<T, CNT>() % 128 == 0 && union_box_bytes<T>() % 128 == 0 &&
+           union_stage_tx<T, CNT>() <= union_stage_bytes<T, CNT>() && union_stage_tx<T, CNT>() < (1u << 20) &&
+           union_smem<T, CNT>() <= 227u * 1024u && union_stages<T, CNT>() >= 2;
+}
+static_assert(union_layout_ok<double, true>() && union_layout_ok<double, false>() &&
+                  union_layout_ok<float, true>() && union_layout_ok<float, false>(),
+              "union kernel shared-memory layout");
+
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_u32(dst)),
