@@ -627,13 +627,22 @@ ComputeStatus subsample_batch_v3(const support_biom_t *table_data, const support
     read_inputs(table_data, tree_data, table, tree);
     st = validate(table, tree);
     if (st != okay) return st;
-    std::vector<ssu::Table> reps;
-    reps.reserve(n_subsamples);
+    // Replicate i draws from its own stream (seed + i), so the replicates are
+    // rarefied on all host threads, each bit-identical to a serial pass.
+    std::vector<ssu::Table> reps(n_subsamples);
     const uint64_t seed = g_seed.load();
-    for (unsigned int i = 0; i < n_subsamples; i++) {
-        reps.push_back(table.rarefied(depth, with_replacement, seed + i));
-        if (reps.back().n_samples == 0 || reps.back().n_obs == 0) return table_empty;
-    }
+    const unsigned n_threads =
+        std::max(1u, std::min<unsigned>(n_subsamples, std::thread::hardware_concurrency()));
+    auto rarefy_from = [&](unsigned first) {
+        for (unsigned i = first; i < n_subsamples; i += n_threads)
+            reps[i] = table.rarefied(depth, with_replacement, seed + i);
+    };
+    std::vector<std::thread> workers;
+    for (unsigned t = 1; t < n_threads; t++) workers.emplace_back(rarefy_from, t);
+    rarefy_from(0);
+    for (std::thread &w : workers) w.join();
+    for (const ssu::Table &t : reps)
+        if (t.n_samples == 0 || t.n_obs == 0) return table_empty;
     std::vector<const ssu::Table *> ptrs;
     for (const ssu::Table &t : reps) ptrs.push_back(&t);
     return batch_matrices<TReal, TMat>(ptrs, tree, r, results);
