@@ -315,7 +315,8 @@ SSU_EXTERN void ssu_b200_plan_destroy(ssu_b200_plan_t **plan);
  * n_embedded rows of ld doubles (ld a multiple of 128, >= n_samples), row e
  * the proportions of embedded branch e per sample; d_lengths the n_embedded
  * branch lengths; d_out receives the full n_samples x n_samples fp64 matrix.
- * The call allocates nothing: its scratch (split-K partial tiles, per-sample
+ * d_embedding must be 16-byte aligned and d_lengths, d_out 8-byte aligned
+ * (output_error otherwise).  The call allocates nothing: its scratch (split-K partial tiles, per-sample
  * weighted sums, tile list) lives in one 32 MiB file-scope device array that
  * every GPU loading the library holds until exit.  n_samples is limited to
  * 100000 and a call whose scratch needs exceed the array returns

@@ -83,11 +83,12 @@ def torch_cuda():
 
 def test_noalloc_matches_full_matrix_entry_point_on_consecutive_calls(ssu, torch_cuda):
     cases = []
-    for seed, n_samples, n_tips in [(71, 150, 400), (72, 300, 250)]:
+    # 129 samples: the last diagonal block holds one sample and has no tile
+    for seed, n_samples, n_tips in [(71, 150, 400), (72, 300, 250), (73, 129, 300)]:
         tree = ssu_synth.random_binary_tree(n_tips, 0.1, seed)
         table = ssu_synth.geometric_table(tree.tip_names()[: n_tips - 20], n_samples, 0.08, 12.0, seed + 1)
         cases.append((tree, table))
-    calls = [(0, True), (0, True), (1, False), (0, True), (1, True)]
+    calls = [(0, True), (0, True), (1, False), (2, True), (0, True), (1, True), (2, False)]
     for idx, normalized in calls:
         tree, table = cases[idx]
         U, lens = host_embedding(ssu, tree, table)
@@ -110,3 +111,6 @@ def test_noalloc_rejects_sizes_beyond_its_limit(ssu, torch_cuda):
     assert f(p, p, 1, 100001, 100096, 1, p, None) == 6   # beyond the sample limit
     assert f(p, p, 1, 200, 100, 1, p, None) == 6         # ld smaller than n_samples
     assert f(p, p, 1, 0, 128, 1, p, None) == 3           # no samples
+    assert f(p + 8, p, 1, 100, 128, 1, p, None) == 6     # embedding not 16-byte aligned
+    assert f(p, p + 4, 1, 100, 128, 1, p, None) == 6     # lengths not 8-byte aligned
+    assert f(p, p, 1, 100, 128, 1, p + 4, None) == 6     # output not 8-byte aligned

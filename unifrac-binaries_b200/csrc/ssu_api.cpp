@@ -11,7 +11,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <fcntl.h>
+#include <sched.h>
+#include <system_error>
 #include <fstream>
 #include <memory>
 #include <sstream>
@@ -39,6 +42,61 @@ constexpr uint32_t kPinnedFlag = 0x2000;  // matrix from the page-locked result 
 constexpr size_t kHugeAlign = size_t(2) << 20;
 
 std::atomic<uint64_t> g_seed{5489u};
+
+// Host threads for the library's own parallel loops: OMP_NUM_THREADS when
+// set (the reference's OpenMP loops honour it), else the CPUs this process
+// may run on (affinity mask, so cgroup/taskset limits hold), at most `cap`.
+unsigned host_threads(unsigned cap) {
+    unsigned n = 0;
+    if (const char *v = std::getenv("OMP_NUM_THREADS")) {
+        const long x = std::strtol(v, nullptr, 10);
+        if (x > 0) n = static_cast<unsigned>(x);
+    }
+    if (n == 0) {
+        cpu_set_t set;
+        CPU_ZERO(&set);
+        if (sched_getaffinity(0, sizeof(set), &set) == 0) n = static_cast<unsigned>(CPU_COUNT(&set));
+    }
+    if (n == 0) n = std::thread::hardware_concurrency();
+    return std::max(1u, std::min(n, std::max(1u, cap)));
+}
+
+// Run fn(i) for i in [0, n) on up to `threads` threads (the caller's included)
+// pulling indices from a shared counter.  A thread that cannot be started
+// leaves its share to the others; every started thread is joined, also when
+// fn throws; the first exception is rethrown on the calling thread.
+template <class F>
+void parallel_for(unsigned n, unsigned threads, F &&fn) {
+    std::atomic<unsigned> next{0};
+    std::mutex err_mu;
+    std::exception_ptr err;
+    auto work = [&] {
+        try {
+            for (unsigned i = next.fetch_add(1); i < n; i = next.fetch_add(1)) fn(i);
+        } catch (...) {
+            std::lock_guard<std::mutex> lock(err_mu);
+            if (!err) err = std::current_exception();
+            next.store(n);  // the others stop at their next index
+        }
+    };
+    struct Joiner {
+        std::vector<std::thread> v;
+        ~Joiner() {
+            for (std::thread &t : v)
+                if (t.joinable()) t.join();
+        }
+    } pool;
+    for (unsigned t = 1; t < std::min(threads, n); t++) {
+        try {
+            pool.v.emplace_back(work);
+        } catch (const std::system_error &) {
+            break;
+        }
+    }
+    work();
+    for (std::thread &t : pool.v) t.join();
+    if (err) std::rethrow_exception(err);
+}
 
 bool env_yes(const char *name) {
     const char *v = std::getenv(name);
@@ -347,16 +405,13 @@ bool alloc_full(TMat *&result, const std::vector<std::string_view> &ids, const c
 // Touch every page of a fresh host buffer on a few threads (run while the
 // GPU computes, so the copy-out finds resident pages).
 void prefault(void *p, size_t bytes) {
-    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const unsigned hw = host_threads(8);
     const size_t slice = ((bytes / hw) + kHugeAlign - 1) / kHugeAlign * kHugeAlign;
-    std::vector<std::thread> threads;
-    for (unsigned t = 0; t < hw; t++) {
+    const unsigned parts = static_cast<unsigned>((bytes + slice - 1) / slice);
+    parallel_for(parts, hw, [&](unsigned t) {
         const size_t a = t * slice;
-        if (a >= bytes) break;
-        const size_t len = std::min(slice, bytes - a);
-        threads.emplace_back([p, a, len] { std::memset(static_cast<char *>(p) + a, 0, len); });
-    }
-    for (auto &th : threads) th.join();
+        std::memset(static_cast<char *>(p) + a, 0, std::min(slice, bytes - a));
+    });
 }
 
 template <class TMat, class TReal>
@@ -628,19 +683,25 @@ ComputeStatus subsample_batch_v3(const support_biom_t *table_data, const support
     st = validate(table, tree);
     if (st != okay) return st;
     // Replicate i draws from its own stream (seed + i), so the replicates are
-    // rarefied on all host threads, each bit-identical to a serial pass.
+    // rarefied on host threads, each bit-identical to a serial pass.  Each
+    // draw holds temporaries of about three times the table's entries, so the
+    // thread count is bounded by a 4 GiB budget for them as well as by
+    // host_threads (OMP_NUM_THREADS / affinity, at most 16).
     std::vector<ssu::Table> reps(n_subsamples);
     const uint64_t seed = g_seed.load();
-    const unsigned n_threads =
-        std::max(1u, std::min<unsigned>(n_subsamples, std::thread::hardware_concurrency()));
-    auto rarefy_from = [&](unsigned first) {
-        for (unsigned i = first; i < n_subsamples; i += n_threads)
-            reps[i] = table.rarefied(depth, with_replacement, seed + i);
-    };
-    std::vector<std::thread> workers;
-    for (unsigned t = 1; t < n_threads; t++) workers.emplace_back(rarefy_from, t);
-    rarefy_from(0);
-    for (std::thread &w : workers) w.join();
+    const size_t per_draw = 3 * (table.nnz() * (sizeof(double) + sizeof(uint32_t)) +
+                                 static_cast<size_t>(depth) * table.n_samples * sizeof(uint32_t)) + 1;
+    const unsigned by_memory = static_cast<unsigned>(std::max<size_t>(1, (size_t(4) << 30) / per_draw));
+    try {
+        parallel_for(n_subsamples, std::min(host_threads(16), by_memory),
+                     [&](unsigned i) { reps[i] = table.rarefied(depth, with_replacement, seed + i); });
+    } catch (const std::bad_alloc &) {
+        report("subsample", "out of host memory while rarefying");
+        return output_error;
+    } catch (const std::exception &e) {
+        report("subsample", e.what());
+        return output_error;
+    }
     for (const ssu::Table &t : reps)
         if (t.n_samples == 0 || t.n_obs == 0) return table_empty;
     std::vector<const ssu::Table *> ptrs;

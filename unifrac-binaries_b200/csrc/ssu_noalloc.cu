@@ -20,7 +20,10 @@
 //    last call left there; calls that overlap on the GPU (different streams,
 //    or different host threads without ordering) race on it;
 //  * nothing in the scratch has to start at zero: every value a call reads is
-//    written earlier in the same call;
+//    written earlier in the same call (the tile list and the table descriptor
+//    by a small kernel, so no call reads host memory once it has returned);
+//  * d_embedding must be 16-byte aligned, d_lengths and d_out 8-byte aligned
+//    (output_error otherwise);
 //  * the first call on a device resolves the array's device address
 //    (cudaGetSymbolAddress) and sets the pair kernel's shared-memory limit,
 //    so that first call should come before any stream capture.
@@ -92,20 +95,36 @@ bool setup_device(int dev, DeviceSetup &out) {
     return true;
 }
 
+// Tiles of the pair kernel: every 128 x 128 block (kb, lb) with kb <= lb,
+// row-major, except the last diagonal block when it holds one sample (no pair
+// k < l there): the blocks (kb, lb) with kb * 128 < min(n, (lb + 1) * 128) - 1.
+uint32_t tile_count(uint32_t n) {
+    const uint32_t nb = (n + BM - 1) / BM;
+    return nb * (nb + 1) / 2 - (n % BM == 1 ? 1u : 0u);
+}
+
+// One thread per block row kb writes that row's tiles at their closed-form
+// offset kb * nb - kb (kb - 1) / 2; thread 0 also writes the table descriptor.
+__global__ void write_tiles_kernel(uint4 *tiles, ssu::dev::TableDesc *table, uint32_t n, uint32_t nb,
+                                   uint32_t n_tiles) {
+    const uint32_t kb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kb == 0) {
+        ssu::dev::TableDesc t{};
+        t.n = n;
+        *table = t;
+    }
+    if (kb >= nb) return;
+    const uint32_t first = kb * nb - kb * (kb - 1) / 2;
+    for (uint32_t lb = kb; lb < nb; lb++)
+        if (first + (lb - kb) < n_tiles) tiles[first + (lb - kb)] = make_uint4(kb, lb, 0, 0);
+}
+
 template <bool NORM>
 int run(const DeviceSetup &ds, const double *U, const double *len, uint32_t E, uint32_t n, uint64_t ld,
         double *out, cudaStream_t stream) {
     using Op = WeightedOp<NORM>;
-    // tile list: every (kb, lb) holding a pair k < l, all of table 0
-    std::vector<uint4> tiles;
-    const uint32_t nbk = (n + BM - 1) / BM, nbl = (n + BN - 1) / BN;
-    for (uint32_t kb = 0; kb < nbk; kb++)
-        for (uint32_t lb = 0; lb < nbl; lb++)
-            if (static_cast<uint64_t>(kb) * BM < std::min<uint64_t>(n, static_cast<uint64_t>(lb + 1) * BN) - 1)
-                tiles.push_back(make_uint4(kb, lb, 0, 0));
-    const uint32_t n_tiles = static_cast<uint32_t>(tiles.size());
-    ssu::dev::TableDesc table{};
-    table.n = n;
+    const uint32_t nb = (n + BM - 1) / BM;
+    const uint32_t n_tiles = tile_count(n);
 
     // scratch layout: [table][tiles][W][W partials][split partials], 256-byte aligned
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
@@ -158,13 +177,9 @@ int run(const DeviceSetup &ds, const double *U, const double *len, uint32_t E, u
     if (splits == 0) splits = 1;
     double *d_split = splits > 1 ? reinterpret_cast<double *>(base + off) : nullptr;
 
-    cudaError_t e = cudaMemcpyAsync(d_tiles, tiles.data(), sizeof(uint4) * n_tiles, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_table, &table, sizeof(table), cudaMemcpyHostToDevice, stream);
-    if (e != cudaSuccess) {
-        note(cudaGetErrorString(e));
-        return output_error;
-    }
+    // the tile list and the table descriptor are written on the device: the
+    // call reads no host memory after it returns
+    write_tiles_kernel<<<(nb + 127) / 128, 128, 0, stream>>>(d_tiles, d_table, n, nb, n_tiles);
     if (NORM) {
         dim3 grid(static_cast<uint32_t>((ld + 255) / 256), n_parts);
         ssu::dev::weighted_sums_partial_kernel<double><<<grid, 256, 0, stream>>>(U, len, E, ld, chunk, d_part,
@@ -197,7 +212,7 @@ int run(const DeviceSetup &ds, const double *U, const double *len, uint32_t E, u
                 <<<n_tiles, (BM / TM) * (BN / TN), 0, stream>>>(a, splits);
     }
     ssu::dev::zero_diagonal_kernel<<<dim3((n + 255) / 256, 1), 256, 0, stream>>>(out, d_table, 1);
-    e = cudaGetLastError();
+    const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         note(cudaGetErrorString(e));
         return output_error;
@@ -221,6 +236,13 @@ extern "C" ComputeStatus ssu_b200_weighted_pairs_noalloc(const double *d_embeddi
     }
     if (!d_embedding || !d_lengths || !d_out) {
         note("null device pointer");
+        return output_error;
+    }
+    // the pair kernel stages embedding rows with 16-byte copies and reads
+    // lengths and writes the matrix as doubles
+    if (reinterpret_cast<uintptr_t>(d_embedding) % 16 != 0 || reinterpret_cast<uintptr_t>(d_lengths) % 8 != 0 ||
+        reinterpret_cast<uintptr_t>(d_out) % 8 != 0) {
+        note("d_embedding must be 16-byte aligned, d_lengths and d_out 8-byte aligned");
         return output_error;
     }
     int dev = 0;
