@@ -1,8 +1,9 @@
 """The tensor-core (tcgen05) unweighted contraction, selected with
 UNIFRAC_B200_UNWEIGHTED_MODE=gemm, against the fp64 oracle.  Bar: max
 relative error 1e-6 on every pair (the contraction's stated bound; lengths
-carried as fp16 hi+lo per 256-node chunk, fp32 accumulation per chunk, fp64
-across chunks and in the final ratio)."""
+carried as an integer fp16 hi part and an fp16 lo part per chunk of lengths
+within a factor of two, exact hi sums, fp64 across chunks and in the final
+ratio)."""
 import os
 
 import numpy as np
@@ -78,3 +79,54 @@ def test_tc_plan_agrees_with_stripe_form(ssu, gemm_mode):
     os.environ["UNIFRAC_B200_UNWEIGHTED_MODE"] = "stripe"
     stripe, _ = ssu.one_off_matrix(tree, table, "unweighted_fp64")
     assert rel_err(tc, stripe)[0] <= TC_REL
+
+
+@pytest.mark.parametrize("n_samples", [2, 128, 129, 255, 256, 257, 383, 511, 513])
+@pytest.mark.parametrize("method", ["unweighted_fp64", "unweighted_unnormalized_fp64"])
+def test_tc_sample_counts_at_work_unit_edges(ssu, oracle_mod, gemm_mode, n_samples, method):
+    """A work unit covers 256 rows x 128 columns: counts around those edges,
+    where units straddle the diagonal or hold a single row or column."""
+    tree, table = _case(n_samples, 300, n_samples, density=0.08)
+    gpu, _ = ssu.one_off_matrix(tree, table, method)
+    ref = oracle_mod.oracle_one_off(tree, table, method)["matrix"]
+    r, z = rel_err(gpu, ref)
+    assert r <= TC_REL and z <= 1e-9, (r, z)
+
+
+def test_tc_close_and_identical_samples(ssu, oracle_mod, gemm_mode):
+    """Samples equal to another one, or differing from it by one short tip:
+    the xor sum is small next to the samples' own lengths, where a contraction
+    of the shared length (r_k + r_l - 2 X L X^T) would cancel."""
+    tree, table = _case(21, 800, 60, density=0.15)
+    dense = table.dense()
+    lengths = dict(zip(tree.tip_names(), tree.tip_lengths()))
+    obs = list(table.obs_ids)
+    shortest = min(range(len(obs)), key=lambda i: lengths.get(obs[i], 1e9))
+    for j in range(0, 30, 2):
+        dense[:, j + 1] = dense[:, j]
+        if j % 4 == 0:
+            dense[shortest, j + 1] = 0.0 if dense[shortest, j] > 0 else 3.0
+    table = ssu_synth.Table.from_dense(dense, obs, table.sample_ids)
+    for method in ("unweighted_fp64", "unweighted_unnormalized_fp64"):
+        gpu, _ = ssu.one_off_matrix(tree, table, method)
+        ref = oracle_mod.oracle_one_off(tree, table, method)["matrix"]
+        r, z = rel_err(gpu, ref)
+        assert r <= TC_REL and z <= 1e-12, (method, r, z)
+
+
+def test_tc_wait_that_runs_out_is_an_error_and_the_device_stays_usable(ssu, oracle_mod, gemm_mode, monkeypatch):
+    """Failure injection without a fault: with UNIFRAC_B200_TEST_STALL the
+    tensor-core kernel's producers issue no copy, so the MMA issuer's and the
+    epilogues' bounded waits (here ~1 ms) run out; the call returns
+    output_error instead of hanging, and the next call is correct."""
+    tree, table = _case(31, 300, 300)
+    monkeypatch.setenv("UNIFRAC_B200_TEST_STALL", "1")
+    monkeypatch.setenv("UNIFRAC_B200_WAIT_CYCLES", "2000000")
+    with pytest.raises(ssu.SSUError) as e:
+        ssu.one_off_matrix(tree, table, "unweighted_fp64")
+    assert e.value.status == 6  # output_error
+    monkeypatch.delenv("UNIFRAC_B200_TEST_STALL")
+    monkeypatch.delenv("UNIFRAC_B200_WAIT_CYCLES")
+    gpu, _ = ssu.one_off_matrix(tree, table, "unweighted_fp64")
+    ref = oracle_mod.oracle_one_off(tree, table, "unweighted_fp64")["matrix"]
+    assert rel_err(gpu, ref)[0] <= TC_REL

@@ -116,7 +116,7 @@ bool make_fp16_map(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols) {
     if (!f) return false;
     const cuuint64_t dims[2] = {cols, rows};
     const cuuint64_t strides[1] = {cols * 2};
-    const cuuint32_t box[2] = {static_cast<cuuint32_t>(tc::BLOCK_K), static_cast<cuuint32_t>(tc::BLOCK_M)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(tc::BLOCK_K), static_cast<cuuint32_t>(tc::ROWS)};
     const cuuint32_t estr[2] = {1, 1};
     return f(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -317,6 +317,9 @@ struct PlanImpl {
     // returns output_error: host-side failure injection, no fault)
     long long union_wait_cycles = 2000000000LL;
     int union_stall = 0;
+    // the same for the tensor-core kernel, whose longest legitimate wait (a
+    // chunk of 127 K blocks) is about 35 us: default about 0.1 s
+    long long gemm_wait_cycles = 200000000LL;
     int sparse_prep_alloc();
     template <typename T>
     int sparse_prep(cudaStream_t s, const Group &g, uint32_t div);
@@ -338,10 +341,9 @@ struct PlanImpl {
     bool gemm = false;
     uint32_t n_pad = 0, k_pad = 0, n_chunks = 0;
     __half *d_A = nullptr, *d_Bh = nullptr, *d_Bl = nullptr, *d_lhi = nullptr, *d_llo = nullptr;
-    double *d_r = nullptr, *d_lsorted = nullptr, *d_chunk_scale = nullptr, *d_G = nullptr;
+    double *d_r = nullptr, *d_lsorted = nullptr, *d_chunk_scale = nullptr;
+    uint32_t *d_chunk_end = nullptr;
     int32_t *d_parent_col = nullptr;
-    std::vector<tc::GemmTable> gtables;
-    tc::GemmTable *d_gtables = nullptr;
     int *d_error = nullptr;
     CUtensorMap map_A{}, map_Bh{}, map_Bl{};
     int setup_gemm(const TableSet &set, const FlatTree &tree);
@@ -479,10 +481,10 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
     size_t per_col = el * std::max<uint32_t>(K, 1) * (counts ? 2 : 1) + sizeof(double) + (counts ? el : 0) +
                      sizeof(unsigned long long) * n_words + (n_parts ? el * (n_parts + 1) : 0);
     if (gemm) {
-        // fp16 operand rows A, B_hi, B_lo over the padded nodes, r, and a row
-        // of the table's fp64 G block
-        const uint64_t kp = (static_cast<uint64_t>(E) + 255) / 256 * 256;
-        per_col = 3 * sizeof(uint16_t) * kp + sizeof(double) + sizeof(double) * ((max_table_n + 127) / 128 * 128);
+        // fp16 operand rows A, B_hi, B_lo over the padded nodes (chunk
+        // padding included, allowing for 128 chunks) and r
+        const uint64_t kp = (static_cast<uint64_t>(E) + 63) / 64 * 64 + 128 * 64;
+        per_col = 3 * sizeof(uint16_t) * kp + sizeof(double);
     }
     size_t budget = opts.group_bytes;
     if (!budget) {
@@ -1248,39 +1250,61 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
 // --------------------------------------------------- tensor-core unweighted
 
 int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
-    const uint32_t chunk_nodes = tc::CHUNK_KB * tc::BLOCK_K;
-    k_pad = std::max<uint32_t>(chunk_nodes, ((E + chunk_nodes - 1) / chunk_nodes) * chunk_nodes);
-    n_chunks = k_pad / chunk_nodes;
-    // embedded nodes sorted by decreasing length
+    // Embedded nodes by decreasing |length|, packed into chunks of whole
+    // 64-node K blocks: a chunk closes (its last block padded with
+    // zero-length columns) when the next length is below half the chunk's
+    // first, or at MAX_CHUNK_KB blocks.  Chunk c is scaled by 2^s_c so that
+    // its largest |length| lies in [1024, 2048): every length of the chunk in
+    // [512, 2048), hi = nearest integer (exact in fp16), lo = fp16(rest).
     std::vector<uint32_t> order(E);
     for (uint32_t e = 0; e < E; e++) order[e] = e;
     std::stable_sort(order.begin(), order.end(),
-                     [&](uint32_t a, uint32_t b) { return tree.length[a] > tree.length[b]; });
+                     [&](uint32_t a, uint32_t b) { return std::fabs(tree.length[a]) > std::fabs(tree.length[b]); });
     std::vector<int32_t> col_of_row(tree.n_nodes, -1);
-    for (uint32_t c = 0; c < E; c++) col_of_row[order[c]] = static_cast<int32_t>(c);
-    std::vector<double> lsorted(k_pad, 0.0), scale(n_chunks, 1.0);
-    std::vector<__half> lhi(k_pad, __float2half(0.0f)), llo(k_pad, __float2half(0.0f));
-    for (uint32_t c = 0; c < E; c++) lsorted[c] = tree.length[order[c]];
-    for (uint32_t ch = 0; ch < n_chunks; ch++) {
-        const double mx = lsorted[ch * chunk_nodes];
-        int sig = 0;
-        if (mx > 0) sig = 14 - static_cast<int>(std::floor(std::log2(mx)));
-        scale[ch] = std::ldexp(1.0, -sig);
-        for (uint32_t c = ch * chunk_nodes; c < (ch + 1) * chunk_nodes; c++) {
-            const double x = std::ldexp(lsorted[c], sig);
-            const __half h = __double2half(x);
-            lhi[c] = h;
-            llo[c] = __double2half(x - static_cast<double>(__half2float(h)));
+    std::vector<double> lsorted, scale;
+    std::vector<__half> lhi, llo;
+    std::vector<uint32_t> chunk_end;
+    const uint32_t max_cols = static_cast<uint32_t>(tc::MAX_CHUNK_KB) * tc::BLOCK_K;
+    auto pad_to_block = [&] {
+        while (lsorted.size() % tc::BLOCK_K) {
+            lsorted.push_back(0.0);
+            lhi.push_back(__float2half(0.0f));
+            llo.push_back(__float2half(0.0f));
         }
+        chunk_end.push_back(static_cast<uint32_t>(lsorted.size() / tc::BLOCK_K));
+    };
+    double first = -1.0;
+    size_t chunk_first = 0;
+    int sig = 0;
+    for (uint32_t i = 0; i < E; i++) {
+        const double L = tree.length[order[i]];
+        const double a = std::fabs(L);
+        if (first < 0 || a < first / 2 || lsorted.size() - chunk_first >= max_cols) {
+            if (first >= 0) pad_to_block();
+            first = a;
+            chunk_first = lsorted.size();
+            sig = a > 0 ? 10 - static_cast<int>(std::floor(std::log2(a))) : 0;
+            scale.push_back(std::ldexp(1.0, -sig));
+        }
+        col_of_row[order[i]] = static_cast<int32_t>(lsorted.size());
+        const double x = std::ldexp(L, sig);
+        const double hi = std::nearbyint(x);
+        lsorted.push_back(L);
+        lhi.push_back(__double2half(hi));
+        llo.push_back(__double2half(x - hi));
     }
+    if (first < 0) scale.push_back(1.0);  // no embedded node: one chunk of padding
+    pad_to_block();
+    k_pad = static_cast<uint32_t>(lsorted.size());
+    n_chunks = static_cast<uint32_t>(chunk_end.size());
     // parents among embedded nodes
     std::vector<int32_t> parent_row(tree.n_nodes, -1);
     for (uint32_t r = 0; r < tree.n_nodes; r++)
         for (uint32_t c = tree.child_ptr[r]; c < tree.child_ptr[r + 1]; c++) parent_row[tree.child_rows[c]] = r;
     std::vector<int32_t> parent_col(k_pad, -1);
-    for (uint32_t c = 0; c < E; c++) {
-        const int32_t p = parent_row[order[c]];
-        parent_col[c] = (p >= 0 && static_cast<uint32_t>(p) < E) ? col_of_row[p] : -1;
+    for (uint32_t r = 0; r < E; r++) {
+        const int32_t p = parent_row[r];
+        parent_col[col_of_row[r]] = (p >= 0 && static_cast<uint32_t>(p) < E) ? col_of_row[p] : -1;
     }
     // starting column of each tree observation: its tip, or the tip's parent
     // when tips are bypassed
@@ -1324,30 +1348,25 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
         SSU_CK(upload(&g.d_sample_ptr, sample_ptr.data(), sizeof(uint32_t) * sample_ptr.size()));
         SSU_CK(upload(&g.d_start_col, start_col.data(), sizeof(int32_t) * start_col.size()));
     }
-    // G blocks per table, relative to the group's G buffer; every ordered
-    // tile of each table, grouped 12 x 12 so concurrent CTAs share row
-    // blocks in L2
-    gtables.assign(tdesc.size(), tc::GemmTable{});
-    uint64_t g_max = 0;
+    // work units: per table, the (256-row block, 128-column block) pairs
+    // holding some pair k < l, in 8 x 16 super-blocks so that the clusters
+    // running at the same time share operand rows in L2
     for (Group &g : groups) {
-        uint64_t off = 0;
         std::vector<uint4> tiles;
         for (uint32_t t = g.t0; t < g.t1; t++) {
-            const uint32_t np = (tdesc[t].n + tc::BLOCK_M - 1) / tc::BLOCK_M * tc::BLOCK_M;
-            gtables[t] = tc::GemmTable{off, np, tdesc[t].base};
-            off += static_cast<uint64_t>(np) * np;
-            const uint32_t nb = np / tc::BLOCK_M, b0 = tdesc[t].base / tc::BLOCK_M;
-            for (uint32_t gk = 0; gk < nb; gk += 12)
-                for (uint32_t gl = 0; gl < nb; gl += 12)
-                    for (uint32_t kb = gk; kb < std::min(nb, gk + 12); kb++)
-                        for (uint32_t lb = gl; lb < std::min(nb, gl + 12); lb++)
-                            tiles.push_back(make_uint4(b0 + kb, b0 + lb, t, 0));
+            const uint32_t n = tdesc[t].n;
+            const uint32_t nkb = (n + tc::UMMA_M - 1) / tc::UMMA_M, nlb = (n + tc::COLS - 1) / tc::COLS;
+            for (uint32_t gk = 0; gk < nkb; gk += 8)
+                for (uint32_t gl = 0; gl < nlb; gl += 16)
+                    for (uint32_t kb = gk; kb < std::min(nkb, gk + 8); kb++)
+                        for (uint32_t lb = gl; lb < std::min(nlb, gl + 16); lb++)
+                            if (static_cast<uint64_t>(kb) * tc::UMMA_M <
+                                std::min<uint64_t>(n, static_cast<uint64_t>(lb + 1) * tc::COLS) - 1)
+                                tiles.push_back(make_uint4(kb, lb, t, 0));
         }
-        g_max = std::max(g_max, off);
         g.n_tiles = static_cast<uint32_t>(tiles.size());
-        SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * tiles.size()));
+        SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * std::max<size_t>(tiles.size(), 1)));
     }
-    SSU_CK(upload(&d_gtables, gtables.data(), sizeof(tc::GemmTable) * std::max<size_t>(gtables.size(), 1)));
 
     n_pad = static_cast<uint32_t>(ld);
     const size_t op_bytes = sizeof(__half) * static_cast<size_t>(n_pad) * k_pad;
@@ -1355,14 +1374,16 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     SSU_CK(alloc(&d_Bh, op_bytes));
     SSU_CK(alloc(&d_Bl, op_bytes));
     SSU_CK(alloc(&d_r, sizeof(double) * n_pad));
-    SSU_CK(alloc(&d_G, sizeof(double) * std::max<uint64_t>(g_max, 1)));
     SSU_CK(upload(&d_lhi, lhi.data(), sizeof(__half) * k_pad));
     SSU_CK(upload(&d_llo, llo.data(), sizeof(__half) * k_pad));
     SSU_CK(upload(&d_lsorted, lsorted.data(), sizeof(double) * k_pad));
     SSU_CK(upload(&d_chunk_scale, scale.data(), sizeof(double) * n_chunks));
+    SSU_CK(upload(&d_chunk_end, chunk_end.data(), sizeof(uint32_t) * n_chunks));
     SSU_CK(upload(&d_parent_col, parent_col.data(), sizeof(int32_t) * k_pad));
     SSU_CK(alloc(&d_error, sizeof(int)));
     SSU_CK(cudaMemsetAsync(d_error, 0, sizeof(int), stream));
+    if (const char *w = std::getenv("UNIFRAC_B200_WAIT_CYCLES")) gemm_wait_cycles = std::max(0LL, std::atoll(w));
+    union_stall = env_int("UNIFRAC_B200_TEST_STALL", 0) ? 1 : 0;
     if (!make_fp16_map(&map_A, d_A, n_pad, k_pad) || !make_fp16_map(&map_Bh, d_Bh, n_pad, k_pad) ||
         !make_fp16_map(&map_Bl, d_Bl, n_pad, k_pad)) {
         last_error = "cuTensorMapEncodeTiled failed";
@@ -1397,24 +1418,23 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
             tc::GemmArgs a{};
             a.tiles = g.d_tiles;
             a.n_tiles = g.n_tiles;
-            a.tables = d_gtables;
+            a.tables = d_tdesc;
             a.n_kblocks = k_pad / tc::BLOCK_K;
+            a.n_chunks = n_chunks;
+            a.chunk_end = d_chunk_end;
             a.chunk_scale = d_chunk_scale;
-            a.G = d_G;
+            a.r = d_r;
+            a.normalized = spec.method == Method::unweighted ? 1 : 0;
+            a.out_fp64 = spec.fp64 ? 1 : 0;
+            a.out = out;
             a.error = d_error;
-            a.wait_cycles = 2000000000LL;  // about one second per wait at B200 clocks
-            tc::unweighted_tc_kernel<<<g.n_tiles, tc::THREADS, tc::SMEM_BYTES, s>>>(map_A, map_Bh, map_Bl, a);
+            a.wait_cycles = gemm_wait_cycles;
+            a.stall = union_stall;
+            // two CTAs (one cluster) per work unit
+            tc::unweighted_tc_kernel<<<2 * g.n_tiles, tc::THREADS, tc::SMEM_BYTES, s>>>(map_A, map_Bh, map_Bl, a);
             launches++;
         }
         if (gi + 1 == groups.size() && timed()) SSU_CK(cudaEventRecord(ev[2], s));
-        const uint32_t nb = (max_table_n + 31) / 32;
-        if (nb) {
-            const dim3 grid(nb, nb, g.t1 - g.t0);
-            tc::finish_unweighted_kernel<<<grid, dim3(32, 8), 0, s>>>(
-                d_G, d_gtables + g.t0, d_tdesc + g.t0, d_r, spec.method == Method::unweighted ? 1 : 0,
-                spec.fp64 ? 1 : 0, out);
-            launches++;
-        }
     }
     if (out.mode == 0) zero_diagonal(s, out.ptr);
     if (timed()) SSU_CK(cudaEventRecord(ev[3], s));

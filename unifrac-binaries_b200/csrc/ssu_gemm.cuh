@@ -3,31 +3,42 @@
 // For presence X (samples x embedded nodes, 0/1) and branch lengths L:
 //   G[k][l] = sum_n X[k][n] L[n] (1 - X[l][n])  (length in k and not in l)
 //   r[k]    = sum_n X[k][n] L[n]                 (fp64)
-//   xor sum  num = G[k][l] + G[l][k]
-//   or  sum  den = r[k] + G[l][k]
-//   unweighted d = num / den, unnormalized d = num
+// and for a pair k < l
+//   or  sum  = r[l] + G[k][l]                    (l, plus what only k has)
+//   xor sum  = 2 G[k][l] + r[l] - r[k]           (= G[k][l] + G[l][k])
+//   unweighted d = xor / or, unnormalized d = xor
 // which are the xor / or sums of the reference's unweighted tasks
-// (src/unifrac_task_impl.hpp:1193-1278).  Every term is positive: unlike
-// r_k + r_l - 2 X L X^T, nothing cancels when two samples share most of
-// their length, so the relative error does not grow for close samples.
+// (src/unifrac_task_impl.hpp:1193-1278).  Only G[k][l] with k < l is
+// contracted: the upper triangle of tiles.  The subtraction in the xor sum
+// cannot lose relative accuracy to G's error: G[k][l] <= xor, so an error
+// e * G[k][l] in G is at most 2 e of the result; r is an fp64 sum of the
+// true lengths.
 //
 // Operands (fp16, K-major, built by `presence_rows_kernel`): A = X, and
-// B_hi / B_lo = (1 - X) * (L 2^s_c) split into two fp16 terms (hi = fp16(x),
-// lo = fp16(x - hi)), nodes sorted by decreasing length and scaled per
-// 256-node chunk c by a power of two 2^s_c.  Each chunk is accumulated in
-// fp32 in tensor memory (TMEM), then promoted to fp64 registers scaled back
-// by 2^-s_c.  The contraction covers every ordered tile (kb, lb) and stores G
-// in fp64; `finish_unweighted_kernel` forms num and den from G and its
-// transpose.
+// B_hi / B_lo = (1 - X) * (L 2^s_c) split into an integer part hi (at most
+// 2048, exact in fp16) and lo = fp16(L 2^s_c - hi).  Nodes are sorted by
+// decreasing length and packed into chunks of whole 64-node K blocks whose
+// lengths lie within a factor of two of the chunk's largest (zero-length
+// padding columns close a chunk); chunk c is scaled by 2^s_c so its lengths
+// fall in [512, 2048).  So every term keeps 22 significant bits, and a
+// chunk's hi sums are exact in the fp32 accumulator (at most 127 blocks x 64
+// nodes x 2048 < 2^24).  Each chunk is accumulated in tensor memory (TMEM),
+// then promoted to fp64 registers scaled back by 2^-s_c.
 //
-// CTA: one 128 x 128 tile of G.  Warp 0 issues TMA loads (A, B_hi,
-// B_lo: 128 rows x 64 nodes each, 128-byte swizzle) into a 4-stage ring;
-// warp 1 (one thread) issues tcgen05.mma (M=128, N=128, K=16, two per K-step:
-// hi and lo into the same accumulator) into one of two TMEM accumulators;
-// warps 2..9 drain a finished accumulator (tcgen05.ld) into fp64 while the
-// next chunk accumulates in the other.  Every mbarrier wait is bounded: on
-// expiry the CTA records an error code, stops issuing, waits (bounded) for its
-// own TMA copies and MMAs, frees its TMEM and returns.
+// Work unit: a cluster of two CTAs (cta_group::2) owns 256 rows k x 128
+// columns l of one table.  One MMA per 16 nodes is M = 256 (128 rows per
+// CTA) x N = 256: the first 128 columns of B are B_hi of the 128 columns l
+// (held by CTA 0), the last 128 are B_lo of the same columns (held by CTA 1),
+// so the hi and lo sums land in separate accumulators.  Per CTA: warp 0
+// issues its TMA loads (its 128 rows of A and its half of B, 64 nodes,
+// 128-byte swizzle, no multicast) into a 6-stage ring whose full barriers
+// live in CTA 0; in CTA 0 one thread of warp 1 issues the MMAs, into one of
+// two 256-column TMEM accumulators per CTA, and commits each stage's release
+// and each chunk's completion to both CTAs; warps 2..9 of both CTAs drain a
+// finished accumulator into fp64 registers while the next chunk accumulates,
+// and finally form the distances and write them.  Every mbarrier wait is
+// bounded: on expiry the CTA records an error code, stops issuing, lets its
+// copies and MMAs finish, frees TMEM and returns.
 #pragma once
 
 #include <cstdint>
@@ -40,49 +51,48 @@
 namespace ssu {
 namespace tc {
 
-constexpr int BLOCK_M = 128;
-constexpr int BLOCK_N = 128;
-constexpr int BLOCK_K = 64;  // fp16 nodes per stage row: one 128-byte swizzle atom
+constexpr int ROWS = 128;        // rows k per CTA (M = 256 per cluster)
+constexpr int COLS = 128;        // columns l per work unit
+constexpr int BLOCK_K = 64;      // fp16 nodes per stage row: one 128-byte swizzle atom
 constexpr int UMMA_K = 16;
-constexpr int STAGES = 4;
-constexpr int CHUNK_KB = 4;  // K blocks per fp64 promotion (256 nodes)
-constexpr int TMEM_COLS = 2 * BLOCK_N;
+constexpr int UMMA_M = 2 * ROWS;
+constexpr int UMMA_N = 2 * COLS; // hi and lo planes
+constexpr int STAGES = 6;
+constexpr int MAX_CHUNK_KB = 127;  // 127 x 64 x 2048 < 2^24: exact hi sums
+constexpr int ACC_COLS = UMMA_N;
+constexpr int TMEM_COLS = 2 * ACC_COLS;
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
-constexpr uint32_t TILE_BYTES = BLOCK_M * BLOCK_K * 2;
-constexpr uint32_t STAGE_BYTES = 3 * TILE_BYTES;
+constexpr uint32_t TILE_BYTES = ROWS * BLOCK_K * 2;
+constexpr uint32_t STAGE_BYTES = 2 * TILE_BYTES;  // A rows + one B plane, per CTA
 constexpr size_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+static_assert(TMEM_COLS <= 512, "two accumulators must fit the 512 TMEM columns");
+static_assert(SMEM_BYTES <= 227 * 1024, "stage ring exceeds shared memory");
+static_assert(static_cast<long long>(MAX_CHUNK_KB) * BLOCK_K * 2048 < (1LL << 24), "hi sums must stay exact");
 
 enum : int { ERR_NONE = 0, ERR_FULL_WAIT = 1, ERR_EMPTY_WAIT = 2, ERR_ACC_FULL_WAIT = 3, ERR_ACC_EMPTY_WAIT = 4,
              ERR_DONE_WAIT = 5, ERR_DRAIN_WAIT = 6 };
 
-// G block of one table: table t's rows are operand rows [base, base + ldg)
-// and its G is ldg x ldg (row major) at G + g_off.
-struct GemmTable {
-    uint64_t g_off;
-    uint32_t ldg;   // the table's samples rounded up to BLOCK_M
-    uint32_t base;  // first operand row of the table
-};
-
 struct GemmArgs {
-    const uint4 *tiles;   // x = row block of k, y = row block of l, z = table
+    const uint4 *tiles;         // x = 256-row block k, y = 128-column block l, z = table
     uint32_t n_tiles;
-    const GemmTable *tables;
-    uint32_t n_kblocks;   // padded nodes / BLOCK_K, a multiple of CHUNK_KB
+    const dev::TableDesc *tables;
+    uint32_t n_kblocks;         // padded nodes / BLOCK_K
+    uint32_t n_chunks;
+    const uint32_t *chunk_end;  // first K block after chunk c
     const double *chunk_scale;  // 2^-s_c per chunk
-    double *G;
-    int *error;           // first error code of any CTA
-    long long wait_cycles;  // budget of one mbarrier wait
+    const double *r;            // per operand row: fp64 sum of the present lengths
+    int normalized;
+    int out_fp64;
+    dev::OutSpec out;
+    int *error;                 // first error code of any CTA
+    long long wait_cycles;      // budget of one mbarrier wait
+    int stall;                  // test switch: no copy is issued, so every wait runs out
 };
 
-using dev::mbar_arrive;
 using dev::mbar_expect_tx;
 using dev::mbar_init;
-using dev::mbar_try_wait;
-using dev::mbar_wait;
 using dev::smem_u32;
-
-using dev::tma_load_2d;
 
 // K-major operand tile in shared memory with 128-byte swizzle: rows of 128
 // bytes, 8-row groups 1024 bytes apart (SBO), LBO unused (1), descriptor
@@ -97,22 +107,78 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     return d;
 }
 
-// Instruction descriptor, kind::f16: D f32, A and B f16, both K-major, M x N.
+// Instruction descriptor, kind::f16: D f32, A and B f16, both K-major, M x N
+// (M counts both CTAs of the pair).
 __host__ __device__ constexpr uint32_t f16_idesc(int m, int n) {
     return (1u << 4) | (0u << 7) | (0u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
            (static_cast<uint32_t>(m >> 4) << 24);
 }
 
-__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// shared::cluster address of the same shared-memory offset in CTA `rank`
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t saddr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+// Bounded wait on a barrier of this CTA that other CTAs of the cluster
+// arrive on (acquire at cluster scope).
+__device__ __forceinline__ bool mbar_try_wait_cl(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cl(uint64_t *bar, uint32_t parity, long long budget) {
+    const uint32_t a = smem_u32(bar);
+    if (mbar_try_wait_cl(a, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait_cl(a, parity))
+        if (clock64() - t0 > budget) return false;
+    return true;
+}
+// arrive on a barrier given by its shared::cluster address (any CTA of the cluster)
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cl_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cl_addr) : "memory");
+}
+// 2-D tiled TMA load into this CTA's shared memory completing on a barrier of
+// either CTA of the pair (given by its shared::cluster address); no multicast.
+__device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *map, uint32_t bar_cl, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+        "%4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(bar_cl), "r"(x), "r"(y)
+        : "memory");
+}
+__device__ __forceinline__ void umma_f16_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(
+            d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0));
 }
-__device__ __forceinline__ void umma_commit(uint64_t *bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
+// Arrive once on the barrier at this offset in both CTAs of the pair when
+// every MMA issued so far has completed.
+__device__ __forceinline__ void umma_commit_pair(uint64_t *bar) {
+    const uint16_t mask = 0x3;
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"(mask)
+        : "memory");
 }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -132,25 +198,27 @@ __device__ __forceinline__ void fail(int *shared_abort, int *global_err, int cod
     atomicCAS(global_err, ERR_NONE, code);
 }
 
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
     unweighted_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmBh,
                          const __grid_constant__ CUtensorMap tmBl, const GemmArgs args) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);  // used in CTA 0
     uint64_t *empty = full + STAGES;
     uint64_t *accf = empty + STAGES;
-    uint64_t *acce = accf + 2;
+    uint64_t *acce = accf + 2;  // used in CTA 0: released by the epilogues of both CTAs
     uint64_t *done = acce + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
     int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
+    const uint32_t rank = cluster_rank();
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const uint4 tile = args.tiles[blockIdx.x];
-    const int m0 = static_cast<int>(tile.x) * BLOCK_M, n0 = static_cast<int>(tile.y) * BLOCK_N;
-    const GemmTable gt = args.tables[tile.z];
-    const uint32_t nkb = args.n_kblocks;
-    const uint32_t nchunks = nkb / CHUNK_KB;
+    const uint4 tile = args.tiles[blockIdx.x >> 1];
+    const dev::TableDesc td = args.tables[tile.z];
+    const uint32_t k0 = tile.x * UMMA_M + rank * ROWS;  // this CTA's first row, table-local
+    const uint32_t l0 = tile.y * COLS;
+    const int arow = static_cast<int>(td.base + k0), brow = static_cast<int>(td.base + l0);
+    const uint32_t nkb = args.n_kblocks, nchunks = args.n_chunks;
     const long long budget = args.wait_cycles;
 
     if (threadIdx.x == 0) {
@@ -160,135 +228,168 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(accf + b, 1);
-            mbar_init(acce + b, EPI_WARPS);
+            mbar_init(acce + b, 2 * EPI_WARPS);
         }
         mbar_init(done, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(TMEM_COLS)
                      : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
     }
     __syncthreads();
+    // both CTAs' barriers are initialised before either signals the other
+    cluster_sync();
     tc_fence_after();
     const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(tmem_slot);
     volatile int *vabort = abort_flag;
+    const uint32_t full0 = map_to_rank(smem_u32(full), 0);
+    const uint32_t acce0 = map_to_rank(smem_u32(acce), 0);
+    // once any cluster of the launch has recorded an error, the others stop
+    // at once instead of each waiting out its budget
+    if (threadIdx.x == 0 && *reinterpret_cast<volatile int *>(args.error) != ERR_NONE) *abort_flag = 1;
+    __syncthreads();
+    bool ok = true;
+    uint32_t issued = 0;
 
     if (warp == 0) {
         if (lane == 0) {
-            // TMA producer
-            uint32_t issued = 0;
-            for (uint32_t kb = 0; kb < nkb; kb++) {
+            // TMA producer of this CTA; the pair's stage completes on CTA 0's barrier
+            const CUtensorMap *mb = rank == 0 ? &tmBh : &tmBl;
+            for (uint32_t kb = 0; kb < (args.stall ? 0u : nkb); kb++) {
                 const uint32_t s = kb % STAGES, use = kb / STAGES;
                 if (*vabort) break;
-                if (use > 0 && !mbar_wait(empty + s, (use - 1) & 1, budget)) {
+                if (use > 0 && !mbar_wait_cl(empty + s, (use - 1) & 1, budget)) {
                     fail(abort_flag, args.error, ERR_EMPTY_WAIT);
                     break;
                 }
                 uint8_t *st = smem + s * STAGE_BYTES;
-                mbar_expect_tx(full + s, STAGE_BYTES);
-                tma_load_2d(st, &tmA, full + s, static_cast<int>(kb) * BLOCK_K, m0);
-                tma_load_2d(st + TILE_BYTES, &tmBh, full + s, static_cast<int>(kb) * BLOCK_K, n0);
-                tma_load_2d(st + 2 * TILE_BYTES, &tmBl, full + s, static_cast<int>(kb) * BLOCK_K, n0);
+                if (rank == 0) mbar_expect_tx(full + s, 2 * STAGE_BYTES);
+                tma_load_2d_pair(st, &tmA, full0 + s * 8, static_cast<int>(kb) * BLOCK_K, arow);
+                tma_load_2d_pair(st + TILE_BYTES, mb, full0 + s * 8, static_cast<int>(kb) * BLOCK_K, brow);
                 issued = kb + 1;
-            }
-            // never leave with copies in flight: each stage's last load must land
-            for (uint32_t kb = issued > STAGES ? issued - STAGES : 0; kb < issued; kb++) {
-                if (!mbar_wait(full + kb % STAGES, (kb / STAGES) & 1, budget))
-                    fail(abort_flag, args.error, ERR_DRAIN_WAIT);
             }
         }
     } else if (warp == 1) {
-        if (lane == 0) {
-            // MMA issuer
-            constexpr uint32_t idesc = f16_idesc(BLOCK_M, BLOCK_N);
+        if (lane == 0 && rank == 0) {
+            // MMA issuer for the pair
+            constexpr uint32_t idesc = f16_idesc(UMMA_M, UMMA_N);
+            uint32_t kb = 0;
             for (uint32_t c = 0; c < nchunks && !*vabort; c++) {
                 const uint32_t buf = c & 1, reuse = c >> 1;
-                if (reuse > 0 && !mbar_wait(acce + buf, (reuse - 1) & 1, budget)) {
+                if (reuse > 0 && !mbar_wait_cl(acce + buf, (reuse - 1) & 1, budget)) {
                     fail(abort_flag, args.error, ERR_ACC_EMPTY_WAIT);
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d = tmem + buf * BLOCK_N;
-                bool ok = true;
-                for (uint32_t kk = 0; kk < CHUNK_KB; kk++) {
-                    const uint32_t kb = c * CHUNK_KB + kk;
+                const uint32_t d = tmem + buf * ACC_COLS;
+                const uint32_t kstart = kb, kend = args.chunk_end[c];
+                bool good = true;
+                for (; kb < kend; kb++) {
                     const uint32_t s = kb % STAGES, use = kb / STAGES;
-                    if (!mbar_wait(full + s, use & 1, budget)) {
+                    if (!mbar_wait_cl(full + s, use & 1, budget)) {
                         fail(abort_flag, args.error, ERR_FULL_WAIT);
-                        ok = false;
+                        good = false;
                         break;
                     }
                     tc_fence_after();
                     const uint32_t st = smem_u32(smem + s * STAGE_BYTES);
                     const uint64_t a0 = sw128_desc(st);
-                    const uint64_t h0 = sw128_desc(st + TILE_BYTES);
-                    const uint64_t l0 = sw128_desc(st + 2 * TILE_BYTES);
+                    const uint64_t b0 = sw128_desc(st + TILE_BYTES);
 #pragma unroll
                     for (int ks = 0; ks < BLOCK_K / UMMA_K; ks++) {
                         // advance 16 fp16 = 32 bytes along K inside the swizzle atom
                         const uint64_t koff = static_cast<uint64_t>((ks * UMMA_K * 2) >> 4);
-                        umma_f16(d, a0 + koff, h0 + koff, idesc, (kk | ks) != 0 ? 1u : 0u);
-                        umma_f16(d, a0 + koff, l0 + koff, idesc, 1u);
+                        umma_f16_pair(d, a0 + koff, b0 + koff, idesc, (kb != kstart || ks != 0) ? 1u : 0u);
                     }
-                    umma_commit(empty + s);
+                    umma_commit_pair(empty + s);
                 }
-                if (!ok) break;
-                umma_commit(accf + buf);
+                if (!good) break;
+                umma_commit_pair(accf + buf);
             }
-            umma_commit(done);
+            umma_commit_pair(done);
         }
     } else {
-        // epilogue: warp w reads TMEM lanes 32*(w%4).. and half (w-2)/4 of the columns
+        // epilogue: warp w reads TMEM lanes 32*(w%4).. and half (w-2)/4 of the
+        // 128 columns, each column's hi and lo sums
         const int q = warp & 3;
         const int half = (warp - 2) >> 2;
-        const int row = q * 32 + lane;
-        double acc[BLOCK_N / 2];
+        double acc[COLS / 2];
 #pragma unroll
-        for (int i = 0; i < BLOCK_N / 2; i++) acc[i] = 0.0;
-        bool ok = true;
+        for (int i = 0; i < COLS / 2; i++) acc[i] = 0.0;
         for (uint32_t c = 0; c < nchunks; c++) {
             const uint32_t buf = c & 1, use = c >> 1;
-            if (!mbar_wait(accf + buf, use & 1, budget)) {
+            if (*vabort || !mbar_wait_cl(accf + buf, use & 1, budget)) {
                 fail(abort_flag, args.error, ERR_ACC_FULL_WAIT);
                 ok = false;
                 break;
             }
             tc_fence_after();
             const double sc = args.chunk_scale[c];
-            const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16) + buf * BLOCK_N + half * (BLOCK_N / 2);
+            const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16) + buf * ACC_COLS + half * (COLS / 2);
 #pragma unroll
-            for (int j = 0; j < BLOCK_N / 2 / 16; j++) {
-                uint32_t v[16];
-                tmem_ld16(base + j * 16, v);
+            for (int j = 0; j < COLS / 2 / 16; j++) {
+                uint32_t hv[16], lv[16];
+                tmem_ld16(base + j * 16, hv);
+                tmem_ld16(base + COLS + j * 16, lv);
                 tmem_wait_ld();
 #pragma unroll
                 for (int i = 0; i < 16; i++)
-                    acc[j * 16 + i] = fma(static_cast<double>(__uint_as_float(v[i])), sc, acc[j * 16 + i]);
+                    acc[j * 16 + i] = fma(static_cast<double>(__uint_as_float(hv[i])) +
+                                              static_cast<double>(__uint_as_float(lv[i])),
+                                          sc, acc[j * 16 + i]);
             }
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(acce + buf);
+            if (lane == 0) mbar_arrive_cluster(acce0 + buf * 8);
         }
-        if (ok && !*vabort) {
-            double *g = args.G + gt.g_off + static_cast<uint64_t>(m0 - gt.base + row) * gt.ldg + (n0 - gt.base) +
-                        half * (BLOCK_N / 2);
+        const uint32_t n = td.n;
+        const uint32_t k = k0 + q * 32 + lane;
+        if (ok && !*vabort && k < n) {
+            dev::OutSpec o = args.out;
+            if (o.mode == 0)
+                o.ptr = static_cast<char *>(o.ptr) + td.out_off * (args.out_fp64 ? sizeof(double) : sizeof(float));
+            const double *rt = args.r + td.base;
+            const double rk = rt[k];
+            const uint32_t lb = l0 + half * (COLS / 2);
+            // fully unrolled: acc stays in registers
 #pragma unroll
-            for (int i = 0; i < BLOCK_N / 2; i += 2)
-                *reinterpret_cast<double2 *>(g + i) = make_double2(acc[i], acc[i + 1]);
+            for (int j = 0; j < COLS / 2; j++) {
+                const uint32_t l = lb + j;
+                if (k < l && l < n) {
+                    const double rl = rt[l];
+                    const double g = acc[j];
+                    const double x = 2.0 * g + (rl - rk);
+                    const double v = args.normalized ? x / (rl + g) : x;
+                    if (o.mode == 0 && !args.out_fp64)
+                        dev::emit_pair<float>(o, n, k, l, static_cast<float>(v));
+                    else
+                        dev::emit_pair<double>(o, n, k, l, v);
+                }
+            }
         }
     }
     __syncthreads();
     if (warp == 1) {
-        // every MMA this CTA issued has completed before its TMEM is freed
-        if (!mbar_wait(done, 0, budget)) fail(abort_flag, args.error, ERR_DONE_WAIT);
-        tc_fence_after();
+        // every MMA that writes this CTA's TMEM or reads its shared memory has completed
+        if (lane == 0 && !mbar_wait_cl(done, 0, budget)) fail(abort_flag, args.error, ERR_DONE_WAIT);
         __syncwarp();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        tc_fence_after();
     }
+    if (threadIdx.x == 0 && *vabort && issued > 0) {
+        // after an expired wait, give copies still in flight into this CTA's
+        // shared memory time to land (about 20 ms at B200 clocks) before it is released
+        const long long t0 = clock64();
+        while (clock64() - t0 < budget / 100) __nanosleep(1000);
+    }
+    __syncthreads();
+    // neither CTA frees TMEM or leaves while the other may still signal it
+    cluster_sync();
+    if (warp == 1)
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
 // Presence rows for the contraction, one CTA per sample (padding rows too):
@@ -342,43 +443,6 @@ __global__ void presence_rows_kernel(const uint32_t *__restrict__ sample_ptr, co
         double s = 0.0;
         for (int t = 0; t < 256; t++) s += red[t];
         r[j] = s;
-    }
-}
-
-// num = G[k][l] + G[l][k], den = r[k] + G[l][k] for k < l, then the output
-// layout of the other pair kernels; grid.z = table of the group.
-__global__ void finish_unweighted_kernel(const double *__restrict__ G, const GemmTable *__restrict__ gtables,
-                                         const dev::TableDesc *__restrict__ tables, const double *__restrict__ r,
-                                         int normalized, int out_fp64, dev::OutSpec out) {
-    // 32 x 32 block of pairs per CTA; both G tiles through shared memory
-    __shared__ double gt[32][33];
-    const GemmTable g = gtables[blockIdx.z];
-    const dev::TableDesc td = tables[blockIdx.z];
-    const uint32_t n = td.n;
-    const uint32_t k0 = blockIdx.y * 32, l0 = blockIdx.x * 32;
-    if (k0 > l0 + 31 || k0 >= n || l0 >= n) return;
-    const double *Gt = G + g.g_off;
-    const uint32_t ldg = g.ldg;
-    const double *rt = r + g.base;
-    if (out.mode == 0) out.ptr = static_cast<char *>(out.ptr) + td.out_off * (out_fp64 ? sizeof(double) : sizeof(float));
-    const uint32_t tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-    for (uint32_t i = ty; i < 32; i += 8) {
-        const uint32_t l = l0 + i, k = k0 + tx;
-        gt[i][tx] = (l < n && k < n) ? Gt[static_cast<uint64_t>(l) * ldg + k] : 0.0;  // G[l][k]
-    }
-    __syncthreads();
-    for (uint32_t i = ty; i < 32; i += 8) {
-        const uint32_t k = k0 + i, l = l0 + tx;
-        if (k < l && l < n) {
-            const double gkl = Gt[static_cast<uint64_t>(k) * ldg + l];
-            const double glk = gt[tx][i];
-            const double num = gkl + glk;
-            const double v = normalized ? num / (rt[k] + glk) : num;
-            if (out.mode == 0 && !out_fp64)
-                dev::emit_pair<float>(out, n, k, l, static_cast<float>(v));
-            else
-                dev::emit_pair<double>(out, n, k, l, v);
-        }
     }
 }
 

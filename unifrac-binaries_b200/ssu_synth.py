@@ -32,6 +32,10 @@ class BPTree:
         s = self.structure
         return [self.names[i] for i in range(len(s) - 1) if s[i] and not s[i + 1]]
 
+    def tip_lengths(self):
+        s = self.structure
+        return [float(self.lengths[i]) for i in range(len(s) - 1) if s[i] and not s[i + 1]]
+
 
 @dataclass
 class Table:
@@ -53,6 +57,17 @@ class Table:
     @property
     def nnz(self) -> int:
         return int(self.indptr[-1])
+
+    @classmethod
+    def from_dense(cls, dense, obs_ids, sample_ids) -> "Table":
+        """Observation-major CSR of a dense features x samples array (non-zero
+        entries kept)."""
+        dense = np.asarray(dense, dtype=np.float64)
+        rows, cols = np.nonzero(dense)
+        indptr = np.zeros(dense.shape[0] + 1, dtype=np.uint32)
+        np.add.at(indptr, rows + 1, 1)
+        return cls(list(obs_ids), list(sample_ids), np.cumsum(indptr).astype(np.uint32),
+                   cols.astype(np.uint32), dense[rows, cols].copy())
 
     def dense(self) -> np.ndarray:
         out = np.zeros((self.n_obs, self.n_samples), dtype=np.float64)
