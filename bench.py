@@ -1,19 +1,26 @@
 """Benchmark: pair-branch updates/s of the B200 Strided State UniFrac engine.
 
-Workload (one step): the full 2,048 x 2,048 weighted-normalized UniFrac matrix
-in fp64 of the 20,000-tip / 20,000-feature x 2,048-sample synthetic table
-(1% non-zero, counts round(LogNormal(2, 1.5)) + 1, branch lengths
-Exponential(mean 0.05), seed 2): proportion embedding, pair kernel and the
-matrix written to HBM.  Units: U = n(n-1)/2 x E pair-branch updates, E the
+Default line (one step): the full 25,000 x 25,000 unweighted UniFrac matrix
+(fp64 ratios) of a 25,000-sample presence table on a 100,000-tip random
+binary tree (branch lengths Exponential(mean 0.02), per-sample richness
+log-uniform in [50, 2000] distinct tips, seed 3), computed as a tcgen05
+tensor-core contraction: presence rows, the contraction with the distances
+formed in its epilogue, the matrix written to HBM.  The same plan on the
+plain stripe (presence-word) form is timed beside it, and the two are
+compared pair by pair.  Units: U = n(n-1)/2 x E pair-branch updates, E the
 embedded branches of the sheared tree.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--workload NAME]
 
 value: U*K / (sum of per-step device times), inputs resident in HBM, L2
 flushed between steps, max over ranks.  e2e: the same metric through the C
-API (one_off_matrix_inmem_v3) from host buffers, host<->device copies and the
-host-side tree work inside the timed region.  Under torchrun each rank runs
-its own table (seed + rank): weak scaling, no data-path collective.
+API (one_off_matrix_inmem_v3, unweighted_fp64 with
+UNIFRAC_B200_UNWEIGHTED_MODE=gemm) from host buffers: host tree and table
+work, upload, compute and the 5 GB copy-out inside the timed region.  Under
+torchrun each rank runs its own table (seed + rank): weak scaling, no
+data-path collective.  --impl reference times the reference's own CPU build
+(oracle/_ref) on a stripe window of the same workload.
 """
 import argparse
 import json
@@ -28,23 +35,26 @@ sys.path.insert(0, os.path.join(ROOT, "unifrac-binaries_b200"))
 
 METRIC = "pair-branch updates/s"
 UNIT = "updates/s"
-WORKLOAD = "weighted_normalized_fp64 UniFrac, 20k-tip tree, 20k features x 2048 samples, full matrix"
+PRESENCE_WORKLOAD = ("unweighted_fp64 UniFrac, 100,000-tip tree (Exponential(0.02) lengths), 25,000 presence "
+                     "samples (log-uniform richness 50-2,000), full 25,000 x 25,000 matrix")
+WEIGHTED_WORKLOAD = "weighted_normalized_fp64 UniFrac, 20k-tip tree, 20k features x 2048 samples, full matrix"
 METHOD = "weighted_normalized_fp64"
 # --workload choices: each names the data it runs
 WORKLOADS = {
-    "20k-tips-2048-samples": "weighted_normalized_fp64, 20,000-tip tree, 20,000 x 2,048 table (the default line)",
-    "1k-tips-128-samples": "unweighted + weighted_normalized fp64, 1,000-tip tree, 1,000 x 128 table, condensed form",
     "100k-tips-25k-presence": "unweighted fp64, 100,000-tip tree, 25,000 presence samples: tensor-core contraction "
-                              "vs the plain stripe form",
+                              "vs the plain stripe form (the default line)",
+    "20k-tips-2048-samples": "weighted_normalized_fp64, 20,000-tip tree, 20,000 x 2,048 table",
+    "1k-tips-128-samples": "unweighted + weighted_normalized fp64, 1,000-tip tree, 1,000 x 128 table, condensed form",
     "100-replicates-5k-samples": "unweighted + weighted_normalized fp32, 100 rarefied replicates of a 10,000 x 5,000 "
                                  "table, 10,000-tip tree",
     "64-uneven-tables": "generalized + four VAW methods fp64, 64 tables of 64-4,096 samples, 50,000-tip tree",
 }
-# reference-form algorithmic bytes per pair-branch update of this method
-# (accumulator read-modify-write of two fp64 stripes per 112-node batch:
-# 2 * 2 * 8 / 112)
+# reference-form algorithmic bytes per pair-branch update of the weighted
+# normalized fp64 method (accumulator read-modify-write of two fp64 stripes
+# per 112-node batch: 2 * 2 * 8 / 112)
 ALGO_BYTES_PER_UPDATE = 2 * 2 * 8 / 112.0
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "pair_hybrid_weighted_normalized_fp64_20k_tips_2048_samples.md")
+PROFILE_TC = os.path.join(ROOT, "profiles", "unweighted_tc_kernel_100k_tips_25k_presence.md")
 
 
 def parse():
@@ -56,15 +66,18 @@ def parse():
     p.add_argument("--samples", type=int, default=2048)
     p.add_argument("--tips", type=int, default=20000)
     p.add_argument("--method", default=METHOD)
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--replicates", type=int, default=100)
     p.add_argument("--uneven-tables", type=int, default=64)
     p.add_argument("--uneven-tips", type=int, default=50000)
-    p.add_argument("--workload", default="20k-tips-2048-samples", choices=list(WORKLOADS),
+    p.add_argument("--workload", default="100k-tips-25k-presence", choices=list(WORKLOADS),
                    help="; ".join(f"{k}: {v}" for k, v in WORKLOADS.items()))
     p.add_argument("--presence-samples", type=int, default=25000)
     p.add_argument("--presence-tips", type=int, default=100000)
+    p.add_argument("--no-secondary", action="store_true", help="skip the weighted (20k-tips-2048-samples) keys "
+                   "of the default line")
+    p.add_argument("--no-stripe-form", action="store_true", help="skip the stripe-form comparison of the default line")
     return p.parse_args()
 
 
@@ -219,31 +232,53 @@ class ClockSampler:
         return rows
 
 
-def read_traffic():
-    """dram bytes per pair-kernel launch from the committed ncu summary."""
+def read_profile_value(path, key):
+    """A `key: value ...` figure from a committed ncu summary (first token)."""
     try:
-        for line in open(PROFILE_TRAFFIC):
-            if line.startswith("dram_bytes_per_launch_full_size:"):
+        for line in open(path):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1].split()[0])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+def read_traffic():
+    """dram bytes per hybrid pair-kernel launch from the committed ncu summary."""
+    return read_profile_value(PROFILE_TRAFFIC, "dram_bytes_per_launch_full_size")
+
+
+def peaks():
+    """Measured peaks of this pool's B200s (MEASURED_PEAKS.json), else the
+    fallback figures: (HBM GB/s, bf16 TFLOP/s burst, sustained, kind)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), float(d.get("bf16_tflops_sustained", 1400.0)), "measured"
+    except Exception:
+        return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
     except OSError:
         pass
     return None
 
 
-def peaks():
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
-    except Exception:
-        return 6650.0, "fallback"
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    return oracle_py
 
 
 def cpu_baseline(tree, table, method, target_s=8.0):
     """The reference's own CPU path (oracle/_ref) on a stripe sub-range of the
     same workload, all host threads; grown until it runs ~target_s."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_py
+    oracle_py = _oracle()
     n = table.n_samples
     s_total = (n + 1) // 2
     kind = "reference"
@@ -253,9 +288,9 @@ def cpu_baseline(tree, table, method, target_s=8.0):
     while True:
         stop = min(s_total, stripes)
         if kind == "reference":
-            r = oracle_py.ref_one_off(tree, table, method, stripe_start=0, stripe_stop=stop, want_matrix=False,
-                                      with_timing=True)
-            secs = r["seconds"][0]
+            r = oracle_py.ref_one_off(tree, table, method, stripe_start=0, stripe_stop=stop,
+                                      want_matrix=(stop == s_total), with_timing=True)
+            secs = r["seconds"][0] + r["seconds"][1]
             e = r["n_embedded"]
         else:
             t0 = time.perf_counter()
@@ -266,15 +301,85 @@ def cpu_baseline(tree, table, method, target_s=8.0):
             break
         stripes = int(stripes * max(2.0, min(8.0, target_s / max(secs, 1e-3))))
     units = stop * n * e
-    cores = os.cpu_count()
-    return {"value": units / secs, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", cores)),
-            "kind": kind, "sample": f"stripes [0,{stop}) of {s_total} ({stop * n} pairs x {e} branches), "
-                                    f"{secs:.2f} s, process_stripes only"}
+    what = ("all stripes, process_stripes + stripes_to_matrix_T" if stop == s_total else
+            f"stripes [0,{stop}) of {s_total}, process_stripes")
+    return {"value": units / secs, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())),
+            "cpu_model": cpu_model(), "kind": kind,
+            "sample": f"{what} ({stop * n} pairs x {e} branches), {secs:.2f} s"}
+
+
+def presence_reference_sample(tree, table, method="unweighted_fp64", target_s=6.0, fixed_s=None):
+    """The reference's CPU build (oracle/_ref, all host threads) on a stripe
+    window [0, S) of the presence workload.  Each call embeds every node
+    for every sample before its stripes (~2 s here whatever S), so the rate
+    is the marginal one: (S x n x E) / (t(S) - t(1)), t(1) the time of a
+    one-stripe window - the reference's best case, extrapolated linearly to
+    all stripes.  Returns (rate, sample dict, fixed seconds)."""
+    oracle_py = _oracle()
+    kind = "reference" if oracle_py.ref_available() else "port"
+
+    def run(a, b):
+        if kind == "reference":
+            return oracle_py.ref_one_off(tree, table, method, stripe_start=a, stripe_stop=b, want_matrix=False,
+                                         with_timing=True)["seconds"][0]
+        t0 = time.perf_counter()
+        oracle_py.oracle_one_off(tree, table, method, stripe_start=a, stripe_stop=b)
+        return time.perf_counter() - t0
+
+    n = table.n_samples
+    s_total = (n + 1) // 2
+    if fixed_s is None:
+        fixed_s = run(0, 1)
+    stripes = 16
+    while True:
+        secs = run(0, stripes)
+        if secs - fixed_s >= target_s / 2 or stripes >= s_total:
+            break
+        stripes = min(s_total, int(stripes * max(2.0, min(8.0, target_s / max(secs - fixed_s, 1e-3)))))
+    e = (oracle_py.ref_one_off if kind == "reference" else oracle_py.oracle_one_off)(
+        tree, table, method, stripe_start=0, stripe_stop=1)["n_embedded"]
+    marginal = max(secs - fixed_s, 1e-9)
+    rate = stripes * n * e / marginal
+    full_s = fixed_s + marginal * s_total / stripes
+    sample = {"kind": kind, "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())), "cpu_model": cpu_model(),
+              "sample": f"stripes [0,{stripes}) of {s_total} ({stripes * n} pairs x {e} branches): {secs:.2f} s, of "
+                        f"which {fixed_s:.2f} s is the per-call embedding (timed on a one-stripe window); rate = "
+                        f"marginal stripes / (t - t_embed), full matrix extrapolated to {full_s:.0f} s "
+                        f"(process_stripes only)"}
+    return rate, sample, fixed_s
 
 
 def run_reference(args):
+    """--impl reference: the reference's own CPU build on the box's host
+    cores, same workload string, metric and unit as this arm's line."""
     world, rank, _ = dist_init()
     if rank != 0:
+        return
+    if args.workload == "100k-tips-25k-presence":
+        import ssu_synth
+        tree, table = ssu_synth.presence_100k_tips_25k_samples(seed=3, n_samples=args.presence_samples,
+                                                               n_tips=args.presence_tips)
+        fixed = None
+        fixed_runs, rates = [], []
+        sample = None
+        for i in range(args.warmup + args.steps):
+            rate, sample, f = presence_reference_sample(tree, table, fixed_s=None if i < max(args.warmup, 1) else
+                                                        statistics.median(fixed_runs))
+            if i < max(args.warmup, 1):
+                fixed_runs.append(f)
+            if i >= args.warmup:
+                rates.append(rate)
+        value = statistics.median(rates)
+        cb = dict(sample)
+        cb.update({"value": value, "unit": UNIT})
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generator presence_100k_tips_25k_samples)",
+                "config": {"workload": PRESENCE_WORKLOAD, "method": "unweighted_fp64"},
+                "impl": "reference", "cpu_baseline": cb,
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
         return
     tree, table = make_workload(2, args)
     samples = []
@@ -288,7 +393,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator lognormal_20k_tips_2048_samples)",
-            "config": {"workload": WORKLOAD + " (CPU: stripe sub-range sample)", "method": args.method,
+            "config": {"workload": WEIGHTED_WORKLOAD, "method": args.method,
                        "n_samples": args.samples, "n_tips": args.tips},
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -307,12 +412,11 @@ def _device_copy(torch, src_ptr, n, dtype):
     return out
 
 
-def _timed_steps(torch, plan, stream, steps, warmup, flush):
-    for _ in range(warmup):
-        plan.execute(stream.cuda_stream)
-    torch.cuda.synchronize()
+def _step_loop(torch, plan, stream, steps, barrier, flush):
+    """K timed executes: per-step CUDA-event time on the plan's stream (L2
+    flushed before each, outside the events) and the pair stage's time."""
     plan.set_timing(True)
-    total, kern = 0.0, 0.0
+    step_ms, pair_ms = [], []
     for _ in range(steps):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -320,81 +424,178 @@ def _timed_steps(torch, plan, stream, steps, warmup, flush):
         plan.execute(stream.cuda_stream)
         e1.record(stream)
         e1.synchronize()
-        total += e0.elapsed_time(e1)
-        kern += plan.stage_ms()[1]
-    return total / steps, kern / steps
+        step_ms.append(e0.elapsed_time(e1))
+        pair_ms.append(plan.stage_ms()[1])
+    barrier()
+    plan.set_timing(False)
+    return step_ms, pair_ms
+
+
+def tc_work_units(n):
+    """Work units of the tensor-core kernel for one table of n samples: the
+    (256-row, 128-column) blocks holding a pair k < l."""
+    nkb, nlb = (n + 255) // 256, (n + 127) // 128
+    return sum(1 for kb in range(nkb) for lb in range(nlb) if kb * 256 < min(n, (lb + 1) * 128) - 1)
 
 
 def run_presence(args):
-    """Unweighted fp64 on the 100,000-tip / 25,000-sample presence table:
-    the tcgen05 contraction against the plain stripe (presence-word) form."""
+    """The default line: unweighted fp64 on the 100,000-tip / 25,000-sample
+    presence table through the tcgen05 contraction, with the plain stripe
+    (presence-word) form timed beside it on the same plan inputs."""
     import torch
+    import torch.distributed as dist
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     import ssu_b200
     import ssu_synth
-    torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    tree, table = ssu_synth.presence_100k_tips_25k_samples(seed=3, n_samples=args.presence_samples, n_tips=args.presence_tips)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # the 5 GB result comes back into page-locked memory recycled between calls
+    os.environ.setdefault("UNIFRAC_B200_PINNED_BYTES", str(8 << 30))
+    t0 = time.perf_counter()
+    tree, table = ssu_synth.presence_100k_tips_25k_samples(seed=3 + rank, n_samples=args.presence_samples,
+                                                           n_tips=args.presence_tips)
+    gen_s = time.perf_counter() - t0
     method = "unweighted_fp64"
     os.environ["UNIFRAC_B200_UNWEIGHTED_MODE"] = "gemm"
     gp = ssu_b200.Plan(tree, table, method)
-    assert gp.pair_kernel() == "unweighted_tc_kernel"
+    assert gp.pair_kernel() == "unweighted_tc_kernel", gp.pair_kernel()
     units = gp.work_units()
-    clocks = ClockSampler(0)
-    clocks.start()
-    g_step, g_kern = _timed_steps(torch, gp, stream, args.steps, args.warmup, flush)
-    clk = clocks.stop()
+    flops_issued = gp.tensor_flops()
     n = table.n_samples
-    g_res = _device_copy(torch, gp.device_result(), n, torch.float64)
-    g_launches = gp.launches()
-    gp.close()
-    os.environ["UNIFRAC_B200_UNWEIGHTED_MODE"] = "stripe"
-    sp = ssu_b200.Plan(tree, table, method)
-    s_step, s_kern = _timed_steps(torch, sp, stream, 1, 1, flush)
-    s_res = _device_copy(torch, sp.device_result(), n, torch.float64)
-    s_name = sp.pair_kernel()
-    sp.close()
-    # relative error of every pair k < l, in row blocks
-    worst, errs = 0.0, []
-    iu = None
-    for r0 in range(0, n, 2048):
-        a = g_res[r0:r0 + 2048]
-        b = s_res[r0:r0 + 2048]
-        rows = torch.arange(r0, min(n, r0 + 2048), device="cuda").unsqueeze(1)
-        cols = torch.arange(n, device="cuda").unsqueeze(0)
-        mask = (cols > rows) & (b != 0)
-        rel = ((a - b).abs() / b.abs())[mask]
-        if rel.numel():
-            worst = max(worst, rel.max().item())
-            errs.append(torch.quantile(rel[torch.randint(0, rel.numel(), (200000,), device="cuda")], 0.999).item())
-    peak_tf = None
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peak_tf = float(json.load(f)["bf16_tflops"])
-    except Exception:
-        peak_tf = 1590.0
-    algo_flops = 2.0 * units
-    achieved = algo_flops / (g_kern / 1e3) / 1e12
-    line = {
-        "metric": METRIC, "value": units / (g_step / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": g_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f16 operands, f32 accumulate per 256 nodes, f64 across chunks and ratio",
-        "data": "synthetic (seeded generator presence_100k_tips_25k_samples)",
-        "config": {"workload": f"unweighted_fp64 UniFrac, {args.presence_tips}-tip tree, {n} samples (presence, "
-                               f"log-uniform richness 50-2000), full matrix", "embedded_branches": gp_units_e(units, n),
-                   "tc_kernel_ms": g_kern, "launches_per_step": g_launches},
-        "stripe_form": {"kernel": s_name, "ms_per_step": s_step, "kernel_ms": s_kern,
-                        "value": units / (s_step / 1e3)},
-        "speedup_tc_vs_stripe": s_step / g_step,
-        "rel_err_vs_fp64_stripe": {"max": worst, "p99.9": max(errs) if errs else None, "pairs": n * (n - 1) // 2},
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
-                     "frac": achieved / peak_tf, "traffic": None,
-                     "note": "algorithmic flops = 2 x pair-branch updates; the kernel issues 4x that "
-                             "(hi + lo terms, both orientations of the cancellation-free form)"},
-        "clocks": clk,
-    }
-    print(json.dumps(line), flush=True)
+    for _ in range(args.warmup):
+        gp.execute(stream.cuda_stream)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    step_ms, tc_ms = _step_loop(torch, gp, stream, args.steps, barrier, flush)
+    clk = clocks.stop()
+    launches_per_step = gp.launches()
+    total_ms, _, all_units, mean_tc_ms = combine_ranks([sum(step_ms), 0.0, float(units), sum(tc_ms) / len(tc_ms)],
+                                                       world, "cuda")
+
+    extra = {}
+    if world == 1 and not args.no_stripe_form:
+        # the plain stripe form on the same inputs, and every pair compared
+        g_res = _device_copy(torch, gp.device_result(), n, torch.float64)
+        gp.close()
+        gp = None
+        os.environ["UNIFRAC_B200_UNWEIGHTED_MODE"] = "stripe"
+        sp = ssu_b200.Plan(tree, table, method)
+        sp.execute(stream.cuda_stream)
+        torch.cuda.synchronize()
+        s_step, s_pair = _step_loop(torch, sp, stream, 1, barrier, flush)
+        s_res = _device_copy(torch, sp.device_result(), n, torch.float64)
+        s_name = sp.pair_kernel()
+        sp.close()
+        worst, q999 = 0.0, []
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(0)
+        for r0 in range(0, n, 2048):
+            a = g_res[r0:r0 + 2048]
+            b = s_res[r0:r0 + 2048]
+            rows = torch.arange(r0, min(n, r0 + 2048), device="cuda").unsqueeze(1)
+            cols = torch.arange(n, device="cuda").unsqueeze(0)
+            mask = (cols > rows) & (b != 0)
+            rel = ((a - b).abs() / b.abs())[mask]
+            if rel.numel():
+                worst = max(worst, rel.max().item())
+                pick = torch.randint(0, rel.numel(), (200000,), device="cuda", generator=gen)
+                q999.append(torch.quantile(rel[pick], 0.999).item())
+        del g_res, s_res
+        extra["stripe_form"] = {"kernel": s_name, "ms_per_step": s_step[0], "kernel_ms": s_pair[0],
+                                "value": units / (s_step[0] / 1e3)}
+        extra["tc_vs_stripe"] = s_step[0] / (sum(step_ms) / len(step_ms))
+        extra["rel_err_vs_fp64_stripe"] = {"max": worst, "p99.9": max(q999) if q999 else None,
+                                           "pairs": n * (n - 1) // 2,
+                                           "bar": 1e-6}
+    if gp is not None:
+        gp.close()
+
+    # end to end through the C API: host buffers in, the host matrix out
+    os.environ["UNIFRAC_B200_UNWEIGHTED_MODE"] = "gemm"
+    e2e_ms = []
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
+        barrier()
+        t0 = time.perf_counter()
+        m, _ = ssu_b200.one_off_matrix(tree, table, method, copy=False)
+        dt = (time.perf_counter() - t0) * 1e3
+        del m  # the caller is done with the result: destroy_mat_full_fp64
+        if i > 0:
+            e2e_ms.append(dt)
+    h2d = int(table.indptr.nbytes + table.indices.nbytes + table.data.nbytes + tree.structure.nbytes +
+              tree.lengths.nbytes)
+    d2h = n * n * 8
+    _, e2e_total, _, _ = combine_ranks([0.0, sum(e2e_ms), 0.0, 0.0], world, "cuda")
+
+    if rank == 0:
+        value = all_units * args.steps / (total_ms / 1e3)
+        _, peak_burst, peak_sus, peak_kind = peaks()
+        algo_flops = 2.0 * units
+        achieved = algo_flops / (mean_tc_ms / 1e3) / 1e12
+        issued = flops_issued / (mean_tc_ms / 1e3) / 1e12
+        traffic_per_unit = read_profile_value(PROFILE_TC, "dram_bytes_per_work_unit")
+        n_units = tc_work_units(n)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f16 operands (0/1 presence; integer hi + fp16 lo lengths), f32 accumulate per chunk, f64 "
+                     "across chunks and ratios",
+            "data": "synthetic (seeded generator presence_100k_tips_25k_samples)",
+            "config": {"workload": PRESENCE_WORKLOAD, "method": method, "pair_kernel": "unweighted_tc_kernel",
+                       "n_samples": n, "embedded_branches": gp_units_e(units, n), "per_gpu_units": units,
+                       "l2": "flushed between steps (256 MiB write outside the step events); operands 30 GB > L2",
+                       "generation_s": gen_s},
+            "tc_kernel_ms": mean_tc_ms,
+            **extra,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak_sus, "unit": "TFLOP/s",
+                         "frac": achieved / peak_sus, "traffic": traffic_per_unit * n_units if traffic_per_unit else None,
+                         "peak_kind": f"{peak_kind} bf16 sustained (the kernel runs ~0.2 s per launch, back to back)",
+                         "frac_of_burst": achieved / peak_burst,
+                         "algorithmic_flops_per_launch": algo_flops, "issued_flops_per_launch": flops_issued,
+                         "issued_tflops": issued, "issued_frac": issued / peak_sus,
+                         "note": "algorithmic flops = 2 x pair-branch updates (one multiply-add per pair and "
+                                 "branch); the kernel issues ~2x that: hi and lo length planes, padding of the "
+                                 "length chunks and of 256 x 128 work units on the diagonal; traffic = ncu DRAM "
+                                 "bytes per work unit x work units"},
+            "e2e": {"value": all_units * len(e2e_ms) / (e2e_total / 1e3) if e2e_ms else None, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_total / len(e2e_ms) if e2e_ms else None,
+                    "path": "one_off_matrix_inmem_v3 (unweighted_fp64, UNIFRAC_B200_UNWEIGHTED_MODE=gemm), host CSR "
+                            "and tree arrays in, 25,000 x 25,000 fp64 matrix out (UNIFRAC_B200_PINNED_BYTES="
+                            + os.environ.get("UNIFRAC_B200_PINNED_BYTES", "") + ")"},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                rate, sample, _ = presence_reference_sample(tree, table, target_s=8.0)
+                line["cpu_baseline"] = dict(sample, value=rate, unit=UNIT)
+            except Exception as exc:  # the reported baseline never blocks the bench line
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
+        if world == 1 and not args.no_secondary:
+            try:
+                w = measure_weighted(args, 1, 0, local, stream=stream, flush=flush, cpu=not args.no_cpu_baseline)
+                line["secondary_weighted_20k_tips_2048_samples"] = {
+                    k: w.get(k) for k in ("value", "ms_per_step", "pair_kernel_ms", "e2e", "roofline",
+                                          "cpu_baseline", "config", "gpu_launches")}
+            except Exception as exc:
+                line["secondary_weighted_20k_tips_2048_samples"] = {"error": str(exc)[:300]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def _time_batch(torch, plan, stream, steps, warmup, flush):
@@ -647,36 +848,20 @@ def gp_units_e(units, n):
     return int(units // (n * (n - 1) // 2)) if n > 1 else 0
 
 
-def main():
-    args = parse()
-    if args.impl == "reference":
-        return run_reference(args)
-    if args.workload == "1k-tips-128-samples":
-        return run_small(args)
-    if args.workload == "100k-tips-25k-presence":
-        return run_presence(args)
-    if args.workload == "100-replicates-5k-samples":
-        return run_replicates(args)
-    if args.workload == "64-uneven-tables":
-        return run_uneven_tables(args)
+def measure_weighted(args, world, rank, local, stream=None, flush=None, cpu=True):
+    """Weighted normalized fp64 on the 20,000-tip / 2,048-sample table: the
+    line's dict (rank 0) with an HBM roofline in reference-form bytes."""
     import torch
     import torch.distributed as dist
-    world, rank, local = dist_init()
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     import ssu_b200
-    import numpy as np
-
     tree, table = make_workload(2 + rank, args)
     plan = ssu_b200.Plan(tree, table, args.method)
     units = plan.work_units()
-    # a side stream: its handle is non-zero, so the plan's kernels and the
-    # step events share it
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    sptr = stream.cuda_stream
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    if stream is None:
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+    if flush is None:
+        flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
 
     def barrier():
         torch.cuda.synchronize()
@@ -685,28 +870,15 @@ def main():
         torch.cuda.synchronize()
 
     for _ in range(args.warmup):
-        plan.execute(sptr)
+        plan.execute(stream.cuda_stream)
     barrier()
-
-    # per-step device time of the whole step and of the pair kernel
-    plan.set_timing(True)
     clocks = ClockSampler(local)
     clocks.start()
-    step_ms, pair_ms = [], []
-    for _ in range(args.steps):
-        flush.zero_()
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        plan.execute(sptr)
-        ev1.record(stream)
-        ev1.synchronize()
-        step_ms.append(ev0.elapsed_time(ev1))
-        pair_ms.append(plan.stage_ms()[1])
-    barrier()
+    step_ms, pair_ms = _step_loop(torch, plan, stream, args.steps, barrier, flush)
     clk = clocks.stop()
     launches_per_step = plan.launches()
-    total_ms = sum(step_ms)
-    mean_pair_ms = sum(pair_ms) / len(pair_ms)
+    n_emb, kernel = plan.n_embedded(), plan.pair_kernel()
+    plan.close()
 
     # end to end through the C API, host buffers in and out
     e2e_ms = []
@@ -722,55 +894,75 @@ def main():
     h2d = int(table.indptr.nbytes + table.indices.nbytes + table.data.nbytes + tree.structure.nbytes +
               tree.lengths.nbytes)
     d2h = int(args.samples) ** 2 * 8
-
     total_ms, e2e_total, all_units, mean_pair_ms = combine_ranks(
-        [total_ms, sum(e2e_ms), float(units), mean_pair_ms], world, "cuda")
+        [sum(step_ms), sum(e2e_ms), float(units), sum(pair_ms) / len(pair_ms)], world, "cuda")
+    if rank != 0:
+        return None
+    value = all_units * args.steps / (total_ms / 1e3)
+    peak, _, _, peak_kind = peaks()
+    algo_bytes = ALGO_BYTES_PER_UPDATE * units
+    achieved = algo_bytes / (mean_pair_ms / 1e3) / 1e9
+    sm_mhz = clk["sm_mhz"] if clk else 1965.0
+    fp64_peak = 148 * 64 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
+    # dense-form arithmetic the stage stands in for: sub + mul + add per update
+    fp64_achieved = 3.0 * units / (mean_pair_ms / 1e3) / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator lognormal_20k_tips_2048_samples)",
+        "config": {"workload": WEIGHTED_WORKLOAD, "method": args.method, "n_samples": args.samples,
+                   "n_tips": args.tips, "embedded_branches": n_emb, "pair_kernel": kernel,
+                   "l2": "flushed between steps (256 MiB write outside the step events); embedding 655 MB > L2",
+                   "per_gpu_units": units},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": read_traffic(), "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": algo_bytes,
+                     "note": "reference-form bytes (2 fp64 accumulators RMW per 112-node batch) over the "
+                             "pair stage; the hybrid kernel keeps its accumulators on chip (traffic = its "
+                             "measured DRAM bytes per launch), so the binding bound is instruction issue: "
+                             "see fp64_dense_equivalent and the profile summary",
+                     "fp64_dense_equivalent": {"achieved_tflops": fp64_achieved,
+                                               "peak_tflops_at_clock": fp64_peak,
+                                               "frac": fp64_achieved / fp64_peak}},
+        "pair_kernel_ms": mean_pair_ms,
+        "e2e": {"value": all_units * len(e2e_ms) / (e2e_total / 1e3) if e2e_ms else None, "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_total / len(e2e_ms) if e2e_ms else None},
+        "gpu_launches": launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    if world == 1 and cpu:
+        try:
+            line["cpu_baseline"] = cpu_baseline(tree, table, args.method)
+        except Exception as exc:  # the reported baseline never blocks the bench line
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
+    return line
 
+
+def run_weighted(args):
+    import torch
+    import torch.distributed as dist
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    line = measure_weighted(args, world, rank, local, cpu=not args.no_cpu_baseline)
     if rank == 0:
-        value = all_units * args.steps / (total_ms / 1e3)
-        e2e_value = all_units * len(e2e_ms) / (e2e_total / 1e3) if e2e_ms else None
-        peak, peak_kind = peaks()
-        algo_bytes = ALGO_BYTES_PER_UPDATE * units
-        achieved = algo_bytes / (mean_pair_ms / 1e3) / 1e9
-        traffic = read_traffic()
-        sm_mhz = clk["sm_mhz"] if clk else 1965.0
-        fp64_peak = 148 * 64 * 2 * sm_mhz * 1e6 / 1e12  # TFLOP/s at the sampled clock
-        # dense-form arithmetic the stage stands in for: sub + mul + add per update
-        fp64_achieved = 3.0 * units / (mean_pair_ms / 1e3) / 1e12
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator lognormal_20k_tips_2048_samples)",
-            "config": {"workload": WORKLOAD, "method": args.method, "n_samples": args.samples, "n_tips": args.tips,
-                       "embedded_branches": plan.n_embedded(), "pair_kernel": plan.pair_kernel(),
-                       "l2": "flushed between steps (256 MiB write outside the step events); embedding 655 MB > L2",
-                       "per_gpu_units": units},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": algo_bytes,
-                         "note": "reference-form bytes (2 fp64 accumulators RMW per 112-node batch) over the "
-                                 "pair stage (dense/sparse row lists, one-sided sums, hybrid tile kernel; the "
-                                 "presence masks are written by the embedding, outside the stage); traffic is "
-                                 "the hybrid kernel's measured DRAM bytes per launch",
-                         "fp64_dense_equivalent": {"achieved_tflops": fp64_achieved,
-                                                   "peak_tflops_at_clock": fp64_peak,
-                                                   "frac": fp64_achieved / fp64_peak}},
-            "pair_kernel_ms": mean_pair_ms,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": e2e_total / len(e2e_ms) if e2e_ms else None},
-            "gpu_launches": launches_per_step * args.steps,
-            "clocks": clk,
-        }
-        if world == 1 and not args.no_cpu_baseline:
-            try:
-                line["cpu_baseline"] = cpu_baseline(tree, table, args.method)
-            except Exception as exc:  # the reported baseline never blocks the bench line
-                line["cpu_baseline"] = {"value": None, "unit": UNIT, "error": str(exc)[:200]}
         print(json.dumps(line), flush=True)
-    plan.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    runners = {"100k-tips-25k-presence": run_presence, "20k-tips-2048-samples": run_weighted,
+               "1k-tips-128-samples": run_small, "100-replicates-5k-samples": run_replicates,
+               "64-uneven-tables": run_uneven_tables}
+    return runners[args.workload](args)
 
 
 if __name__ == "__main__":

@@ -11,13 +11,23 @@ Reads the reference checkout as text only (nothing is compiled or run):
 * src/test*.tre     - the newick trees the API tests load.
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
+(default: $UNIFRAC_REFERENCE_PATH, else BASELINE.json's reference_path)
 """
 import json
 import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+def _default_reference():
+    """UNIFRAC_REFERENCE_PATH, else BASELINE.json's reference_path."""
+    if os.environ.get("UNIFRAC_REFERENCE_PATH"):
+        return os.environ["UNIFRAC_REFERENCE_PATH"]
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "..", "..", "BASELINE.json")) as f:
+        return json.load(f)["reference_path"]
+
+
+REF = sys.argv[1] if len(sys.argv) > 1 else _default_reference()
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
 
 

@@ -95,20 +95,22 @@ def test_clock_sampler_returns_promptly_without_a_gpu():
     assert clk is None or {"sm_mhz", "sm_max_mhz", "reasons", "samples"} <= set(clk)
 
 
-def _reference_arm(env_extra):
+def _reference_arm(env_extra, workload="100k-tips-25k-presence"):
     import json
     import subprocess
     env = dict(os.environ)
     env.update(env_extra)
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "0", "--samples", "96", "--tips", "600"],
+                          "--warmup", "0", "--samples", "96", "--tips", "600", "--presence-samples", "96",
+                          "--presence-tips", "600", "--workload", workload],
                          capture_output=True, text=True, env=env, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     return [json.loads(x) for x in out.stdout.splitlines() if x.startswith("{")]
 
 
-def test_reference_arm_prints_one_contract_line_on_rank_0():
-    lines = _reference_arm({"RANK": "0", "WORLD_SIZE": "1"})
+@pytest.mark.parametrize("workload", ["100k-tips-25k-presence", "20k-tips-2048-samples"])
+def test_reference_arm_prints_one_contract_line_on_rank_0(workload):
+    lines = _reference_arm({"RANK": "0", "WORLD_SIZE": "1"}, workload)
     assert len(lines) == 1
     d = lines[0]
     assert d["impl"] == "reference" and d["metric"] == "pair-branch updates/s" and d["unit"] == "updates/s"
@@ -116,6 +118,10 @@ def test_reference_arm_prints_one_contract_line_on_rank_0():
     assert d["cpu_baseline"]["kind"] in ("reference", "port") and d["cpu_baseline"]["cores"] >= 1
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    sys.path.insert(0, ROOT)
+    import bench
+    expected = bench.PRESENCE_WORKLOAD if workload == "100k-tips-25k-presence" else bench.WEIGHTED_WORKLOAD
+    assert d["config"]["workload"] == expected  # the same string as this arm's line
 
 
 def test_reference_arm_other_ranks_exit_without_work():

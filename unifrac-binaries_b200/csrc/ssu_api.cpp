@@ -1250,6 +1250,7 @@ uint64_t ssu_b200_plan_work_units(const ssu_b200_plan_t *plan) { return plan ? p
 uint32_t ssu_b200_plan_n_samples(const ssu_b200_plan_t *plan) { return plan ? plan->plan->n_samples() : 0; }
 uint64_t ssu_b200_plan_n_embedded(const ssu_b200_plan_t *plan) { return plan ? plan->plan->n_embedded() : 0; }
 uint32_t ssu_b200_plan_launches(const ssu_b200_plan_t *plan) { return plan ? plan->plan->launches() : 0; }
+uint64_t ssu_b200_plan_tensor_flops(const ssu_b200_plan_t *plan) { return plan ? plan->plan->tensor_flops() : 0; }
 void ssu_b200_plan_set_timing(ssu_b200_plan_t *plan, int enable) {
     if (plan) plan->plan->set_timing(enable != 0);
 }

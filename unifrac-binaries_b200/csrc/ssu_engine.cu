@@ -1349,20 +1349,23 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
         SSU_CK(upload(&g.d_start_col, start_col.data(), sizeof(int32_t) * start_col.size()));
     }
     // work units: per table, the (256-row block, 128-column block) pairs
-    // holding some pair k < l, in 8 x 16 super-blocks so that the clusters
-    // running at the same time share operand rows in L2
+    // holding some pair k < l, ordered in bands of 8 row blocks walked
+    // column by column.  Clusters start in launch order as SMs free up (one
+    // unit every ~20 us on the 25,000-sample table), so a unit reads the
+    // column block of B that its predecessor is reading and the row block of
+    // A that the unit 8 places earlier read, both still in L2: each B block
+    // comes from DRAM about once per band, each A block about once per table.
     for (Group &g : groups) {
         std::vector<uint4> tiles;
         for (uint32_t t = g.t0; t < g.t1; t++) {
             const uint32_t n = tdesc[t].n;
             const uint32_t nkb = (n + tc::UMMA_M - 1) / tc::UMMA_M, nlb = (n + tc::COLS - 1) / tc::COLS;
-            for (uint32_t gk = 0; gk < nkb; gk += 8)
-                for (uint32_t gl = 0; gl < nlb; gl += 16)
-                    for (uint32_t kb = gk; kb < std::min(nkb, gk + 8); kb++)
-                        for (uint32_t lb = gl; lb < std::min(nlb, gl + 16); lb++)
-                            if (static_cast<uint64_t>(kb) * tc::UMMA_M <
-                                std::min<uint64_t>(n, static_cast<uint64_t>(lb + 1) * tc::COLS) - 1)
-                                tiles.push_back(make_uint4(kb, lb, t, 0));
+            for (uint32_t k0 = 0; k0 < nkb; k0 += 8)
+                for (uint32_t lb = 0; lb < nlb; lb++)
+                    for (uint32_t kb = k0; kb < std::min(nkb, k0 + 8); kb++)
+                        if (static_cast<uint64_t>(kb) * tc::UMMA_M <
+                            std::min<uint64_t>(n, static_cast<uint64_t>(lb + 1) * tc::COLS) - 1)
+                            tiles.push_back(make_uint4(kb, lb, t, 0));
         }
         g.n_tiles = static_cast<uint32_t>(tiles.size());
         SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * std::max<size_t>(tiles.size(), 1)));
@@ -1430,7 +1433,7 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
             a.error = d_error;
             a.wait_cycles = gemm_wait_cycles;
             a.stall = union_stall;
-            // two CTAs (one cluster) per work unit
+            // two CTAs (one cluster) per work unit, started in unit order
             tc::unweighted_tc_kernel<<<2 * g.n_tiles, tc::THREADS, tc::SMEM_BYTES, s>>>(map_A, map_Bh, map_Bl, a);
             launches++;
         }
@@ -1787,6 +1790,12 @@ uint64_t Plan::work_units() const {
         u += n * (n - (n ? 1 : 0)) / 2 * impl_->table_E[t];
     }
     return u;
+}
+uint64_t Plan::tensor_flops() const {
+    if (!impl_->gemm) return 0;
+    uint64_t units = 0;
+    for (const auto &g : impl_->groups) units += g.n_tiles;
+    return 2ull * tc::UMMA_M * tc::UMMA_N * impl_->k_pad * units;
 }
 uint32_t Plan::launches() const { return impl_->launches; }
 const char *Plan::pair_kernel_name() const {

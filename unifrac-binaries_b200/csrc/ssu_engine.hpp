@@ -128,6 +128,9 @@ class Plan {
     const char *tuning() const;
     uint64_t n_embedded() const;
     uint64_t work_units() const;
+    // tensor-core flops (2 x multiply-adds) one execute issues; 0 off the
+    // tensor-core path
+    uint64_t tensor_flops() const;
     uint32_t launches() const;
     const char *pair_kernel_name() const;
     void set_timing(bool on);

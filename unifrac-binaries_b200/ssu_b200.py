@@ -131,6 +131,8 @@ def lib():
         L.ssu_b200_plan_n_embedded.restype = C.c_uint64
         L.ssu_b200_plan_launches.argtypes = [C.c_void_p]
         L.ssu_b200_plan_launches.restype = C.c_uint32
+        L.ssu_b200_plan_tensor_flops.argtypes = [C.c_void_p]
+        L.ssu_b200_plan_tensor_flops.restype = C.c_uint64
         L.ssu_b200_plan_set_timing.argtypes = [C.c_void_p, C.c_int]
         L.ssu_b200_plan_set_timing.restype = None
         L.ssu_b200_plan_stage_ms.argtypes = [C.c_void_p, P(C.c_float), P(C.c_float), P(C.c_float)]
@@ -566,6 +568,9 @@ class Plan:
     def launches(self):
         return int(lib().ssu_b200_plan_launches(self.ptr))
 
+    def tensor_flops(self):
+        return int(lib().ssu_b200_plan_tensor_flops(self.ptr))
+
     def pair_kernel(self):
         return lib().ssu_b200_plan_pair_kernel(self.ptr).decode()
 
@@ -619,6 +624,21 @@ class BatchPlan(Plan):
 
     def table_embedded(self, t):
         return int(lib().ssu_b200_plan_table_embedded(self.ptr, t))
+
+    def result_of(self, t):
+        """Table t's n x n result alone, copied from the plan's device buffer
+        (after execute; synchronous)."""
+        dt = np.float64 if is_fp64(self.method) else np.float32
+        n = self.sizes[t]
+        out = np.empty((n, n), dtype=dt)
+        rt = C.CDLL("libcudart.so.12")
+        rt.cudaMemcpy.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_int]
+        if rt.cudaDeviceSynchronize() != 0:  # the plan's work runs on its own stream
+            raise SSUError(6, "cudaDeviceSynchronize")
+        src = self.device_result() + self.offsets[t] * out.itemsize
+        if n and rt.cudaMemcpy(out.ctypes.data_as(C.c_void_p), C.c_void_p(src), out.nbytes, 2) != 0:
+            raise SSUError(6, "cudaMemcpy of one table's result")
+        return out
 
     def results(self, stream=None):
         dt = np.float64 if is_fp64(self.method) else np.float32
