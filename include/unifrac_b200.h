@@ -212,7 +212,13 @@ SSU_EXTERN ComputeStatus one_dense_pair_v2(unsigned int n_obs, const char **obs_
                                            bool bypass_tips, double *result);
 
 /* File-based entry points (BIOM-HDF5 table + newick tree).
- * src/api.hpp:228-244, 348-436, 492-493, 805-814 */
+ * src/api.hpp:228-244, 348-436, 492-493, 805-814.  The table file is read by
+ * this library's own BIOM-HDF5 reader (/observation/ids, /sample/ids and the
+ * observation-major CSR, as src/biom.cpp:18-255); a missing or unreadable
+ * table file is table_missing, a missing or unparsable tree file
+ * tree_missing.  The one_off_matrix* calls compute in the method's precision
+ * and write the result type's (an fp32 method through one_off_matrix_v3
+ * gives fp32 arithmetic in an fp64 matrix), as the reference. */
 SSU_EXTERN ComputeStatus one_off_v3(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
                                     bool variance_adjust, double alpha, bool bypass_tips,
                                     bool normalize_sample_counts, unsigned int n_substeps, mat_t **result);
@@ -237,6 +243,50 @@ SSU_EXTERN ComputeStatus one_off_matrix_fp32_v3(const char *biom_filename, const
                                                 unsigned int n_substeps, unsigned int subsample_depth,
                                                 bool subsample_with_replacement, const char *mmap_dir,
                                                 mat_full_fp32_t **result);
+/* From a pre-parsed tree (read_bptree_opaque / load_bptree_opaque /
+ * convert_bptree_opaque): src/api.hpp:355-359. */
+SSU_EXTERN ComputeStatus one_off_matrix_v3t(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                            const char *unifrac_method, bool variance_adjust, double alpha,
+                                            bool bypass_tips, bool normalize_sample_counts, unsigned int n_substeps,
+                                            unsigned int subsample_depth, bool subsample_with_replacement,
+                                            const char *mmap_dir, mat_full_fp64_t **result);
+/* Normalised sample counts: src/api.hpp:362-373. */
+SSU_EXTERN ComputeStatus one_off_matrix_v2(const char *biom_filename, const char *tree_filename,
+                                           const char *unifrac_method, bool variance_adjust, double alpha,
+                                           bool bypass_tips, unsigned int n_substeps, unsigned int subsample_depth,
+                                           bool subsample_with_replacement, const char *mmap_dir,
+                                           mat_full_fp64_t **result);
+SSU_EXTERN ComputeStatus one_off_matrix_v2t(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                            const char *unifrac_method, bool variance_adjust, double alpha,
+                                            bool bypass_tips, unsigned int n_substeps, unsigned int subsample_depth,
+                                            bool subsample_with_replacement, const char *mmap_dir,
+                                            mat_full_fp64_t **result);
+/* No subsampling: src/api.hpp:375-379. */
+SSU_EXTERN ComputeStatus one_off_matrix(const char *biom_filename, const char *tree_filename,
+                                        const char *unifrac_method, bool variance_adjust, double alpha,
+                                        bool bypass_tips, unsigned int n_substeps, const char *mmap_dir,
+                                        mat_full_fp64_t **result);
+/* fp32 twins: src/api.hpp:412-436. */
+SSU_EXTERN ComputeStatus one_off_matrix_fp32_v3t(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                                 const char *unifrac_method, bool variance_adjust, double alpha,
+                                                 bool bypass_tips, bool normalize_sample_counts,
+                                                 unsigned int n_substeps, unsigned int subsample_depth,
+                                                 bool subsample_with_replacement, const char *mmap_dir,
+                                                 mat_full_fp32_t **result);
+SSU_EXTERN ComputeStatus one_off_matrix_fp32_v2(const char *biom_filename, const char *tree_filename,
+                                                const char *unifrac_method, bool variance_adjust, double alpha,
+                                                bool bypass_tips, unsigned int n_substeps,
+                                                unsigned int subsample_depth, bool subsample_with_replacement,
+                                                const char *mmap_dir, mat_full_fp32_t **result);
+SSU_EXTERN ComputeStatus one_off_matrix_fp32_v2t(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                                 const char *unifrac_method, bool variance_adjust, double alpha,
+                                                 bool bypass_tips, unsigned int n_substeps,
+                                                 unsigned int subsample_depth, bool subsample_with_replacement,
+                                                 const char *mmap_dir, mat_full_fp32_t **result);
+SSU_EXTERN ComputeStatus one_off_matrix_fp32(const char *biom_filename, const char *tree_filename,
+                                             const char *unifrac_method, bool variance_adjust, double alpha,
+                                             bool bypass_tips, unsigned int n_substeps, const char *mmap_dir,
+                                             mat_full_fp32_t **result);
 SSU_EXTERN ComputeStatus faith_pd_one_off(const char *biom_filename, const char *tree_filename, r_vec **result);
 SSU_EXTERN ComputeStatus partial_v3(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
                                     bool variance_adjust, double alpha, bool bypass_tips,
@@ -246,7 +296,40 @@ SSU_EXTERN ComputeStatus partial(const char *biom_filename, const char *tree_fil
                                  bool variance_adjust, double alpha, bool bypass_tips, unsigned int n_substeps,
                                  unsigned int stripe_start, unsigned int stripe_stop, partial_mat_t **result);
 
+/* Partial results on disk (src/api.hpp:22-23, 816-991): the reference's
+ * version-2 file (magic 0x088ABA02, LZ4 blocks of the sample ids and of each
+ * stripe), written and read with this library's own LZ4 block codec.
+ * Statuses are the reference's; unlike it, a malformed file or an
+ * out-of-range stripe index is reported, never fatal.  read_partial_header
+ * reads only the header; stripes are then read on demand
+ * (read_partial_one_stripe) or by the merges.  validate_partial and the
+ * merges need the same samples, stripe total and triangle flag in every
+ * partial, no stripe twice and every stripe present (zero partials:
+ * incomplete_stripe_set, where the reference exits). */
+SSU_EXTERN IOStatus write_partial(const char *filename, const partial_mat_t *result);
+SSU_EXTERN IOStatus read_partial(const char *filename, partial_mat_t **result);
+SSU_EXTERN IOStatus read_partial_header(const char *input_filename, partial_dyn_mat_t **result_out);
+SSU_EXTERN IOStatus read_partial_one_stripe(partial_dyn_mat_t *result, uint32_t stripe_idx);
+SSU_EXTERN MergeStatus validate_partial(const partial_dyn_mat_t *const *partial_mats, int n_partials);
+SSU_EXTERN MergeStatus merge_partial_to_matrix(partial_dyn_mat_t **partial_mats, int n_partials,
+                                               mat_full_fp64_t **result);
+SSU_EXTERN MergeStatus merge_partial_to_matrix_fp32(partial_dyn_mat_t **partial_mats, int n_partials,
+                                                    mat_full_fp32_t **result);
+SSU_EXTERN MergeStatus merge_partial_to_mmap_matrix(partial_dyn_mat_t **partial_mats, int n_partials,
+                                                    const char *mmap_dir, mat_full_fp64_t **result);
+SSU_EXTERN MergeStatus merge_partial_to_mmap_matrix_fp32(partial_dyn_mat_t **partial_mats, int n_partials,
+                                                         const char *mmap_dir, mat_full_fp32_t **result);
+
 /* ------------------------------------------- extensions (no reference twin) */
+
+/* A BIOM-HDF5 table file read into a malloc'ed support_biom_t (ids copied,
+ * observation-major CSR), for callers without an HDF5 library; the reference
+ * reads the same datasets inside su::biom (src/biom.cpp:18-255) but does not
+ * export it.  open_error for a missing file, read_error for a file that is not
+ * a readable BIOM-HDF5 table (a message goes to stderr).  Release with
+ * ssu_b200_destroy_biom. */
+SSU_EXTERN IOStatus ssu_b200_read_biom(const char *biom_filename, support_biom_t **table);
+SSU_EXTERN void ssu_b200_destroy_biom(support_biom_t **table);
 
 /* one_off / partial / faith_pd_one_off over in-memory inputs: the compute
  * paths of the file-based calls above without the file parsing.  Method names,

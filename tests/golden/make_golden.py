@@ -10,6 +10,18 @@ Reads the reference checkout as text only (nothing is compiled or run):
                       ids, indices, indptr, data);
 * src/test*.tre     - the newick trees the API tests load.
 
+It also copies, byte for byte, the data files the reference's own checks run
+on into tests/golden/fixtures/ (the BIOM-HDF5 tables, their trees and the
+expected outputs the reference compares against):
+
+* ci/crawford.biom, ci/crawford.tre and the outputs ci/crawford_test.sh
+  compares with: ci/test.ssu.exp (unweighted_fp64), ci/test.ssu_vaw.exp
+  (unweighted_fp64, variance adjusted), ci/test.faith.exp (Faith PD);
+* src/testdata/absquant.biom, absquant.tree and the weighted-normalized
+  matrices without and with sample-count normalisation
+  (test.absquant.wn.dm, test.absquant_not.wn.dm);
+* src/test.biom, the 6 x 5 table of the reference's unit tests.
+
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 (default: $UNIFRAC_REFERENCE_PATH, else BASELINE.json's reference_path)
 """
@@ -129,6 +141,19 @@ def main():
     with open(OUT, "w") as f:
         json.dump(golden, f, indent=1, sort_keys=True)
     print("wrote", OUT)
+    fixtures = os.path.join(os.path.dirname(OUT), "fixtures")
+    os.makedirs(fixtures, exist_ok=True)
+    for rel in FIXTURES:
+        src = os.path.join(REF, rel)
+        dst = os.path.join(fixtures, os.path.basename(rel))
+        with open(src, "rb") as a, open(dst, "wb") as b:
+            b.write(a.read())
+        print("copied", rel)
+
+
+FIXTURES = ["ci/crawford.biom", "ci/crawford.tre", "ci/test.ssu.exp", "ci/test.ssu_vaw.exp", "ci/test.faith.exp",
+            "src/testdata/absquant.biom", "src/testdata/absquant.tree", "src/testdata/test.absquant.wn.dm",
+            "src/testdata/test.absquant_not.wn.dm", "src/test.biom"]
 
 
 if __name__ == "__main__":

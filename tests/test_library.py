@@ -154,11 +154,10 @@ def test_file_entry_points_statuses(ssu, L, tmp_path):
     tre.write_text("(GG_OTU_1:1,GG_OTU_2:1);")
     biom = tmp_path / "t.biom"
     biom.write_bytes(b"\x89HDF\r\n\x1a\n")
-    res = ctypes.c_void_p()
-    assert L.faith_pd_one_off(missing.encode(), str(tre).encode(), ctypes.byref(res)) == 2       # table_missing
-    assert L.faith_pd_one_off(str(biom).encode(), missing.encode(), ctypes.byref(res)) == 1      # tree_missing
-    # no HDF5 reader in this build: an existing table file reports table_missing
-    assert L.faith_pd_one_off(str(biom).encode(), str(tre).encode(), ctypes.byref(res)) == 2
+    for b, t, want in [(missing, str(tre), 2), (str(biom), missing, 1), (str(biom), str(tre), 2)]:
+        with pytest.raises(ssu.SSUError) as e:   # an HDF5 signature alone is not a readable table
+            ssu.file_faith_pd(b, t)
+        assert e.value.status == want
     t = ssu.OpaqueTree(path=str(tre))
     assert t.n_tips() == 2
 

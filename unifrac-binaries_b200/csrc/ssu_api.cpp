@@ -30,7 +30,9 @@
 
 #include <cuda_runtime.h>
 
+#include "ssu_biom.hpp"
 #include "ssu_engine.hpp"
+#include "ssu_partial.hpp"
 #include "ssu_table.hpp"
 #include "ssu_tree.hpp"
 
@@ -459,12 +461,27 @@ ComputeStatus full_matrix(const ssu::Table &table, const ssu::BPTree &tree, cons
         return output_error;
     }
     std::string err;
+    bool method_fp64 = false;
+    is_fp64_method(r.method, method_fp64);
     int rc = plan->execute(nullptr);
-    if (rc == 0) {
+    const size_t elems = static_cast<size_t>(table.n_samples) * table.n_samples;
+    if (rc == 0 && method_fp64 != (sizeof(TReal) == sizeof(double))) {
+        // the file-based calls compute in the method's precision and write
+        // the result type's (stripes_to_matrix_T<TReal>, src/api.cpp:684-690)
+        if (method_fp64) {
+            std::vector<double> tmp(elems);
+            rc = plan->download_full(tmp.data(), false, err);
+            for (size_t i = 0; rc == 0 && i < elems; i++) (*result)->matrix[i] = static_cast<TReal>(tmp[i]);
+        } else {
+            std::vector<float> tmp(elems);
+            rc = plan->download_full(tmp.data(), false, err);
+            for (size_t i = 0; rc == 0 && i < elems; i++) (*result)->matrix[i] = static_cast<TReal>(tmp[i]);
+        }
+    } else if (rc == 0) {
         // a fresh pageable result is faulted in while the device computes and
         // page-locked for the copy; a pooled one is page-locked already
         const bool fresh = allocated && (*result)->flags == 0;
-        const size_t bytes = sizeof(TReal) * static_cast<size_t>(table.n_samples) * table.n_samples;
+        const size_t bytes = sizeof(TReal) * elems;
         if (fresh && bytes >= kHugeAlign) prefault((*result)->matrix, bytes);
         rc = plan->download_full((*result)->matrix, fresh, err);
     } else {
@@ -832,26 +849,127 @@ bool read_text(const char *path, std::string &out) {
     return true;
 }
 
-// BIOM-HDF5 tables need an HDF5 reader, which this build does not carry.
-ComputeStatus load_biom(const char *biom_filename) {
-    std::fprintf(stderr,
-                 "unifrac-b200: %s: BIOM-HDF5 input is not available in this build; use the in-memory "
-                 "entry points\n",
-                 biom_filename);
-    return table_missing;
+// CHECK_FILE + PARSE_TREE_TABLE (src/api.cpp:115-121, 127-135): the table
+// file read as BIOM-HDF5 (ssu_biom.cpp), the tree file as newick.
+ComputeStatus load_table_file(const char *biom_filename, ssu::Table &table) {
+    std::string err;
+    if (!ssu::read_biom_hdf5(biom_filename, table, err)) {
+        report("table", std::string(biom_filename) + ": " + err);
+        return table_missing;
+    }
+    return okay;
+}
+
+ComputeStatus load_tree_file(const char *tree_filename, ssu::BPTree &tree) {
+    std::string text;
+    if (!read_text(tree_filename, text) || !ssu::BPTree::from_newick(text, tree)) return tree_missing;
+    return okay;
 }
 
 struct OpaqueTree {
     ssu::BPTree tree;
 };
 
-ComputeStatus file_front(const char *biom_filename, const char *tree_filename) {
+// Both files (or the table file and a pre-parsed tree), read and validated:
+// table_missing / tree_missing for missing or unreadable files, then
+// VALIDATE_TREE_TABLE's statuses.
+ComputeStatus load_files(const char *biom_filename, const char *tree_filename, ssu::Table &table,
+                         ssu::BPTree &tree) {
     if (!file_exists(biom_filename)) return table_missing;
     if (!file_exists(tree_filename)) return tree_missing;
-    std::string text;
-    ssu::BPTree tree;
-    if (!read_text(tree_filename, text) || !ssu::BPTree::from_newick(text, tree)) return tree_missing;
-    return load_biom(biom_filename);
+    ComputeStatus st = load_tree_file(tree_filename, tree);
+    if (st != okay) return st;
+    st = load_table_file(biom_filename, table);
+    if (st != okay) return st;
+    return validate(table, tree);
+}
+
+ComputeStatus load_files_wtree(const char *biom_filename, const opaque_bptree_t *tree_data, ssu::Table &table,
+                               ssu::BPTree &tree) {
+    if (!tree_data) return tree_missing;
+    if (!file_exists(biom_filename)) return table_missing;
+    tree = reinterpret_cast<const OpaqueTree *>(tree_data)->tree;
+    const ComputeStatus st = load_table_file(biom_filename, table);
+    if (st != okay) return st;
+    return validate(table, tree);
+}
+
+// merge_partial_to_matrix_T (src/api.cpp:2454-2478): the partials checked,
+// the result allocated (malloc, or a file under mmap_dir), every stripe read
+// (from memory, or its file when only the header was read), scattered to
+// both triangles and released; stripes are independent, so they go to host
+// threads.
+template <class TReal, class TMat>
+MergeStatus merge_partials(partial_dyn_mat_t **mats, int n, const char *mmap_dir, TMat **result) {
+    if (!result) return incomplete_stripe_set;
+    if (mmap_dir && !mmap_dir[0]) mmap_dir = nullptr;
+    const MergeStatus err = ssu::partial_check(mats, n, false);
+    if (err != merge_okay) return err;
+    const uint32_t ns = mats[0]->n_samples;
+    std::vector<std::string_view> ids(ns);
+    for (uint32_t j = 0; j < ns; j++) ids[j] = mats[0]->sample_ids[j];
+    struct Job {
+        partial_dyn_mat_t *p;
+        uint32_t idx;
+        uint64_t off;
+    };
+    std::vector<Job> jobs;
+    for (int i = 0; i < n; i++) {
+        partial_dyn_mat_t *p = mats[i];
+        const uint32_t cnt = p->stripe_stop - p->stripe_start;
+        bool all_in_memory = true;
+        for (uint32_t s = 0; s < cnt; s++) all_in_memory = all_in_memory && p->stripes && p->stripes[s];
+        std::vector<uint64_t> offs(cnt, 0);
+        if (!all_in_memory) {
+            if (!p->filename || !p->offsets ||
+                ssu::partial_stripe_offsets(p->filename, p->offsets[0], cnt, offs) != read_okay)
+                return incomplete_stripe_set;
+        }
+        for (uint32_t s = 0; s < cnt; s++) jobs.push_back(Job{p, s, offs[s]});
+    }
+    *result = nullptr;
+    if (!alloc_full<TReal, TMat>(*result, ids, mmap_dir)) {
+        destroy_full<TMat, TReal>(result);
+        return incomplete_stripe_set;
+    }
+    TReal *m = (*result)->matrix;
+    std::atomic<bool> bad{false};
+    try {
+        parallel_for(static_cast<unsigned>(jobs.size()), host_threads(16), [&](unsigned j) {
+            const Job &jb = jobs[j];
+            double *owned = jb.p->stripes ? jb.p->stripes[jb.idx] : nullptr;
+            const double *stripe = owned;
+            std::vector<double> local;
+            if (!stripe) {
+                local.resize(ns);
+                if (ssu::partial_read_stripe_at(jb.p->filename, jb.off, ns, local.data()) != read_okay) {
+                    bad = true;
+                    return;
+                }
+                stripe = local.data();
+            }
+            const uint64_t s = jb.p->stripe_start + jb.idx;
+            for (uint64_t k = 0; k < ns; k++) {
+                const uint64_t l = (k + s + 1) % ns;
+                m[k * ns + l] = static_cast<TReal>(stripe[k]);
+                m[l * ns + k] = static_cast<TReal>(stripe[k]);
+            }
+            // a stripe held in memory is released once used (the reference's
+            // PartialStripes::release_stripe, src/api.cpp:2441-2450)
+            if (owned) {
+                std::free(owned);
+                jb.p->stripes[jb.idx] = nullptr;
+            }
+        });
+    } catch (const std::exception &) {
+        bad = true;
+    }
+    if (bad) {
+        destroy_full<TMat, TReal>(result);
+        return incomplete_stripe_set;
+    }
+    for (uint64_t k = 0; k < ns; k++) m[k * ns + k] = 0;
+    return merge_okay;
 }
 
 }  // namespace
@@ -942,6 +1060,25 @@ void destroy_partial_dyn_mat(partial_dyn_mat_t **result) {
     std::free(p->filename);
     std::free(p);
     *result = nullptr;
+}
+
+MergeStatus merge_partial_to_matrix(partial_dyn_mat_t **partial_mats, int n_partials, mat_full_fp64_t **result) {
+    return merge_partials<double, mat_full_fp64_t>(partial_mats, n_partials, nullptr, result);
+}
+
+MergeStatus merge_partial_to_matrix_fp32(partial_dyn_mat_t **partial_mats, int n_partials,
+                                         mat_full_fp32_t **result) {
+    return merge_partials<float, mat_full_fp32_t>(partial_mats, n_partials, nullptr, result);
+}
+
+MergeStatus merge_partial_to_mmap_matrix(partial_dyn_mat_t **partial_mats, int n_partials, const char *mmap_dir,
+                                         mat_full_fp64_t **result) {
+    return merge_partials<double, mat_full_fp64_t>(partial_mats, n_partials, mmap_dir, result);
+}
+
+MergeStatus merge_partial_to_mmap_matrix_fp32(partial_dyn_mat_t **partial_mats, int n_partials,
+                                              const char *mmap_dir, mat_full_fp32_t **result) {
+    return merge_partials<float, mat_full_fp32_t>(partial_mats, n_partials, mmap_dir, result);
 }
 
 void destroy_results_vec(r_vec **result) {
@@ -1071,16 +1208,26 @@ ComputeStatus one_dense_pair_v2(unsigned int n_obs, const char **obs_ids, const 
                              bypass_tips, true, result);
 }
 
-ComputeStatus one_off_v3(const char *biom_filename, const char *tree_filename, const char *, bool, double, bool,
-                         bool, unsigned int, mat_t **) {
-    return file_front(biom_filename, tree_filename);
+ComputeStatus one_off_v3(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                         bool variance_adjust, double alpha, bool bypass_tips, bool normalize_sample_counts,
+                         unsigned int, mat_t **result) {
+    ssu::Table table;
+    ssu::BPTree tree;
+    const ComputeStatus st = load_files(biom_filename, tree_filename, table, tree);
+    if (st != okay) return st;
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return condensed(table, tree, r, result);
 }
 
-ComputeStatus one_off_wtree_v3(const char *biom_filename, const opaque_bptree_t *tree_data, const char *, bool,
-                               double, bool, bool, unsigned int, mat_t **) {
-    if (!tree_data) return tree_missing;
-    if (!file_exists(biom_filename)) return table_missing;
-    return load_biom(biom_filename);
+ComputeStatus one_off_wtree_v3(const char *biom_filename, const opaque_bptree_t *tree_data,
+                               const char *unifrac_method, bool variance_adjust, double alpha, bool bypass_tips,
+                               bool normalize_sample_counts, unsigned int, mat_t **result) {
+    ssu::Table table;
+    ssu::BPTree tree;
+    const ComputeStatus st = load_files_wtree(biom_filename, tree_data, table, tree);
+    if (st != okay) return st;
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return condensed(table, tree, r, result);
 }
 
 ComputeStatus one_off(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
@@ -1096,24 +1243,149 @@ ComputeStatus one_off_wtree(const char *biom_filename, const opaque_bptree_t *tr
                             n_substeps, result);
 }
 
-ComputeStatus one_off_matrix_v3(const char *biom_filename, const char *tree_filename, const char *, bool, double,
-                                bool, bool, unsigned int, unsigned int, bool, const char *, mat_full_fp64_t **) {
-    return file_front(biom_filename, tree_filename);
+}  // extern "C"
+
+namespace {
+
+// one_off_matrix_v3_T over a loaded table (src/api.cpp:700-717): optional
+// rarefaction, the method's precision for the arithmetic, TReal for the result.
+template <class TReal, class TMat>
+ComputeStatus file_matrix(ComputeStatus loaded, const ssu::Table &table, const ssu::BPTree &tree, const Request &r,
+                          unsigned int subsample_depth, bool with_replacement, const char *mmap_dir, TMat **result) {
+    if (loaded != okay) return loaded;
+    if (!result) return output_error;
+    if (mmap_dir && mmap_dir[0] == 0) mmap_dir = nullptr;
+    if (subsample_depth > 0) {
+        ssu::Table sub = table.rarefied(subsample_depth, with_replacement, g_seed.load());
+        if (sub.n_samples == 0 || sub.n_obs == 0) return table_empty;
+        return full_matrix<TReal, TMat>(sub, tree, r, mmap_dir, result);
+    }
+    return full_matrix<TReal, TMat>(table, tree, r, mmap_dir, result);
 }
 
-ComputeStatus one_off_matrix_fp32_v3(const char *biom_filename, const char *tree_filename, const char *, bool,
-                                     double, bool, bool, unsigned int, unsigned int, bool, const char *,
-                                     mat_full_fp32_t **) {
-    return file_front(biom_filename, tree_filename);
+}  // namespace
+
+extern "C" {
+
+ComputeStatus one_off_matrix_v3(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                                bool variance_adjust, double alpha, bool bypass_tips, bool normalize_sample_counts,
+                                unsigned int, unsigned int subsample_depth, bool subsample_with_replacement,
+                                const char *mmap_dir, mat_full_fp64_t **result) {
+    ssu::Table table;
+    ssu::BPTree tree;
+    const ComputeStatus st = load_files(biom_filename, tree_filename, table, tree);
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return file_matrix<double, mat_full_fp64_t>(st, table, tree, r, subsample_depth, subsample_with_replacement,
+                                                mmap_dir, result);
 }
 
-ComputeStatus faith_pd_one_off(const char *biom_filename, const char *tree_filename, r_vec **) {
-    return file_front(biom_filename, tree_filename);
+ComputeStatus one_off_matrix_fp32_v3(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                                     bool variance_adjust, double alpha, bool bypass_tips,
+                                     bool normalize_sample_counts, unsigned int, unsigned int subsample_depth,
+                                     bool subsample_with_replacement, const char *mmap_dir,
+                                     mat_full_fp32_t **result) {
+    ssu::Table table;
+    ssu::BPTree tree;
+    const ComputeStatus st = load_files(biom_filename, tree_filename, table, tree);
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return file_matrix<float, mat_full_fp32_t>(st, table, tree, r, subsample_depth, subsample_with_replacement,
+                                               mmap_dir, result);
 }
 
-ComputeStatus partial_v3(const char *biom_filename, const char *tree_filename, const char *, bool, double, bool,
-                         bool, unsigned int, unsigned int, unsigned int, partial_mat_t **) {
-    return file_front(biom_filename, tree_filename);
+ComputeStatus one_off_matrix_v3t(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                 const char *unifrac_method, bool variance_adjust, double alpha, bool bypass_tips,
+                                 bool normalize_sample_counts, unsigned int, unsigned int subsample_depth,
+                                 bool subsample_with_replacement, const char *mmap_dir, mat_full_fp64_t **result) {
+    ssu::Table table;
+    ssu::BPTree tree;
+    const ComputeStatus st = load_files_wtree(biom_filename, tree_data, table, tree);
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return file_matrix<double, mat_full_fp64_t>(st, table, tree, r, subsample_depth, subsample_with_replacement,
+                                                mmap_dir, result);
+}
+
+ComputeStatus one_off_matrix_fp32_v3t(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                      const char *unifrac_method, bool variance_adjust, double alpha,
+                                      bool bypass_tips, bool normalize_sample_counts, unsigned int,
+                                      unsigned int subsample_depth, bool subsample_with_replacement,
+                                      const char *mmap_dir, mat_full_fp32_t **result) {
+    ssu::Table table;
+    ssu::BPTree tree;
+    const ComputeStatus st = load_files_wtree(biom_filename, tree_data, table, tree);
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return file_matrix<float, mat_full_fp32_t>(st, table, tree, r, subsample_depth, subsample_with_replacement,
+                                               mmap_dir, result);
+}
+
+ComputeStatus one_off_matrix_v2(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                                bool variance_adjust, double alpha, bool bypass_tips, unsigned int n_substeps,
+                                unsigned int subsample_depth, bool subsample_with_replacement, const char *mmap_dir,
+                                mat_full_fp64_t **result) {
+    return one_off_matrix_v3(biom_filename, tree_filename, unifrac_method, variance_adjust, alpha, bypass_tips, true,
+                             n_substeps, subsample_depth, subsample_with_replacement, mmap_dir, result);
+}
+
+ComputeStatus one_off_matrix_v2t(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                 const char *unifrac_method, bool variance_adjust, double alpha, bool bypass_tips,
+                                 unsigned int n_substeps, unsigned int subsample_depth,
+                                 bool subsample_with_replacement, const char *mmap_dir, mat_full_fp64_t **result) {
+    return one_off_matrix_v3t(biom_filename, tree_data, unifrac_method, variance_adjust, alpha, bypass_tips, true,
+                              n_substeps, subsample_depth, subsample_with_replacement, mmap_dir, result);
+}
+
+ComputeStatus one_off_matrix(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                             bool variance_adjust, double alpha, bool bypass_tips, unsigned int n_substeps,
+                             const char *mmap_dir, mat_full_fp64_t **result) {
+    return one_off_matrix_v3(biom_filename, tree_filename, unifrac_method, variance_adjust, alpha, bypass_tips, true,
+                             n_substeps, 0, false, mmap_dir, result);
+}
+
+ComputeStatus one_off_matrix_fp32_v2(const char *biom_filename, const char *tree_filename,
+                                     const char *unifrac_method, bool variance_adjust, double alpha,
+                                     bool bypass_tips, unsigned int n_substeps, unsigned int subsample_depth,
+                                     bool subsample_with_replacement, const char *mmap_dir,
+                                     mat_full_fp32_t **result) {
+    return one_off_matrix_fp32_v3(biom_filename, tree_filename, unifrac_method, variance_adjust, alpha, bypass_tips,
+                                  true, n_substeps, subsample_depth, subsample_with_replacement, mmap_dir, result);
+}
+
+ComputeStatus one_off_matrix_fp32_v2t(const char *biom_filename, const opaque_bptree_t *tree_data,
+                                      const char *unifrac_method, bool variance_adjust, double alpha,
+                                      bool bypass_tips, unsigned int n_substeps, unsigned int subsample_depth,
+                                      bool subsample_with_replacement, const char *mmap_dir,
+                                      mat_full_fp32_t **result) {
+    return one_off_matrix_fp32_v3t(biom_filename, tree_data, unifrac_method, variance_adjust, alpha, bypass_tips,
+                                   true, n_substeps, subsample_depth, subsample_with_replacement, mmap_dir, result);
+}
+
+ComputeStatus one_off_matrix_fp32(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                                  bool variance_adjust, double alpha, bool bypass_tips, unsigned int n_substeps,
+                                  const char *mmap_dir, mat_full_fp32_t **result) {
+    return one_off_matrix_fp32_v3(biom_filename, tree_filename, unifrac_method, variance_adjust, alpha, bypass_tips,
+                                  true, n_substeps, 0, false, mmap_dir, result);
+}
+
+ComputeStatus faith_pd_one_off(const char *biom_filename, const char *tree_filename, r_vec **result) {
+    ssu::Table table;
+    ssu::BPTree tree;
+    const ComputeStatus st = load_files(biom_filename, tree_filename, table, tree);
+    if (st != okay) return st;
+    return faith_pd(table, tree, result);
+}
+
+ComputeStatus partial_v3(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
+                         bool variance_adjust, double alpha, bool bypass_tips, bool normalize_sample_counts,
+                         unsigned int, unsigned int stripe_start, unsigned int stripe_stop, partial_mat_t **result) {
+    if (!file_exists(biom_filename)) return table_missing;
+    if (!file_exists(tree_filename)) return tree_missing;
+    bool fp64 = false;
+    if (is_fp64_method(unifrac_method, fp64) != okay) return unknown_method;  // SET_METHOD before parsing
+    ssu::Table table;
+    ssu::BPTree tree;
+    const ComputeStatus st = load_files(biom_filename, tree_filename, table, tree);
+    if (st != okay) return st;
+    const Request r{unifrac_method, variance_adjust, alpha, bypass_tips, normalize_sample_counts};
+    return partial_stripes(table, tree, r, stripe_start, stripe_stop, result);
 }
 
 ComputeStatus partial(const char *biom_filename, const char *tree_filename, const char *unifrac_method,
@@ -1124,6 +1396,46 @@ ComputeStatus partial(const char *biom_filename, const char *tree_filename, cons
 }
 
 // ================================================================ extensions
+
+IOStatus ssu_b200_read_biom(const char *biom_filename, support_biom_t **table) {
+    if (!table) return unexpected_end;
+    *table = nullptr;
+    if (!file_exists(biom_filename)) return open_error;
+    ssu::Table t;
+    std::string err;
+    if (!ssu::read_biom_hdf5(biom_filename, t, err)) {
+        report("table", std::string(biom_filename) + ": " + err);
+        return read_error;
+    }
+    support_biom_t *b = static_cast<support_biom_t *>(std::calloc(1, sizeof(support_biom_t)));
+    b->n_obs = static_cast<int>(t.n_obs);
+    b->n_samples = static_cast<int>(t.n_samples);
+    b->nnz = static_cast<int>(t.nnz());
+    b->obs_ids = copy_ids(t.obs_ids);
+    b->sample_ids = copy_ids(t.sample_ids);
+    b->indptr = static_cast<uint32_t *>(std::malloc(sizeof(uint32_t) * (t.n_obs + 1)));
+    b->indices = static_cast<uint32_t *>(std::malloc(sizeof(uint32_t) * std::max<uint64_t>(t.nnz(), 1)));
+    b->data = static_cast<double *>(std::malloc(sizeof(double) * std::max<uint64_t>(t.nnz(), 1)));
+    std::memcpy(b->indptr, t.indptr, sizeof(uint32_t) * (t.n_obs + 1));
+    std::memcpy(b->indices, t.indices, sizeof(uint32_t) * t.nnz());
+    std::memcpy(b->data, t.data, sizeof(double) * t.nnz());
+    *table = b;
+    return read_okay;
+}
+
+void ssu_b200_destroy_biom(support_biom_t **table) {
+    if (!table || !*table) return;
+    support_biom_t *b = *table;
+    for (int i = 0; i < b->n_obs; i++) std::free(b->obs_ids[i]);
+    for (int j = 0; j < b->n_samples; j++) std::free(b->sample_ids[j]);
+    std::free(b->obs_ids);
+    std::free(b->sample_ids);
+    std::free(b->indptr);
+    std::free(b->indices);
+    std::free(b->data);
+    std::free(b);
+    *table = nullptr;
+}
 
 ComputeStatus ssu_b200_one_off_inmem_v3(const support_biom_t *table_data, const support_bptree_t *tree_data,
                                         const char *unifrac_method, bool variance_adjust, double alpha,

@@ -1349,20 +1349,23 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
         SSU_CK(upload(&g.d_start_col, start_col.data(), sizeof(int32_t) * start_col.size()));
     }
     // work units: per table, the (256-row block, 128-column block) pairs
-    // holding some pair k < l, ordered in bands of 8 row blocks walked
+    // holding some pair k < l, ordered in bands of row blocks walked
     // column by column.  Clusters start in launch order as SMs free up (one
     // unit every ~20 us on the 25,000-sample table), so a unit reads the
     // column block of B that its predecessor is reading and the row block of
-    // A that the unit 8 places earlier read, both still in L2: each B block
+    // A that the unit a band height earlier read, both still in L2: each B block
     // comes from DRAM about once per band, each A block about once per table.
+    // UNIFRAC_B200_TC_BAND sets the band height (row blocks, default 4: on the
+    // 25,000-sample table 164 ms against 166.6 at 8, 173.9 at 2, 190.4 at 1).
+    const uint32_t band = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_TC_BAND", 4)));
     for (Group &g : groups) {
         std::vector<uint4> tiles;
         for (uint32_t t = g.t0; t < g.t1; t++) {
             const uint32_t n = tdesc[t].n;
             const uint32_t nkb = (n + tc::UMMA_M - 1) / tc::UMMA_M, nlb = (n + tc::COLS - 1) / tc::COLS;
-            for (uint32_t k0 = 0; k0 < nkb; k0 += 8)
+            for (uint32_t k0 = 0; k0 < nkb; k0 += band)
                 for (uint32_t lb = 0; lb < nlb; lb++)
-                    for (uint32_t kb = k0; kb < std::min(nkb, k0 + 8); kb++)
+                    for (uint32_t kb = k0; kb < std::min(nkb, k0 + band); kb++)
                         if (static_cast<uint64_t>(kb) * tc::UMMA_M <
                             std::min<uint64_t>(n, static_cast<uint64_t>(lb + 1) * tc::COLS) - 1)
                             tiles.push_back(make_uint4(kb, lb, t, 0));

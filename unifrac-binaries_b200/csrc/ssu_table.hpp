@@ -44,9 +44,11 @@ struct Table {
     mutable uint32_t distinct_names = 0;
     mutable std::shared_ptr<const TipMatch> tip_match;
 
-    // storage when the table owns its arrays
+    // storage when the table owns its arrays (and, for tables read from a
+    // file, the bytes its id views point into)
     std::vector<uint32_t> own_indptr, own_indices;
     std::vector<double> own_data;
+    std::unique_ptr<char[]> own_names;
 
     uint64_t nnz() const { return n_obs ? indptr[n_obs] : 0; }
 
@@ -69,6 +71,8 @@ struct Table {
 
     void compute_totals();
     std::unordered_map<std::string_view, uint32_t> obs_index() const;
+    // point indptr / indices / data at the owned arrays
+    void adopt() { adopt_owned(); }
 
   private:
     void adopt_owned();

@@ -24,6 +24,8 @@ STATUS = ["okay", "tree_missing", "table_missing", "table_empty", "unknown_metho
           "table_and_tree_do_not_overlap", "output_error", "invalid_method", "grouping_missing"]
 IO_STATUS = ["read_okay", "write_okay", "open_error", "read_error", "magic_incompatible", "bad_header",
              "unexpected_end", "write_error"]
+MERGE_STATUS = ["merge_okay", "incomplete_stripe_set", "sample_id_consistency", "square_mismatch",
+                "partials_mismatch", "stripes_overlap"]
 
 _strpp = C.POINTER(C.c_char_p)
 
@@ -56,6 +58,13 @@ class Mat(C.Structure):
 
 class RVec(C.Structure):
     _fields_ = [("n_samples", C.c_uint), ("values", C.POINTER(C.c_double)), ("sample_ids", _strpp)]
+
+
+class PartialDynMat(C.Structure):
+    _fields_ = [("n_samples", C.c_uint32), ("sample_ids", _strpp), ("offsets", C.POINTER(C.c_uint64)),
+                ("stripes", C.POINTER(C.POINTER(C.c_double))), ("stripe_start", C.c_uint32),
+                ("stripe_stop", C.c_uint32), ("stripe_total", C.c_uint32), ("is_upper_triangle", C.c_bool),
+                ("filename", C.c_char_p)]
 
 
 class PartialMat(C.Structure):
@@ -115,9 +124,33 @@ def lib():
             f.restype = None
         for name in ["one_off_v3", "one_off_matrix_v3", "faith_pd_one_off", "partial_v3"]:
             getattr(L, name).restype = C.c_int
-        L.faith_pd_one_off.argtypes = [C.c_char_p, C.c_char_p, C.c_void_p]
+        L.faith_pd_one_off.argtypes = [C.c_char_p, C.c_char_p, PP(P(RVec))]
         L.ssu_set_random_seed.argtypes = [C.c_uint]
         L.ssu_set_random_seed.restype = None
+        L.write_partial.argtypes = [C.c_char_p, P(PartialMat)]
+        L.read_partial_header.argtypes = [C.c_char_p, PP(P(PartialDynMat))]
+        L.destroy_partial_dyn_mat.argtypes = [PP(P(PartialDynMat))]
+        L.destroy_partial_dyn_mat.restype = None
+        L.validate_partial.argtypes = [P(P(PartialDynMat)), C.c_int]
+        L.merge_partial_to_mmap_matrix.argtypes = [P(P(PartialDynMat)), C.c_int, C.c_char_p, PP(P(MatFull64))]
+        L.merge_partial_to_mmap_matrix_fp32.argtypes = [P(P(PartialDynMat)), C.c_int, C.c_char_p,
+                                                        PP(P(MatFull32))]
+        L.ssu_b200_read_biom.argtypes = [C.c_char_p, PP(P(SupportBiom))]
+        L.ssu_b200_destroy_biom.argtypes = [PP(P(SupportBiom))]
+        L.ssu_b200_destroy_biom.restype = None
+        fcommon = [C.c_char_p, C.c_void_p, C.c_char_p, C.c_bool, C.c_double, C.c_bool]
+        for name, res in [("one_off_matrix_v3", MatFull64), ("one_off_matrix_v3t", MatFull64),
+                          ("one_off_matrix_fp32_v3", MatFull32), ("one_off_matrix_fp32_v3t", MatFull32)]:
+            getattr(L, name).argtypes = fcommon + [C.c_bool, C.c_uint, C.c_uint, C.c_bool, C.c_char_p,
+                                                   PP(P(res))]
+        for name, res in [("one_off_matrix_v2", MatFull64), ("one_off_matrix_v2t", MatFull64),
+                          ("one_off_matrix_fp32_v2", MatFull32), ("one_off_matrix_fp32_v2t", MatFull32)]:
+            getattr(L, name).argtypes = fcommon + [C.c_uint, C.c_uint, C.c_bool, C.c_char_p, PP(P(res))]
+        L.one_off_matrix.argtypes = fcommon + [C.c_uint, C.c_char_p, PP(P(MatFull64))]
+        L.one_off_matrix_fp32.argtypes = fcommon + [C.c_uint, C.c_char_p, PP(P(MatFull32))]
+        L.one_off_v3.argtypes = fcommon + [C.c_bool, C.c_uint, PP(P(Mat))]
+        L.one_off_wtree_v3.argtypes = fcommon + [C.c_bool, C.c_uint, PP(P(Mat))]
+        L.partial_v3.argtypes = fcommon + [C.c_bool, C.c_uint, C.c_uint, C.c_uint, PP(P(PartialMat))]
         L.ssu_b200_plan_create.argtypes = common[:-1] + [P(C.c_void_p)]
         L.ssu_b200_plan_execute.argtypes = [C.c_void_p, C.c_void_p]
         L.ssu_b200_plan_device_result.argtypes = [C.c_void_p]
@@ -435,6 +468,52 @@ def partial(tree, table, method, stripe_start, stripe_stop, variance_adjust=Fals
     return stripes, meta
 
 
+def partial_to_file(tree, table, method, stripe_start, stripe_stop, path, variance_adjust=False, alpha=1.0,
+                    bypass_tips=False, normalize=True):
+    """Stripes [start, stop) through ssu_b200_partial_inmem_v3, written to
+    `path` with write_partial (the reference's partial file format)."""
+    L = lib()
+    x = Inputs(tree, table)
+    res = C.POINTER(PartialMat)()
+    st = L.ssu_b200_partial_inmem_v3(C.byref(x.biom), C.byref(x.tree), method.encode(), variance_adjust, alpha,
+                                     bypass_tips, normalize, 1, stripe_start, stripe_stop, C.byref(res))
+    if st != 0:
+        raise SSUError(st, "ssu_b200_partial_inmem_v3")
+    io = L.write_partial(str(path).encode(), res)
+    L.destroy_partial_mat(C.byref(res))
+    if io != 1:
+        raise RuntimeError(f"write_partial: {IO_STATUS[io]}")
+
+
+def merge_partial_files(paths, fp32=False, mmap_dir=None):
+    """Headers of the partial files read (read_partial_header), checked and
+    merged (merge_partial_to_mmap_matrix[_fp32]); the stripes are read on
+    demand by the merge.  Returns (matrix, ids)."""
+    L = lib()
+    mats = []
+    try:
+        for p in paths:
+            d = C.POINTER(PartialDynMat)()
+            io = L.read_partial_header(str(p).encode(), C.byref(d))
+            if io != 0:
+                raise RuntimeError(f"read_partial_header({p}): {IO_STATUS[io]}")
+            mats.append(d)
+        arr = (C.POINTER(PartialDynMat) * len(mats))(*mats)
+        res = C.POINTER(MatFull32 if fp32 else MatFull64)()
+        fn = L.merge_partial_to_mmap_matrix_fp32 if fp32 else L.merge_partial_to_mmap_matrix
+        st = fn(arr, len(mats), mmap_dir.encode() if mmap_dir else None, C.byref(res))
+        if st != 0:
+            raise RuntimeError(f"merge of partial files: {MERGE_STATUS[st]}")
+        n = res.contents.n_samples
+        out = np.ctypeslib.as_array(res.contents.matrix, shape=(n, n)).copy()
+        ids = _ids(res.contents.sample_ids, n)
+        (L.destroy_mat_full_fp32 if fp32 else L.destroy_mat_full_fp64)(C.byref(res))
+        return out, ids
+    finally:
+        for d in mats:
+            L.destroy_partial_dyn_mat(C.byref(d))
+
+
 def faith_pd(tree, table):
     L = lib()
     x = Inputs(tree, table)
@@ -507,6 +586,100 @@ class OpaqueTree:
             self.close()
         except Exception:
             pass
+
+
+def read_biom(path):
+    """A BIOM-HDF5 table file as a synthetic-module Table (ssu_b200_read_biom)."""
+    import ssu_synth
+    L = lib()
+    res = C.POINTER(SupportBiom)()
+    st = L.ssu_b200_read_biom(str(path).encode(), C.byref(res))
+    if st != 0:
+        raise RuntimeError(f"ssu_b200_read_biom: {IO_STATUS[st]}")
+    b = res.contents
+    nnz = b.nnz
+    t = ssu_synth.Table(_ids(b.obs_ids, b.n_obs), _ids(b.sample_ids, b.n_samples),
+                        np.ctypeslib.as_array(b.indptr, shape=(b.n_obs + 1,)).copy(),
+                        np.ctypeslib.as_array(b.indices, shape=(max(nnz, 1),))[:nnz].copy(),
+                        np.ctypeslib.as_array(b.data, shape=(max(nnz, 1),))[:nnz].copy())
+    L.ssu_b200_destroy_biom(C.byref(res))
+    return t
+
+
+def file_matrix(entry, biom_path, tree, method, variance_adjust=False, alpha=1.0, bypass_tips=False,
+                normalize=True, subsample_depth=0, with_replacement=False, mmap_dir=None):
+    """One of the file-based one_off_matrix* calls by name.  `tree` is a
+    newick file path for the plain forms and an OpaqueTree for the *t forms.
+    Returns (matrix, ids); raises SSUError with the status otherwise."""
+    L = lib()
+    f = getattr(L, entry)
+    fp32 = "fp32" in entry
+    res = C.POINTER(MatFull32 if fp32 else MatFull64)()
+    tree_arg = tree.ptr if isinstance(tree, OpaqueTree) else str(tree).encode()
+    md = mmap_dir.encode() if mmap_dir else None
+    head = [str(biom_path).encode(), tree_arg, method.encode(), variance_adjust, alpha, bypass_tips]
+    if entry.endswith("_v3") or entry.endswith("_v3t"):
+        args = head + [normalize, 1, subsample_depth, with_replacement, md]
+    elif entry.endswith("_v2") or entry.endswith("_v2t"):
+        args = head + [1, subsample_depth, with_replacement, md]
+    else:
+        args = head + [1, md]
+    st = f(*args, C.byref(res))
+    if st != 0:
+        raise SSUError(st, entry)
+    n = res.contents.n_samples
+    ids = _ids(res.contents.sample_ids, n)
+    out = np.ctypeslib.as_array(res.contents.matrix, shape=(n, n)).copy()
+    (L.destroy_mat_full_fp32 if fp32 else L.destroy_mat_full_fp64)(C.byref(res))
+    return out, ids
+
+
+def file_one_off(biom_path, tree_path, method, variance_adjust=False, alpha=1.0, bypass_tips=False,
+                 normalize=True):
+    """one_off_v3: the condensed matrix.  Returns (condensed, ids)."""
+    L = lib()
+    res = C.POINTER(Mat)()
+    st = L.one_off_v3(str(biom_path).encode(), str(tree_path).encode(), method.encode(), variance_adjust, alpha,
+                      bypass_tips, normalize, 1, C.byref(res))
+    if st != 0:
+        raise SSUError(st, "one_off_v3")
+    m = res.contents
+    cf = np.ctypeslib.as_array(m.condensed_form, shape=(max(m.cf_size, 1),))[:m.cf_size].copy()
+    ids = _ids(m.sample_ids, m.n_samples)
+    L.destroy_mat(C.byref(res))
+    return cf, ids
+
+
+def file_partial(biom_path, tree_path, method, stripe_start, stripe_stop, variance_adjust=False, alpha=1.0,
+                 bypass_tips=False, normalize=True):
+    """partial_v3: stripes [start, stop) as a (stop - start, n) array, ids."""
+    L = lib()
+    res = C.POINTER(PartialMat)()
+    st = L.partial_v3(str(biom_path).encode(), str(tree_path).encode(), method.encode(), variance_adjust, alpha,
+                      bypass_tips, normalize, 1, stripe_start, stripe_stop, C.byref(res))
+    if st != 0:
+        raise SSUError(st, "partial_v3")
+    p = res.contents
+    n = p.n_samples
+    out = np.array([np.ctypeslib.as_array(p.stripes[s], shape=(n,)).copy()
+                    for s in range(p.stripe_stop - p.stripe_start)])
+    ids = _ids(p.sample_ids, n)
+    L.destroy_partial_mat(C.byref(res))
+    return out, ids
+
+
+def file_faith_pd(biom_path, tree_path):
+    """faith_pd_one_off: (values, ids)."""
+    L = lib()
+    res = C.POINTER(RVec)()
+    st = L.faith_pd_one_off(str(biom_path).encode(), str(tree_path).encode(), C.byref(res))
+    if st != 0:
+        raise SSUError(st, "faith_pd_one_off")
+    r = res.contents
+    vals = np.ctypeslib.as_array(r.values, shape=(r.n_samples,)).copy()
+    ids = _ids(r.sample_ids, r.n_samples)
+    L.destroy_results_vec(C.byref(res))
+    return vals, ids
 
 
 def shear_collapse(tree, names=None, collapse=True):
