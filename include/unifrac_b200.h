@@ -331,6 +331,21 @@ SSU_EXTERN MergeStatus merge_partial_to_mmap_matrix_fp32(partial_dyn_mat_t **par
 SSU_EXTERN IOStatus ssu_b200_read_biom(const char *biom_filename, support_biom_t **table);
 SSU_EXTERN void ssu_b200_destroy_biom(support_biom_t **table);
 
+/* n_subsamples rarefied replicates of a table, drawn on the GPU: samples with
+ * a total below `depth` dropped, each kept sample reduced to `depth` counts
+ * drawn without replacement (integer-truncated counts, every subset of units
+ * equally likely; all units kept when fewer than depth) or with replacement
+ * (counts as weights), observations left without counts dropped - the rules
+ * of su::skbio_biom_subsampled (src/biom_subsampled.cpp:287-353), whose
+ * random stream (libstdc++, thread-count dependent) is not reproduced.
+ * Replicate r depends only on seed + r (ssu_set_random_seed) and the
+ * sample; the subsample_depth of one_off_matrix_inmem_v3 and of the file
+ * calls draws replicate 0.  results[0..n_subsamples) receive malloc'ed tables to release with
+ * ssu_b200_destroy_biom.  The ssu_b200_subsample_batch_* calls use the same
+ * draws. */
+SSU_EXTERN ComputeStatus ssu_b200_rarefy_batch(const support_biom_t *table, unsigned int n_subsamples,
+                                               unsigned int depth, bool with_replacement, support_biom_t **results);
+
 /* one_off / partial / faith_pd_one_off over in-memory inputs: the compute
  * paths of the file-based calls above without the file parsing.  Method names,
  * statuses and result layouts are those of the file-based calls.  An
@@ -447,10 +462,11 @@ SSU_EXTERN ComputeStatus ssu_b200_one_off_batch_inmem_fp32_v3(const support_biom
                                                               bool normalize_sample_counts,
                                                               mat_full_fp32_t **results);
 /* The compute part of unifrac_multi_to_file_v3 in memory: n_subsamples
- * replicates of table_data, each rarefied to subsample_depth with this
- * library's sampler (seeded by ssu_set_random_seed's seed + replicate
- * index), computed as one batch; results[r] holds replicate r's matrix over
- * the samples that reached the depth. */
+ * replicates of table_data, each rarefied to subsample_depth on the GPU
+ * (ssu_b200_rarefy_batch's draws: replicate r under seed s is what
+ * one_off_matrix_inmem_v3's subsample_depth draws under seed s + r),
+ * computed as one batch; results[r] holds replicate r's matrix over the
+ * samples that reached the depth. */
 SSU_EXTERN ComputeStatus ssu_b200_subsample_batch_inmem_v3(const support_biom_t *table_data,
                                                            const support_bptree_t *tree_data,
                                                            const char *unifrac_method, bool variance_adjust,

@@ -33,6 +33,7 @@
 #include "ssu_biom.hpp"
 #include "ssu_engine.hpp"
 #include "ssu_partial.hpp"
+#include "ssu_rarefy.hpp"
 #include "ssu_table.hpp"
 #include "ssu_tree.hpp"
 
@@ -496,6 +497,23 @@ ComputeStatus full_matrix(const ssu::Table &table, const ssu::BPTree &tree, cons
     return okay;
 }
 
+// skbio_biom_subsampled (src/biom_subsampled.cpp:287-353) once, drawn on the
+// device with the current seed (the replicate-batch calls' replicate 0).
+ComputeStatus rarefied_once(const ssu::Table &table, unsigned int depth, bool with_replacement, ssu::Table &out) {
+    std::string err;
+    if (!select_device(err)) {
+        report("device", err);
+        return output_error;
+    }
+    std::vector<ssu::Table> reps;
+    if (ssu::rarefy_on_device(table, depth, with_replacement, g_seed.load(), 1, reps, err)) {
+        report("subsample", err);
+        return output_error;
+    }
+    out = std::move(reps[0]);
+    return out.n_samples == 0 || out.n_obs == 0 ? table_empty : okay;
+}
+
 // one_off_matrix_v3_T (src/api.cpp:700-717): optional rarefaction first.
 template <class TReal, class TMat>
 ComputeStatus full_matrix_v3(const support_biom_t *table_data, const support_bptree_t *tree_data, const Request &r,
@@ -516,8 +534,9 @@ ComputeStatus full_matrix_v3(const support_biom_t *table_data, const support_bpt
     timer.step("validate");
     if (st != okay) return st;
     if (subsample_depth > 0) {
-        ssu::Table sub = table.rarefied(subsample_depth, with_replacement, g_seed.load());
-        if (sub.n_samples == 0 || sub.n_obs == 0) return table_empty;
+        ssu::Table sub;
+        st = rarefied_once(table, subsample_depth, with_replacement, sub);
+        if (st != okay) return st;
         return full_matrix<TReal, TMat>(sub, tree, r, mmap_dir, result);
     }
     return full_matrix<TReal, TMat>(table, tree, r, mmap_dir, result);
@@ -699,24 +718,16 @@ ComputeStatus subsample_batch_v3(const support_biom_t *table_data, const support
     read_inputs(table_data, tree_data, table, tree);
     st = validate(table, tree);
     if (st != okay) return st;
-    // Replicate i draws from its own stream (seed + i), so the replicates are
-    // rarefied on host threads, each bit-identical to a serial pass.  Each
-    // draw holds temporaries of about three times the table's entries, so the
-    // thread count is bounded by a 4 GiB budget for them as well as by
-    // host_threads (OMP_NUM_THREADS / affinity, at most 16).
-    std::vector<ssu::Table> reps(n_subsamples);
-    const uint64_t seed = g_seed.load();
-    const size_t per_draw = 3 * (table.nnz() * (sizeof(double) + sizeof(uint32_t)) +
-                                 static_cast<size_t>(depth) * table.n_samples * sizeof(uint32_t)) + 1;
-    const unsigned by_memory = static_cast<unsigned>(std::max<size_t>(1, (size_t(4) << 30) / per_draw));
-    try {
-        parallel_for(n_subsamples, std::min(host_threads(16), by_memory),
-                     [&](unsigned i) { reps[i] = table.rarefied(depth, with_replacement, seed + i); });
-    } catch (const std::bad_alloc &) {
-        report("subsample", "out of host memory while rarefying");
+    // The replicates are drawn on the device (ssu_rarefy.cu): replicate i's
+    // draws depend only on the seed, i and the sample.
+    std::string err;
+    if (!select_device(err)) {
+        report("device", err);
         return output_error;
-    } catch (const std::exception &e) {
-        report("subsample", e.what());
+    }
+    std::vector<ssu::Table> reps;
+    if (ssu::rarefy_on_device(table, depth, with_replacement, g_seed.load(), n_subsamples, reps, err)) {
+        report("subsample", err);
         return output_error;
     }
     for (const ssu::Table &t : reps)
@@ -1256,8 +1267,9 @@ ComputeStatus file_matrix(ComputeStatus loaded, const ssu::Table &table, const s
     if (!result) return output_error;
     if (mmap_dir && mmap_dir[0] == 0) mmap_dir = nullptr;
     if (subsample_depth > 0) {
-        ssu::Table sub = table.rarefied(subsample_depth, with_replacement, g_seed.load());
-        if (sub.n_samples == 0 || sub.n_obs == 0) return table_empty;
+        ssu::Table sub;
+        const ComputeStatus st = rarefied_once(table, subsample_depth, with_replacement, sub);
+        if (st != okay) return st;
         return full_matrix<TReal, TMat>(sub, tree, r, mmap_dir, result);
     }
     return full_matrix<TReal, TMat>(table, tree, r, mmap_dir, result);
@@ -1421,6 +1433,48 @@ IOStatus ssu_b200_read_biom(const char *biom_filename, support_biom_t **table) {
     std::memcpy(b->data, t.data, sizeof(double) * t.nnz());
     *table = b;
     return read_okay;
+}
+
+ComputeStatus ssu_b200_rarefy_batch(const support_biom_t *table_data, unsigned int n_subsamples,
+                                    unsigned int depth, bool with_replacement, support_biom_t **results) {
+    if (!table_data || table_data->n_samples <= 0 || table_data->n_obs <= 0 || n_subsamples == 0 || depth == 0 ||
+        !results)
+        return table_empty;
+    ssu::Table table = table_from(table_data);
+    if (table.malformed) {
+        report("table", "malformed CSR (offsets or sample positions out of range)");
+        return table_missing;
+    }
+    std::string err;
+    if (!select_device(err)) {
+        report("device", err);
+        return output_error;
+    }
+    std::vector<ssu::Table> reps;
+    if (ssu::rarefy_on_device(table, depth, with_replacement, g_seed.load(), n_subsamples, reps, err)) {
+        report("subsample", err);
+        return output_error;
+    }
+    for (unsigned int r = 0; r < n_subsamples; r++) {
+        const ssu::Table &t = reps[r];
+        support_biom_t *b = static_cast<support_biom_t *>(std::calloc(1, sizeof(support_biom_t)));
+        b->n_obs = static_cast<int>(t.n_obs);
+        b->n_samples = static_cast<int>(t.n_samples);
+        b->nnz = static_cast<int>(t.nnz());
+        b->obs_ids = copy_ids(t.obs_ids);
+        b->sample_ids = copy_ids(t.sample_ids);
+        b->indptr = static_cast<uint32_t *>(std::malloc(sizeof(uint32_t) * (t.n_obs + 1)));
+        b->indices = static_cast<uint32_t *>(std::malloc(sizeof(uint32_t) * std::max<uint64_t>(t.nnz(), 1)));
+        b->data = static_cast<double *>(std::malloc(sizeof(double) * std::max<uint64_t>(t.nnz(), 1)));
+        if (t.n_obs) std::memcpy(b->indptr, t.indptr, sizeof(uint32_t) * (t.n_obs + 1));
+        else b->indptr[0] = 0;
+        if (t.nnz()) {
+            std::memcpy(b->indices, t.indices, sizeof(uint32_t) * t.nnz());
+            std::memcpy(b->data, t.data, sizeof(double) * t.nnz());
+        }
+        results[r] = b;
+    }
+    return okay;
 }
 
 void ssu_b200_destroy_biom(support_biom_t **table) {

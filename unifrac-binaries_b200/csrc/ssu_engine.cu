@@ -1192,6 +1192,7 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
     append_tiles(tiles, 0, 0, tdesc[0].n, BM, BN, mode == 1, start, stop);
     uint4 *d_t = nullptr;
     SSU_CK(upload(&d_t, tiles.data(), sizeof(uint4) * tiles.size()));
+    // (the hybrid and union stages below also take the full matrix's splits)
     if (union_mode) {
         dev::OutSpec o{mode, d_out, start, stop};
         launches = 0;
@@ -1199,10 +1200,10 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
         int rc = 0;
         if (spec.fp64) {
             rc = embed<double>(stream, g);
-            if (!rc) rc = union_stage<double>(stream, g, o, d_t, nt, 1, true);
+            if (!rc) rc = union_stage<double>(stream, g, o, d_t, nt, g.splits, true);
         } else {
             rc = embed<float>(stream, g);
-            if (!rc) rc = union_stage<float>(stream, g, o, d_t, nt, 1, true);
+            if (!rc) rc = union_stage<float>(stream, g, o, d_t, nt, g.splits, true);
         }
         return rc;
     }
@@ -1214,23 +1215,19 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
         if (spec.fp64) {
             rc = embed<double>(stream, g);
             if (!rc) rc = prepare<double>(stream, g);
-            if (!rc) rc = hybrid_stage<double>(stream, g, o, d_t, nt, 1, true);
+            if (!rc) rc = hybrid_stage<double>(stream, g, o, d_t, nt, g.splits, true);
         } else {
             rc = embed<float>(stream, g);
             if (!rc) rc = prepare<float>(stream, g);
-            if (!rc) rc = hybrid_stage<float>(stream, g, o, d_t, nt, 1, true);
+            if (!rc) rc = hybrid_stage<float>(stream, g, o, d_t, nt, g.splits, true);
         }
         return rc;
     }
-    uint32_t s = 1, rows = 0;
-    if (spec.fp64)
-        choose_splits<double>(kd, static_cast<uint32_t>(tiles.size()), s, rows);
-    else
-        choose_splits<float>(kf, static_cast<uint32_t>(tiles.size()), s, rows);
-    // the window never holds more tiles than the full matrix, so the plan's
-    // partial buffer is large enough when the split count does not grow
-    const size_t per_tile = spec.fp64 ? kd.partial_per_tile * sizeof(double) : kf.partial_per_tile * sizeof(float);
-    if (s > 1 && per_tile * tiles.size() * s > partial_bytes) s = 1;
+    // the full matrix's node splits: every tile of the window sums its nodes
+    // in the same order as in the full matrix, so stripes of a window are
+    // bit-identical to the full matrix's (the window never holds more tiles,
+    // so the plan's partial buffer fits)
+    const uint32_t s = g.splits, rows = g.rows_per_split;
     dev::OutSpec o{mode, d_out, start, stop};
     launches = 0;
     const uint32_t nt = static_cast<uint32_t>(tiles.size());

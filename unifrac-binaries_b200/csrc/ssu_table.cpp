@@ -1,7 +1,6 @@
 // Host-side feature table: borrow, dense pair, filter, rarefy, totals.
 #include "ssu_table.hpp"
 
-#include <random>
 
 namespace ssu {
 
@@ -95,71 +94,6 @@ Table Table::filtered(double min_total) const {
         t.n_samples = 0;
     }
     t.adopt_owned();
-    return t;
-}
-
-Table Table::rarefied(uint32_t depth, bool with_replacement, uint64_t seed) const {
-    // sample-major view of the kept samples
-    std::vector<uint32_t> keep;
-    for (uint32_t j = 0; j < n_samples; j++)
-        if (totals[j] >= depth) keep.push_back(j);
-    std::vector<uint32_t> new_idx(n_samples, UINT32_MAX);
-    for (uint32_t jj = 0; jj < keep.size(); jj++) new_idx[keep[jj]] = jj;
-    std::vector<std::vector<std::pair<uint32_t, double>>> cols(keep.size());
-    for (uint32_t i = 0; i < n_obs; i++)
-        for (uint32_t q = indptr[i]; q < indptr[i + 1]; q++)
-            if (new_idx[indices[q]] != UINT32_MAX) cols[new_idx[indices[q]]].emplace_back(i, data[q]);
-
-    std::mt19937_64 gen(seed);
-    std::vector<std::vector<double>> sub(keep.size());
-    for (uint32_t jj = 0; jj < keep.size(); jj++) {
-        auto &col = cols[jj];
-        std::vector<double> out(col.size(), 0.0);
-        if (with_replacement) {
-            std::vector<double> w(col.size());
-            for (size_t e = 0; e < col.size(); e++) w[e] = col[e].second;
-            std::discrete_distribution<size_t> pick(w.begin(), w.end());
-            for (uint32_t d = 0; d < depth; d++) out[pick(gen)] += 1.0;
-        } else {
-            // `depth` draws without replacement from the multiset of integer
-            // counts: partial Fisher-Yates over the expanded items
-            std::vector<uint32_t> items;
-            for (size_t e = 0; e < col.size(); e++) {
-                const uint64_t c = static_cast<uint64_t>(col[e].second);
-                items.insert(items.end(), c, static_cast<uint32_t>(e));
-            }
-            for (uint32_t d = 0; d < depth && d < items.size(); d++) {
-                std::uniform_int_distribution<size_t> u(d, items.size() - 1);
-                std::swap(items[d], items[u(gen)]);
-                out[items[d]] += 1.0;
-            }
-        }
-        sub[jj] = std::move(out);
-    }
-    // back to observation-major, dropping observations left without counts
-    std::vector<std::vector<std::pair<uint32_t, double>>> rows(n_obs);
-    for (uint32_t jj = 0; jj < keep.size(); jj++)
-        for (size_t e = 0; e < cols[jj].size(); e++)
-            rows[cols[jj][e].first].emplace_back(jj, sub[jj][e]);
-    Table t;
-    t.n_samples = static_cast<uint32_t>(keep.size());
-    for (uint32_t jj = 0; jj < keep.size(); jj++) t.sample_ids.push_back(sample_ids[keep[jj]]);
-    t.own_indptr.push_back(0);
-    for (uint32_t i = 0; i < n_obs; i++) {
-        bool any = false;
-        for (auto &e : rows[i]) any = any || e.second > 0.0;
-        if (!any) continue;
-        for (auto &e : rows[i]) {
-            if (e.second <= 0.0) continue;
-            t.own_indices.push_back(e.first);
-            t.own_data.push_back(e.second);
-        }
-        t.obs_ids.push_back(obs_ids[i]);
-        t.own_indptr.push_back(static_cast<uint32_t>(t.own_indices.size()));
-    }
-    t.n_obs = static_cast<uint32_t>(t.obs_ids.size());
-    t.adopt_owned();
-    t.compute_totals();
     return t;
 }
 

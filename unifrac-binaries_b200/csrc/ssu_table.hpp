@@ -63,11 +63,6 @@ struct Table {
     // keep at least one entry (src/biom_inmem.cpp:284-338).  Totals are the
     // parent's.
     Table filtered(double min_total) const;
-    // Every sample with total >= depth subsampled to `depth` counts (without
-    // or with replacement); lighter samples and observations left without a
-    // positive count are dropped (src/biom_subsampled.cpp:287-353).  The
-    // random stream is this library's own.
-    Table rarefied(uint32_t depth, bool with_replacement, uint64_t seed) const;
 
     void compute_totals();
     std::unordered_map<std::string_view, uint32_t> obs_index() const;

@@ -136,6 +136,7 @@ def lib():
         L.merge_partial_to_mmap_matrix_fp32.argtypes = [P(P(PartialDynMat)), C.c_int, C.c_char_p,
                                                         PP(P(MatFull32))]
         L.ssu_b200_read_biom.argtypes = [C.c_char_p, PP(P(SupportBiom))]
+        L.ssu_b200_rarefy_batch.argtypes = [P(SupportBiom), C.c_uint, C.c_uint, C.c_bool, P(P(SupportBiom))]
         L.ssu_b200_destroy_biom.argtypes = [PP(P(SupportBiom))]
         L.ssu_b200_destroy_biom.restype = None
         fcommon = [C.c_char_p, C.c_void_p, C.c_char_p, C.c_bool, C.c_double, C.c_bool]
@@ -590,20 +591,40 @@ class OpaqueTree:
 
 def read_biom(path):
     """A BIOM-HDF5 table file as a synthetic-module Table (ssu_b200_read_biom)."""
-    import ssu_synth
     L = lib()
     res = C.POINTER(SupportBiom)()
     st = L.ssu_b200_read_biom(str(path).encode(), C.byref(res))
     if st != 0:
         raise RuntimeError(f"ssu_b200_read_biom: {IO_STATUS[st]}")
-    b = res.contents
-    nnz = b.nnz
-    t = ssu_synth.Table(_ids(b.obs_ids, b.n_obs), _ids(b.sample_ids, b.n_samples),
-                        np.ctypeslib.as_array(b.indptr, shape=(b.n_obs + 1,)).copy(),
-                        np.ctypeslib.as_array(b.indices, shape=(max(nnz, 1),))[:nnz].copy(),
-                        np.ctypeslib.as_array(b.data, shape=(max(nnz, 1),))[:nnz].copy())
+    t = _table_of(res.contents)
     L.ssu_b200_destroy_biom(C.byref(res))
     return t
+
+
+def _table_of(b):
+    import ssu_synth
+    nnz = b.nnz
+    return ssu_synth.Table(_ids(b.obs_ids, b.n_obs), _ids(b.sample_ids, b.n_samples),
+                           np.ctypeslib.as_array(b.indptr, shape=(b.n_obs + 1,)).copy(),
+                           np.ctypeslib.as_array(b.indices, shape=(max(nnz, 1),))[:nnz].copy(),
+                           np.ctypeslib.as_array(b.data, shape=(max(nnz, 1),))[:nnz].copy())
+
+
+def rarefy_batch(table, n_subsamples, depth, with_replacement=False):
+    """n_subsamples replicates of `table` rarefied to `depth` on the GPU
+    (ssu_b200_rarefy_batch), as synthetic-module Tables."""
+    L = lib()
+    x = TableInputs(table)
+    res = (C.POINTER(SupportBiom) * n_subsamples)()
+    st = L.ssu_b200_rarefy_batch(C.byref(x.biom), n_subsamples, depth, with_replacement, res)
+    if st != 0:
+        raise SSUError(st, "ssu_b200_rarefy_batch")
+    out = []
+    for r in range(n_subsamples):
+        out.append(_table_of(res[r].contents))
+        p = C.POINTER(SupportBiom)(res[r].contents)
+        L.ssu_b200_destroy_biom(C.byref(p))
+    return out
 
 
 def file_matrix(entry, biom_path, tree, method, variance_adjust=False, alpha=1.0, bypass_tips=False,
