@@ -8,11 +8,11 @@
  * reference declaration it replaces.  Results are allocated by the library
  * with malloc and released only through the matching destroy_*() call.
  *
- * The file-based entry points (one_off, partial, faith_pd_one_off, ...) read
- * BIOM-HDF5 tables.  This build has no HDF5 library: they check that both
- * files exist (table_missing / tree_missing as the reference), parse the
- * newick tree, and report table_missing for the table with a message on
- * stderr.  The in-memory entry points carry the whole compute path.
+ * The file-based entry points (one_off, one_off_matrix*, partial,
+ * faith_pd_one_off) read BIOM 2.x HDF5 tables with the library's own reader
+ * of the HDF5 subset such files use (no HDF5 library) and newick trees;
+ * missing or unreadable files give table_missing / tree_missing as the
+ * reference, with a message on stderr.
  *
  * The second part (ssu_b200_*) has no counterpart in the reference: in-memory
  * forms of one_off / partial / faith_pd, and a device-resident plan for
@@ -499,6 +499,75 @@ SSU_EXTERN uint64_t ssu_b200_plan_table_embedded(const ssu_b200_plan_t *plan, ui
 SSU_EXTERN void ssu_b200_plan_set_graph(ssu_b200_plan_t *plan, int enable);
 /* How the pair kernel's tile shape was chosen, and the shape. */
 SSU_EXTERN const char *ssu_b200_plan_tuning(const ssu_b200_plan_t *plan);
+
+/* ---- statistics on the distance matrix, on the device ------------------
+ *
+ * The reference hands these to scikit-bio-binaries (src/skbio_alt.cpp:144-234).
+ * Matrices are n_samples x n_samples row-major, in host memory (copied to the
+ * device) or device memory (read in place); arithmetic is fp64 throughout.
+ * PCoA: the eigenpairs of the Gower-centred -D^2/2 by randomized subspace
+ * iteration (Halko, Martinsson and Tropp, 10 extra columns, Rayleigh-Ritz
+ * after every multiply, stopped when the wanted Ritz values settle to 1e-12
+ * of the largest), the method of scikit-bio's "fsvd" carried to convergence
+ * (the reference's fsvd stops after a fixed few steps); each axis has its
+ * largest-magnitude entry positive (the reference's signs are arbitrary).
+ * Outputs are malloc'ed, released with free(); after a failure (reported on
+ * stderr) they are NULL. */
+
+/* src/api.hpp:1008-1010 (C++ linkage there).  eigenvalues[n_dims] descending,
+ * samples[n_samples][n_dims] = eigenvector * sqrt(eigenvalue),
+ * proportion_explained[n_dims] = eigenvalue / trace of the centred matrix. */
+SSU_EXTERN void pcoa(const double *mat, const uint32_t n_samples, const uint32_t n_dims, double **eigenvalues,
+                     double **samples, double **proportion_explained);
+SSU_EXTERN void pcoa_fp32(const float *mat, const uint32_t n_samples, const uint32_t n_dims, float **eigenvalues,
+                          float **samples, float **proportion_explained);
+SSU_EXTERN void pcoa_mixed(const double *mat, const uint32_t n_samples, const uint32_t n_dims,
+                           float **eigenvalues, float **samples, float **proportion_explained);
+/* src/api.hpp:1001-1002, src/api.cpp:2501-2507 (C++ linkage there; the header
+ * names the fp32 form find_eigens_fast_p32, the source find_eigens_fast_fp32,
+ * which is the one defined).  The n_dims largest eigenpairs of an already
+ * centred symmetric matrix: eigenvectors[n_samples][n_dims], unit length.
+ * The matrix is not modified. */
+SSU_EXTERN void find_eigens_fast(const uint32_t n_samples, const uint32_t n_dims, double *centered,
+                                 double **eigenvalues, double **eigenvectors);
+SSU_EXTERN void find_eigens_fast_fp32(const uint32_t n_samples, const uint32_t n_dims, float *centered,
+                                      float **eigenvalues, float **eigenvectors);
+/* src/api.hpp:616-638.  For each of the n_columns grouping columns of the
+ * metadata TSV (header line, first field the sample id, tab-separated, as
+ * src/tsv.cpp:118-180 reads it): scikit-bio's PERMANOVA pseudo-F over the
+ * matrix's upper triangle and its p-value from permanova_perms permutations
+ * ((1 + #F_perm >= F) / (1 + perms); NaN with no permutations), drawn from
+ * the library seed (ssu_set_random_seed) + column index.  grouping_missing
+ * when the file, a column or a sample's line is missing (the reference does
+ * not check the first sample; this checks all).  F and p are NaN when there
+ * are fewer than 2 groups or as many groups as samples. */
+SSU_EXTERN ComputeStatus compute_permanova_fp64(const char *grouping_filename, unsigned int n_columns,
+                                                const char **columns, mat_full_fp64_t *result,
+                                                unsigned int permanova_perms, double *fstats, double *pvalues);
+SSU_EXTERN ComputeStatus compute_permanova_fp32(const char *grouping_filename, unsigned int n_columns,
+                                                const char **columns, mat_full_fp32_t *result,
+                                                unsigned int permanova_perms, float *fstats, float *pvalues);
+/* The grouping column alone: grouping[n_samples] receives group numbers
+ * 0, 1, ... in the order their values first appear in the file. */
+SSU_EXTERN ComputeStatus ssu_b200_read_grouping(const char *grouping_filename, const char *column,
+                                                uint32_t n_samples, const char *const *sample_ids,
+                                                uint32_t *grouping, uint32_t *n_groups);
+/* PERMANOVA of one grouping given as labels (any values; at most 65535
+ * distinct), permutations from the library seed. */
+SSU_EXTERN ComputeStatus ssu_b200_permanova_fp64(const double *mat, uint32_t n_samples, const uint32_t *grouping,
+                                                 unsigned int permanova_perms, double *fstat, double *pvalue);
+SSU_EXTERN ComputeStatus ssu_b200_permanova_fp32(const float *mat, uint32_t n_samples, const uint32_t *grouping,
+                                                 unsigned int permanova_perms, float *fstat, float *pvalue);
+/* One dataset of an HDF5 file of the subset BIOM files and the reference's
+ * outputs use (src/api.cpp:1160-1290: "matrix", "order", "pcoa_eigvals",
+ * "pcoa_samples", "pcoa_proportion_explained", "stat_*"): numbers as
+ * malloc'ed doubles in row-major order with rank and dims[0..rank) (rank <= 8),
+ * strings as a malloc'ed array released with ssu_b200_free_h5_strings. */
+SSU_EXTERN IOStatus ssu_b200_read_h5_doubles(const char *filename, const char *dataset, double **values,
+                                             uint32_t *rank, uint64_t *dims);
+SSU_EXTERN IOStatus ssu_b200_read_h5_strings(const char *filename, const char *dataset, char ***strings,
+                                             uint64_t *n);
+SSU_EXTERN void ssu_b200_free_h5_strings(char **strings, uint64_t n);
 
 /* Name of the kernel family the plan's pair stage launches (for profiling). */
 SSU_EXTERN const char *ssu_b200_plan_pair_kernel(const ssu_b200_plan_t *plan);

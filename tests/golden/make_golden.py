@@ -20,7 +20,19 @@ expected outputs the reference compares against):
 * src/testdata/absquant.biom, absquant.tree and the weighted-normalized
   matrices without and with sample-count normalisation
   (test.absquant.wn.dm, test.absquant_not.wn.dm);
-* src/test.biom, the 6 x 5 table of the reference's unit tests.
+* src/test.biom, the 6 x 5 table of the reference's unit tests;
+* src/test_ska_pcoa_big.dat (57 x 57 matrix with its PCoA, test_pcoa_big),
+  src/testdata/test500.tsv (sample metadata) and two of the reference's
+  HDF5 outputs on its 500-sample table (distance matrix, sample order and
+  4-axis PCoA): test500.unweighted_fp32.f.h5 and
+  test500.weighted_unnormalized_fp32.h5.
+
+From src/test_ska.cpp (the statistics tests) it keeps, per test function,
+every numeric array and every `exp_*` scalar; from
+src/testdata/validation_tests.sh every PERMANOVA check
+(compare_unifrac_stats.py arguments with the method and grouping column of
+the ssu run before it) and every PCoA check (compare_unifrac_pcoa.py: file,
+axes compared, relative precision).
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 (default: $UNIFRAC_REFERENCE_PATH, else BASELINE.json's reference_path)
@@ -108,6 +120,49 @@ def parse_test_su(path):
     return out
 
 
+def parse_test_ska(path):
+    text = open(path).read()
+    out = {}
+    for name, body in _split_functions(text).items():
+        entry = {"arrays": {}, "scalars": {}}
+        for m in re.finditer(r"(?:const\s+)?(double|float|uint32_t)\s+(\w+)\s*\[\d*\]\s*=\s*\{([^}]*)\}", body):
+            vals = _numbers(m.group(3))
+            if vals is not None:
+                entry["arrays"].setdefault(m.group(2), []).append(vals)
+        for m in re.finditer(r"(?:const\s+)?(?:float|double)\s+(exp_\w+)\s*=\s*([-+0-9.eE]+)\s*;", body):
+            entry["scalars"][m.group(1)] = float(m.group(2))
+        if entry["arrays"] or entry["scalars"]:
+            out[name] = entry
+    return out
+
+
+def parse_validation(path):
+    """PERMANOVA and PCoA checks of validation_tests.sh."""
+    stats, pcoa = [], []
+    method = column = perms = None
+    for line in open(path):
+        m = re.search(r"\bssu\s.*?-m\s+(\S+)", line)
+        if m:
+            method = m.group(1)
+            c = re.search(r"\s-c\s+(\S+)", line)
+            column = c.group(1) if c else None
+            q = re.search(r"--permanova\s+(\d+)", line)
+            perms = int(q.group(1)) if q else None
+            continue
+        m = re.search(r"compare_unifrac_stats\.py\s+\S+\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)\s+(\S+)", line)
+        if m:
+            g, n, v, pv, pr_v, pr_p = m.groups()
+            stats.append({"method": method, "column": column, "permanova_flag": perms, "n_groups": int(g),
+                          "n_perms": int(n), "value": float(v), "pvalue": float(pv), "prec_value": float(pr_v),
+                          "prec_pvalue": float(pr_p)})
+            continue
+        m = re.search(r"compare_unifrac_pcoa\.py\s+(\S+)\s+\S+\s+(\d+)\s+(\S+)", line)
+        if m:
+            pcoa.append({"method": method, "expected": m.group(1), "axes": int(m.group(2)),
+                         "precision": float(m.group(3))})
+    return {"permanova": stats, "pcoa": pcoa}
+
+
 def parse_capi_inmem(path):
     text = open(path).read()
 
@@ -134,6 +189,8 @@ def main():
         "test_su": parse_test_su(os.path.join(REF, "src", "test_su.cpp")),
         "table_csr": parse_capi_inmem(os.path.join(REF, "test", "capi_inmem_test.c")),
         "trees": {},
+        "test_ska": parse_test_ska(os.path.join(REF, "src", "test_ska.cpp")),
+        "validation": parse_validation(os.path.join(REF, "src", "testdata", "validation_tests.sh")),
     }
     for fn in sorted(os.listdir(os.path.join(REF, "src"))):
         if fn.endswith(".tre"):
@@ -153,7 +210,9 @@ def main():
 
 FIXTURES = ["ci/crawford.biom", "ci/crawford.tre", "ci/test.ssu.exp", "ci/test.ssu_vaw.exp", "ci/test.faith.exp",
             "src/testdata/absquant.biom", "src/testdata/absquant.tree", "src/testdata/test.absquant.wn.dm",
-            "src/testdata/test.absquant_not.wn.dm", "src/test.biom"]
+            "src/testdata/test.absquant_not.wn.dm", "src/test.biom", "src/test_ska_pcoa_big.dat",
+            "src/testdata/test500.tsv", "src/testdata/test500.unweighted_fp32.f.h5",
+            "src/testdata/test500.weighted_unnormalized_fp32.h5"]
 
 
 if __name__ == "__main__":

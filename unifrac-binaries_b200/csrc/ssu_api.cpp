@@ -32,8 +32,10 @@
 
 #include "ssu_biom.hpp"
 #include "ssu_engine.hpp"
+#include "ssu_grouping.hpp"
 #include "ssu_partial.hpp"
 #include "ssu_rarefy.hpp"
+#include "ssu_stats.hpp"
 #include "ssu_table.hpp"
 #include "ssu_tree.hpp"
 
@@ -1730,5 +1732,244 @@ const char *ssu_b200_plan_pair_kernel(const ssu_b200_plan_t *plan) {
 }
 
 const char *ssu_b200_version(void) { return "unifrac-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"
+
+// ============================================= PCoA and PERMANOVA (device)
+
+namespace {
+
+template <typename TOut>
+void free_outputs(TOut **a, TOut **b, TOut **c) {
+    for (TOut **p : {a, b, c}) {
+        std::free(*p);
+        *p = nullptr;
+    }
+}
+
+// src/api.cpp:2537-2547 (su::pcoa, src/skbio_alt.cpp:176-199): malloc'ed
+// eigenvalues[n_dims], samples[n_samples][n_dims], proportion[n_dims]; all
+// three NULL after a failure (reported on stderr).
+template <typename TOut, typename TIn>
+void pcoa_T(const TIn *mat, uint32_t n, uint32_t dims, TOut **eigenvalues, TOut **samples, TOut **proportion) {
+    if (!eigenvalues || !samples || !proportion) return;
+    const size_t nd = static_cast<size_t>(n) * dims;
+    *eigenvalues = static_cast<TOut *>(std::malloc(sizeof(TOut) * std::max<size_t>(dims, 1)));
+    *samples = static_cast<TOut *>(std::malloc(sizeof(TOut) * std::max<size_t>(nd, 1)));
+    *proportion = static_cast<TOut *>(std::malloc(sizeof(TOut) * std::max<size_t>(dims, 1)));
+    if (!*eigenvalues || !*samples || !*proportion) {
+        free_outputs(eigenvalues, samples, proportion);
+        report("pcoa", "out of host memory");
+        return;
+    }
+    std::string err;
+    try {
+        if (!mat && n) throw std::invalid_argument("no matrix");
+        if (!select_device(err)) throw std::runtime_error(err);
+        std::vector<double> ev(dims), sm(nd), pr(dims);
+        if (ssu::pcoa_device(mat, n, dims, ev.data(), sm.data(), pr.data(), err)) throw std::runtime_error(err);
+        for (uint32_t c = 0; c < dims; c++) {
+            (*eigenvalues)[c] = static_cast<TOut>(ev[c]);
+            (*proportion)[c] = static_cast<TOut>(pr[c]);
+        }
+        for (size_t k = 0; k < nd; k++) (*samples)[k] = static_cast<TOut>(sm[k]);
+    } catch (const std::exception &e) {
+        free_outputs(eigenvalues, samples, proportion);
+        report("pcoa", e.what());
+    }
+}
+
+// src/api.cpp:2501-2507 (su::find_eigens_fast): eigenvalues[n_dims] and
+// unit eigenvectors[n_samples][n_dims] of an already centred matrix.
+template <typename TReal>
+void eigens_T(uint32_t n, uint32_t dims, const TReal *centered, TReal **eigenvalues, TReal **eigenvectors) {
+    if (!eigenvalues || !eigenvectors) return;
+    const size_t nd = static_cast<size_t>(n) * dims;
+    *eigenvalues = static_cast<TReal *>(std::malloc(sizeof(TReal) * std::max<size_t>(dims, 1)));
+    *eigenvectors = static_cast<TReal *>(std::malloc(sizeof(TReal) * std::max<size_t>(nd, 1)));
+    std::string err;
+    try {
+        if (!*eigenvalues || !*eigenvectors) throw std::runtime_error("out of host memory");
+        if (!centered && n) throw std::invalid_argument("no matrix");
+        if (!select_device(err)) throw std::runtime_error(err);
+        std::vector<double> ev(dims), vec(nd);
+        if (ssu::eigens_device(centered, n, dims, ev.data(), vec.data(), err)) throw std::runtime_error(err);
+        for (uint32_t c = 0; c < dims; c++) (*eigenvalues)[c] = static_cast<TReal>(ev[c]);
+        for (size_t k = 0; k < nd; k++) (*eigenvectors)[k] = static_cast<TReal>(vec[k]);
+    } catch (const std::exception &e) {
+        std::free(*eigenvalues);
+        std::free(*eigenvectors);
+        *eigenvalues = nullptr;
+        *eigenvectors = nullptr;
+        report("find_eigens_fast", e.what());
+    }
+}
+
+// Labels of any values renumbered 0, 1, ... by first appearance.
+uint32_t dense_labels(const uint32_t *grouping, uint32_t n, std::vector<uint32_t> &out) {
+    std::unordered_map<uint32_t, uint32_t> ids;
+    out.resize(n);
+    for (uint32_t i = 0; i < n; i++)
+        out[i] = ids.emplace(grouping[i], static_cast<uint32_t>(ids.size())).first->second;
+    return static_cast<uint32_t>(ids.size());
+}
+
+template <typename TReal>
+ComputeStatus permanova_T(const TReal *mat, uint32_t n, const uint32_t *grouping, uint32_t n_groups,
+                          unsigned int perms, uint64_t seed, TReal &fstat, TReal &pvalue) {
+    std::string err;
+    try {
+        if (!select_device(err)) throw std::runtime_error(err);
+        double f = 0.0, p = 0.0;
+        if (ssu::permanova_device(mat, n, grouping, n_groups, perms, seed, f, p, err)) throw std::runtime_error(err);
+        fstat = static_cast<TReal>(f);
+        pvalue = static_cast<TReal>(p);
+        return okay;
+    } catch (const std::exception &e) {
+        report("permanova", e.what());
+        return output_error;
+    }
+}
+
+// src/api.cpp:949-975: each grouping column read from the TSV (any failure:
+// grouping_missing) and tested on the matrix.  Column i's permutations are
+// drawn from the library seed (ssu_set_random_seed) + i.
+template <typename TReal, typename TMat>
+ComputeStatus compute_permanova_T(const char *grouping_filename, unsigned int n_columns, const char **columns,
+                                  TMat *result, unsigned int perms, TReal *fstats, TReal *pvalues) {
+    if (!result || !result->matrix || !result->sample_ids || (n_columns && (!columns || !fstats || !pvalues)))
+        return grouping_missing;
+    if (!grouping_filename || !file_exists(grouping_filename)) return grouping_missing;
+    std::vector<uint32_t> grouping;
+    for (unsigned int i = 0; i < n_columns; i++) {
+        uint32_t n_groups = 0;
+        std::string err;
+        if (!columns[i] || !ssu::read_grouping_tsv(grouping_filename, columns[i], result->n_samples,
+                                                   result->sample_ids, grouping, n_groups, err)) {
+            report("grouping", err);
+            return grouping_missing;
+        }
+        const ComputeStatus st = permanova_T<TReal>(result->matrix, result->n_samples, grouping.data(), n_groups,
+                                                    perms, g_seed.load() + i, fstats[i], pvalues[i]);
+        if (st != okay) return st;
+    }
+    return okay;
+}
+
+}  // namespace
+
+extern "C" {
+
+void pcoa(const double *mat, const uint32_t n_samples, const uint32_t n_dims, double **eigenvalues,
+          double **samples, double **proportion_explained) {
+    pcoa_T<double>(mat, n_samples, n_dims, eigenvalues, samples, proportion_explained);
+}
+
+void pcoa_fp32(const float *mat, const uint32_t n_samples, const uint32_t n_dims, float **eigenvalues,
+               float **samples, float **proportion_explained) {
+    pcoa_T<float>(mat, n_samples, n_dims, eigenvalues, samples, proportion_explained);
+}
+
+void pcoa_mixed(const double *mat, const uint32_t n_samples, const uint32_t n_dims, float **eigenvalues,
+                float **samples, float **proportion_explained) {
+    pcoa_T<float>(mat, n_samples, n_dims, eigenvalues, samples, proportion_explained);
+}
+
+void find_eigens_fast(const uint32_t n_samples, const uint32_t n_dims, double *centered, double **eigenvalues,
+                      double **eigenvectors) {
+    eigens_T<double>(n_samples, n_dims, centered, eigenvalues, eigenvectors);
+}
+
+void find_eigens_fast_fp32(const uint32_t n_samples, const uint32_t n_dims, float *centered, float **eigenvalues,
+                           float **eigenvectors) {
+    eigens_T<float>(n_samples, n_dims, centered, eigenvalues, eigenvectors);
+}
+
+ComputeStatus compute_permanova_fp64(const char *grouping_filename, unsigned int n_columns, const char **columns,
+                                     mat_full_fp64_t *result, unsigned int permanova_perms, double *fstats,
+                                     double *pvalues) {
+    return compute_permanova_T<double>(grouping_filename, n_columns, columns, result, permanova_perms, fstats,
+                                       pvalues);
+}
+
+ComputeStatus compute_permanova_fp32(const char *grouping_filename, unsigned int n_columns, const char **columns,
+                                     mat_full_fp32_t *result, unsigned int permanova_perms, float *fstats,
+                                     float *pvalues) {
+    return compute_permanova_T<float>(grouping_filename, n_columns, columns, result, permanova_perms, fstats,
+                                      pvalues);
+}
+
+ComputeStatus ssu_b200_read_grouping(const char *grouping_filename, const char *column, uint32_t n_samples,
+                                     const char *const *sample_ids, uint32_t *grouping, uint32_t *n_groups) {
+    if (!grouping_filename || !column || (n_samples && (!sample_ids || !grouping)) || !n_groups)
+        return grouping_missing;
+    std::vector<uint32_t> g;
+    std::string err;
+    if (!ssu::read_grouping_tsv(grouping_filename, column, n_samples, sample_ids, g, *n_groups, err)) {
+        report("grouping", err);
+        return grouping_missing;
+    }
+    std::copy(g.begin(), g.end(), grouping);
+    return okay;
+}
+
+ComputeStatus ssu_b200_permanova_fp64(const double *mat, uint32_t n_samples, const uint32_t *grouping,
+                                      unsigned int permanova_perms, double *fstat, double *pvalue) {
+    if (!mat || !grouping || !fstat || !pvalue) return output_error;
+    std::vector<uint32_t> labels;
+    const uint32_t g = dense_labels(grouping, n_samples, labels);
+    return permanova_T<double>(mat, n_samples, labels.data(), g, permanova_perms, g_seed.load(), *fstat, *pvalue);
+}
+
+ComputeStatus ssu_b200_permanova_fp32(const float *mat, uint32_t n_samples, const uint32_t *grouping,
+                                      unsigned int permanova_perms, float *fstat, float *pvalue) {
+    if (!mat || !grouping || !fstat || !pvalue) return output_error;
+    std::vector<uint32_t> labels;
+    const uint32_t g = dense_labels(grouping, n_samples, labels);
+    return permanova_T<float>(mat, n_samples, labels.data(), g, permanova_perms, g_seed.load(), *fstat, *pvalue);
+}
+
+IOStatus ssu_b200_read_h5_doubles(const char *filename, const char *dataset, double **values, uint32_t *rank,
+                                  uint64_t *dims) {
+    if (!filename || !dataset || !values || !rank || !dims) return read_error;
+    *values = nullptr;
+    *rank = 0;
+    if (!file_exists(filename)) return open_error;
+    ssu::H5Data d;
+    std::string err;
+    if (!ssu::read_hdf5_dataset(filename, dataset, d, err) || d.is_string || d.dims.size() > 8) {
+        report("hdf5", std::string(filename) + ":" + dataset + ": " + (err.empty() ? "not a numeric dataset" : err));
+        return read_error;
+    }
+    *values = static_cast<double *>(std::malloc(sizeof(double) * std::max<size_t>(d.values.size(), 1)));
+    if (!*values) return read_error;
+    std::copy(d.values.begin(), d.values.end(), *values);
+    *rank = static_cast<uint32_t>(d.dims.size());
+    std::copy(d.dims.begin(), d.dims.end(), dims);
+    return read_okay;
+}
+
+IOStatus ssu_b200_read_h5_strings(const char *filename, const char *dataset, char ***strings, uint64_t *n) {
+    if (!filename || !dataset || !strings || !n) return read_error;
+    *strings = nullptr;
+    *n = 0;
+    if (!file_exists(filename)) return open_error;
+    ssu::H5Data d;
+    std::string err;
+    if (!ssu::read_hdf5_dataset(filename, dataset, d, err) || !d.is_string) {
+        report("hdf5", std::string(filename) + ":" + dataset + ": " + (err.empty() ? "not a string dataset" : err));
+        return read_error;
+    }
+    std::vector<std::string_view> views(d.strings.begin(), d.strings.end());
+    *strings = copy_ids(views);
+    *n = d.strings.size();
+    return read_okay;
+}
+
+void ssu_b200_free_h5_strings(char **strings, uint64_t n) {
+    if (!strings) return;
+    for (uint64_t i = 0; i < n; i++) std::free(strings[i]);
+    std::free(strings);
+}
 
 }  // extern "C"

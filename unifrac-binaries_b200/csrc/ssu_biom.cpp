@@ -167,15 +167,25 @@ class Reader {
             else if (m.type == 0x000B) read_filters(m, d);
         }
         if (d.type.cls < 0 || d.layout < 0) throw std::runtime_error("HDF5 dataset without a datatype or layout");
-        if (d.dims.size() != 1) throw std::runtime_error("only one-dimensional HDF5 datasets are read");
+        if (d.layout == 2 && d.dims.size() != 1)
+            throw std::runtime_error("only one-dimensional chunked HDF5 datasets are read");
         if (d.type.big_endian && (d.type.cls == 0 || d.type.cls == 1))
             throw std::runtime_error("big-endian HDF5 datasets are not supported");
         return d;
     }
 
     // The dataset's elements as stored (elements x type size bytes).
+    static uint64_t count(const Dataset &d) {
+        uint64_t n = 1;
+        for (uint64_t x : d.dims) {
+            if (x && n > (uint64_t(1) << 40) / x) throw std::runtime_error("HDF5 dataset too large");
+            n *= x;
+        }
+        return n;
+    }
+
     std::vector<uint8_t> raw(const Dataset &d) const {
-        const uint64_t n = d.dims[0];
+        const uint64_t n = count(d);
         const uint64_t es = d.type.size;
         if (es == 0 || (n && n > (uint64_t(1) << 40) / es)) throw std::runtime_error("HDF5 dataset too large");
         std::vector<uint8_t> out(n * es, 0);
@@ -194,7 +204,7 @@ class Reader {
     // Elements as doubles (integer or floating-point datasets).
     std::vector<double> doubles(const Dataset &d) const {
         const std::vector<uint8_t> b = raw(d);
-        const uint64_t n = d.dims[0];
+        const uint64_t n = count(d);
         std::vector<double> v(n);
         for (uint64_t i = 0; i < n; i++) v[i] = number(b.data() + i * d.type.size, d.type);
         return v;
@@ -202,7 +212,7 @@ class Reader {
 
     std::vector<std::string> strings(const Dataset &d) const {
         const std::vector<uint8_t> b = raw(d);
-        const uint64_t n = d.dims[0];
+        const uint64_t n = count(d);
         std::vector<std::string> out(n);
         if (d.type.cls == 3) {
             for (uint64_t i = 0; i < n; i++) {
@@ -230,7 +240,7 @@ class Reader {
                               std::min(obj.second, len));
             }
         } else {
-            throw std::runtime_error("HDF5 id dataset is not a string dataset");
+            throw std::runtime_error("HDF5 dataset is not a string dataset");
         }
         return out;
     }
@@ -522,6 +532,26 @@ class Reader {
 };
 
 }  // namespace
+
+bool read_hdf5_dataset(const std::string &path, const std::string &name, H5Data &out, std::string &err) {
+    try {
+        Reader r(path);
+        r.superblock();
+        const Dataset d = r.dataset(r.find(name));
+        H5Data o;
+        o.dims = d.dims;
+        o.is_string = d.type.cls == 3 || (d.type.cls == 9 && d.type.vlen_kind == 1);
+        if (o.is_string)
+            o.strings = r.strings(d);
+        else
+            o.values = r.doubles(d);
+        out = std::move(o);
+        return true;
+    } catch (const std::exception &e) {
+        err = e.what();
+        return false;
+    }
+}
 
 bool read_biom_hdf5(const std::string &path, Table &out, std::string &err) {
     try {

@@ -14,7 +14,9 @@
 // collections).  Other files are refused with a message, never guessed at.
 #pragma once
 
+#include <cstdint>
 #include <string>
+#include <vector>
 
 #include "ssu_table.hpp"
 
@@ -23,5 +25,18 @@ namespace ssu {
 // Fills `out` (an owning table, totals computed) from a BIOM 2.x HDF5 file.
 // Returns false and sets `err` when the file cannot be read as one.
 bool read_biom_hdf5(const std::string &path, Table &out, std::string &err);
+
+// One dataset of such a file, e.g. the reference's own output files
+// (src/api.cpp:1160-1290: "matrix", "order", "pcoa_eigvals", "pcoa_samples",
+// "pcoa_proportion_explained", "stat_*").  Compact and contiguous layouts of
+// any rank, chunked ones of rank 1.  Numbers come back as doubles in storage
+// (row-major) order, strings as strings.
+struct H5Data {
+    std::vector<uint64_t> dims;
+    bool is_string = false;
+    std::vector<double> values;
+    std::vector<std::string> strings;
+};
+bool read_hdf5_dataset(const std::string &path, const std::string &name, H5Data &out, std::string &err);
 
 }  // namespace ssu

@@ -195,6 +195,28 @@ def lib():
         L.ssu_b200_plan_set_graph.restype = None
         L.ssu_b200_plan_tuning.argtypes = [C.c_void_p]
         L.ssu_b200_plan_tuning.restype = C.c_char_p
+        for name, real, out in (("pcoa", C.c_double, C.c_double), ("pcoa_fp32", C.c_float, C.c_float),
+                                ("pcoa_mixed", C.c_double, C.c_float)):
+            getattr(L, name).argtypes = [P(real), C.c_uint32, C.c_uint32, PP(P(out)), PP(P(out)), PP(P(out))]
+            getattr(L, name).restype = None
+        for name, real in (("find_eigens_fast", C.c_double), ("find_eigens_fast_fp32", C.c_float)):
+            getattr(L, name).argtypes = [C.c_uint32, C.c_uint32, P(real), PP(P(real)), PP(P(real))]
+            getattr(L, name).restype = None
+        L.compute_permanova_fp64.argtypes = [C.c_char_p, C.c_uint, _strpp, P(MatFull64), C.c_uint,
+                                             P(C.c_double), P(C.c_double)]
+        L.compute_permanova_fp32.argtypes = [C.c_char_p, C.c_uint, _strpp, P(MatFull32), C.c_uint,
+                                             P(C.c_float), P(C.c_float)]
+        L.ssu_b200_read_grouping.argtypes = [C.c_char_p, C.c_char_p, C.c_uint32, _strpp, P(C.c_uint32),
+                                             P(C.c_uint32)]
+        L.ssu_b200_permanova_fp64.argtypes = [P(C.c_double), C.c_uint32, P(C.c_uint32), C.c_uint,
+                                              P(C.c_double), P(C.c_double)]
+        L.ssu_b200_permanova_fp32.argtypes = [P(C.c_float), C.c_uint32, P(C.c_uint32), C.c_uint,
+                                              P(C.c_float), P(C.c_float)]
+        L.ssu_b200_read_h5_doubles.argtypes = [C.c_char_p, C.c_char_p, PP(P(C.c_double)), P(C.c_uint32),
+                                               P(C.c_uint64)]
+        L.ssu_b200_read_h5_strings.argtypes = [C.c_char_p, C.c_char_p, P(_strpp), P(C.c_uint64)]
+        L.ssu_b200_free_h5_strings.argtypes = [_strpp, C.c_uint64]
+        L.ssu_b200_free_h5_strings.restype = None
         _lib = L
     return _lib
 
@@ -843,3 +865,132 @@ class BatchPlan(Plan):
         if st != 0:
             raise SSUError(st, "ssu_b200_plan_copy_result")
         return [flat[o:o + n * n].reshape(n, n) for o, n in zip(self.offsets, self.sizes)]
+
+
+# ------------------------------------------------- statistics on the matrix
+
+_libc = C.CDLL(None)
+_libc.free.argtypes = [C.c_void_p]
+_libc.free.restype = None
+
+
+def _take(ptr, shape, dtype):
+    """Copy of a malloc'ed array returned by the library, which is then freed."""
+    if not ptr:
+        raise SSUError(6, "statistics call failed (see stderr)")
+    n = int(np.prod(shape))
+    out = np.ctypeslib.as_array(ptr, shape=(max(n, 1),))[:n].astype(dtype, copy=True).reshape(shape)
+    _libc.free(C.cast(ptr, C.c_void_p))
+    return out
+
+
+def pcoa(mat, n_dims, entry="pcoa"):
+    """pcoa / pcoa_fp32 / pcoa_mixed on an n x n matrix: (eigenvalues[n_dims],
+    samples[n, n_dims], proportion_explained[n_dims])."""
+    L = lib()
+    real, out = {"pcoa": (C.c_double, C.c_double), "pcoa_fp32": (C.c_float, C.c_float),
+                 "pcoa_mixed": (C.c_double, C.c_float)}[entry]
+    dt = np.float64 if real is C.c_double else np.float32
+    m = np.ascontiguousarray(mat, dtype=dt)
+    n = m.shape[0]
+    ev, sm, pr = C.POINTER(out)(), C.POINTER(out)(), C.POINTER(out)()
+    getattr(L, entry)(m.ctypes.data_as(C.POINTER(real)), n, n_dims, C.byref(ev), C.byref(sm), C.byref(pr))
+    odt = np.float64 if out is C.c_double else np.float32
+    if not (ev and sm and pr):
+        raise SSUError(6, entry)
+    return _take(ev, (n_dims,), odt), _take(sm, (n, n_dims), odt), _take(pr, (n_dims,), odt)
+
+
+def pcoa_device(dptr, n, n_dims):
+    """pcoa on an n x n fp64 matrix in device memory (address dptr), read in place."""
+    L = lib()
+    ev, sm, pr = C.POINTER(C.c_double)(), C.POINTER(C.c_double)(), C.POINTER(C.c_double)()
+    L.pcoa(C.cast(C.c_void_p(dptr), C.POINTER(C.c_double)), n, n_dims, C.byref(ev), C.byref(sm), C.byref(pr))
+    if not (ev and sm and pr):
+        raise SSUError(6, "pcoa")
+    return (_take(ev, (n_dims,), np.float64), _take(sm, (n, n_dims), np.float64),
+            _take(pr, (n_dims,), np.float64))
+
+
+def find_eigens_fast(centered, n_dims, fp32=False):
+    """find_eigens_fast(_fp32): (eigenvalues[n_dims], eigenvectors[n, n_dims])."""
+    L = lib()
+    real = C.c_float if fp32 else C.c_double
+    dt = np.float32 if fp32 else np.float64
+    m = np.ascontiguousarray(centered, dtype=dt)
+    n = m.shape[0]
+    ev, vec = C.POINTER(real)(), C.POINTER(real)()
+    getattr(L, "find_eigens_fast_fp32" if fp32 else "find_eigens_fast")(
+        n, n_dims, m.ctypes.data_as(C.POINTER(real)), C.byref(ev), C.byref(vec))
+    if not (ev and vec):
+        raise SSUError(6, "find_eigens_fast")
+    return _take(ev, (n_dims,), dt), _take(vec, (n, n_dims), dt)
+
+
+def permanova(mat, grouping, perms, fp32=False):
+    """ssu_b200_permanova_fp64/_fp32: (pseudo-F, p-value)."""
+    L = lib()
+    real = C.c_float if fp32 else C.c_double
+    m = np.ascontiguousarray(mat, dtype=np.float32 if fp32 else np.float64)
+    g = np.ascontiguousarray(grouping, dtype=np.uint32)
+    f, p = real(), real()
+    st = getattr(L, "ssu_b200_permanova_fp32" if fp32 else "ssu_b200_permanova_fp64")(
+        m.ctypes.data_as(C.POINTER(real)), m.shape[0], g.ctypes.data_as(C.POINTER(C.c_uint32)), perms,
+        C.byref(f), C.byref(p))
+    if st != 0:
+        raise SSUError(st, "ssu_b200_permanova")
+    return f.value, p.value
+
+
+def compute_permanova(path, columns, mat, ids, perms, fp32=False):
+    """compute_permanova_fp64/_fp32 over a full matrix with sample ids:
+    (status, fstats, pvalues)."""
+    L = lib()
+    real = C.c_float if fp32 else C.c_double
+    m = np.ascontiguousarray(mat, dtype=np.float32 if fp32 else np.float64)
+    res = (MatFull32 if fp32 else MatFull64)()
+    res.n_samples = m.shape[0]
+    res.flags = 0
+    res.matrix = m.ctypes.data_as(C.POINTER(real))
+    id_arr = _strarr(ids)
+    res.sample_ids = C.cast(id_arr, _strpp)
+    cols = _strarr(columns)
+    fs = (real * max(len(columns), 1))()
+    ps = (real * max(len(columns), 1))()
+    f = L.compute_permanova_fp32 if fp32 else L.compute_permanova_fp64
+    st = f(str(path).encode() if path is not None else None, len(columns), C.cast(cols, _strpp), C.byref(res),
+           perms, fs, ps)
+    return st, list(fs)[:len(columns)], list(ps)[:len(columns)]
+
+
+def read_grouping(path, column, ids):
+    """ssu_b200_read_grouping: (status, grouping array, n_groups)."""
+    L = lib()
+    g = np.zeros(max(len(ids), 1), dtype=np.uint32)
+    ng = C.c_uint32()
+    id_arr = _strarr(ids)
+    st = L.ssu_b200_read_grouping(str(path).encode(), column.encode(), len(ids), C.cast(id_arr, _strpp),
+                                  g.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(ng))
+    return st, g[:len(ids)], ng.value
+
+
+def read_h5(path, dataset, strings=False):
+    """A numeric dataset (as a float64 array of its shape) or, with strings,
+    a string dataset (as a list) of an HDF5 file, through the library's reader."""
+    L = lib()
+    if not strings:
+        vals = C.POINTER(C.c_double)()
+        rank = C.c_uint32()
+        dims = (C.c_uint64 * 8)()
+        st = L.ssu_b200_read_h5_doubles(str(path).encode(), dataset.encode(), C.byref(vals), C.byref(rank), dims)
+        if st != 0:
+            raise RuntimeError(f"{path}:{dataset}: {IO_STATUS[st]}")
+        return _take(vals, tuple(int(dims[i]) for i in range(rank.value)), np.float64)
+    strs = _strpp()
+    n = C.c_uint64()
+    st = L.ssu_b200_read_h5_strings(str(path).encode(), dataset.encode(), C.byref(strs), C.byref(n))
+    if st != 0:
+        raise RuntimeError(f"{path}:{dataset}: {IO_STATUS[st]}")
+    out = _ids(strs, n.value)
+    L.ssu_b200_free_h5_strings(strs, n.value)
+    return out
