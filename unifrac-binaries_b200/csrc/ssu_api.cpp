@@ -306,8 +306,9 @@ ComputeStatus make_plan(const ssu::Table &table, const ssu::BPTree &tree, const 
 // Page-locked host memory for full results: the copy-out then runs at the
 // link's rate with no per-call page registration.  Blocks released through
 // destroy_mat_full_* are kept for later results (best fit, up to twice the
-// request) while the pool holds at most UNIFRAC_B200_PINNED_BYTES (default
-// 4 GiB) live and cached together; beyond that results use pageable memory.
+// request) while the pool holds at most UNIFRAC_B200_PINNED_BYTES (default:
+// a sixteenth of the host's memory, within [4, 16] GiB) live and cached
+// together; beyond that results use pageable memory.
 class PinnedPool {
   public:
     static PinnedPool &get() {
@@ -353,6 +354,10 @@ class PinnedPool {
 
   private:
     PinnedPool() {
+        const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGESIZE);
+        if (pages > 0 && page > 0)
+            limit_ = std::min(std::max(static_cast<size_t>(pages) * static_cast<size_t>(page) / 16, size_t(4) << 30),
+                              size_t(16) << 30);
         if (const char *v = std::getenv("UNIFRAC_B200_PINNED_BYTES")) limit_ = std::strtoull(v, nullptr, 10);
     }
     size_t held() const { return live_bytes_ + cached_; }
@@ -466,9 +471,10 @@ ComputeStatus full_matrix(const ssu::Table &table, const ssu::BPTree &tree, cons
     std::string err;
     bool method_fp64 = false;
     is_fp64_method(r.method, method_fp64);
-    int rc = plan->execute(nullptr);
     const size_t elems = static_cast<size_t>(table.n_samples) * table.n_samples;
-    if (rc == 0 && method_fp64 != (sizeof(TReal) == sizeof(double))) {
+    const bool convert = method_fp64 != (sizeof(TReal) == sizeof(double));
+    int rc = convert ? plan->execute(nullptr) : 0;
+    if (rc == 0 && convert) {
         // the file-based calls compute in the method's precision and write
         // the result type's (stripes_to_matrix_T<TReal>, src/api.cpp:684-690)
         if (method_fp64) {
@@ -485,8 +491,18 @@ ComputeStatus full_matrix(const ssu::Table &table, const ssu::BPTree &tree, cons
         // page-locked for the copy; a pooled one is page-locked already
         const bool fresh = allocated && (*result)->flags == 0;
         const size_t bytes = sizeof(TReal) * elems;
-        if (fresh && bytes >= kHugeAlign) prefault((*result)->matrix, bytes);
-        rc = plan->download_full((*result)->matrix, fresh, err);
+        if ((*result)->flags & kPinnedFlag) {
+            // page-locked: the copy-out runs alongside the computation
+            rc = plan->execute_download((*result)->matrix, false, err);
+        } else {
+            rc = plan->execute(nullptr);
+            if (rc == 0) {
+                if (fresh && bytes >= kHugeAlign) prefault((*result)->matrix, bytes);
+                rc = plan->download_full((*result)->matrix, fresh, err);
+            } else {
+                err = "launch failed";
+            }
+        }
     } else {
         err = "launch failed";
     }

@@ -4,6 +4,7 @@
 #include "ssu_engine.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -222,6 +223,22 @@ int log2_bucket(uint64_t x) {
     return b;
 }
 
+// UNIFRAC_TIMING_INFO: host time of the plan's setup steps, printed as the
+// API layer prints its own steps.
+struct SetupTimer {
+    bool on;
+    std::chrono::steady_clock::time_point t0;
+    SetupTimer() : on(std::getenv("UNIFRAC_TIMING_INFO") != nullptr), t0(std::chrono::steady_clock::now()) {}
+    void step(const char *name) {
+        if (!on) return;
+        const auto t1 = std::chrono::steady_clock::now();
+        std::printf("INFO (unifrac): dt %8.3f ms : plan.%s\n",
+                    std::chrono::duration<double, std::milli>(t1 - t0).count(), name);
+        std::fflush(stdout);
+        t0 = t1;
+    }
+};
+
 int env_int(const char *name, int fallback) {
     const char *v = std::getenv(name);
     return (v && *v) ? std::atoi(v) : fallback;
@@ -243,6 +260,9 @@ struct Group {
     // tensor-core path: per operand row, the starting columns of its tips
     uint32_t *d_sample_ptr = nullptr;
     int32_t *d_start_col = nullptr;
+    // tensor-core path, one table: first work unit and first row of each
+    // band of row blocks (one extra entry closes the list)
+    std::vector<uint32_t> band_unit, band_row;
 };
 
 struct PlanImpl {
@@ -348,6 +368,11 @@ struct PlanImpl {
     CUtensorMap map_A{}, map_Bh{}, map_Bl{};
     int setup_gemm(const TableSet &set, const FlatTree &tree);
     int execute_gemm(cudaStream_t s, const dev::OutSpec &out);
+    int execute_gemm_overlap(void *host);
+    // overlapped copy-out: a second compute stream, the copy stream, and an
+    // event per band of rows
+    cudaStream_t aux[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> band_ev;
 
     // CUDA graph of execute()
     bool graph_on = false, capturing = false;
@@ -418,6 +443,7 @@ PairKernel<float> &PlanImpl::kern<float>() {
 }
 
 int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOptions &opts) {
+    SetupTimer timer;
     const uint32_t n_tables = static_cast<uint32_t>(set.tables.size());
     K = tree.n_nodes;
     E = faith ? tree.n_nodes : tree.n_embedded;
@@ -470,6 +496,7 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
         }
     }
 
+    timer.step("csr_upload");
     // groups of tables whose embedding fits the budget together
     const size_t el = (spec.fp64 || faith) ? sizeof(double) : sizeof(float);
     n_words = bits() ? (E + 63) / 64 : 0;
@@ -567,6 +594,7 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
         }
     }
     SSU_CK(upload(&d_tdesc, tdesc.data(), sizeof(dev::TableDesc) * std::max<uint32_t>(n_tables, 1)));
+    timer.step("groups");
 
     // tree
     SSU_CK(upload(&d_tip_rows, tree.leaf_rows.data(), sizeof(uint32_t) * n_tips));
@@ -598,6 +626,7 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
         SSU_CK(upload(reinterpret_cast<float **>(&d_len), len.data(), sizeof(float) * len.size()));
     }
     for (auto &e : ev) SSU_CK(cudaEventCreate(&e));
+    timer.step("tree_upload");
     return 0;
 }
 
@@ -1247,16 +1276,37 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
 // --------------------------------------------------- tensor-core unweighted
 
 int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
+    SetupTimer timer;
     // Embedded nodes by decreasing |length|, packed into chunks of whole
     // 64-node K blocks: a chunk closes (its last block padded with
     // zero-length columns) when the next length is below half the chunk's
     // first, or at MAX_CHUNK_KB blocks.  Chunk c is scaled by 2^s_c so that
     // its largest |length| lies in [1024, 2048): every length of the chunk in
     // [512, 2048), hi = nearest integer (exact in fp16), lo = fp16(rest).
-    std::vector<uint32_t> order(E);
-    for (uint32_t e = 0; e < E; e++) order[e] = e;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](uint32_t a, uint32_t b) { return std::fabs(tree.length[a]) > std::fabs(tree.length[b]); });
+    // (stable order by decreasing |length|: an LSD radix sort of the
+    // complemented bit patterns, which order non-negative doubles)
+    std::vector<uint32_t> order(E), tmp(E);
+    std::vector<uint64_t> key(E), key_tmp(E);
+    for (uint32_t e = 0; e < E; e++) {
+        order[e] = e;
+        const double a = std::fabs(tree.length[e]);
+        uint64_t b;
+        std::memcpy(&b, &a, sizeof b);
+        key[e] = ~b;
+    }
+    for (int shift = 0; shift < 64; shift += 16) {
+        std::vector<uint32_t> count(65537, 0);
+        for (uint32_t i = 0; i < E; i++) count[((key[i] >> shift) & 0xFFFF) + 1]++;
+        if (std::count(count.begin(), count.end(), 0u) == 65536) continue;  // one digit value: order kept
+        for (int d = 0; d < 65536; d++) count[d + 1] += count[d];
+        for (uint32_t i = 0; i < E; i++) {
+            const uint32_t pos = count[(key[i] >> shift) & 0xFFFF]++;
+            key_tmp[pos] = key[i];
+            tmp[pos] = order[i];
+        }
+        key.swap(key_tmp);
+        order.swap(tmp);
+    }
     std::vector<int32_t> col_of_row(tree.n_nodes, -1);
     std::vector<double> lsorted, scale;
     std::vector<__half> lhi, llo;
@@ -1292,6 +1342,7 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     }
     if (first < 0) scale.push_back(1.0);  // no embedded node: one chunk of padding
     pad_to_block();
+    timer.step("gemm_chunks");
     k_pad = static_cast<uint32_t>(lsorted.size());
     n_chunks = static_cast<uint32_t>(chunk_end.size());
     // parents among embedded nodes
@@ -1315,36 +1366,52 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
         if (r >= E) node = parent_row[r];
         start_of_obs[obs] = (node >= 0 && static_cast<uint32_t>(node) < E) ? col_of_row[node] : -1;
     }
+    timer.step("gemm_parents");
     // per group: operand rows = the group's columns; each row's list of
-    // starting columns (table rows of an observation with a positive count)
+    // starting columns (one per table row of an observation with a positive
+    // count), built on the device from the uploaded CSR: count, scan, place
     for (Group &g : groups) {
-        std::vector<uint32_t> sample_ptr(g.ld + 1, 0);
-        std::vector<std::pair<uint32_t, int32_t>> entries;  // (operand row, start column)
+        uint64_t nnz_g = 0;
+        for (uint32_t t = g.t0; t < g.t1; t++) nnz_g += set.tables[t]->nnz();
+        uint32_t *d_count = nullptr, *d_fill = nullptr;
+        SSU_CK(alloc(&d_count, sizeof(uint32_t) * g.ld));
+        SSU_CK(alloc(&d_fill, sizeof(uint32_t) * g.ld));
+        SSU_CK(alloc(&g.d_sample_ptr, sizeof(uint32_t) * (g.ld + 1)));
+        SSU_CK(alloc(&g.d_start_col, sizeof(int32_t) * std::max<uint64_t>(nnz_g, 1)));
+        SSU_CK(cudaMemsetAsync(d_count, 0, sizeof(uint32_t) * g.ld, stream));
+        std::vector<int32_t *> d_row_start(g.t1 - g.t0, nullptr);
         for (uint32_t t = g.t0; t < g.t1; t++) {
             const Table &tb = *set.tables[t];
-            const uint32_t base = tdesc[t].base;
-            auto add_row = [&](uint32_t i, int32_t start) {
-                if (start < 0) return;
-                for (uint32_t q = tb.indptr[i]; q < tb.indptr[i + 1]; q++)
-                    if (tb.data[q] > 0.0) entries.emplace_back(base + tb.indices[q], start);
-            };
+            std::vector<int32_t> row_start(std::max<uint32_t>(tb.n_obs, 1), -1);
             if (set.obs_row.empty()) {
-                for (uint32_t o = 0; o < n_obs_tree; o++)
-                    if (o < tb.n_obs) add_row(o, start_of_obs[o]);
+                for (uint32_t o = 0; o < n_obs_tree && o < tb.n_obs; o++) row_start[o] = start_of_obs[o];
             } else {
                 const std::vector<int32_t> &m = set.obs_row[t];
                 for (uint32_t o = 0; o < n_obs_tree && o < m.size(); o++)
-                    if (m[o] >= 0) add_row(static_cast<uint32_t>(m[o]), start_of_obs[o]);
+                    if (m[o] >= 0 && static_cast<uint32_t>(m[o]) < tb.n_obs) row_start[m[o]] = start_of_obs[o];
+            }
+            SSU_CK(upload(&d_row_start[t - g.t0], row_start.data(), sizeof(int32_t) * row_start.size()));
+        }
+        for (int pass = 0; pass < 2; pass++) {
+            if (pass == 1) {
+                tc::exclusive_scan_kernel<<<1, 1024, 0, stream>>>(d_count, static_cast<uint32_t>(g.ld),
+                                                                  g.d_sample_ptr);
+                SSU_CK(cudaMemcpyAsync(d_fill, g.d_sample_ptr, sizeof(uint32_t) * g.ld, cudaMemcpyDeviceToDevice,
+                                       stream));
+            }
+            for (uint32_t t = g.t0; t < g.t1; t++) {
+                const Table &tb = *set.tables[t];
+                const dev::TableDesc &d = tdesc[t];
+                if (tb.n_obs == 0 || tb.nnz() == 0) continue;
+                const uint64_t threads = static_cast<uint64_t>(tb.n_obs) * 32;
+                tc::sample_lists_kernel<<<static_cast<uint32_t>((threads + 255) / 256), 256, 0, stream>>>(
+                    d_indptr + d.indptr_off, d_indices + d.nnz_off, d_data + d.nnz_off, d_row_start[t - g.t0],
+                    tb.n_obs, d.base, d_count, pass ? d_fill : nullptr, g.d_start_col);
             }
         }
-        for (const auto &e : entries) sample_ptr[e.first + 1]++;
-        for (uint64_t j = 0; j < g.ld; j++) sample_ptr[j + 1] += sample_ptr[j];
-        std::vector<int32_t> start_col(std::max<size_t>(entries.size(), 1));
-        std::vector<uint32_t> fill(sample_ptr.begin(), sample_ptr.end() - 1);
-        for (const auto &e : entries) start_col[fill[e.first]++] = e.second;
-        SSU_CK(upload(&g.d_sample_ptr, sample_ptr.data(), sizeof(uint32_t) * sample_ptr.size()));
-        SSU_CK(upload(&g.d_start_col, start_col.data(), sizeof(int32_t) * start_col.size()));
+        SSU_CK(cudaGetLastError());
     }
+    timer.step("gemm_sample_lists");
     // work units: per table, the (256-row block, 128-column block) pairs
     // holding some pair k < l, ordered in bands of row blocks walked
     // column by column.  Clusters start in launch order as SMs free up (one
@@ -1357,20 +1424,28 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     const uint32_t band = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_TC_BAND", 4)));
     for (Group &g : groups) {
         std::vector<uint4> tiles;
+        g.band_unit.clear();
+        g.band_row.clear();
         for (uint32_t t = g.t0; t < g.t1; t++) {
             const uint32_t n = tdesc[t].n;
             const uint32_t nkb = (n + tc::UMMA_M - 1) / tc::UMMA_M, nlb = (n + tc::COLS - 1) / tc::COLS;
-            for (uint32_t k0 = 0; k0 < nkb; k0 += band)
+            for (uint32_t k0 = 0; k0 < nkb; k0 += band) {
+                g.band_unit.push_back(static_cast<uint32_t>(tiles.size()));
+                g.band_row.push_back(k0 * tc::UMMA_M);
                 for (uint32_t lb = 0; lb < nlb; lb++)
                     for (uint32_t kb = k0; kb < std::min(nkb, k0 + band); kb++)
                         if (static_cast<uint64_t>(kb) * tc::UMMA_M <
                             std::min<uint64_t>(n, static_cast<uint64_t>(lb + 1) * tc::COLS) - 1)
                             tiles.push_back(make_uint4(kb, lb, t, 0));
+            }
+            g.band_unit.push_back(static_cast<uint32_t>(tiles.size()));
+            g.band_row.push_back(n);
         }
         g.n_tiles = static_cast<uint32_t>(tiles.size());
         SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * std::max<size_t>(tiles.size(), 1)));
     }
 
+    timer.step("gemm_tiles");
     n_pad = static_cast<uint32_t>(ld);
     const size_t op_bytes = sizeof(__half) * static_cast<size_t>(n_pad) * k_pad;
     SSU_CK(alloc(&d_A, op_bytes));
@@ -1402,6 +1477,8 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     SSU_CK(cudaFuncSetAttribute(tc::presence_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 static_cast<int>(bits_smem)));
     SSU_CK(alloc(&d_full, (spec.fp64 ? sizeof(double) : sizeof(float)) * std::max<uint64_t>(full_elems, 1)));
+    SSU_CK(cudaStreamSynchronize(stream));
+    timer.step("gemm_buffers");
     tuning = "fixed";
     return 0;
 }
@@ -1442,6 +1519,77 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
     if (out.mode == 0) zero_diagonal(s, out.ptr);
     if (timed()) SSU_CK(cudaEventRecord(ev[3], s));
     SSU_CK(cudaGetLastError());
+    return 0;
+}
+
+// One table on the tensor-core path, result copied out while it is being
+// computed.  The work units are ordered in bands of row blocks, and a unit of
+// band p writes the upper-triangle entries of its rows (band p) and their
+// mirror images in rows of bands >= p.  So rows of band p are final once the
+// launches of bands 0..p are done: each band is one launch, alternating
+// between two streams (the next band's clusters fill SMs as the previous
+// band drains), and the copy stream copies band p's rows after waiting for
+// band p's launch - the earlier bands' copies having waited for theirs.
+int PlanImpl::execute_gemm_overlap(void *host) {
+    const Group &g = groups[0];
+    const uint32_t nb = static_cast<uint32_t>(g.band_unit.size()) - 1;
+    const uint32_t n_t = tdesc[0].n;
+    const size_t el = spec.fp64 ? sizeof(double) : sizeof(float);
+    for (cudaStream_t &a : aux)
+        if (!a) SSU_CK(cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking));
+    while (band_ev.size() < nb + 2) {
+        cudaEvent_t e = nullptr;
+        SSU_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        band_ev.push_back(e);
+    }
+    cudaStream_t s = stream, s1 = aux[0], sc = aux[1];
+    launches = 0;
+    dev::OutSpec out{};
+    out.mode = 0;
+    out.ptr = d_full;
+    zero_diagonal(s, d_full);  // the units never write the diagonal
+    const size_t bits_smem = sizeof(uint32_t) * (k_pad / 32);
+    tc::presence_rows_kernel<<<static_cast<uint32_t>(g.ld), 256, bits_smem, s>>>(
+        g.d_sample_ptr, g.d_start_col, d_parent_col, d_lhi, d_llo, d_lsorted, static_cast<uint32_t>(g.ld), k_pad,
+        d_A, d_Bh, d_Bl, d_r);
+    launches++;
+    SSU_CK(cudaEventRecord(band_ev[nb], s));
+    SSU_CK(cudaStreamWaitEvent(s1, band_ev[nb], 0));
+    for (uint32_t p = 0; p < nb; p++) {
+        cudaStream_t st = (p & 1) ? s1 : s;
+        const uint32_t u0 = g.band_unit[p], u1 = g.band_unit[p + 1];
+        if (u1 > u0) {
+            tc::GemmArgs a{};
+            a.tiles = g.d_tiles + u0;
+            a.n_tiles = u1 - u0;
+            a.tables = d_tdesc;
+            a.n_kblocks = k_pad / tc::BLOCK_K;
+            a.n_chunks = n_chunks;
+            a.chunk_end = d_chunk_end;
+            a.chunk_scale = d_chunk_scale;
+            a.r = d_r;
+            a.normalized = spec.method == Method::unweighted ? 1 : 0;
+            a.out_fp64 = spec.fp64 ? 1 : 0;
+            a.out = out;
+            a.error = d_error;
+            a.wait_cycles = gemm_wait_cycles;
+            a.stall = union_stall;
+            tc::unweighted_tc_kernel<<<2 * (u1 - u0), tc::THREADS, tc::SMEM_BYTES, st>>>(map_A, map_Bh, map_Bl, a);
+            launches++;
+        }
+        SSU_CK(cudaEventRecord(band_ev[p], st));
+        SSU_CK(cudaStreamWaitEvent(sc, band_ev[p], 0));
+        const uint64_t r0 = g.band_row[p], r1 = std::min<uint64_t>(g.band_row[p + 1], n_t);
+        if (r1 > r0)
+            SSU_CK(cudaMemcpyAsync(static_cast<char *>(host) + el * r0 * n_t,
+                                   static_cast<const char *>(d_full) + el * r0 * n_t, el * (r1 - r0) * n_t,
+                                   cudaMemcpyDeviceToHost, sc));
+    }
+    SSU_CK(cudaGetLastError());
+    SSU_CK(cudaEventRecord(band_ev[nb + 1], sc));
+    SSU_CK(cudaStreamWaitEvent(s, band_ev[nb + 1], 0));
+    SSU_CK(cudaEventRecord(band_ev[nb], s1));
+    SSU_CK(cudaStreamWaitEvent(s, band_ev[nb], 0));
     return 0;
 }
 
@@ -1564,6 +1712,13 @@ Plan::~Plan() {
     }
     for (auto &e : m.ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : m.band_ev)
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t a : m.aux)
+        if (a) {
+            cudaStreamSynchronize(a);
+            cudaStreamDestroy(a);
+        }
     if (m.own_stream && m.stream) cudaStreamDestroy(m.stream);
     delete impl_;
 }
@@ -1642,6 +1797,41 @@ int Plan::run_full(void *host_out, bool out_fp64, std::string &err) {
     }
     if (rc) err = m.last_error;
     return rc;
+}
+
+int Plan::execute_download(void *host_out, bool pin, std::string &err) {
+    PlanImpl &m = *impl_;
+    const bool overlap = m.gemm && !m.graph_on && m.groups.size() == 1 && m.groups[0].t1 - m.groups[0].t0 == 1 &&
+                         m.groups[0].band_unit.size() > 2 && m.full_elems > 0;
+    if (!overlap) {
+        const int rc = execute(nullptr);
+        if (rc) {
+            err = m.last_error.empty() ? "launch failed" : m.last_error;
+            return rc;
+        }
+        return download_full(host_out, pin, err);
+    }
+    const size_t bytes = (m.spec.fp64 ? sizeof(double) : sizeof(float)) * m.full_elems;
+    bool registered = false;
+    if (pin && bytes >= (size_t(1) << 20))
+        registered = cudaHostRegister(host_out, bytes, cudaHostRegisterDefault) == cudaSuccess;
+    if (pin && !registered) cudaGetLastError();  // a refused registration only means pageable copies
+    int rc = m.execute_gemm_overlap(host_out);
+    cudaError_t e = cudaStreamSynchronize(m.stream);
+    if (registered) cudaHostUnregister(host_out);
+    if (rc) {
+        err = m.last_error;
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        err = cudaGetErrorString(e);
+        return kOutputError;
+    }
+    if (const int de = device_error()) {
+        err = "device wait expired (code " + std::to_string(de) + ")";
+        return kOutputError;
+    }
+    return 0;
 }
 
 int Plan::download_full(void *host_out, bool pin, std::string &err) {

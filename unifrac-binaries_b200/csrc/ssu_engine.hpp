@@ -107,6 +107,11 @@ class Plan {
     // `pin`, the destination is page-locked for the copy (cudaHostRegister)
     // and released after.  Synchronises and checks device-side errors.
     int download_full(void *host_out, bool pin, std::string &err);
+    // execute(nullptr) then download_full, with the copy-out overlapped with
+    // the computation where the plan allows it (one table on the tensor-core
+    // path: bands of rows are copied as soon as every launch writing to them
+    // has finished); otherwise the two calls in turn.
+    int execute_download(void *host_out, bool pin, std::string &err);
     // Same for `count` result elements starting at element `offset` (one
     // table of a batch: table_offset(t), n_t * n_t).
     int download_range(uint64_t offset, uint64_t count, void *host_out, bool pin, std::string &err);

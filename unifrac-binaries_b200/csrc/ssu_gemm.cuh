@@ -392,6 +392,70 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
         asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
+// Per-sample lists of starting columns, built from one table's CSR on the
+// device: table row i (one warp) whose observation starts at column
+// row_start[i] >= 0 gives every sample j with a positive count one entry in
+// operand row base + j.  Counting pass (fill == nullptr): count[base + j]++;
+// placing pass: start_col[fill[base + j]++] = row_start[i].  The order within
+// a sample's list varies; the rows kernel only takes the union of the paths.
+__global__ void sample_lists_kernel(const uint32_t *__restrict__ indptr, const uint32_t *__restrict__ indices,
+                                    const double *__restrict__ data, const int32_t *__restrict__ row_start,
+                                    uint32_t n_rows, uint32_t base, uint32_t *__restrict__ count,
+                                    uint32_t *__restrict__ fill, int32_t *__restrict__ start_col) {
+    const uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
+    const uint32_t lane = threadIdx.x % 32;
+    if (w >= n_rows) return;
+    const int32_t st = row_start[w];
+    if (st < 0) return;
+    for (uint32_t q = indptr[w] + lane; q < indptr[w + 1]; q += 32) {
+        if (!(data[q] > 0.0)) continue;
+        const uint32_t col = base + indices[q];
+        if (fill)
+            start_col[atomicAdd(fill + col, 1u)] = st;
+        else
+            atomicAdd(count + col, 1u);
+    }
+}
+
+// out[0] = 0, out[i + 1] = in[0] + ... + in[i] for i < n; one CTA of 1024.
+__global__ void __launch_bounds__(1024) exclusive_scan_kernel(const uint32_t *__restrict__ in, uint32_t n,
+                                                              uint32_t *__restrict__ out) {
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t carry;
+    const uint32_t lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+    if (threadIdx.x == 0) {
+        carry = 0;
+        out[0] = 0;
+    }
+    __syncthreads();
+    for (uint32_t b = 0; b < n; b += 1024) {
+        const uint32_t i = b + threadIdx.x;
+        uint32_t v = i < n ? in[i] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= static_cast<uint32_t>(o)) v += y;
+        }
+        if (lane == 31) warp_tot[warp] = v;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t t = warp_tot[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= static_cast<uint32_t>(o)) t += y;
+            }
+            warp_tot[lane] = t;  // inclusive over warps
+        }
+        __syncthreads();
+        const uint32_t before = carry + (warp ? warp_tot[warp - 1] : 0u);
+        if (i < n) out[i + 1] = before + v;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_tot[31];
+        __syncthreads();
+    }
+}
+
 // Presence rows for the contraction, one CTA per sample (padding rows too):
 // walk up from every present tip, marking embedded ancestors in a shared
 // bitmap (stopping at nodes already marked), then write the sample's rows of
