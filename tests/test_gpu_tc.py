@@ -1,9 +1,9 @@
 """The tensor-core (tcgen05) unweighted contraction, selected with
 UNIFRAC_B200_UNWEIGHTED_MODE=gemm, against the fp64 oracle.  Bar: max
 relative error 1e-6 on every pair (the contraction's stated bound; lengths
-carried as an integer fp16 hi part and an fp16 lo part per chunk of lengths
-within a factor of two, exact hi sums, fp64 across chunks and in the final
-ratio)."""
+carried as 24-bit fixed point in three byte planes per chunk of lengths
+within a factor of two, exact int32 plane sums, fp64 across chunks and in
+the final ratio)."""
 import os
 
 import numpy as np
@@ -81,10 +81,10 @@ def test_tc_plan_agrees_with_stripe_form(ssu, gemm_mode):
     assert rel_err(tc, stripe)[0] <= TC_REL
 
 
-@pytest.mark.parametrize("n_samples", [2, 128, 129, 255, 256, 257, 383, 511, 513])
+@pytest.mark.parametrize("n_samples", [2, 63, 64, 65, 128, 129, 255, 256, 257, 319, 383, 511, 513])
 @pytest.mark.parametrize("method", ["unweighted_fp64", "unweighted_unnormalized_fp64"])
 def test_tc_sample_counts_at_work_unit_edges(ssu, oracle_mod, gemm_mode, n_samples, method):
-    """A work unit covers 256 rows x 128 columns: counts around those edges,
+    """A work unit covers 256 rows x 64 columns: counts around those edges,
     where units straddle the diagonal or hold a single row or column."""
     tree, table = _case(n_samples, 300, n_samples, density=0.08)
     gpu, _ = ssu.one_off_matrix(tree, table, method)
@@ -130,3 +130,17 @@ def test_tc_wait_that_runs_out_is_an_error_and_the_device_stays_usable(ssu, orac
     gpu, _ = ssu.one_off_matrix(tree, table, "unweighted_fp64")
     ref = oracle_mod.oracle_one_off(tree, table, "unweighted_fp64")["matrix"]
     assert rel_err(gpu, ref)[0] <= TC_REL
+
+
+def test_tc_negative_lengths_keep_the_stripe_form(ssu, oracle_mod, gemm_mode):
+    """Lengths are fixed-point magnitudes on the tensor cores: a tree with a
+    negative branch length runs on the stripe form instead, and still
+    matches the oracle."""
+    tree, table = _case(31, 400, 70, density=0.15)
+    lengths = tree.lengths.copy()
+    lengths[np.flatnonzero(tree.structure)[5]] = -0.01
+    tree.lengths = lengths
+    gpu, _ = ssu.one_off_matrix(tree, table, "unweighted_fp64")
+    ref = oracle_mod.oracle_one_off(tree, table, "unweighted_fp64")["matrix"]
+    r, z = rel_err(gpu, ref)
+    assert r <= 1e-12 and z <= 1e-13, (r, z)

@@ -9,7 +9,6 @@
 #include <cstdio>
 #include <cstring>
 #include <cuda.h>
-#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <fstream>
 #include <map>
@@ -110,16 +109,17 @@ EncodeTiledFn encode_tiled() {
     return fn;
 }
 
-// 2-D fp16 tensor map over a row-major [rows][cols] matrix with a
-// 64-column x 128-row box and 128-byte swizzle (the UMMA K-major layout).
-bool make_fp16_map(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols) {
+// 2-D tensor map over a row-major [rows][cols] matrix of bytes with a
+// 128-column x box_rows box and 128-byte swizzle (the UMMA K-major layout);
+// rows past `rows` read as zero.
+bool make_u8_map(CUtensorMap *map, void *base, uint64_t rows, uint64_t cols, uint32_t box_rows) {
     EncodeTiledFn f = encode_tiled();
     if (!f) return false;
     const cuuint64_t dims[2] = {cols, rows};
-    const cuuint64_t strides[1] = {cols * 2};
-    const cuuint32_t box[2] = {static_cast<cuuint32_t>(tc::BLOCK_K), static_cast<cuuint32_t>(tc::ROWS)};
+    const cuuint64_t strides[1] = {cols};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(tc::BLOCK_K), box_rows};
     const cuuint32_t estr[2] = {1, 1};
-    return f(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+    return f(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -360,12 +360,12 @@ struct PlanImpl {
     // tensor-core unweighted path (one table)
     bool gemm = false;
     uint32_t n_pad = 0, k_pad = 0, n_chunks = 0;
-    __half *d_A = nullptr, *d_Bh = nullptr, *d_Bl = nullptr, *d_lhi = nullptr, *d_llo = nullptr;
+    uint8_t *d_A = nullptr, *d_B = nullptr, *d_lq = nullptr;
     double *d_r = nullptr, *d_lsorted = nullptr, *d_chunk_scale = nullptr;
     uint32_t *d_chunk_end = nullptr;
     int32_t *d_parent_col = nullptr;
     int *d_error = nullptr;
-    CUtensorMap map_A{}, map_Bh{}, map_Bl{};
+    CUtensorMap map_A{}, map_B{};
     int setup_gemm(const TableSet &set, const FlatTree &tree);
     int execute_gemm(cudaStream_t s, const dev::OutSpec &out);
     int execute_gemm_overlap(void *host);
@@ -508,10 +508,10 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
     size_t per_col = el * std::max<uint32_t>(K, 1) * (counts ? 2 : 1) + sizeof(double) + (counts ? el : 0) +
                      sizeof(unsigned long long) * n_words + (n_parts ? el * (n_parts + 1) : 0);
     if (gemm) {
-        // fp16 operand rows A, B_hi, B_lo over the padded nodes (chunk
-        // padding included, allowing for 128 chunks) and r
-        const uint64_t kp = (static_cast<uint64_t>(E) + 63) / 64 * 64 + 128 * 64;
-        per_col = 3 * sizeof(uint16_t) * kp + sizeof(double);
+        // 8-bit operand rows (A and three B planes) over the padded nodes
+        // (chunk padding included, allowing for 128 chunks) and r
+        const uint64_t kp = (static_cast<uint64_t>(E) + tc::BLOCK_K - 1) / tc::BLOCK_K * tc::BLOCK_K + 128 * tc::BLOCK_K;
+        per_col = (1 + tc::PLANES) * kp + sizeof(double);
     }
     size_t budget = opts.group_bytes;
     if (!budget) {
@@ -1309,14 +1309,13 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     }
     std::vector<int32_t> col_of_row(tree.n_nodes, -1);
     std::vector<double> lsorted, scale;
-    std::vector<__half> lhi, llo;
+    std::vector<uint32_t> lq;  // 24-bit fixed-point lengths
     std::vector<uint32_t> chunk_end;
     const uint32_t max_cols = static_cast<uint32_t>(tc::MAX_CHUNK_KB) * tc::BLOCK_K;
     auto pad_to_block = [&] {
         while (lsorted.size() % tc::BLOCK_K) {
             lsorted.push_back(0.0);
-            lhi.push_back(__float2half(0.0f));
-            llo.push_back(__float2half(0.0f));
+            lq.push_back(0u);
         }
         chunk_end.push_back(static_cast<uint32_t>(lsorted.size() / tc::BLOCK_K));
     };
@@ -1330,15 +1329,14 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
             if (first >= 0) pad_to_block();
             first = a;
             chunk_first = lsorted.size();
-            sig = a > 0 ? 10 - static_cast<int>(std::floor(std::log2(a))) : 0;
+            // the chunk's largest length to [2^23, 2^24)
+            sig = a > 0 ? (tc::QBITS - 1) - static_cast<int>(std::floor(std::log2(a))) : 0;
             scale.push_back(std::ldexp(1.0, -sig));
         }
         col_of_row[order[i]] = static_cast<int32_t>(lsorted.size());
-        const double x = std::ldexp(L, sig);
-        const double hi = std::nearbyint(x);
+        const double x = std::nearbyint(std::ldexp(L, sig));
         lsorted.push_back(L);
-        lhi.push_back(__double2half(hi));
-        llo.push_back(__double2half(x - hi));
+        lq.push_back(static_cast<uint32_t>(std::min(std::max(x, 0.0), std::ldexp(1.0, tc::QBITS) - 1.0)));
     }
     if (first < 0) scale.push_back(1.0);  // no embedded node: one chunk of padding
     pad_to_block();
@@ -1447,13 +1445,17 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
 
     timer.step("gemm_tiles");
     n_pad = static_cast<uint32_t>(ld);
-    const size_t op_bytes = sizeof(__half) * static_cast<size_t>(n_pad) * k_pad;
+    const size_t op_bytes = static_cast<size_t>(n_pad) * k_pad;
     SSU_CK(alloc(&d_A, op_bytes));
-    SSU_CK(alloc(&d_Bh, op_bytes));
-    SSU_CK(alloc(&d_Bl, op_bytes));
+    SSU_CK(alloc(&d_B, tc::PLANES * op_bytes));
     SSU_CK(alloc(&d_r, sizeof(double) * n_pad));
-    SSU_CK(upload(&d_lhi, lhi.data(), sizeof(__half) * k_pad));
-    SSU_CK(upload(&d_llo, llo.data(), sizeof(__half) * k_pad));
+    {
+        std::vector<uint8_t> planes(static_cast<size_t>(tc::PLANES) * k_pad);
+        for (uint32_t c = 0; c < k_pad; c++)
+            for (int p = 0; p < tc::PLANES; p++)
+                planes[static_cast<size_t>(p) * k_pad + c] = static_cast<uint8_t>(lq[c] >> (8 * p));
+        SSU_CK(upload(&d_lq, planes.data(), planes.size()));
+    }
     SSU_CK(upload(&d_lsorted, lsorted.data(), sizeof(double) * k_pad));
     SSU_CK(upload(&d_chunk_scale, scale.data(), sizeof(double) * n_chunks));
     SSU_CK(upload(&d_chunk_end, chunk_end.data(), sizeof(uint32_t) * n_chunks));
@@ -1462,8 +1464,8 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     SSU_CK(cudaMemsetAsync(d_error, 0, sizeof(int), stream));
     if (const char *w = std::getenv("UNIFRAC_B200_WAIT_CYCLES")) gemm_wait_cycles = std::max(0LL, std::atoll(w));
     union_stall = env_int("UNIFRAC_B200_TEST_STALL", 0) ? 1 : 0;
-    if (!make_fp16_map(&map_A, d_A, n_pad, k_pad) || !make_fp16_map(&map_Bh, d_Bh, n_pad, k_pad) ||
-        !make_fp16_map(&map_Bl, d_Bl, n_pad, k_pad)) {
+    if (!make_u8_map(&map_A, d_A, n_pad, k_pad, tc::ROWS) ||
+        !make_u8_map(&map_B, d_B, static_cast<uint64_t>(tc::PLANES) * n_pad, k_pad, tc::B_ROWS)) {
         last_error = "cuTensorMapEncodeTiled failed";
         return kOutputError;
     }
@@ -1490,8 +1492,8 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
     for (size_t gi = 0; gi < groups.size(); gi++) {
         const Group &g = groups[gi];
         tc::presence_rows_kernel<<<static_cast<uint32_t>(g.ld), 256, bits_smem, s>>>(
-            g.d_sample_ptr, g.d_start_col, d_parent_col, d_lhi, d_llo, d_lsorted, static_cast<uint32_t>(g.ld),
-            k_pad, d_A, d_Bh, d_Bl, d_r);
+            g.d_sample_ptr, g.d_start_col, d_parent_col, d_lq, d_lsorted, static_cast<uint32_t>(g.ld), k_pad,
+            d_A, d_B, d_r);
         launches++;
         if (gi == 0 && timed()) SSU_CK(cudaEventRecord(ev[1], s));
         if (g.n_tiles) {
@@ -1511,7 +1513,7 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
             a.wait_cycles = gemm_wait_cycles;
             a.stall = union_stall;
             // two CTAs (one cluster) per work unit, started in unit order
-            tc::unweighted_tc_kernel<<<2 * g.n_tiles, tc::THREADS, tc::SMEM_BYTES, s>>>(map_A, map_Bh, map_Bl, a);
+            tc::unweighted_tc_kernel<<<2 * g.n_tiles, tc::THREADS, tc::SMEM_BYTES, s>>>(map_A, map_B, a);
             launches++;
         }
         if (gi + 1 == groups.size() && timed()) SSU_CK(cudaEventRecord(ev[2], s));
@@ -1550,8 +1552,8 @@ int PlanImpl::execute_gemm_overlap(void *host) {
     zero_diagonal(s, d_full);  // the units never write the diagonal
     const size_t bits_smem = sizeof(uint32_t) * (k_pad / 32);
     tc::presence_rows_kernel<<<static_cast<uint32_t>(g.ld), 256, bits_smem, s>>>(
-        g.d_sample_ptr, g.d_start_col, d_parent_col, d_lhi, d_llo, d_lsorted, static_cast<uint32_t>(g.ld), k_pad,
-        d_A, d_Bh, d_Bl, d_r);
+        g.d_sample_ptr, g.d_start_col, d_parent_col, d_lq, d_lsorted, static_cast<uint32_t>(g.ld), k_pad, d_A, d_B,
+        d_r);
     launches++;
     SSU_CK(cudaEventRecord(band_ev[nb], s));
     SSU_CK(cudaStreamWaitEvent(s1, band_ev[nb], 0));
@@ -1574,7 +1576,7 @@ int PlanImpl::execute_gemm_overlap(void *host) {
             a.error = d_error;
             a.wait_cycles = gemm_wait_cycles;
             a.stall = union_stall;
-            tc::unweighted_tc_kernel<<<2 * (u1 - u0), tc::THREADS, tc::SMEM_BYTES, st>>>(map_A, map_Bh, map_Bl, a);
+            tc::unweighted_tc_kernel<<<2 * (u1 - u0), tc::THREADS, tc::SMEM_BYTES, st>>>(map_A, map_B, a);
             launches++;
         }
         SSU_CK(cudaEventRecord(band_ev[p], st));
@@ -1607,16 +1609,19 @@ int resolve_autotune(int requested, bool batch) {
 namespace {
 
 // Unweighted methods (not variance adjusted) on the tensor-core contraction:
-// by default for fp32 results (its ~2.5e-7 relative error is inside the
+// by default for fp32 results (its ~1e-8 relative error is far inside the
 // fp32 stripe form's own), on request for fp64.  Presence is "proportion >
 // 0", the OR of the tips below a node, so it needs counts that are not
-// negative.  A batch with bypassed tips keeps the stripe form (its tables'
-// trees differ in which rows carry length).
-bool use_tensor_cores(const MethodSpec &spec, const TableSet &set, bool batch) {
+// negative, and the lengths are fixed-point magnitudes, so they must not be
+// negative either.  A batch with bypassed tips keeps the stripe form (its
+// tables' trees differ in which rows carry length).
+bool use_tensor_cores(const MethodSpec &spec, const TableSet &set, const FlatTree &tree, bool batch) {
     if (spec.vaw || !(spec.method == Method::unweighted || spec.method == Method::unweighted_unnormalized))
         return false;
     bool want = spec.unweighted_gemm || (!spec.fp64 && !spec.unweighted_stripe);
     if (batch && spec.bypass_tips) want = false;
+    for (uint32_t e = 0; want && e < tree.n_embedded; e++)
+        if (!(tree.length[e] >= 0.0 && std::isfinite(tree.length[e]))) want = false;
     for (const Table *t : set.tables)
         for (uint64_t q = 0; want && q < t->nnz(); q++)
             if (!(t->data[q] >= 0.0)) want = false;
@@ -1636,7 +1641,7 @@ int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spe
     TableSet set;
     set.tables.push_back(&table);
     set.embedded.push_back(tree.n_embedded);
-    m.gemm = use_tensor_cores(spec, set, false);
+    m.gemm = use_tensor_cores(spec, set, tree, false);
     int rc = m.setup(set, tree, BatchOptions{});
     if (!rc) rc = m.gemm ? m.setup_gemm(set, tree) : spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
     if (rc) {
@@ -1663,7 +1668,7 @@ int Plan::create_batch(const TableSet &set, const FlatTree &tree, const MethodSp
     m.batch = true;
     m.stream = static_cast<cudaStream_t>(stream);
     m.autotune = resolve_autotune(opts.autotune, true);
-    m.gemm = use_tensor_cores(spec, set, true);
+    m.gemm = use_tensor_cores(spec, set, tree, true);
     int rc = m.setup(set, tree, opts);
     if (!rc) rc = m.gemm ? m.setup_gemm(set, tree) : spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
     if (rc) {

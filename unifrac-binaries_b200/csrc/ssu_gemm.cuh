@@ -14,26 +14,29 @@
 // e * G[k][l] in G is at most 2 e of the result; r is an fp64 sum of the
 // true lengths.
 //
-// Operands (fp16, K-major, built by `presence_rows_kernel`): A = X, and
-// B_hi / B_lo = (1 - X) * (L 2^s_c) split into an integer part hi (at most
-// 2048, exact in fp16) and lo = fp16(L 2^s_c - hi).  Nodes are sorted by
-// decreasing length and packed into chunks of whole 64-node K blocks whose
+// Operands (8-bit, K-major, built by `presence_rows_kernel`): A = X (0/1),
+// and B = (1 - X) * q where q is the length in 24-bit fixed point, split
+// into three byte planes q = q0 + 2^8 q1 + 2^16 q2 (`kind::i8`, unsigned,
+// int32 accumulate: every plane sum is exact).  Nodes are sorted by
+// decreasing length and packed into chunks of whole 128-node K blocks whose
 // lengths lie within a factor of two of the chunk's largest (zero-length
-// padding columns close a chunk); chunk c is scaled by 2^s_c so its lengths
-// fall in [512, 2048).  So every term keeps 22 significant bits, and a
-// chunk's hi sums are exact in the fp32 accumulator (at most 127 blocks x 64
-// nodes x 2048 < 2^24).  Each chunk is accumulated in tensor memory (TMEM),
-// then promoted to fp64 registers scaled back by 2^-s_c.
+// padding columns close a chunk); chunk c is scaled by 2^s_c so its largest
+// length lies in [2^23, 2^24): q = round(L 2^s_c) keeps 23 significant bits
+// of every length, and a chunk's plane sums stay below 2^31 (at most 4096
+// blocks x 128 nodes x 255).  Each chunk is accumulated in tensor memory
+// (TMEM), then S0 + 2^8 S1 + 2^16 S2 (exact in int64) is promoted to fp64
+// registers scaled back by 2^-s_c.  The only rounding before fp64 is the
+// quantisation of each length (relative 2^-24 .. 2^-23).
 //
-// Work unit: a cluster of two CTAs (cta_group::2) owns 256 rows k x 128
-// columns l of one table.  One MMA per 16 nodes is M = 256 (128 rows per
-// CTA) x N = 256: the first 128 columns of B are B_hi of the 128 columns l
-// (held by CTA 0), the last 128 are B_lo of the same columns (held by CTA 1),
-// so the hi and lo sums land in separate accumulators.  Per CTA: warp 0
-// issues its TMA loads (its 128 rows of A and its half of B, 64 nodes,
-// 128-byte swizzle, no multicast) into a 6-stage ring whose full barriers
+// Work unit: a cluster of two CTAs (cta_group::2) owns 256 rows k x 64
+// columns l of one table.  One MMA per 32 nodes is M = 256 (128 rows per
+// CTA) x N = 192: B's rows are ordered 3 l + p (column l, plane p), so the
+// unit's 192 B rows are its 64 columns' three planes, 96 held by each CTA,
+// and TMEM column 3 c + p holds column c's plane-p sum.  Per CTA: warp 0
+// issues its TMA loads (its 128 rows of A and its 96 rows of B, 128 nodes,
+// 128-byte swizzle, no multicast) into a 7-stage ring whose full barriers
 // live in CTA 0; in CTA 0 one thread of warp 1 issues the MMAs, into one of
-// two 256-column TMEM accumulators per CTA, and commits each stage's release
+// two 192-column TMEM accumulators per CTA, and commits each stage's release
 // and each chunk's completion to both CTAs; warps 2..9 of both CTAs drain a
 // finished accumulator into fp64 registers while the next chunk accumulates,
 // and finally form the distances and write them.  Every mbarrier wait is
@@ -43,7 +46,6 @@
 
 #include <cstdint>
 #include <cuda.h>
-#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "ssu_kernels.cuh"
@@ -52,29 +54,35 @@ namespace ssu {
 namespace tc {
 
 constexpr int ROWS = 128;        // rows k per CTA (M = 256 per cluster)
-constexpr int COLS = 128;        // columns l per work unit
-constexpr int BLOCK_K = 64;      // fp16 nodes per stage row: one 128-byte swizzle atom
-constexpr int UMMA_K = 16;
+constexpr int COLS = 64;         // columns l per work unit
+constexpr int PLANES = 3;        // byte planes of a length
+constexpr int BLOCK_K = 128;     // 8-bit nodes per stage row: one 128-byte swizzle atom
+constexpr int UMMA_K = 32;
 constexpr int UMMA_M = 2 * ROWS;
-constexpr int UMMA_N = 2 * COLS; // hi and lo planes
-constexpr int STAGES = 6;
-constexpr int MAX_CHUNK_KB = 127;  // 127 x 64 x 2048 < 2^24: exact hi sums
-constexpr int ACC_COLS = UMMA_N;
-constexpr int TMEM_COLS = 2 * ACC_COLS;
+constexpr int UMMA_N = PLANES * COLS;  // 192
+constexpr int B_ROWS = UMMA_N / 2;     // B rows held by each CTA of the pair
+constexpr int STAGES = 7;
+constexpr int MAX_CHUNK_KB = 4096;     // 4096 x 128 x 255 < 2^31: exact plane sums
+constexpr int QBITS = 24;              // fixed-point bits of the largest length of a chunk
+constexpr int ACC_STRIDE = 256;        // TMEM columns between the two accumulators
+constexpr int TMEM_COLS = 512;
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
-constexpr uint32_t TILE_BYTES = ROWS * BLOCK_K * 2;
-constexpr uint32_t STAGE_BYTES = 2 * TILE_BYTES;  // A rows + one B plane, per CTA
+constexpr uint32_t A_BYTES = ROWS * BLOCK_K;
+constexpr uint32_t B_BYTES = B_ROWS * BLOCK_K;
+constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;  // per CTA
 constexpr size_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-static_assert(TMEM_COLS <= 512, "two accumulators must fit the 512 TMEM columns");
+static_assert(UMMA_N % 32 == 0 && UMMA_N <= 256, "kind::i8 with cta_group::2 takes N in multiples of 32 up to 256");
+static_assert(UMMA_N <= ACC_STRIDE && 2 * ACC_STRIDE <= TMEM_COLS, "two accumulators must fit the TMEM allocation");
+static_assert(A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "operand tiles must keep 1024-byte swizzle alignment");
 static_assert(SMEM_BYTES <= 227 * 1024, "stage ring exceeds shared memory");
-static_assert(static_cast<long long>(MAX_CHUNK_KB) * BLOCK_K * 2048 < (1LL << 24), "hi sums must stay exact");
+static_assert(static_cast<long long>(MAX_CHUNK_KB) * BLOCK_K * 255 < (1LL << 31), "plane sums must stay exact");
 
 enum : int { ERR_NONE = 0, ERR_FULL_WAIT = 1, ERR_EMPTY_WAIT = 2, ERR_ACC_FULL_WAIT = 3, ERR_ACC_EMPTY_WAIT = 4,
              ERR_DONE_WAIT = 5, ERR_DRAIN_WAIT = 6 };
 
 struct GemmArgs {
-    const uint4 *tiles;         // x = 256-row block k, y = 128-column block l, z = table
+    const uint4 *tiles;         // x = 256-row block k, y = 64-column block l, z = table
     uint32_t n_tiles;
     const dev::TableDesc *tables;
     uint32_t n_kblocks;         // padded nodes / BLOCK_K
@@ -107,10 +115,10 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     return d;
 }
 
-// Instruction descriptor, kind::f16: D f32, A and B f16, both K-major, M x N
-// (M counts both CTAs of the pair).
-__host__ __device__ constexpr uint32_t f16_idesc(int m, int n) {
-    return (1u << 4) | (0u << 7) | (0u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
+// Instruction descriptor, kind::i8: D s32, A and B unsigned 8-bit, both
+// K-major, M x N (M counts both CTAs of the pair).
+__host__ __device__ constexpr uint32_t i8_idesc(int m, int n) {
+    return (2u << 4) | (0u << 7) | (0u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
            (static_cast<uint32_t>(m >> 4) << 24);
 }
 
@@ -162,11 +170,11 @@ __device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *m
         "l"(map), "r"(bar_cl), "r"(x), "r"(y)
         : "memory");
 }
-__device__ __forceinline__ void umma_f16_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+__device__ __forceinline__ void umma_i8_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}" ::"r"(
             d_tmem),
         "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0), "r"(0));
 }
@@ -199,8 +207,8 @@ __device__ __forceinline__ void fail(int *shared_abort, int *global_err, int cod
 }
 
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
-    unweighted_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmBh,
-                         const __grid_constant__ CUtensorMap tmBl, const GemmArgs args) {
+    unweighted_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                         const GemmArgs args) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);  // used in CTA 0
@@ -217,7 +225,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
     const dev::TableDesc td = args.tables[tile.z];
     const uint32_t k0 = tile.x * UMMA_M + rank * ROWS;  // this CTA's first row, table-local
     const uint32_t l0 = tile.y * COLS;
-    const int arow = static_cast<int>(td.base + k0), brow = static_cast<int>(td.base + l0);
+    // this CTA's rows: 128 of A, and B rows 3 l + p of its half of the 192
+    const int arow = static_cast<int>(td.base + k0);
+    const int brow = static_cast<int>(PLANES * (td.base + l0) + rank * B_ROWS);
     const uint32_t nkb = args.n_kblocks, nchunks = args.n_chunks;
     const long long budget = args.wait_cycles;
 
@@ -258,7 +268,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
     if (warp == 0) {
         if (lane == 0) {
             // TMA producer of this CTA; the pair's stage completes on CTA 0's barrier
-            const CUtensorMap *mb = rank == 0 ? &tmBh : &tmBl;
             for (uint32_t kb = 0; kb < (args.stall ? 0u : nkb); kb++) {
                 const uint32_t s = kb % STAGES, use = kb / STAGES;
                 if (*vabort) break;
@@ -269,14 +278,14 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                 uint8_t *st = smem + s * STAGE_BYTES;
                 if (rank == 0) mbar_expect_tx(full + s, 2 * STAGE_BYTES);
                 tma_load_2d_pair(st, &tmA, full0 + s * 8, static_cast<int>(kb) * BLOCK_K, arow);
-                tma_load_2d_pair(st + TILE_BYTES, mb, full0 + s * 8, static_cast<int>(kb) * BLOCK_K, brow);
+                tma_load_2d_pair(st + A_BYTES, &tmB, full0 + s * 8, static_cast<int>(kb) * BLOCK_K, brow);
                 issued = kb + 1;
             }
         }
     } else if (warp == 1) {
         if (lane == 0 && rank == 0) {
             // MMA issuer for the pair
-            constexpr uint32_t idesc = f16_idesc(UMMA_M, UMMA_N);
+            constexpr uint32_t idesc = i8_idesc(UMMA_M, UMMA_N);
             uint32_t kb = 0;
             for (uint32_t c = 0; c < nchunks && !*vabort; c++) {
                 const uint32_t buf = c & 1, reuse = c >> 1;
@@ -285,7 +294,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d = tmem + buf * ACC_COLS;
+                const uint32_t d = tmem + buf * ACC_STRIDE;
                 const uint32_t kstart = kb, kend = args.chunk_end[c];
                 bool good = true;
                 for (; kb < kend; kb++) {
@@ -298,12 +307,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                     tc_fence_after();
                     const uint32_t st = smem_u32(smem + s * STAGE_BYTES);
                     const uint64_t a0 = sw128_desc(st);
-                    const uint64_t b0 = sw128_desc(st + TILE_BYTES);
+                    const uint64_t b0 = sw128_desc(st + A_BYTES);
 #pragma unroll
                     for (int ks = 0; ks < BLOCK_K / UMMA_K; ks++) {
-                        // advance 16 fp16 = 32 bytes along K inside the swizzle atom
-                        const uint64_t koff = static_cast<uint64_t>((ks * UMMA_K * 2) >> 4);
-                        umma_f16_pair(d, a0 + koff, b0 + koff, idesc, (kb != kstart || ks != 0) ? 1u : 0u);
+                        // advance 32 bytes along K inside the swizzle atom
+                        const uint64_t koff = static_cast<uint64_t>((ks * UMMA_K) >> 4);
+                        umma_i8_pair(d, a0 + koff, b0 + koff, idesc, (kb != kstart || ks != 0) ? 1u : 0u);
                     }
                     umma_commit_pair(empty + s);
                 }
@@ -314,12 +323,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
         }
     } else {
         // epilogue: warp w reads TMEM lanes 32*(w%4).. and half (w-2)/4 of the
-        // 128 columns, each column's hi and lo sums
+        // 64 columns, each column's three plane sums
         const int q = warp & 3;
         const int half = (warp - 2) >> 2;
-        double acc[COLS / 2];
+        constexpr int HC = COLS / 2;  // columns per epilogue warp
+        double acc[HC];
 #pragma unroll
-        for (int i = 0; i < COLS / 2; i++) acc[i] = 0.0;
+        for (int i = 0; i < HC; i++) acc[i] = 0.0;
         for (uint32_t c = 0; c < nchunks; c++) {
             const uint32_t buf = c & 1, use = c >> 1;
             if (*vabort || !mbar_wait_cl(accf + buf, use & 1, budget)) {
@@ -329,18 +339,24 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
             }
             tc_fence_after();
             const double sc = args.chunk_scale[c];
-            const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16) + buf * ACC_COLS + half * (COLS / 2);
+            const uint32_t base =
+                tmem + (static_cast<uint32_t>(q * 32) << 16) + buf * ACC_STRIDE + half * (PLANES * HC);
 #pragma unroll
-            for (int j = 0; j < COLS / 2 / 16; j++) {
-                uint32_t hv[16], lv[16];
-                tmem_ld16(base + j * 16, hv);
-                tmem_ld16(base + COLS + j * 16, lv);
+            for (int g = 0; g < HC / 16; g++) {
+                // 16 columns = 48 consecutive TMEM columns (3 c + p)
+                uint32_t v0[16], v1[16], v2[16];
+                tmem_ld16(base + g * 48, v0);
+                tmem_ld16(base + g * 48 + 16, v1);
+                tmem_ld16(base + g * 48 + 32, v2);
                 tmem_wait_ld();
 #pragma unroll
-                for (int i = 0; i < 16; i++)
-                    acc[j * 16 + i] = fma(static_cast<double>(__uint_as_float(hv[i])) +
-                                              static_cast<double>(__uint_as_float(lv[i])),
-                                          sc, acc[j * 16 + i]);
+                for (int i = 0; i < 16; i++) {
+                    auto plane = [&](int t) -> unsigned long long {
+                        return t < 16 ? v0[t] : t < 32 ? v1[t - 16] : v2[t - 32];
+                    };
+                    const unsigned long long t = plane(3 * i) + (plane(3 * i + 1) << 8) + (plane(3 * i + 2) << 16);
+                    acc[g * 16 + i] = fma(static_cast<double>(t), sc, acc[g * 16 + i]);
+                }
             }
             tc_fence_before();
             __syncwarp();
@@ -354,10 +370,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                 o.ptr = static_cast<char *>(o.ptr) + td.out_off * (args.out_fp64 ? sizeof(double) : sizeof(float));
             const double *rt = args.r + td.base;
             const double rk = rt[k];
-            const uint32_t lb = l0 + half * (COLS / 2);
+            const uint32_t lb = l0 + half * HC;
             // fully unrolled: acc stays in registers
 #pragma unroll
-            for (int j = 0; j < COLS / 2; j++) {
+            for (int j = 0; j < HC; j++) {
                 const uint32_t l = lb + j;
                 if (k < l && l < n) {
                     const double rl = rt[l];
@@ -458,14 +474,14 @@ __global__ void __launch_bounds__(1024) exclusive_scan_kernel(const uint32_t *__
 
 // Presence rows for the contraction, one CTA per sample (padding rows too):
 // walk up from every present tip, marking embedded ancestors in a shared
-// bitmap (stopping at nodes already marked), then write the sample's rows of
-// A = X and B_hi, B_lo = (1 - X) L (fp16) in full, 16 bytes per thread, and
-// r = sum L of the present nodes (fp64, fixed reduction order).
+// bitmap (stopping at nodes already marked), then write the sample's row of
+// A = X and its three rows 3 j + p of B = (1 - X) q_p (8-bit, 16 nodes and
+// 16 bytes per store), and r = sum L of the present nodes (fp64, fixed
+// reduction order).  lq holds the length planes: plane p at lq + p * k_pad.
 __global__ void presence_rows_kernel(const uint32_t *__restrict__ sample_ptr, const int32_t *__restrict__ start_col,
-                                     const int32_t *__restrict__ parent_col, const __half *__restrict__ l_hi,
-                                     const __half *__restrict__ l_lo, const double *__restrict__ l_sorted,
-                                     uint32_t n, uint32_t k_pad, __half *__restrict__ A, __half *__restrict__ Bh,
-                                     __half *__restrict__ Bl, double *__restrict__ r) {
+                                     const int32_t *__restrict__ parent_col, const uint8_t *__restrict__ lq,
+                                     const double *__restrict__ l_sorted, uint32_t n, uint32_t k_pad,
+                                     uint8_t *__restrict__ A, uint8_t *__restrict__ B, double *__restrict__ r) {
     extern __shared__ uint32_t bits[];  // k_pad / 32 words
     __shared__ double red[256];
     const uint32_t j = blockIdx.x;
@@ -484,22 +500,28 @@ __global__ void presence_rows_kernel(const uint32_t *__restrict__ sample_ptr, co
         }
     }
     __syncthreads();
-    const uint64_t row = static_cast<uint64_t>(j) * k_pad;
+    const uint64_t arow = static_cast<uint64_t>(j) * k_pad;
+    const uint64_t brow = static_cast<uint64_t>(PLANES) * j * k_pad;
     double part = 0.0;
-    for (uint32_t c8 = threadIdx.x * 8; c8 < k_pad; c8 += blockDim.x * 8) {
-        const uint32_t b = (bits[c8 >> 5] >> (c8 & 31)) & 0xFFu;
-        __align__(16) __half xa[8], xh[8], xl[8];
+    for (uint32_t c16 = threadIdx.x * 16; c16 < k_pad; c16 += blockDim.x * 16) {
+        const uint32_t b = (bits[c16 >> 5] >> (c16 & 31)) & 0xFFFFu;
+        uint32_t on[4], keep[4];
 #pragma unroll
-        for (int t = 0; t < 8; t++) {
-            const bool on = (b >> t) & 1u;
-            xa[t] = on ? __float2half(1.0f) : __float2half(0.0f);
-            xh[t] = on ? __float2half(0.0f) : l_hi[c8 + t];
-            xl[t] = on ? __float2half(0.0f) : l_lo[c8 + t];
-            if (on) part += l_sorted[c8 + t];
+        for (int w = 0; w < 4; w++) {
+            const uint32_t nib = (b >> (4 * w)) & 0xFu;
+            on[w] = (nib & 1u) | (((nib >> 1) & 1u) << 8) | (((nib >> 2) & 1u) << 16) | (((nib >> 3) & 1u) << 24);
+            keep[w] = ~(on[w] * 0xFFu);  // 0xFF in the bytes of absent nodes
         }
-        *reinterpret_cast<uint4 *>(A + row + c8) = *reinterpret_cast<const uint4 *>(xa);
-        *reinterpret_cast<uint4 *>(Bh + row + c8) = *reinterpret_cast<const uint4 *>(xh);
-        *reinterpret_cast<uint4 *>(Bl + row + c8) = *reinterpret_cast<const uint4 *>(xl);
+        *reinterpret_cast<uint4 *>(A + arow + c16) = make_uint4(on[0], on[1], on[2], on[3]);
+#pragma unroll
+        for (int pl = 0; pl < PLANES; pl++) {
+            const uint4 qv = *reinterpret_cast<const uint4 *>(lq + static_cast<uint64_t>(pl) * k_pad + c16);
+            *reinterpret_cast<uint4 *>(B + brow + static_cast<uint64_t>(pl) * k_pad + c16) =
+                make_uint4(qv.x & keep[0], qv.y & keep[1], qv.z & keep[2], qv.w & keep[3]);
+        }
+#pragma unroll
+        for (int t = 0; t < 16; t++)
+            if ((b >> t) & 1u) part += l_sorted[c16 + t];
     }
     red[threadIdx.x] = part;
     __syncthreads();
