@@ -708,6 +708,23 @@ def run_small(args):
     print(json.dumps(line), flush=True)
 
 
+def _batch_e2e(torch, ssu_b200, tree, tables, method, units, steps, **kw):
+    """The batch C API end to end (host tables in, host matrices out): one
+    untimed call (first-use costs: memory pools, page-locked results, tuning),
+    then `steps` timed calls; seconds per call."""
+    times = []
+    for i in range(steps + 1):
+        t0 = time.perf_counter()
+        out = ssu_b200.one_off_batch(tree, tables, method, copy=False, **kw)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        del out
+        if i > 0:
+            times.append(dt)
+    sec = sum(times) / len(times)
+    return {"seconds": sec, "value": units / sec}
+
+
 def run_replicates(args):
     """100 rarefied replicates (depth 1,000) of a 10,000-feature x 5,000-sample
     table on a 10,000-tip tree, unweighted and weighted-normalized fp32, every
@@ -740,12 +757,7 @@ def run_replicates(args):
         plan.close()
         # end to end through the batch C API: host tables in, host matrices out
         if args.e2e_steps > 0:
-            t0 = time.perf_counter()
-            out = ssu_b200.one_off_batch(tree, reps, m, copy=False)
-            torch.cuda.synchronize()
-            dt = time.perf_counter() - t0
-            e2e[m] = {"seconds": dt, "value": units / dt}
-            del out
+            e2e[m] = _batch_e2e(torch, ssu_b200, tree, reps, m, units, args.e2e_steps)
         per_table_ms = _unbatched_ms(torch, ssu_b200, tree, reps, m, stream)
         single = ssu_b200.Plan(tree, reps[0], m)
         single.execute()
@@ -816,11 +828,15 @@ def run_uneven_tables(args):
         total_units += units
         total_ms += ms
         res = plan.results()
+        info = {"groups": plan.n_groups(), "tuning": plan.tuning(), "kernel": plan.pair_kernel(),
+                "launches_per_step": plan.launches()}
+        plan.close()
         per_table_ms = _unbatched_ms(torch, ssu_b200, tree, tables, m, stream, variance_adjust=vaw, alpha=0.5)
         entry = {"method": m, "variance_adjust": vaw, "ms_per_step": ms, "value": units / (ms / 1e3),
                  "one_plan_per_table_ms": per_table_ms, "batched_speedup": per_table_ms / ms,
-                 "units": units, "groups": plan.n_groups(), "tuning": plan.tuning(), "kernel": plan.pair_kernel(),
-                 "launches_per_step": plan.launches(), "plan_create_s": create_s, "clocks": clk}
+                 "units": units, **info, "plan_create_s": create_s, "clocks": clk}
+        if args.e2e_steps > 0:
+            entry["e2e"] = _batch_e2e(torch, ssu_b200, tree, tables, m, units, 1, variance_adjust=vaw, alpha=0.5)
         if oracle_py.ref_available():
             worst = 0.0
             for t in small:
@@ -830,7 +846,7 @@ def run_uneven_tables(args):
                                                  "max_rel": worst}
         per.append(entry)
         del res
-        plan.close()
+    e2e_s = sum(e["e2e"]["seconds"] for e in per if "e2e" in e)
     line = {
         "metric": METRIC, "value": total_units / (total_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms, "higher_is_better": True, "scaling": "weak",
@@ -841,6 +857,12 @@ def run_uneven_tables(args):
                                "weighted_unnormalized / generalized a=0.5, fp64, full matrices",
                    "l2": "flushed between steps; embedding > L2", "generation_s": gen_s},
         "methods": per,
+        "e2e": {"value": total_units / e2e_s if e2e_s else None, "unit": UNIT,
+                "ms_per_step": e2e_s * 1e3 if e2e_s else None,
+                "h2d_bytes_per_step": sum(int(t.indptr.nbytes + t.indices.nbytes + t.data.nbytes) for t in tables)
+                * len(per),
+                "d2h_bytes_per_step": sum(8 * t.n_samples ** 2 for t in tables) * len(per),
+                "path": "ssu_b200_one_off_batch_inmem_v3 per method, one untimed call first"},
         "gpu_launches": launches * args.steps,
     }
     print(json.dumps(line), flush=True)

@@ -317,6 +317,20 @@ def test_weighted_sparse_and_dense_forms_agree(ssu, monkeypatch, method, prec):
         np.testing.assert_allclose(hybrid, dense, rtol=5e-6, atol=1e-7)
 
 
+@pytest.mark.parametrize("method", ["weighted_normalized", "weighted_unnormalized"])
+def test_weighted_fp32_deterministic_mode_repeats_bit_for_bit(ssu, monkeypatch, method):
+    """UNIFRAC_B200_DETERMINISTIC=1 gives fp32 plans the owner-per-element
+    walk of the sparse rows (no atomics): repeated calls agree bit for bit,
+    and with the default (atomic) form to fp32 rounding."""
+    tree, table = _case(64, n_tips=400, n_samples=600, density=0.02)
+    default, _ = ssu.one_off_matrix(tree, table, f"{method}_fp32")
+    monkeypatch.setenv("UNIFRAC_B200_DETERMINISTIC", "1")
+    runs = [ssu.one_off_matrix(tree, table, f"{method}_fp32")[0] for _ in range(3)]
+    for r in runs[1:]:
+        np.testing.assert_array_equal(r, runs[0])
+    np.testing.assert_allclose(runs[0], default, rtol=2e-6, atol=1e-7)
+
+
 UNION_RUNS = [("generalized", False, 0.5), ("generalized", False, 0.0), ("generalized", False, 1.0),
               ("generalized", False, 0.25), ("unweighted", True, 1.0), ("unweighted_unnormalized", True, 1.0),
               ("weighted_normalized", True, 1.0), ("weighted_unnormalized", True, 1.0),

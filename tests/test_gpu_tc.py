@@ -144,3 +144,22 @@ def test_tc_negative_lengths_keep_the_stripe_form(ssu, oracle_mod, gemm_mode):
     ref = oracle_mod.oracle_one_off(tree, table, "unweighted_fp64")["matrix"]
     r, z = rel_err(gpu, ref)
     assert r <= 1e-12 and z <= 1e-13, (r, z)
+
+
+def test_tc_band_tuning_changes_no_result(ssu):
+    """Batch plans time the band height of the unit order (2, 4 or 8 row
+    blocks) and keep the fastest; the order changes no result, bit for bit."""
+    tree = ssu_synth.random_binary_tree(900, 0.05, 41)
+    tables = [ssu_synth.geometric_table(tree.tip_names()[:850], n, 0.08, 6.0, 42 + n) for n in (700, 1100)]
+    method = "unweighted"  # fp32 results: the tensor-core form by default
+    fixed = ssu.BatchPlan(tree, tables, method, autotune=0)
+    fixed.execute()
+    ref = fixed.results()
+    assert "band 4" in fixed.tuning()
+    fixed.close()
+    tuned = ssu.BatchPlan(tree, tables, method, autotune=1)
+    assert "band" in tuned.tuning() and ("measured" in tuned.tuning() or "cache" in tuned.tuning())
+    tuned.execute()
+    for a, b in zip(tuned.results(), ref):
+        np.testing.assert_array_equal(a, b)
+    tuned.close()

@@ -114,3 +114,40 @@ def test_noalloc_rejects_sizes_beyond_its_limit(ssu, torch_cuda):
     assert f(p + 8, p, 1, 100, 128, 1, p, None) == 6     # embedding not 16-byte aligned
     assert f(p, p + 4, 1, 100, 128, 1, p, None) == 6     # lengths not 8-byte aligned
     assert f(p, p, 1, 100, 128, 1, p + 4, None) == 6     # output not 8-byte aligned
+
+
+def test_noalloc_call_captured_in_a_graph_replays_correctly(ssu, torch_cuda):
+    """After a first call on the device, a call made while its stream is
+    being captured becomes part of the graph: it reads no host memory at
+    replay time (the tile list and table descriptor are written on the
+    device), so replaying the graph recomputes the same matrix."""
+    torch = torch_cuda
+    tree = ssu_synth.random_binary_tree(300, 0.1, 81)
+    table = ssu_synth.geometric_table(tree.tip_names()[:280], 140, 0.08, 12.0, 82)
+    U, lens = host_embedding(ssu, tree, table)
+    n = table.n_samples
+    st, first = call_noalloc(ssu, torch, U, lens, n, True)  # the first call sets the device up
+    assert st == 0
+    L = ssu.lib()
+    f = L.ssu_b200_weighted_pairs_noalloc
+    ld = ((n + 127) // 128) * 128
+    padded = np.zeros((U.shape[0], ld))
+    padded[:, :n] = U
+    d_u = torch.from_numpy(padded).cuda()
+    d_len = torch.from_numpy(np.ascontiguousarray(lens)).cuda()
+    d_out = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    status = []
+    with torch.cuda.graph(graph, stream=stream):
+        status.append(f(d_u.data_ptr(), d_len.data_ptr(), U.shape[0], n, ld, 1, d_out.data_ptr(),
+                        ctypes.c_void_p(stream.cuda_stream)))
+    assert status == [0]
+    d_out.fill_(float("nan"))
+    graph.replay()
+    torch.cuda.synchronize()
+    got = d_out.cpu().numpy()
+    r, z = rel_err(got, first)
+    assert r == 0.0 and z == 0.0, (r, z)
+    del graph

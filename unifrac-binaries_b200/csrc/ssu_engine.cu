@@ -313,6 +313,7 @@ struct PlanImpl {
     // sparse rows on their intersections, flagged tiles recomputed exactly)
     bool hybrid = false;
     uint32_t hybrid_div = 8;  // rows non-zero in more than ld / hybrid_div columns are dense
+    bool hybrid_atomic = false;  // sparse updates with shared-memory atomics (fp32 default)
     bool nonneg_data = true;  // no negative count in any table
     unsigned long long *d_masks = nullptr;
     uint32_t *d_counts = nullptr, *d_dense_rows = nullptr, *d_sparse_rows = nullptr, *d_nrows = nullptr;
@@ -367,6 +368,10 @@ struct PlanImpl {
     int *d_error = nullptr;
     CUtensorMap map_A{}, map_B{};
     int setup_gemm(const TableSet &set, const FlatTree &tree);
+    int build_units(uint32_t band);
+    int tune_band();
+    bool device_error_pending();
+    uint32_t tc_band = 4;
     int execute_gemm(cudaStream_t s, const dev::OutSpec &out);
     int execute_gemm_overlap(void *host);
     // overlapped copy-out: a second compute stream, the copy stream, and an
@@ -742,11 +747,18 @@ int PlanImpl::setup_hybrid() {
     part_chunk = part_chunk ? part_chunk : 512;
     n_parts = std::max<uint32_t>(1, (E + part_chunk - 1) / part_chunk);
     SSU_CK(alloc(&d_ws_part, sizeof(double) * ld * n_parts));
-    auto kfn = dev::pair_hybrid_kernel<T, true>;
-    auto kfu = dev::pair_hybrid_kernel<T, false>;
+    // UNIFRAC_B200_DETERMINISTIC=1: fp32 plans also take the owner walk, so
+    // their results repeat bit for bit (about 13% slower on replicate tables)
+    hybrid_atomic = sizeof(T) == 4 && !env_int("UNIFRAC_B200_DETERMINISTIC", 0);
     const int smem = static_cast<int>(dev::hybrid_smem<T>());
-    SSU_CK(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    SSU_CK(cudaFuncSetAttribute(kfu, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    SSU_CK(cudaFuncSetAttribute(dev::pair_hybrid_kernel<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem));
+    SSU_CK(cudaFuncSetAttribute(dev::pair_hybrid_kernel<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem));
+    SSU_CK(cudaFuncSetAttribute(dev::pair_hybrid_kernel<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem));
+    SSU_CK(cudaFuncSetAttribute(dev::pair_hybrid_kernel<T, false, false>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     uint32_t max_tiles = 0;
     hpartial_bytes = 0;
     for (Group &g : groups) {
@@ -831,10 +843,14 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
     const uint32_t ctas = static_cast<uint32_t>(
         std::min<uint64_t>(static_cast<uint64_t>(ntiles) * h.n_splits, static_cast<uint64_t>(n_sms)));
     const size_t smem = dev::hybrid_smem<T>();
-    if (norm)
-        dev::pair_hybrid_kernel<T, true><<<ctas, dev::HTHREADS, smem, s>>>(h);
+    if (norm && hybrid_atomic)
+        dev::pair_hybrid_kernel<T, true, true><<<ctas, dev::HTHREADS, smem, s>>>(h);
+    else if (norm)
+        dev::pair_hybrid_kernel<T, true, false><<<ctas, dev::HTHREADS, smem, s>>>(h);
+    else if (hybrid_atomic)
+        dev::pair_hybrid_kernel<T, false, true><<<ctas, dev::HTHREADS, smem, s>>>(h);
     else
-        dev::pair_hybrid_kernel<T, false><<<ctas, dev::HTHREADS, smem, s>>>(h);
+        dev::pair_hybrid_kernel<T, false, false><<<ctas, dev::HTHREADS, smem, s>>>(h);
     launches++;
     if (h.partial) {
         if (norm)
@@ -1275,6 +1291,95 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
 
 // --------------------------------------------------- tensor-core unweighted
 
+// Tensor-core work units: per table, the (256-row block, 64-column block)
+// pairs holding some pair k < l, ordered in bands of `band` row blocks walked
+// column by column.  Clusters start in launch order as SMs free up, so a
+// unit reads the column block of B that its predecessor is reading and the
+// row block of A that the unit a band height earlier read, both still in L2:
+// each B block comes from DRAM about once per band, each A block about once
+// per table.  The order changes no result (every unit is independent).
+int PlanImpl::build_units(uint32_t band) {
+    band = std::max(1u, band);
+    for (Group &g : groups) {
+        std::vector<uint4> tiles;
+        g.band_unit.clear();
+        g.band_row.clear();
+        for (uint32_t t = g.t0; t < g.t1; t++) {
+            const uint32_t n = tdesc[t].n;
+            const uint32_t nkb = (n + tc::UMMA_M - 1) / tc::UMMA_M, nlb = (n + tc::COLS - 1) / tc::COLS;
+            for (uint32_t k0 = 0; k0 < nkb; k0 += band) {
+                g.band_unit.push_back(static_cast<uint32_t>(tiles.size()));
+                g.band_row.push_back(k0 * tc::UMMA_M);
+                for (uint32_t lb = 0; lb < nlb; lb++)
+                    for (uint32_t kb = k0; kb < std::min(nkb, k0 + band); kb++)
+                        if (static_cast<uint64_t>(kb) * tc::UMMA_M <
+                            std::min<uint64_t>(n, static_cast<uint64_t>(lb + 1) * tc::COLS) - 1)
+                            tiles.push_back(make_uint4(kb, lb, t, 0));
+            }
+            g.band_unit.push_back(static_cast<uint32_t>(tiles.size()));
+            g.band_row.push_back(n);
+        }
+        g.n_tiles = static_cast<uint32_t>(tiles.size());
+        if (!g.d_tiles) SSU_CK(alloc(&g.d_tiles, sizeof(uint4) * std::max<size_t>(tiles.size(), 1)));
+        if (!tiles.empty())
+            SSU_CK(cudaMemcpyAsync(g.d_tiles, tiles.data(), sizeof(uint4) * tiles.size(), cudaMemcpyHostToDevice,
+                                   stream));
+        SSU_CK(cudaStreamSynchronize(stream));  // the host list is released on return
+    }
+    tc_band = band;
+    return 0;
+}
+
+// With tuning on: the band height of the unit order by measurement (one
+// untimed and one timed execute per candidate), cached per (table sizes,
+// nodes, SM count) for the process and UNIFRAC_B200_TUNE_CACHE.
+int PlanImpl::tune_band() {
+    const std::string key = "tc_band|n" + std::to_string(log2_bucket(max_table_n)) + "|c" +
+                            std::to_string(log2_bucket(ld)) + "|E" + std::to_string(log2_bucket(E)) + "|sm" +
+                            std::to_string(n_sms);
+    std::string v;
+    if (TuneCache::get().find(key, v) && v.rfind("band=", 0) == 0) {
+        const int b = std::atoi(v.c_str() + 5);
+        if (b > 0) {
+            tuning = "cache band " + std::to_string(b);
+            return build_units(static_cast<uint32_t>(b));
+        }
+    }
+    cudaEvent_t a = nullptr, b = nullptr;
+    SSU_CK(cudaEventCreate(&a));
+    SSU_CK(cudaEventCreate(&b));
+    const dev::OutSpec out{0, d_full, 0, 0};
+    uint32_t best_band = tc_band;
+    float best = 1e30f;
+    std::string report;
+    int rc = 0;
+    for (uint32_t cand : {2u, 4u, 8u}) {
+        if ((rc = build_units(cand))) break;
+        if ((rc = execute_gemm(stream, out))) break;
+        SSU_CK(cudaEventRecord(a, stream));
+        if ((rc = execute_gemm(stream, out))) break;
+        SSU_CK(cudaEventRecord(b, stream));
+        SSU_CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        SSU_CK(cudaEventElapsedTime(&ms, a, b));
+        report += (report.empty() ? "" : ", ") + std::to_string(cand) + ": " + std::to_string(ms) + " ms";
+        if (ms < best) {
+            best = ms;
+            best_band = cand;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (device_error_pending()) {
+        last_error = "device wait expired while tuning";
+        return kOutputError;
+    }
+    TuneCache::get().put(key, "band=" + std::to_string(best_band));
+    tuning = "measured band " + std::to_string(best_band) + " (" + report + ")";
+    return build_units(best_band);
+}
+
 int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     SetupTimer timer;
     // Embedded nodes by decreasing |length|, packed into chunks of whole
@@ -1410,39 +1515,8 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
         SSU_CK(cudaGetLastError());
     }
     timer.step("gemm_sample_lists");
-    // work units: per table, the (256-row block, 128-column block) pairs
-    // holding some pair k < l, ordered in bands of row blocks walked
-    // column by column.  Clusters start in launch order as SMs free up (one
-    // unit every ~20 us on the 25,000-sample table), so a unit reads the
-    // column block of B that its predecessor is reading and the row block of
-    // A that the unit a band height earlier read, both still in L2: each B block
-    // comes from DRAM about once per band, each A block about once per table.
-    // UNIFRAC_B200_TC_BAND sets the band height (row blocks, default 4: on the
-    // 25,000-sample table 164 ms against 166.6 at 8, 173.9 at 2, 190.4 at 1).
     const uint32_t band = static_cast<uint32_t>(std::max(1, env_int("UNIFRAC_B200_TC_BAND", 4)));
-    for (Group &g : groups) {
-        std::vector<uint4> tiles;
-        g.band_unit.clear();
-        g.band_row.clear();
-        for (uint32_t t = g.t0; t < g.t1; t++) {
-            const uint32_t n = tdesc[t].n;
-            const uint32_t nkb = (n + tc::UMMA_M - 1) / tc::UMMA_M, nlb = (n + tc::COLS - 1) / tc::COLS;
-            for (uint32_t k0 = 0; k0 < nkb; k0 += band) {
-                g.band_unit.push_back(static_cast<uint32_t>(tiles.size()));
-                g.band_row.push_back(k0 * tc::UMMA_M);
-                for (uint32_t lb = 0; lb < nlb; lb++)
-                    for (uint32_t kb = k0; kb < std::min(nkb, k0 + band); kb++)
-                        if (static_cast<uint64_t>(kb) * tc::UMMA_M <
-                            std::min<uint64_t>(n, static_cast<uint64_t>(lb + 1) * tc::COLS) - 1)
-                            tiles.push_back(make_uint4(kb, lb, t, 0));
-            }
-            g.band_unit.push_back(static_cast<uint32_t>(tiles.size()));
-            g.band_row.push_back(n);
-        }
-        g.n_tiles = static_cast<uint32_t>(tiles.size());
-        SSU_CK(upload(&g.d_tiles, tiles.data(), sizeof(uint4) * std::max<size_t>(tiles.size(), 1)));
-    }
-
+    if (const int rc = build_units(band)) return rc;
     timer.step("gemm_tiles");
     n_pad = static_cast<uint32_t>(ld);
     const size_t op_bytes = static_cast<size_t>(n_pad) * k_pad;
@@ -1481,8 +1555,18 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     SSU_CK(alloc(&d_full, (spec.fp64 ? sizeof(double) : sizeof(float)) * std::max<uint64_t>(full_elems, 1)));
     SSU_CK(cudaStreamSynchronize(stream));
     timer.step("gemm_buffers");
-    tuning = "fixed";
+    tuning = "band " + std::to_string(tc_band);
+    if (autotune == 1 && !std::getenv("UNIFRAC_B200_TC_BAND")) {
+        if (const int rc = tune_band()) return rc;
+        timer.step("gemm_tune");
+    }
     return 0;
+}
+
+bool PlanImpl::device_error_pending() {
+    int h = 0;
+    if (!d_error || cudaMemcpy(&h, d_error, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    return h != 0;
 }
 
 int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
@@ -2002,8 +2086,11 @@ const char *Plan::pair_kernel_name() const {
     return impl_->spec.fp64 ? impl_->kd.name : impl_->kf.name;
 }
 const char *Plan::tuning() const {
-    if (impl_->gemm) return "fixed";
     static thread_local std::string s;
+    if (impl_->gemm) {
+        s = "tensor-core units, " + impl_->tuning;
+        return s.c_str();
+    }
     if (impl_->union_mode) return "sparse union 64x64";
     s = impl_->tuning + " " + (impl_->spec.fp64 ? impl_->kd.shape : impl_->kf.shape);
     return s.c_str();

@@ -173,7 +173,10 @@ __device__ __forceinline__ void hybrid_emit(const HybridArgs<T> &a, const TableD
     emit_pair<T>(o, td.n, k, l, v);
 }
 
-template <typename T, bool NORM>
+// ATOMIC: the sparse rows' updates go one warp per row with shared-memory
+// atomics (default for fp32 plans); otherwise the owner-per-element walk
+// (bit-reproducible; always for fp64 plans).
+template <typename T, bool NORM, bool ATOMIC = (sizeof(T) == 4)>
 __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridArgs<T> a) {
     constexpr int TX = 16;         // dense phase: 16 (l) x 32 (k) threads, 4 x 8 pairs each
     constexpr int TM = 4, TN = 8;
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                 Mt[tile_row<HB, TM>(ty, i) * HB + tile_row<HB, TN>(tx, j)] = acc[i][j];
         __syncthreads();
 
-        if constexpr (sizeof(T) == 4) {
+        if constexpr (ATOMIC) {
             // ---- sparse rows, fp32 plans: -2 L min(a, b) where both are non-zero.  Warp w
             // takes batches w, w + 16, ... of 32 consecutive rows (lane i: row i's
             // class, its k-block and l-block mask words and length, fetched two
