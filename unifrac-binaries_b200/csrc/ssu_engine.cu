@@ -542,8 +542,16 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
                  (spec.vaw || spec.method == Method::generalized);
     if (const char *m = std::getenv("UNIFRAC_B200_UNION_MODE"))
         if (std::string(m) == "dense") union_mode = false;
-    if (hybrid || union_mode)
-        max_cols = std::min<uint64_t>(max_cols, std::max<uint64_t>(8192, (max_table_n + 127) / 128 * 128));
+    // Sparse-kernel groups hold as many tables as the memory budget allows:
+    // the whole batch in one embedding pass and one persistent pair launch
+    // where it fits (100 config-4 replicates: 1,440 ms as one group against
+    // 1,432 ms as 100 groups of one; 64 config-5 tables: generalized 1,449
+    // against 1,468 ms as 10 groups of <= 8,192 columns, VAW weighted 1,822
+    // against 1,847 ms).  UNIFRAC_B200_SPARSE_GROUP_COLS caps their columns.
+    if ((hybrid || union_mode) && env_int("UNIFRAC_B200_SPARSE_GROUP_COLS", 0) > 0) {
+        const uint64_t cap = static_cast<uint64_t>(std::max(128, env_int("UNIFRAC_B200_SPARSE_GROUP_COLS", 0)));
+        max_cols = std::min<uint64_t>(max_cols, std::max<uint64_t>(cap, (max_table_n + 127) / 128 * 128));
+    }
     groups.clear();
     uint64_t cols = 0;
     for (uint32_t t = 0; t < n_tables; t++) {
