@@ -233,3 +233,18 @@ def test_compute_permanova_on_reference_outputs(ssu, golden):
     ids = ssu.read_h5(H5_WU, "order", strings=True)
     st, fs, ps = ssu.compute_permanova(TSV, ["empo_2", "empo_3"], m, ids, 99)
     assert st == 0 and len(fs) == 2 and fs[0] != fs[1]
+
+
+def test_permanova_chunked_labels_change_nothing(ssu, monkeypatch):
+    """Permutations evaluated in chunks of columns (a label budget far below
+    one pass) give the same F and p, bit for bit, as one chunk."""
+    L = ssu.lib()
+    m = euclidean_matrix(500, 8, 9)
+    g = np.arange(500) % 4
+    L.ssu_set_random_seed(21)
+    whole = ssu.permanova(m, g, 999)
+    monkeypatch.setenv("UNIFRAC_B200_PERMANOVA_LABEL_BYTES", str(500 * 2 * 64))  # 64 groupings per chunk
+    L.ssu_set_random_seed(21)
+    chunked = ssu.permanova(m, g, 999)
+    L.ssu_set_random_seed(5489)
+    assert chunked == whole

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <numeric>
@@ -201,6 +202,18 @@ __global__ void __launch_bounds__(kRows * 32) permanova_kernel(const TIn *__rest
         else if (total_partial)
             total_partial[blockIdx.x] = s;
     }
+}
+
+// s_w[c] = sum over blocks (in order) of the per-block sums of grouping c,
+// from partial[(c / 32) * blocks + b][c % 32].
+__global__ void column_sums_kernel(const double *__restrict__ partial, uint32_t blocks, uint32_t cols,
+                                   double *__restrict__ s_w) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    const double *p = partial + static_cast<size_t>(c / kPb) * blocks * kPb + c % kPb;
+    double s = 0.0;
+    for (uint32_t b = 0; b < blocks; b++) s += p[static_cast<size_t>(b) * kPb];
+    s_w[c] = s;
 }
 
 // Cyclic Jacobi eigen-decomposition of a symmetric m x m matrix (row-major):
@@ -509,50 +522,69 @@ int permanova_device(const TIn *mat, uint32_t n, const uint32_t *grouping, uint3
     }
     std::vector<double> inv(n_groups);
     for (uint32_t g = 0; g < n_groups; g++) inv[g] = size[g] > 0 ? 1.0 / size[g] : 0.0;
-    // grouping 0 is the observed one, 1..perms permuted (Fisher-Yates)
-    const uint32_t cols = (perms + 1 + kPb - 1) / kPb * kPb;
-    std::vector<uint16_t> lab(static_cast<size_t>(n) * cols, 0);
-    std::vector<uint32_t> cur(grouping, grouping + n);
-    std::mt19937_64 gen(seed);
-    for (uint32_t p = 0; p <= perms; p++) {
-        if (p > 0)
-            for (uint32_t i = n - 1; i > 0; i--) {
-                std::uniform_int_distribution<uint32_t> pick(0, i);
-                std::swap(cur[i], cur[pick(gen)]);
-            }
-        for (uint32_t i = 0; i < n; i++) lab[static_cast<size_t>(i) * cols + p] = static_cast<uint16_t>(cur[i]);
-    }
+    // grouping 0 is the observed one, 1..perms permuted (Fisher-Yates, one
+    // stream from `seed`), evaluated in chunks of columns so that the labels
+    // on the device stay within about 256 MiB whatever the permutation count;
+    // the host draws chunk c + 1 while the device evaluates chunk c.
+    const uint32_t total = (perms + 1 + kPb - 1) / kPb * kPb;
+    uint64_t budget = uint64_t(256) << 20;  // UNIFRAC_B200_PERMANOVA_LABEL_BYTES
+    if (const char *v = std::getenv("UNIFRAC_B200_PERMANOVA_LABEL_BYTES"))
+        budget = std::max<uint64_t>(1, std::strtoull(v, nullptr, 10));
+    const uint64_t fit = budget / (2ull * n) / kPb * kPb;
+    const uint32_t chunk = static_cast<uint32_t>(std::min<uint64_t>(total, std::max<uint64_t>(kPb, fit)));
     Dev dv;
     ST_CK(cudaStreamCreateWithFlags(&dv.s, cudaStreamNonBlocking));
     const uint32_t blocks = (n + kRows - 1) / kRows;
     const TIn *dD = nullptr;
     if (stage_matrix(dv, mat, n, dD, err)) return 6;
     uint16_t *dl = nullptr;
-    double *dinv = nullptr, *dpart = nullptr, *dtot = nullptr;
-    ST_CK(dv.alloc(&dl, sizeof(uint16_t) * lab.size()));
+    double *dinv = nullptr, *dpart = nullptr, *dtot = nullptr, *dsw = nullptr;
+    ST_CK(dv.alloc(&dl, sizeof(uint16_t) * n * chunk));
     ST_CK(dv.alloc(&dinv, sizeof(double) * n_groups));
-    ST_CK(dv.alloc(&dpart, sizeof(double) * blocks * cols));
+    ST_CK(dv.alloc(&dpart, sizeof(double) * blocks * chunk));
     ST_CK(dv.alloc(&dtot, sizeof(double) * blocks));
-    ST_CK(cudaMemcpyAsync(dl, lab.data(), sizeof(uint16_t) * lab.size(), cudaMemcpyHostToDevice, dv.s));
+    ST_CK(dv.alloc(&dsw, sizeof(double) * chunk));
     ST_CK(cudaMemcpyAsync(dinv, inv.data(), sizeof(double) * n_groups, cudaMemcpyHostToDevice, dv.s));
-    for (uint32_t p0 = 0; p0 < cols; p0 += kPb)
-        permanova_kernel<TIn><<<blocks, kRows * 32, 0, dv.s>>>(dD, n, dl, cols, p0, dinv,
-                                                               dpart + static_cast<size_t>(p0 / kPb) * blocks * kPb,
-                                                               p0 == 0 ? dtot : nullptr);
-    ST_CK(cudaGetLastError());
-    std::vector<double> part(static_cast<size_t>(blocks) * cols), tot(blocks);
-    ST_CK(cudaMemcpyAsync(part.data(), dpart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, dv.s));
+    std::vector<uint16_t> lab(static_cast<size_t>(n) * chunk, 0);
+    std::vector<uint32_t> cur(grouping, grouping + n);
+    std::mt19937_64 gen(seed);
+    std::vector<double> s_w(total, 0.0);
+    uint32_t next_p = 0;  // next grouping to draw
+    auto draw = [&](uint32_t cn) {  // the next cn groupings, row stride cn
+        for (uint32_t c = 0; c < cn; c++, next_p++) {
+            if (next_p > 0 && next_p <= perms)
+                for (uint32_t i = n - 1; i > 0; i--) {
+                    std::uniform_int_distribution<uint32_t> pick(0, i);
+                    std::swap(cur[i], cur[pick(gen)]);
+                }
+            // columns past `perms` (padding to whole passes) repeat the last grouping; never read
+            for (uint32_t i = 0; i < n; i++) lab[static_cast<size_t>(i) * cn + c] = static_cast<uint16_t>(cur[i]);
+        }
+    };
+    uint32_t c0 = 0, cn = std::min(chunk, total);
+    draw(cn);
+    while (cn > 0) {
+        ST_CK(cudaMemcpyAsync(dl, lab.data(), sizeof(uint16_t) * n * cn, cudaMemcpyHostToDevice, dv.s));
+        for (uint32_t p0 = 0; p0 < cn; p0 += kPb)
+            permanova_kernel<TIn><<<blocks, kRows * 32, 0, dv.s>>>(dD, n, dl, cn, p0, dinv,
+                                                                   dpart + static_cast<size_t>(p0 / kPb) * blocks * kPb,
+                                                                   c0 == 0 && p0 == 0 ? dtot : nullptr);
+        column_sums_kernel<<<(cn + 255) / 256, 256, 0, dv.s>>>(dpart, blocks, cn, dsw);
+        ST_CK(cudaGetLastError());
+        const uint32_t c1 = c0 + cn, cn1 = std::min(chunk, total - c1);
+        if (cn1 > 0) draw(cn1);  // overlaps the device's chunk
+        ST_CK(cudaMemcpyAsync(s_w.data() + c0, dsw, sizeof(double) * cn, cudaMemcpyDeviceToHost, dv.s));
+        ST_CK(cudaStreamSynchronize(dv.s));
+        c0 = c1;
+        cn = cn1;
+    }
+    std::vector<double> tot(blocks);
     ST_CK(cudaMemcpyAsync(tot.data(), dtot, sizeof(double) * blocks, cudaMemcpyDeviceToHost, dv.s));
     ST_CK(cudaStreamSynchronize(dv.s));
     double s_t = 0.0;
     for (uint32_t b = 0; b < blocks; b++) s_t += tot[b];
     s_t /= n;
-    auto f_of = [&](uint32_t p) {
-        const uint32_t batch = p / kPb, pp = p % kPb;
-        double s_w = 0.0;
-        for (uint32_t b = 0; b < blocks; b++) s_w += part[(static_cast<size_t>(batch) * blocks + b) * kPb + pp];
-        return ((s_t - s_w) / (n_groups - 1)) / (s_w / (n - n_groups));
-    };
+    auto f_of = [&](uint32_t p) { return ((s_t - s_w[p]) / (n_groups - 1)) / (s_w[p] / (n - n_groups)); };
     fstat = f_of(0);
     if (perms > 0) {
         uint32_t ge = 0;
