@@ -20,8 +20,7 @@
 namespace ssu {
 namespace {
 
-constexpr int kRows = 16;   // rows (one warp each) per multiply block
-constexpr int kJt = 128;    // distance-matrix columns per staged tile
+constexpr int kRows = 16;   // rows (one warp each) per PERMANOVA block
 constexpr int kLmax = 32;   // basis columns per multiply pass
 constexpr int kPb = 32;     // permutations per PERMANOVA pass
 constexpr int kOversample = 10;
@@ -67,44 +66,82 @@ __global__ void row_means_kernel(const TIn *__restrict__ D, uint32_t n, double *
     }
 }
 
-// Yt[c0 + c][i] = sum_j e(d_ij) Qt[c0 + c][j] for c < lc; basis columns
-// stored column-major ([column][row]).  One warp per row, the lanes over
-// consecutive j (coalesced), the basis tile staged in shared memory.
+// Yt[c0 + c][i] = sum_j e(d_ij) Qt[c0 + c][j] for c < lc (<= 32); basis
+// columns stored column-major ([column][row]).  A register-blocked tile
+// product: a CTA of 128 threads owns 64 rows i x 32 columns c, each thread
+// 4 x 4 of them; per step it stages e(d) of 64 rows x 32 j (transposed, so
+// a thread reads its 4 rows of one j at once) and 32 j x 32 columns of Q in
+// shared memory (the next step's tiles are loaded into registers while this
+// one is multiplied), and every pair of staged loads feeds 16 FMAs.
+constexpr int MI = 64, MC = 32, MJ = 32;  // rows, columns, j per step
+
 template <typename TIn, bool kSquare>
-__global__ void __launch_bounds__(kRows * 32) multiply_kernel(const TIn *__restrict__ D, uint32_t n,
-                                                                const double *__restrict__ Qt, uint32_t c0,
-                                                                uint32_t lc, double *__restrict__ Yt) {
-    __shared__ double qs[kLmax][kJt];
-    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-    const uint32_t i = blockIdx.x * kRows + warp;
-    double acc[kLmax];
+__global__ void __launch_bounds__(128) multiply_kernel(const TIn *__restrict__ D, uint32_t n,
+                                                       const double *__restrict__ Qt, uint32_t c0, uint32_t lc,
+                                                       double *__restrict__ Yt) {
+    __shared__ __align__(16) double ds[MJ][MI + 2];  // e(d) transposed: [j][i]
+    __shared__ __align__(16) double qs[MJ][MC + 2];  // [j][c]
+    const int tid = threadIdx.x;
+    const int ti = tid % 16, tc = tid / 16;  // 16 x 8 threads, 4 x 4 each
+    const uint32_t i0 = blockIdx.x * MI;
+    double acc[4][4];
 #pragma unroll
-    for (int c = 0; c < kLmax; c++) acc[c] = 0.0;
-    const TIn *row = D + static_cast<uint64_t>(i < n ? i : 0) * n;
-    for (uint32_t j0 = 0; j0 < n; j0 += kJt) {
-        __syncthreads();
-        for (uint32_t t = threadIdx.x; t < lc * kJt; t += blockDim.x) {
-            const uint32_t c = t / kJt, jj = t % kJt;
-            qs[c][jj] = j0 + jj < n ? Qt[static_cast<uint64_t>(c0 + c) * n + j0 + jj] : 0.0;
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+    // staging assignment: D tile 64 x 32 (16 per thread: row r = tid / 2,
+    // j = 16 (tid % 2) .. + 15), Q tile 32 x 32 (8 per thread: column
+    // cq = tid / 4, j = 8 (tid % 4) .. + 7)
+    const int dr = tid / 2, dj = 16 * (tid % 2);
+    const int qc = tid / 4, qj = 8 * (tid % 4);
+    const uint32_t drow = i0 + dr;
+    const TIn *dsrc = D + static_cast<uint64_t>(drow < n ? drow : 0) * n;
+    const bool qok = static_cast<uint32_t>(qc) < lc;
+    const double *qsrc = Qt + static_cast<uint64_t>(c0 + (qok ? qc : 0)) * n;
+    double dv[16], qv[8];
+    auto load = [&](uint32_t j0) {
+#pragma unroll
+        for (int t = 0; t < 16; t++) {
+            const uint32_t j = j0 + dj + t;
+            dv[t] = (drow < n && j < n) ? entry<kSquare>(static_cast<double>(dsrc[j])) : 0.0;
         }
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            const uint32_t j = j0 + qj + t;
+            qv[t] = (qok && j < n) ? qsrc[j] : 0.0;
+        }
+    };
+    load(0);
+    for (uint32_t j0 = 0; j0 < n; j0 += MJ) {
         __syncthreads();
-        if (i < n) {
 #pragma unroll
-            for (int k = 0; k < kJt / 32; k++) {
-                const uint32_t jj = k * 32 + lane, j = j0 + jj;
-                const double e = j < n ? entry<kSquare>(static_cast<double>(row[j])) : 0.0;
+        for (int t = 0; t < 16; t++) ds[dj + t][dr] = dv[t];
 #pragma unroll
-                for (int c = 0; c < kLmax; c++)
-                    if (c < static_cast<int>(lc)) acc[c] = fma(e, qs[c][jj], acc[c]);
-            }
+        for (int t = 0; t < 8; t++) qs[qj + t][qc] = qv[t];
+        __syncthreads();
+        if (j0 + MJ < n) load(j0 + MJ);
+#pragma unroll 8
+        for (int j = 0; j < MJ; j++) {
+            double av[4], bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; a++) av[a] = ds[j][4 * ti + a];
+#pragma unroll
+            for (int b = 0; b < 4; b++) bv[b] = qs[j][4 * tc + b];
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int b = 0; b < 4; b++) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
         }
     }
-    if (i >= n) return;
 #pragma unroll
-    for (int c = 0; c < kLmax; c++) {
-        if (c >= static_cast<int>(lc)) break;
-        const double v = warp_sum(acc[c]);
-        if (lane == 0) Yt[static_cast<uint64_t>(c0 + c) * n + i] = v;
+    for (int b = 0; b < 4; b++) {
+        const uint32_t c = 4 * tc + b;
+        if (c >= lc) continue;
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            const uint32_t i = i0 + 4 * ti + a;
+            if (i < n) Yt[static_cast<uint64_t>(c0 + c) * n + i] = acc[a][b];
+        }
     }
 }
 
@@ -392,8 +429,8 @@ int subspace_eigen(const TIn *mat, uint32_t n, uint32_t dims, std::vector<double
     // Yt = A Q for the r columns of Qt (multiply passes of <= 32 columns)
     auto apply = [&](const double *Qt, uint32_t r) -> int {
         for (uint32_t c0 = 0; c0 < r; c0 += kLmax)
-            multiply_kernel<TIn, kSquare><<<(n + kRows - 1) / kRows, kRows * 32, 0, dv.s>>>(
-                dD, n, Qt, c0, std::min<uint32_t>(kLmax, r - c0), dY);
+            multiply_kernel<TIn, kSquare><<<(n + MI - 1) / MI, 128, 0, dv.s>>>(dD, n, Qt, c0,
+                                                                              std::min<uint32_t>(kLmax, r - c0), dY);
         if (kSquare) {
             // s_c = sum_j Q_jc and t_c = sum_j m_j Q_jc in one pass ([ones; m] . Q)
             dot_kernel<<<2 * r, 256, 0, dv.s>>>(dm1, Qt, n, r, dst);
