@@ -317,6 +317,34 @@ def test_weighted_sparse_and_dense_forms_agree(ssu, monkeypatch, method, prec):
         np.testing.assert_allclose(hybrid, dense, rtol=5e-6, atol=1e-7)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("method", ["weighted_normalized", "weighted_unnormalized"])
+def test_weighted_pair_scatter_and_tile_walk_agree(ssu, monkeypatch, method, prec):
+    """The sparse rows as per-pair fixed-point sums (the default) against the
+    tile kernel's own walk: the same to fp64 rounding, and the integer sums
+    make repeated calls agree bit for bit in both precisions."""
+    tree, table = _case(65, n_tips=500, n_samples=700, density=0.02)
+    scatter = [ssu.one_off_matrix(tree, table, f"{method}_{prec}")[0] for _ in range(2)]
+    np.testing.assert_array_equal(scatter[0], scatter[1])
+    monkeypatch.setenv("UNIFRAC_B200_HYBRID_SCATTER", "0")
+    monkeypatch.setenv("UNIFRAC_B200_DETERMINISTIC", "1")
+    walk, _ = ssu.one_off_matrix(tree, table, f"{method}_{prec}")
+    if prec == "fp64":
+        check_fp64(scatter[0], walk)
+    else:
+        np.testing.assert_allclose(scatter[0], walk, rtol=2e-6, atol=1e-7)
+    # raw counts (no sample normalisation): the fixed-point unit follows the largest total
+    monkeypatch.delenv("UNIFRAC_B200_HYBRID_SCATTER")
+    big = ssu_synth.geometric_table(table.obs_ids, 300, 0.02, 5000.0, 66)
+    raw_scatter, _ = ssu.one_off_matrix(tree, big, f"{method}_{prec}", normalize=False)
+    monkeypatch.setenv("UNIFRAC_B200_HYBRID_SCATTER", "0")
+    raw_walk, _ = ssu.one_off_matrix(tree, big, f"{method}_{prec}", normalize=False)
+    if prec == "fp64":
+        check_fp64(raw_scatter, raw_walk)
+    else:
+        np.testing.assert_allclose(raw_scatter, raw_walk, rtol=2e-6, atol=1e-4)
+
+
 @pytest.mark.parametrize("method", ["weighted_normalized", "weighted_unnormalized"])
 def test_weighted_fp32_deterministic_mode_repeats_bit_for_bit(ssu, monkeypatch, method):
     """UNIFRAC_B200_DETERMINISTIC=1 gives fp32 plans the owner-per-element

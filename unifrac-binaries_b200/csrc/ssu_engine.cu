@@ -314,6 +314,9 @@ struct PlanImpl {
     bool hybrid = false;
     uint32_t hybrid_div = 8;  // rows non-zero in more than ld / hybrid_div columns are dense
     bool hybrid_atomic = false;  // sparse updates with shared-memory atomics (fp32 default)
+    bool hybrid_scatter = false;  // sparse rows as per-pair fixed-point sums (sparse_pairs_kernel)
+    unsigned long long *d_Sq = nullptr;  // those sums; the fp64 result buffer doubles as them
+    double sq_scale = 1.0;
     bool nonneg_data = true;  // no negative count in any table
     unsigned long long *d_masks = nullptr;
     uint32_t *d_counts = nullptr, *d_dense_rows = nullptr, *d_sparse_rows = nullptr, *d_nrows = nullptr;
@@ -525,7 +528,9 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
     if (!budget && n_tables > 1) {  // one table is one group whatever the budget
         size_t free_b = 0, total_b = 0;
         SSU_CK(cudaMemGetInfo(&free_b, &total_b));
-        const size_t fixed = el * full_elems + 12 * nnz_total;
+        // (fp32 weighted plans also hold the pair-scatter sums: 8 bytes per result)
+        const bool weighted = spec.method == Method::weighted_normalized || spec.method == Method::weighted_unnormalized;
+        const size_t fixed = el * full_elems + 12 * nnz_total + (weighted && !spec.fp64 && !faith ? 8 * full_elems : 0);
         budget = free_b > fixed ? (free_b - fixed) / 2 : 0;
     }
     uint64_t max_cols = std::max<uint64_t>(128, budget / per_col);
@@ -758,6 +763,28 @@ int PlanImpl::setup_hybrid() {
     // UNIFRAC_B200_DETERMINISTIC=1: fp32 plans also take the owner walk, so
     // their results repeat bit for bit (about 13% slower on replicate tables)
     hybrid_atomic = sizeof(T) == 4 && !env_int("UNIFRAC_B200_DETERMINISTIC", 0);
+    // UNIFRAC_B200_HYBRID_SCATTER=0: the tile kernel walks the sparse rows
+    // itself instead of reading per-pair sums
+    hybrid_scatter = env_int("UNIFRAC_B200_HYBRID_SCATTER", 1) != 0;
+    if (hybrid_scatter) {
+        // no pair's sum of L min(a, b) exceeds the sum of |L| over the
+        // embedded rows times the largest embedded value: 1 for proportions,
+        // the largest sample total for raw counts.  The unit 2^-s keeps
+        // every sum below 2^62.
+        double vmax = 1.0;
+        if (!spec.normalize)
+            for (const Group &g : groups)
+                for (double t : g.totals) vmax = std::max(vmax, std::fabs(t));
+        double bound = 0.0;
+        for (uint32_t e = 0; e < E; e++) bound += std::fabs(host_len[e]);
+        bound *= vmax * (1.0 + 1e-12);
+        const int s2 = 62 - static_cast<int>(std::ceil(std::log2(std::max(bound, 1e-300))));
+        sq_scale = std::ldexp(1.0, std::min(s2, 1000));
+        if (sizeof(T) == sizeof(double))
+            d_Sq = static_cast<unsigned long long *>(d_full);  // written only after its sum is read
+        else
+            SSU_CK(alloc(&d_Sq, sizeof(unsigned long long) * std::max<uint64_t>(full_elems, 1)));
+    }
     const int smem = static_cast<int>(dev::hybrid_smem<T>());
     SSU_CK(cudaFuncSetAttribute(dev::pair_hybrid_kernel<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem));
@@ -824,6 +851,27 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
     launches++;
     if (ntiles == 0) return 0;
     SSU_CK(cudaMemsetAsync(d_flags, 0, sizeof(int) * ntiles, s));
+    if (hybrid_scatter) {
+        const dev::TableDesc &first = tdesc[g.t0], &lastd = tdesc[g.t1 - 1];
+        const uint64_t n_last = lastd.n;
+        const uint64_t span = lastd.out_off + n_last * n_last - first.out_off;
+        SSU_CK(cudaMemsetAsync(d_Sq + first.out_off, 0, sizeof(unsigned long long) * span, s));
+        dev::ScatterArgs<T> sa{};
+        sa.sparse_rows = d_sparse_rows;
+        sa.n_rows = d_nrows;
+        sa.masks = d_masks;
+        sa.E = E;
+        sa.tables = d_tdesc;
+        sa.t0 = g.t0;
+        sa.n_tables = g.t1 - g.t0;
+        sa.U = U;
+        sa.len = static_cast<const T *>(d_len);
+        sa.ld = g.ld;
+        sa.Sq = d_Sq;
+        sa.scale = sq_scale;
+        dev::sparse_pairs_kernel<T><<<static_cast<uint32_t>(n_sms) * 8, dev::SC_WARPS * 32, 0, s>>>(sa);
+        launches++;
+    }
     dev::HybridArgs<T> h{};
     h.tiles = tiles;
     h.n_tiles = ntiles;
@@ -847,6 +895,8 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
         h.partial = nullptr;
     }
     h.out = out;
+    h.Sq = hybrid_scatter ? d_Sq : nullptr;
+    h.sq_unit = 1.0 / sq_scale;
     const bool norm = spec.method == Method::weighted_normalized;
     const uint32_t ctas = static_cast<uint32_t>(
         std::min<uint64_t>(static_cast<uint64_t>(ntiles) * h.n_splits, static_cast<uint64_t>(n_sms)));

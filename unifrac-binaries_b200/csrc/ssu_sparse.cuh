@@ -145,6 +145,11 @@ struct HybridArgs {
     int *tile_flags;     // tiles that need the exact recomputation
     double *partial;     // per (split, tile) 128 x 128 fp64 raw sums; nullptr: no splits
     OutSpec out;
+    // pair-scatter form: the sparse rows' sums S = sum L min(a, b) per pair
+    // k < l of a table, 64-bit fixed point at td.out_off + k n + l (nullptr:
+    // the tile kernel walks the sparse rows itself)
+    const unsigned long long *Sq;
+    double sq_unit;      // value of one fixed-point unit (2^-s)
 };
 
 constexpr int HB = 128;      // tile edge
@@ -166,6 +171,9 @@ __device__ __forceinline__ void hybrid_emit(const HybridArgs<T> &a, const TableD
                                             uint32_t kc, uint32_t lc, double x) {
     const uint32_t k = kc - td.base, l = lc - td.base;
     if (!(k < l && l < td.n)) return;
+    if (a.Sq)
+        x -= 2.0 * static_cast<double>(static_cast<long long>(a.Sq[td.out_off + static_cast<uint64_t>(k) * td.n + l])) *
+             a.sq_unit;
     const double ws = a.Ws[kc] + a.Ws[lc];
     const double d = x + ws;
     if (d < a.tau * ws) atomicOr(a.tile_flags + ti, 1);
@@ -306,7 +314,9 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
                 Mt[tile_row<HB, TM>(ty, i) * HB + tile_row<HB, TN>(tx, j)] = acc[i][j];
         __syncthreads();
 
-        if constexpr (ATOMIC) {
+        if (a.Sq) {
+            // ---- sparse rows: already scattered into Sq (sparse_pairs_kernel)
+        } else if constexpr (ATOMIC) {
             // ---- sparse rows, fp32 plans: -2 L min(a, b) where both are non-zero.  Warp w
             // takes batches w, w + 16, ... of 32 consecutive rows (lane i: row i's
             // class, its k-block and l-block mask words and length, fetched two
@@ -554,6 +564,109 @@ __global__ void __launch_bounds__(HTHREADS, 1) pair_hybrid_kernel(const HybridAr
 }
 
 // Split partials of each tile summed in split order, then the epilogue.
+// ---- pair-scatter form of the sparse rows
+//
+// For each (sparse row e, table t) of a group, one warp lists the table's
+// samples where the row is non-zero (from the presence masks, in column
+// order, up to SC_CAP at a time in shared memory with their values) and adds
+// L min(a, b) of every pair k < l of the list to S[k][l] with a 64-bit
+// integer atomic: the term in fixed point, round(L min(a, b) 2^s), with 2^s
+// chosen on the host so that no pair's sum can reach 2^62.  Integer addition
+// is associative, so the sums (and the results) do not depend on the order
+// of the atomics.  Each (row, table) is visited once, against once per tile
+// of the table in the tile walk; the work is the row's pair count.
+constexpr int SC_WARPS = 8;
+constexpr int SC_CAP = 256;
+
+template <typename T>
+struct ScatterArgs {
+    const uint32_t *sparse_rows;
+    const uint32_t *n_rows;  // {dense, sparse}
+    const unsigned long long *masks;
+    uint32_t E;
+    const TableDesc *tables;
+    uint32_t t0, n_tables;  // the group's tables
+    const T *U;
+    const T *len;
+    uint64_t ld;
+    unsigned long long *Sq;
+    double scale;  // 2^s
+};
+
+template <typename T>
+__global__ void __launch_bounds__(SC_WARPS * 32) sparse_pairs_kernel(const ScatterArgs<T> a) {
+    __shared__ uint32_t col_s[SC_WARPS][2][SC_CAP];
+    __shared__ double val_s[SC_WARPS][2][SC_CAP];
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const uint32_t n_sparse = a.n_rows[1];
+    const uint64_t tasks = static_cast<uint64_t>(n_sparse) * a.n_tables;
+    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * SC_WARPS;
+    for (uint64_t task = static_cast<uint64_t>(blockIdx.x) * SC_WARPS + warp; task < tasks; task += stride) {
+        // table-major: the warps in flight share one table's sums in L2
+        const uint32_t e = a.sparse_rows[task % n_sparse];
+        const TableDesc td = a.tables[a.t0 + static_cast<uint32_t>(task / n_sparse)];
+        const uint64_t w0 = td.base / 64;  // tables start on 128-column boundaries
+        const uint32_t nw = (td.n + 63) / 64;
+        const unsigned long long *mrow = a.masks + w0 * a.E + e;
+        uint32_t P = 0;
+        for (uint32_t w = lane; w < nw; w += 32) P += __popcll(mrow[static_cast<uint64_t>(w) * a.E]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) P += __shfl_xor_sync(0xffffffffu, P, o);
+        if (P < 2) continue;
+        const double L = static_cast<double>(a.len[e]) * a.scale;
+        const T *row = a.U + static_cast<uint64_t>(e) * a.ld + td.base;
+        unsigned long long *S = a.Sq + td.out_off;
+        // list b <- the present columns of rank [r0, r0 + SC_CAP), with values
+        auto collect = [&](int b, uint32_t r0) {
+            uint32_t base = 0;
+            for (uint32_t w = lane; w - lane < nw && base < r0 + SC_CAP; w += 32) {
+                const unsigned long long m = w < nw ? mrow[static_cast<uint64_t>(w) * a.E] : 0ull;
+                const uint32_t c = __popcll(m);
+                uint32_t incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                uint32_t rank = base + incl - c;  // rank of this word's first set bit
+                unsigned long long mm = m;
+                while (mm) {
+                    const int bit = __ffsll(mm) - 1;
+                    mm &= mm - 1;
+                    if (rank >= r0 && rank < r0 + SC_CAP) {
+                        const uint32_t col = w * 64 + bit;
+                        col_s[warp][b][rank - r0] = col;
+                        val_s[warp][b][rank - r0] = static_cast<double>(row[col]);
+                    }
+                    rank++;
+                }
+                base += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            __syncwarp();
+        };
+        for (uint32_t i0 = 0; i0 < P; i0 += SC_CAP) {
+            const uint32_t ni = min(static_cast<uint32_t>(SC_CAP), P - i0);
+            collect(0, i0);
+            for (uint32_t j0 = i0; j0 < P; j0 += SC_CAP) {
+                const bool same = j0 == i0;
+                const uint32_t nj = min(static_cast<uint32_t>(SC_CAP), P - j0);
+                if (!same) collect(1, j0);
+                const int bl = same ? 0 : 1;
+                for (uint32_t i = 0; i < ni; i++) {
+                    const uint32_t k = col_s[warp][0][i];
+                    const double av = val_s[warp][0][i];
+                    unsigned long long *Sk = S + static_cast<uint64_t>(k) * td.n;
+                    for (uint32_t j = (same ? i + 1 : 0) + lane; j < nj; j += 32) {
+                        const double t = L * fmin(av, val_s[warp][bl][j]);
+                        atomicAdd(Sk + col_s[warp][bl][j], static_cast<unsigned long long>(__double2ll_rn(t)));
+                    }
+                }
+                __syncwarp();
+            }
+        }
+    }
+}
+
 template <typename T, bool NORM>
 __global__ void __launch_bounds__(HTHREADS) hybrid_finalize_kernel(const HybridArgs<T> a) {
     const uint32_t ti = blockIdx.x;
