@@ -483,3 +483,22 @@ def test_hybrid_with_every_row_sparse_matches_dense_form(ssu, monkeypatch, prec)
         check_fp64(sparse, dense)
     else:
         np.testing.assert_allclose(sparse, dense, rtol=5e-6, atol=1e-7)
+
+
+def test_page_locked_results_are_recycled(ssu):
+    """Full results of 2 MiB or more come from the page-locked pool, and a
+    result released through destroy_mat_full_fp64 goes back to it: after many
+    large results, large and smaller ones are still page-locked (flag
+    0x2000), so no call falls back to registering pageable memory."""
+    import ctypes
+    L = ssu.lib()
+    tree, table = _case(67, n_tips=300, n_samples=700, density=0.05)
+    small_tree, small = _case(68, n_tips=300, n_samples=520, density=0.05)
+    for t, tb in [(tree, table)] * 4 + [(small_tree, small)] * 2 + [(tree, table)]:
+        x = ssu.Inputs(t, tb)
+        res = ctypes.POINTER(ssu.MatFull64)()
+        st = L.one_off_matrix_inmem_v3(ctypes.byref(x.biom), ctypes.byref(x.tree), b"weighted_normalized_fp64",
+                                       False, 1.0, False, True, 1, 0, False, None, ctypes.byref(res))
+        assert st == 0
+        assert res.contents.flags & 0x2000, "result not page-locked"
+        L.destroy_mat_full_fp64(ctypes.byref(res))

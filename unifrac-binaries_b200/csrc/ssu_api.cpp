@@ -321,6 +321,7 @@ class PinnedPool {
         if (it != free_.end() && it->first <= 2 * bytes) {
             void *p = it->second;
             cached_ -= it->first;
+            live_bytes_ += it->first;
             live_[p] = it->first;
             free_.erase(it);
             return p;
@@ -464,6 +465,7 @@ ComputeStatus full_matrix(const ssu::Table &table, const ssu::BPTree &tree, cons
         }
         allocated = true;
     }
+    timer.step(((*result)->flags & kPinnedFlag) ? "result_alloc (page-locked)" : "result_alloc (pageable)");
     if ((*result)->matrix == nullptr || (*result)->n_samples != table.n_samples) {
         report("one_off_matrix", "caller-provided result does not match the table");
         return output_error;
