@@ -433,9 +433,9 @@ def _step_loop(torch, plan, stream, steps, barrier, flush):
 
 def tc_work_units(n):
     """Work units of the tensor-core kernel for one table of n samples: the
-    (256-row, 64-column) blocks holding a pair k < l."""
-    nkb, nlb = (n + 255) // 256, (n + 63) // 64
-    return sum(1 for kb in range(nkb) for lb in range(nlb) if kb * 256 < min(n, (lb + 1) * 64) - 1)
+    (256-row, 128-column) blocks holding a pair k < l."""
+    nkb, nlb = (n + 255) // 256, (n + 127) // 128
+    return sum(1 for kb in range(nkb) for lb in range(nlb) if kb * 256 < min(n, (lb + 1) * 128) - 1)
 
 
 def run_presence(args):
@@ -550,8 +550,8 @@ def run_presence(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "u8 operands (0/1 presence; lengths as three byte planes of 24-bit fixed point), exact s32 "
-                     "accumulate per chunk, f64 across chunks and ratios",
+            "dtype": "u8 operands (presence times 8-bit digits of 23-bit fixed-point lengths, q = 256 u v + s t), "
+                     "exact s32 accumulate per chunk, f64 across chunks and ratios",
             "data": "synthetic (seeded generator presence_100k_tips_25k_samples)",
             "config": {"workload": PRESENCE_WORKLOAD, "method": method, "pair_kernel": "unweighted_tc_kernel",
                        "n_samples": n, "embedded_branches": gp_units_e(units, n), "per_gpu_units": units,
@@ -567,9 +567,9 @@ def run_presence(args):
                          "issued_int8_tops": issued, "issued_frac": issued / (2.0 * peak_sus),
                          "issued_peak": f"2 x {peak_kind} bf16 sustained (dense int8 : bf16 = 2 : 1 on B200)",
                          "note": "algorithmic flops = 2 x pair-branch updates (one multiply-add per pair and "
-                                 "branch), against the bf16 peak; the kernel issues ~3x that in int8 ops (three "
-                                 "length planes, padding of the length chunks and of 256 x 64 work units on the "
-                                 "diagonal) at twice the bf16 rate; traffic = ncu DRAM bytes per work unit x work "
+                                 "branch), against the bf16 peak; the kernel issues ~2x that in int8 ops (two "
+                                 "digit products per length, padding of the length chunks and of 256 x 128 work "
+                                 "units on the diagonal) at twice the bf16 rate; traffic = ncu DRAM bytes per work unit x work "
                                  "units"},
             "e2e": {"value": all_units * len(e2e_ms) / (e2e_total / 1e3) if e2e_ms else None, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -1,9 +1,9 @@
 """The tensor-core (tcgen05) unweighted contraction, selected with
 UNIFRAC_B200_UNWEIGHTED_MODE=gemm, against the fp64 oracle.  Bar: max
 relative error 1e-6 on every pair (the contraction's stated bound; lengths
-carried as 24-bit fixed point in three byte planes per chunk of lengths
-within a factor of two, exact int32 plane sums, fp64 across chunks and in
-the final ratio)."""
+carried as 23-bit fixed point per chunk of lengths within a factor of two,
+each written as 256 u v + s t with 8-bit digits, exact int32 sums of the
+two products, fp64 across chunks and in the final ratio)."""
 import os
 
 import numpy as np
@@ -70,6 +70,18 @@ def test_tc_wide_length_range(ssu, oracle_mod, gemm_mode):
     assert rel_err(gpu, ref)[0] <= TC_REL
 
 
+def test_tc_chunk_closes_at_its_block_limit(ssu, oracle_mod, gemm_mode):
+    """80,000 embedded nodes whose lengths lie within a factor of two fill one
+    chunk past its limit of 512 blocks of 128 nodes (the int32 product sums'
+    bound), so the contraction runs over two chunks of the same scale."""
+    tree, table = _case(12, 40000, 48, density=0.3)
+    rng = np.random.default_rng(12)
+    tree.lengths = np.where(tree.structure, rng.uniform(1.0, 1.9, size=tree.lengths.shape), 0.0)
+    gpu, _ = ssu.one_off_matrix(tree, table, "unweighted_fp64")
+    ref = oracle_mod.oracle_one_off(tree, table, "unweighted_fp64")["matrix"]
+    assert rel_err(gpu, ref)[0] <= TC_REL
+
+
 def test_tc_plan_agrees_with_stripe_form(ssu, gemm_mode):
     tree, table = _case(9, 2000, 400)
     plan = ssu.Plan(tree, table, "unweighted_fp64")
@@ -81,10 +93,10 @@ def test_tc_plan_agrees_with_stripe_form(ssu, gemm_mode):
     assert rel_err(tc, stripe)[0] <= TC_REL
 
 
-@pytest.mark.parametrize("n_samples", [2, 63, 64, 65, 128, 129, 255, 256, 257, 319, 383, 511, 513])
+@pytest.mark.parametrize("n_samples", [2, 63, 64, 65, 127, 128, 129, 255, 256, 257, 319, 383, 385, 511, 513])
 @pytest.mark.parametrize("method", ["unweighted_fp64", "unweighted_unnormalized_fp64"])
 def test_tc_sample_counts_at_work_unit_edges(ssu, oracle_mod, gemm_mode, n_samples, method):
-    """A work unit covers 256 rows x 64 columns: counts around those edges,
+    """A work unit covers 256 rows x 128 columns: counts around those edges,
     where units straddle the diagonal or hold a single row or column."""
     tree, table = _case(n_samples, 300, n_samples, density=0.08)
     gpu, _ = ssu.one_off_matrix(tree, table, method)

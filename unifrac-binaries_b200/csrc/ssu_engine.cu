@@ -516,10 +516,10 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
     size_t per_col = el * std::max<uint32_t>(K, 1) * (counts ? 2 : 1) + sizeof(double) + (counts ? el : 0) +
                      sizeof(unsigned long long) * n_words + (n_parts ? el * (n_parts + 1) : 0);
     if (gemm) {
-        // 8-bit operand rows (A and three B planes) over the padded nodes
-        // (chunk padding included, allowing for 128 chunks) and r
+        // 8-bit operand rows (A0, A1, B0, B1) over the padded nodes (chunk
+        // padding included, allowing for 128 chunks) and r
         const uint64_t kp = (static_cast<uint64_t>(E) + tc::BLOCK_K - 1) / tc::BLOCK_K * tc::BLOCK_K + 128 * tc::BLOCK_K;
-        per_col = (1 + tc::PLANES) * kp + sizeof(double);
+        per_col = 2 * tc::PRODUCTS * kp + sizeof(double);
     }
     size_t budget = opts.group_bytes;
     if (!budget) {
@@ -1349,7 +1349,37 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
 
 // --------------------------------------------------- tensor-core unweighted
 
-// Tensor-core work units: per table, the (256-row block, 64-column block)
+// q (< 2^23) as 256 u v + s t with u, v, s, t in [0, 255] and u v, s t <=
+// 32767: d = {u, s, v, t}.  p = u v runs down from q / 256 (s t = q - 256 p
+// up from q mod 256) until both are products of two bytes; every q < 2^23
+// has such a pair within 112 steps.  False if none is found.
+static bool split_length(uint32_t q, uint8_t d[4]) {
+    struct Factors {
+        uint16_t f[tc::MAX_PART + 1];  // u | v << 8 for p = u v, or 0xFFFF
+        Factors() {
+            std::fill(std::begin(f), std::end(f), static_cast<uint16_t>(0xFFFF));
+            f[0] = 0;
+            for (uint32_t u = 1; u < 256; u++)
+                for (uint32_t v = u; v < 256 && u * v <= static_cast<uint32_t>(tc::MAX_PART); v++)
+                    if (f[u * v] == 0xFFFF) f[u * v] = static_cast<uint16_t>(u | (v << 8));
+        }
+    };
+    static const Factors tab;
+    if (q >= (1u << tc::QBITS)) return false;
+    for (int64_t p = q >> 8, rest = q & 255; p >= 0 && rest <= tc::MAX_PART; p--, rest += 256) {
+        if (p > tc::MAX_PART) continue;
+        const uint16_t a = tab.f[p], b = tab.f[rest];
+        if (a == 0xFFFF || b == 0xFFFF) continue;
+        d[0] = static_cast<uint8_t>(a & 0xFF);
+        d[2] = static_cast<uint8_t>(a >> 8);
+        d[1] = static_cast<uint8_t>(b & 0xFF);
+        d[3] = static_cast<uint8_t>(b >> 8);
+        return true;
+    }
+    return false;
+}
+
+// Tensor-core work units: per table, the (256-row block, 128-column block)
 // pairs holding some pair k < l, ordered in bands of `band` row blocks walked
 // column by column.  Clusters start in launch order as SMs free up, so a
 // unit reads the column block of B that its predecessor is reading and the
@@ -1441,11 +1471,11 @@ int PlanImpl::tune_band() {
 int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     SetupTimer timer;
     // Embedded nodes by decreasing |length|, packed into chunks of whole
-    // 64-node K blocks: a chunk closes (its last block padded with
+    // 128-node K blocks: a chunk closes (its last block padded with
     // zero-length columns) when the next length is below half the chunk's
     // first, or at MAX_CHUNK_KB blocks.  Chunk c is scaled by 2^s_c so that
-    // its largest |length| lies in [1024, 2048): every length of the chunk in
-    // [512, 2048), hi = nearest integer (exact in fp16), lo = fp16(rest).
+    // its largest length lies in [2^22, 2^23); q = round(L 2^s_c) is then
+    // written as 256 u v + s t with 8-bit digits (`split_length`).
     // (stable order by decreasing |length|: an LSD radix sort of the
     // complemented bit patterns, which order non-negative doubles)
     std::vector<uint32_t> order(E), tmp(E);
@@ -1472,7 +1502,7 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     }
     std::vector<int32_t> col_of_row(tree.n_nodes, -1);
     std::vector<double> lsorted, scale;
-    std::vector<uint32_t> lq;  // 24-bit fixed-point lengths
+    std::vector<uint32_t> lq;  // 23-bit fixed-point lengths
     std::vector<uint32_t> chunk_end;
     const uint32_t max_cols = static_cast<uint32_t>(tc::MAX_CHUNK_KB) * tc::BLOCK_K;
     auto pad_to_block = [&] {
@@ -1492,7 +1522,7 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
             if (first >= 0) pad_to_block();
             first = a;
             chunk_first = lsorted.size();
-            // the chunk's largest length to [2^23, 2^24)
+            // the chunk's largest length to [2^22, 2^23)
             sig = a > 0 ? (tc::QBITS - 1) - static_cast<int>(std::floor(std::log2(a))) : 0;
             scale.push_back(std::ldexp(1.0, -sig));
         }
@@ -1578,15 +1608,21 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     timer.step("gemm_tiles");
     n_pad = static_cast<uint32_t>(ld);
     const size_t op_bytes = static_cast<size_t>(n_pad) * k_pad;
-    SSU_CK(alloc(&d_A, op_bytes));
-    SSU_CK(alloc(&d_B, tc::PLANES * op_bytes));
+    SSU_CK(alloc(&d_A, tc::PRODUCTS * op_bytes));
+    SSU_CK(alloc(&d_B, tc::PRODUCTS * op_bytes));
     SSU_CK(alloc(&d_r, sizeof(double) * n_pad));
     {
-        std::vector<uint8_t> planes(static_cast<size_t>(tc::PLANES) * k_pad);
-        for (uint32_t c = 0; c < k_pad; c++)
-            for (int p = 0; p < tc::PLANES; p++)
-                planes[static_cast<size_t>(p) * k_pad + c] = static_cast<uint8_t>(lq[c] >> (8 * p));
-        SSU_CK(upload(&d_lq, planes.data(), planes.size()));
+        // digits u, s, v, t of every column, one k_pad row each
+        std::vector<uint8_t> digits(static_cast<size_t>(2 * tc::PRODUCTS) * k_pad);
+        for (uint32_t c = 0; c < k_pad; c++) {
+            uint8_t d[4];
+            if (!split_length(lq[c], d)) {
+                last_error = "length has no 8-bit product form";
+                return kOutputError;
+            }
+            for (int i = 0; i < 4; i++) digits[static_cast<size_t>(i) * k_pad + c] = d[i];
+        }
+        SSU_CK(upload(&d_lq, digits.data(), digits.size()));
     }
     SSU_CK(upload(&d_lsorted, lsorted.data(), sizeof(double) * k_pad));
     SSU_CK(upload(&d_chunk_scale, scale.data(), sizeof(double) * n_chunks));
@@ -1596,8 +1632,8 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     SSU_CK(cudaMemsetAsync(d_error, 0, sizeof(int), stream));
     if (const char *w = std::getenv("UNIFRAC_B200_WAIT_CYCLES")) gemm_wait_cycles = std::max(0LL, std::atoll(w));
     union_stall = env_int("UNIFRAC_B200_TEST_STALL", 0) ? 1 : 0;
-    if (!make_u8_map(&map_A, d_A, n_pad, k_pad, tc::ROWS) ||
-        !make_u8_map(&map_B, d_B, static_cast<uint64_t>(tc::PLANES) * n_pad, k_pad, tc::B_ROWS)) {
+    if (!make_u8_map(&map_A, d_A, static_cast<uint64_t>(tc::PRODUCTS) * n_pad, k_pad, tc::ROWS) ||
+        !make_u8_map(&map_B, d_B, static_cast<uint64_t>(tc::PRODUCTS) * n_pad, k_pad, tc::B_ROWS)) {
         last_error = "cuTensorMapEncodeTiled failed";
         return kOutputError;
     }
@@ -1635,7 +1671,7 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
         const Group &g = groups[gi];
         tc::presence_rows_kernel<<<static_cast<uint32_t>(g.ld), 256, bits_smem, s>>>(
             g.d_sample_ptr, g.d_start_col, d_parent_col, d_lq, d_lsorted, static_cast<uint32_t>(g.ld), k_pad,
-            d_A, d_B, d_r);
+            static_cast<uint64_t>(n_pad) * k_pad, d_A, d_B, d_r);
         launches++;
         if (gi == 0 && timed()) SSU_CK(cudaEventRecord(ev[1], s));
         if (g.n_tiles) {
@@ -1644,6 +1680,7 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
             a.n_tiles = g.n_tiles;
             a.tables = d_tdesc;
             a.n_kblocks = k_pad / tc::BLOCK_K;
+            a.plane_rows = n_pad;
             a.n_chunks = n_chunks;
             a.chunk_end = d_chunk_end;
             a.chunk_scale = d_chunk_scale;
@@ -1694,8 +1731,8 @@ int PlanImpl::execute_gemm_overlap(void *host) {
     zero_diagonal(s, d_full);  // the units never write the diagonal
     const size_t bits_smem = sizeof(uint32_t) * (k_pad / 32);
     tc::presence_rows_kernel<<<static_cast<uint32_t>(g.ld), 256, bits_smem, s>>>(
-        g.d_sample_ptr, g.d_start_col, d_parent_col, d_lq, d_lsorted, static_cast<uint32_t>(g.ld), k_pad, d_A, d_B,
-        d_r);
+        g.d_sample_ptr, g.d_start_col, d_parent_col, d_lq, d_lsorted, static_cast<uint32_t>(g.ld), k_pad,
+        static_cast<uint64_t>(n_pad) * k_pad, d_A, d_B, d_r);
     launches++;
     SSU_CK(cudaEventRecord(band_ev[nb], s));
     SSU_CK(cudaStreamWaitEvent(s1, band_ev[nb], 0));
@@ -1708,6 +1745,7 @@ int PlanImpl::execute_gemm_overlap(void *host) {
             a.n_tiles = u1 - u0;
             a.tables = d_tdesc;
             a.n_kblocks = k_pad / tc::BLOCK_K;
+            a.plane_rows = n_pad;
             a.n_chunks = n_chunks;
             a.chunk_end = d_chunk_end;
             a.chunk_scale = d_chunk_scale;
@@ -2132,7 +2170,7 @@ uint64_t Plan::tensor_flops() const {
     if (!impl_->gemm) return 0;
     uint64_t units = 0;
     for (const auto &g : impl_->groups) units += g.n_tiles;
-    return 2ull * tc::UMMA_M * tc::UMMA_N * impl_->k_pad * units;
+    return 2ull * tc::PRODUCTS * tc::UMMA_M * tc::UMMA_N * impl_->k_pad * units;
 }
 uint32_t Plan::launches() const { return impl_->launches; }
 const char *Plan::pair_kernel_name() const {

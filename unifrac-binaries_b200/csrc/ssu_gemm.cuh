@@ -14,32 +14,37 @@
 // e * G[k][l] in G is at most 2 e of the result; r is an fp64 sum of the
 // true lengths.
 //
-// Operands (8-bit, K-major, built by `presence_rows_kernel`): A = X (0/1),
-// and B = (1 - X) * q where q is the length in 24-bit fixed point, split
-// into three byte planes q = q0 + 2^8 q1 + 2^16 q2 (`kind::i8`, unsigned,
-// int32 accumulate: every plane sum is exact).  Nodes are sorted by
-// decreasing length and packed into chunks of whole 128-node K blocks whose
-// lengths lie within a factor of two of the chunk's largest (zero-length
-// padding columns close a chunk); chunk c is scaled by 2^s_c so its largest
-// length lies in [2^23, 2^24): q = round(L 2^s_c) keeps 23 significant bits
-// of every length, and a chunk's plane sums stay below 2^31 (at most 4096
-// blocks x 128 nodes x 255).  Each chunk is accumulated in tensor memory
-// (TMEM), then S0 + 2^8 S1 + 2^16 S2 (exact in int64) is promoted to fp64
-// registers scaled back by 2^-s_c.  The only rounding before fp64 is the
-// quantisation of each length (relative 2^-24 .. 2^-23).
+// Operands (8-bit, K-major, built by `presence_rows_kernel`).  The length of
+// node n, scaled by its chunk's 2^s_c to q < 2^23, is written as
+//   q = 256 u v + s t     (u, v, s, t in [0, 255]; u v, s t <= 32767)
+// (every integer below 2^23 has such a form; the host picks one per node).
+// Row operands A0 = X u and A1 = X s, column operands B0 = (1 - X) v and
+// B1 = (1 - X) t, so that with P0 = A0 B0^T and P1 = A1 B1^T (`kind::i8`,
+// unsigned, int32 accumulate: exact, a chunk holding at most 512 blocks x
+// 128 nodes x 32767 < 2^31)
+//   G[k][l] (chunk c) = 2^-s_c (256 P0[k][l] + P1[k][l]).
+// Two products of 8-bit operands carry the 23-bit lengths: two MMAs per
+// pair and node, where a 0/1 row operand against three byte planes of the
+// lengths takes three.  Nodes are sorted by decreasing length and packed
+// into chunks of whole 128-node K blocks whose lengths lie within a factor
+// of two of the chunk's largest (zero-length padding columns close a chunk);
+// chunk c's largest length lies in [2^22, 2^23) after scaling, so
+// q = round(L 2^s_c) keeps 22 significant bits of every length.  Each chunk
+// is accumulated in tensor memory (TMEM), then 256 P0 + P1 (exact in int64)
+// is promoted to fp64 registers scaled back by 2^-s_c.  The only rounding
+// before fp64 is the quantisation of each length (relative 2^-23 .. 2^-22).
 //
-// Work unit: a cluster of two CTAs (cta_group::2) owns 256 rows k x 64
-// columns l of one table.  One MMA per 32 nodes is M = 256 (128 rows per
-// CTA) x N = 192: B's rows are ordered 3 l + p (column l, plane p), so the
-// unit's 192 B rows are its 64 columns' three planes, 96 held by each CTA,
-// and TMEM column 3 c + p holds column c's plane-p sum.  Per CTA: warp 0
-// issues its TMA loads (its 128 rows of A and its 96 rows of B, 128 nodes,
-// 128-byte swizzle, no multicast) into a 7-stage ring whose full barriers
-// live in CTA 0; in CTA 0 one thread of warp 1 issues the MMAs, into one of
-// two 192-column TMEM accumulators per CTA, and commits each stage's release
-// and each chunk's completion to both CTAs; warps 2..9 of both CTAs drain a
-// finished accumulator into fp64 registers while the next chunk accumulates,
-// and finally form the distances and write them.  Every mbarrier wait is
+// Work unit: a cluster of two CTAs (cta_group::2) owns 256 rows k x 128
+// columns l of one table.  Per 32 nodes, two MMAs of M = 256 (128 rows per
+// CTA) x N = 128 (64 columns of B held by each CTA), one per product, into
+// TMEM columns [0, 128) and [128, 256) of one of two accumulators.  Per
+// CTA: warp 0 issues its TMA loads (its 128 rows of A0 and of A1 and its 64
+// rows of B0 and of B1, 128 nodes, 128-byte swizzle, no multicast) into a
+// 4-stage ring whose full barriers live in CTA 0; in CTA 0 one thread of
+// warp 1 issues the MMAs, and commits each stage's release and each chunk's
+// completion to both CTAs; warps 2..9 of both CTAs drain a finished
+// accumulator into fp64 registers while the next chunk accumulates, and
+// finally form the distances and write them.  Every mbarrier wait is
 // bounded: on expiry the CTA records an error code, stops issuing, lets its
 // copies and MMAs finish, frees TMEM and returns.
 #pragma once
@@ -54,38 +59,43 @@ namespace ssu {
 namespace tc {
 
 constexpr int ROWS = 128;        // rows k per CTA (M = 256 per cluster)
-constexpr int COLS = 64;         // columns l per work unit
-constexpr int PLANES = 3;        // byte planes of a length
+constexpr int COLS = 128;        // columns l per work unit
+constexpr int PRODUCTS = 2;      // operand pairs (A0, B0), (A1, B1)
 constexpr int BLOCK_K = 128;     // 8-bit nodes per stage row: one 128-byte swizzle atom
 constexpr int UMMA_K = 32;
 constexpr int UMMA_M = 2 * ROWS;
-constexpr int UMMA_N = PLANES * COLS;  // 192
-constexpr int B_ROWS = UMMA_N / 2;     // B rows held by each CTA of the pair
-constexpr int STAGES = 7;
-constexpr int MAX_CHUNK_KB = 4096;     // 4096 x 128 x 255 < 2^31: exact plane sums
-constexpr int QBITS = 24;              // fixed-point bits of the largest length of a chunk
+constexpr int UMMA_N = COLS;           // per product
+constexpr int B_ROWS = UMMA_N / 2;     // B rows of each product held by each CTA of the pair
+constexpr int STAGES = 4;
+constexpr int MAX_CHUNK_KB = 512;      // 512 x 128 x 32767 < 2^31: exact product sums
+constexpr int QBITS = 23;              // fixed-point bits of the largest length of a chunk
+constexpr int MAX_PART = 32767;        // largest u v and s t
 constexpr int ACC_STRIDE = 256;        // TMEM columns between the two accumulators
 constexpr int TMEM_COLS = 512;
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
-constexpr uint32_t A_BYTES = ROWS * BLOCK_K;
-constexpr uint32_t B_BYTES = B_ROWS * BLOCK_K;
-constexpr uint32_t STAGE_BYTES = A_BYTES + B_BYTES;  // per CTA
+constexpr uint32_t A_BYTES = ROWS * BLOCK_K;    // one product's A tile
+constexpr uint32_t B_BYTES = B_ROWS * BLOCK_K;  // one product's B tile
+constexpr uint32_t STAGE_BYTES = PRODUCTS * (A_BYTES + B_BYTES);  // per CTA
 constexpr size_t SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-static_assert(UMMA_N % 32 == 0 && UMMA_N <= 256, "kind::i8 with cta_group::2 takes N in multiples of 32 up to 256");
-static_assert(UMMA_N <= ACC_STRIDE && 2 * ACC_STRIDE <= TMEM_COLS, "two accumulators must fit the TMEM allocation");
+static_assert(UMMA_N % 16 == 0 && UMMA_N <= 256, "kind::i8 with M = 256 takes N in multiples of 16 up to 256");
+static_assert(PRODUCTS * UMMA_N <= ACC_STRIDE && 2 * ACC_STRIDE <= TMEM_COLS,
+              "two accumulators must fit the TMEM allocation");
 static_assert(A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "operand tiles must keep 1024-byte swizzle alignment");
 static_assert(SMEM_BYTES <= 227 * 1024, "stage ring exceeds shared memory");
-static_assert(static_cast<long long>(MAX_CHUNK_KB) * BLOCK_K * 255 < (1LL << 31), "plane sums must stay exact");
+static_assert(static_cast<long long>(MAX_CHUNK_KB) * BLOCK_K * MAX_PART < (1LL << 31), "product sums must stay exact");
+static_assert((static_cast<long long>(MAX_PART) << 8) + MAX_PART >= (1LL << QBITS) - 1,
+              "256 u v + s t must reach the largest length");
 
 enum : int { ERR_NONE = 0, ERR_FULL_WAIT = 1, ERR_EMPTY_WAIT = 2, ERR_ACC_FULL_WAIT = 3, ERR_ACC_EMPTY_WAIT = 4,
              ERR_DONE_WAIT = 5, ERR_DRAIN_WAIT = 6 };
 
 struct GemmArgs {
-    const uint4 *tiles;         // x = 256-row block k, y = 64-column block l, z = table
+    const uint4 *tiles;         // x = 256-row block k, y = 128-column block l, z = table
     uint32_t n_tiles;
     const dev::TableDesc *tables;
     uint32_t n_kblocks;         // padded nodes / BLOCK_K
+    uint32_t plane_rows;        // operand rows of one product (A1 and B1 start there)
     uint32_t n_chunks;
     const uint32_t *chunk_end;  // first K block after chunk c
     const double *chunk_scale;  // 2^-s_c per chunk
@@ -225,9 +235,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
     const dev::TableDesc td = args.tables[tile.z];
     const uint32_t k0 = tile.x * UMMA_M + rank * ROWS;  // this CTA's first row, table-local
     const uint32_t l0 = tile.y * COLS;
-    // this CTA's rows: 128 of A, and B rows 3 l + p of its half of the 192
+    // this CTA's rows: 128 of A0 (A1 plane_rows further), and its half of the
+    // unit's 128 columns of B0 (B1 likewise)
     const int arow = static_cast<int>(td.base + k0);
-    const int brow = static_cast<int>(PLANES * (td.base + l0) + rank * B_ROWS);
+    const int brow = static_cast<int>(td.base + l0 + rank * B_ROWS);
+    const int prow = static_cast<int>(args.plane_rows);
     const uint32_t nkb = args.n_kblocks, nchunks = args.n_chunks;
     const long long budget = args.wait_cycles;
 
@@ -276,9 +288,13 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                     break;
                 }
                 uint8_t *st = smem + s * STAGE_BYTES;
+                const int x = static_cast<int>(kb) * BLOCK_K;
                 if (rank == 0) mbar_expect_tx(full + s, 2 * STAGE_BYTES);
-                tma_load_2d_pair(st, &tmA, full0 + s * 8, static_cast<int>(kb) * BLOCK_K, arow);
-                tma_load_2d_pair(st + A_BYTES, &tmB, full0 + s * 8, static_cast<int>(kb) * BLOCK_K, brow);
+                // stage layout: A0, A1, B0, B1
+                tma_load_2d_pair(st, &tmA, full0 + s * 8, x, arow);
+                tma_load_2d_pair(st + A_BYTES, &tmA, full0 + s * 8, x, arow + prow);
+                tma_load_2d_pair(st + 2 * A_BYTES, &tmB, full0 + s * 8, x, brow);
+                tma_load_2d_pair(st + 2 * A_BYTES + B_BYTES, &tmB, full0 + s * 8, x, brow + prow);
                 issued = kb + 1;
             }
         }
@@ -307,12 +323,16 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
                     tc_fence_after();
                     const uint32_t st = smem_u32(smem + s * STAGE_BYTES);
                     const uint64_t a0 = sw128_desc(st);
-                    const uint64_t b0 = sw128_desc(st + A_BYTES);
+                    const uint64_t a1 = sw128_desc(st + A_BYTES);
+                    const uint64_t b0 = sw128_desc(st + 2 * A_BYTES);
+                    const uint64_t b1 = sw128_desc(st + 2 * A_BYTES + B_BYTES);
 #pragma unroll
                     for (int ks = 0; ks < BLOCK_K / UMMA_K; ks++) {
                         // advance 32 bytes along K inside the swizzle atom
                         const uint64_t koff = static_cast<uint64_t>((ks * UMMA_K) >> 4);
-                        umma_i8_pair(d, a0 + koff, b0 + koff, idesc, (kb != kstart || ks != 0) ? 1u : 0u);
+                        const uint32_t accum = (kb != kstart || ks != 0) ? 1u : 0u;
+                        umma_i8_pair(d, a0 + koff, b0 + koff, idesc, accum);
+                        umma_i8_pair(d + UMMA_N, a1 + koff, b1 + koff, idesc, accum);
                     }
                     umma_commit_pair(empty + s);
                 }
@@ -323,7 +343,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
         }
     } else {
         // epilogue: warp w reads TMEM lanes 32*(w%4).. and half (w-2)/4 of the
-        // 64 columns, each column's three plane sums
+        // 128 columns, each column's two product sums
         const int q = warp & 3;
         const int half = (warp - 2) >> 2;
         constexpr int HC = COLS / 2;  // columns per epilogue warp
@@ -339,22 +359,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
             }
             tc_fence_after();
             const double sc = args.chunk_scale[c];
-            const uint32_t base =
-                tmem + (static_cast<uint32_t>(q * 32) << 16) + buf * ACC_STRIDE + half * (PLANES * HC);
+            const uint32_t base = tmem + (static_cast<uint32_t>(q * 32) << 16) + buf * ACC_STRIDE + half * HC;
 #pragma unroll
             for (int g = 0; g < HC / 16; g++) {
-                // 16 columns = 48 consecutive TMEM columns (3 c + p)
-                uint32_t v0[16], v1[16], v2[16];
-                tmem_ld16(base + g * 48, v0);
-                tmem_ld16(base + g * 48 + 16, v1);
-                tmem_ld16(base + g * 48 + 32, v2);
+                // 16 columns of each product
+                uint32_t v0[16], v1[16];
+                tmem_ld16(base + g * 16, v0);
+                tmem_ld16(base + UMMA_N + g * 16, v1);
                 tmem_wait_ld();
 #pragma unroll
                 for (int i = 0; i < 16; i++) {
-                    auto plane = [&](int t) -> unsigned long long {
-                        return t < 16 ? v0[t] : t < 32 ? v1[t - 16] : v2[t - 32];
-                    };
-                    const unsigned long long t = plane(3 * i) + (plane(3 * i + 1) << 8) + (plane(3 * i + 2) << 16);
+                    const unsigned long long t = (static_cast<unsigned long long>(v0[i]) << 8) + v1[i];
                     acc[g * 16 + i] = fma(static_cast<double>(t), sc, acc[g * 16 + i]);
                 }
             }
@@ -474,13 +489,14 @@ __global__ void __launch_bounds__(1024) exclusive_scan_kernel(const uint32_t *__
 
 // Presence rows for the contraction, one CTA per sample (padding rows too):
 // walk up from every present tip, marking embedded ancestors in a shared
-// bitmap (stopping at nodes already marked), then write the sample's row of
-// A = X and its three rows 3 j + p of B = (1 - X) q_p (8-bit, 16 nodes and
-// 16 bytes per store), and r = sum L of the present nodes (fp64, fixed
-// reduction order).  lq holds the length planes: plane p at lq + p * k_pad.
+// bitmap (stopping at nodes already marked), then write the sample's rows of
+// A0 = X u, A1 = X s, B0 = (1 - X) v and B1 = (1 - X) t (8-bit, 16 nodes and
+// 16 bytes per store; A1 and B1 `plane` bytes after A0 and B0), and
+// r = sum L of the present nodes (fp64, fixed reduction order).  lq holds
+// the node digits u, s, v, t: digit i at lq + i * k_pad.
 __global__ void presence_rows_kernel(const uint32_t *__restrict__ sample_ptr, const int32_t *__restrict__ start_col,
                                      const int32_t *__restrict__ parent_col, const uint8_t *__restrict__ lq,
-                                     const double *__restrict__ l_sorted, uint32_t n, uint32_t k_pad,
+                                     const double *__restrict__ l_sorted, uint32_t n, uint32_t k_pad, uint64_t plane,
                                      uint8_t *__restrict__ A, uint8_t *__restrict__ B, double *__restrict__ r) {
     extern __shared__ uint32_t bits[];  // k_pad / 32 words
     __shared__ double red[256];
@@ -500,24 +516,25 @@ __global__ void presence_rows_kernel(const uint32_t *__restrict__ sample_ptr, co
         }
     }
     __syncthreads();
-    const uint64_t arow = static_cast<uint64_t>(j) * k_pad;
-    const uint64_t brow = static_cast<uint64_t>(PLANES) * j * k_pad;
+    const uint64_t row = static_cast<uint64_t>(j) * k_pad;
     double part = 0.0;
     for (uint32_t c16 = threadIdx.x * 16; c16 < k_pad; c16 += blockDim.x * 16) {
         const uint32_t b = (bits[c16 >> 5] >> (c16 & 31)) & 0xFFFFu;
-        uint32_t on[4], keep[4];
+        uint32_t keep[4];  // 0xFF in the bytes of present nodes
 #pragma unroll
         for (int w = 0; w < 4; w++) {
             const uint32_t nib = (b >> (4 * w)) & 0xFu;
-            on[w] = (nib & 1u) | (((nib >> 1) & 1u) << 8) | (((nib >> 2) & 1u) << 16) | (((nib >> 3) & 1u) << 24);
-            keep[w] = ~(on[w] * 0xFFu);  // 0xFF in the bytes of absent nodes
+            keep[w] = ((nib & 1u) | (((nib >> 1) & 1u) << 8) | (((nib >> 2) & 1u) << 16) |
+                       (((nib >> 3) & 1u) << 24)) * 0xFFu;
         }
-        *reinterpret_cast<uint4 *>(A + arow + c16) = make_uint4(on[0], on[1], on[2], on[3]);
 #pragma unroll
-        for (int pl = 0; pl < PLANES; pl++) {
-            const uint4 qv = *reinterpret_cast<const uint4 *>(lq + static_cast<uint64_t>(pl) * k_pad + c16);
-            *reinterpret_cast<uint4 *>(B + brow + static_cast<uint64_t>(pl) * k_pad + c16) =
-                make_uint4(qv.x & keep[0], qv.y & keep[1], qv.z & keep[2], qv.w & keep[3]);
+        for (int i = 0; i < 2 * PRODUCTS; i++) {
+            const uint4 d = *reinterpret_cast<const uint4 *>(lq + static_cast<uint64_t>(i) * k_pad + c16);
+            const bool row_side = i < PRODUCTS;
+            uint8_t *dst = (row_side ? A : B) + static_cast<uint64_t>(i % PRODUCTS) * plane + row + c16;
+            const uint32_t m0 = row_side ? keep[0] : ~keep[0], m1 = row_side ? keep[1] : ~keep[1];
+            const uint32_t m2 = row_side ? keep[2] : ~keep[2], m3 = row_side ? keep[3] : ~keep[3];
+            *reinterpret_cast<uint4 *>(dst) = make_uint4(d.x & m0, d.y & m1, d.z & m2, d.w & m3);
         }
 #pragma unroll
         for (int t = 0; t < 16; t++)
