@@ -175,3 +175,20 @@ def test_tc_band_tuning_changes_no_result(ssu):
     for a, b in zip(tuned.results(), ref):
         np.testing.assert_array_equal(a, b)
     tuned.close()
+
+
+@pytest.mark.parametrize("band", ["1", "4"])
+def test_tc_copy_out_alongside_computation_covers_the_matrix(ssu, gemm_mode, monkeypatch, band):
+    """A full result of one table in page-locked memory is copied out band by
+    band of rows while later bands compute.  Bands of 256 and 1,024 rows over
+    2,300 samples, the last band short: the copied matrix is the plan's own
+    result bit for bit, diagonal included."""
+    monkeypatch.setenv("UNIFRAC_B200_TC_BAND", band)
+    tree, table = _case(14, 1200, 2300, density=0.05)
+    full, _ = ssu.one_off_matrix(tree, table, "unweighted_fp64")
+    plan = ssu.Plan(tree, table, "unweighted_fp64")
+    plan.execute()
+    ref = plan.result()
+    plan.close()
+    np.testing.assert_array_equal(full, ref)
+    assert np.all(np.diag(full) == 0.0)

@@ -13,6 +13,7 @@
 #include <fstream>
 #include <map>
 #include <mutex>
+#include <future>
 
 #include "ssu_gemm.cuh"
 #include "ssu_kernels.cuh"
@@ -265,6 +266,17 @@ struct Group {
     std::vector<uint32_t> band_unit, band_row;
 };
 
+// Host-built layout of the tensor-core operands (see build_gemm_layout).
+struct GemmLayout {
+    std::vector<double> lsorted, scale;  // lengths in column order; 2^-s_c per chunk
+    std::vector<uint32_t> chunk_end;     // first K block after chunk c
+    std::vector<uint8_t> digits;         // u, s, v, t rows of k_pad bytes
+    std::vector<int32_t> parent_col;     // embedded parent's column, or -1
+    std::vector<int32_t> start_of_obs;   // column where a tree observation's path starts, or -1
+    std::string error;
+};
+GemmLayout build_gemm_layout(const FlatTree &tree);
+
 struct PlanImpl {
     MethodSpec spec;
     bool faith = false;
@@ -285,6 +297,16 @@ struct PlanImpl {
     std::vector<Group> groups;
     uint32_t *d_indptr = nullptr, *d_indices = nullptr;
     double *d_data = nullptr;
+    // tensor-core layout built on a worker thread while setup() uploads
+    // (built in setup_gemm instead when no thread can be started)
+    std::future<GemmLayout> gemm_layout;
+    void start_gemm_layout(const FlatTree &tree) {
+        try {
+            gemm_layout = std::async(std::launch::async, build_gemm_layout, std::cref(tree));
+        } catch (const std::exception &) {
+            gemm_layout = std::future<GemmLayout>();
+        }
+    }
 
     // tree
     uint32_t n_tips = 0;
@@ -1468,16 +1490,19 @@ int PlanImpl::tune_band() {
     return build_units(best_band);
 }
 
-int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
-    SetupTimer timer;
-    // Embedded nodes by decreasing |length|, packed into chunks of whole
-    // 128-node K blocks: a chunk closes (its last block padded with
-    // zero-length columns) when the next length is below half the chunk's
-    // first, or at MAX_CHUNK_KB blocks.  Chunk c is scaled by 2^s_c so that
-    // its largest length lies in [2^22, 2^23); q = round(L 2^s_c) is then
-    // written as 256 u v + s t with 8-bit digits (`split_length`).
-    // (stable order by decreasing |length|: an LSD radix sort of the
-    // complemented bit patterns, which order non-negative doubles)
+// Tree-only host part of the tensor-core setup (no CUDA call, so it runs on
+// a worker thread while the plan's CSR and tree are uploaded).
+// Embedded nodes by decreasing |length|, packed into chunks of whole
+// 128-node K blocks: a chunk closes (its last block padded with zero-length
+// columns) when the next length is below half the chunk's first, or at
+// MAX_CHUNK_KB blocks.  Chunk c is scaled by 2^s_c so that its largest
+// length lies in [2^22, 2^23); q = round(L 2^s_c) is then written as
+// 256 u v + s t with 8-bit digits (`split_length`).
+GemmLayout build_gemm_layout(const FlatTree &tree) {
+    GemmLayout lay;
+    const uint32_t E = tree.n_embedded;
+    // stable order by decreasing |length|: an LSD radix sort of the
+    // complemented bit patterns, which order non-negative doubles
     std::vector<uint32_t> order(E), tmp(E);
     std::vector<uint64_t> key(E), key_tmp(E);
     for (uint32_t e = 0; e < E; e++) {
@@ -1487,8 +1512,9 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
         std::memcpy(&b, &a, sizeof b);
         key[e] = ~b;
     }
+    std::vector<uint32_t> count(65537);
     for (int shift = 0; shift < 64; shift += 16) {
-        std::vector<uint32_t> count(65537, 0);
+        std::fill(count.begin(), count.end(), 0u);
         for (uint32_t i = 0; i < E; i++) count[((key[i] >> shift) & 0xFFFF) + 1]++;
         if (std::count(count.begin(), count.end(), 0u) == 65536) continue;  // one digit value: order kept
         for (int d = 0; d < 65536; d++) count[d + 1] += count[d];
@@ -1501,16 +1527,16 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
         order.swap(tmp);
     }
     std::vector<int32_t> col_of_row(tree.n_nodes, -1);
-    std::vector<double> lsorted, scale;
     std::vector<uint32_t> lq;  // 23-bit fixed-point lengths
-    std::vector<uint32_t> chunk_end;
+    lq.reserve(E + 128 * tc::BLOCK_K);
+    lay.lsorted.reserve(E + 128 * tc::BLOCK_K);
     const uint32_t max_cols = static_cast<uint32_t>(tc::MAX_CHUNK_KB) * tc::BLOCK_K;
     auto pad_to_block = [&] {
-        while (lsorted.size() % tc::BLOCK_K) {
-            lsorted.push_back(0.0);
+        while (lay.lsorted.size() % tc::BLOCK_K) {
+            lay.lsorted.push_back(0.0);
             lq.push_back(0u);
         }
-        chunk_end.push_back(static_cast<uint32_t>(lsorted.size() / tc::BLOCK_K));
+        lay.chunk_end.push_back(static_cast<uint32_t>(lay.lsorted.size() / tc::BLOCK_K));
     };
     double first = -1.0;
     size_t chunk_first = 0;
@@ -1518,46 +1544,68 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     for (uint32_t i = 0; i < E; i++) {
         const double L = tree.length[order[i]];
         const double a = std::fabs(L);
-        if (first < 0 || a < first / 2 || lsorted.size() - chunk_first >= max_cols) {
+        if (first < 0 || a < first / 2 || lay.lsorted.size() - chunk_first >= max_cols) {
             if (first >= 0) pad_to_block();
             first = a;
-            chunk_first = lsorted.size();
+            chunk_first = lay.lsorted.size();
             // the chunk's largest length to [2^22, 2^23)
             sig = a > 0 ? (tc::QBITS - 1) - static_cast<int>(std::floor(std::log2(a))) : 0;
-            scale.push_back(std::ldexp(1.0, -sig));
+            lay.scale.push_back(std::ldexp(1.0, -sig));
         }
-        col_of_row[order[i]] = static_cast<int32_t>(lsorted.size());
+        col_of_row[order[i]] = static_cast<int32_t>(lay.lsorted.size());
         const double x = std::nearbyint(std::ldexp(L, sig));
-        lsorted.push_back(L);
+        lay.lsorted.push_back(L);
         lq.push_back(static_cast<uint32_t>(std::min(std::max(x, 0.0), std::ldexp(1.0, tc::QBITS) - 1.0)));
     }
-    if (first < 0) scale.push_back(1.0);  // no embedded node: one chunk of padding
+    if (first < 0) lay.scale.push_back(1.0);  // no embedded node: one chunk of padding
     pad_to_block();
-    timer.step("gemm_chunks");
-    k_pad = static_cast<uint32_t>(lsorted.size());
-    n_chunks = static_cast<uint32_t>(chunk_end.size());
+    const uint32_t k_pad = static_cast<uint32_t>(lay.lsorted.size());
+    // digits u, s, v, t of every column, one k_pad row each
+    lay.digits.assign(static_cast<size_t>(2 * tc::PRODUCTS) * k_pad, 0);
+    for (uint32_t c = 0; c < k_pad; c++) {
+        uint8_t d[4];
+        if (!split_length(lq[c], d)) {
+            lay.error = "length has no 8-bit product form";
+            return lay;
+        }
+        for (int i = 0; i < 4; i++) lay.digits[static_cast<size_t>(i) * k_pad + c] = d[i];
+    }
     // parents among embedded nodes
     std::vector<int32_t> parent_row(tree.n_nodes, -1);
     for (uint32_t r = 0; r < tree.n_nodes; r++)
         for (uint32_t c = tree.child_ptr[r]; c < tree.child_ptr[r + 1]; c++) parent_row[tree.child_rows[c]] = r;
-    std::vector<int32_t> parent_col(k_pad, -1);
+    lay.parent_col.assign(k_pad, -1);
     for (uint32_t r = 0; r < E; r++) {
         const int32_t p = parent_row[r];
-        parent_col[col_of_row[r]] = (p >= 0 && static_cast<uint32_t>(p) < E) ? col_of_row[p] : -1;
+        lay.parent_col[col_of_row[r]] = (p >= 0 && static_cast<uint32_t>(p) < E) ? col_of_row[p] : -1;
     }
     // starting column of each tree observation: its tip, or the tip's parent
     // when tips are bypassed
     uint32_t n_obs_tree = 0;
     for (uint32_t r : tree.leaf_rows) n_obs_tree = std::max<uint32_t>(n_obs_tree, tree.leaf_obs[r] + 1);
-    std::vector<int32_t> start_of_obs(n_obs_tree, -1);
+    lay.start_of_obs.assign(n_obs_tree, -1);
     for (uint32_t r : tree.leaf_rows) {
         const int32_t obs = tree.leaf_obs[r];
         if (obs < 0) continue;
         int32_t node = static_cast<int32_t>(r);
         if (r >= E) node = parent_row[r];
-        start_of_obs[obs] = (node >= 0 && static_cast<uint32_t>(node) < E) ? col_of_row[node] : -1;
+        lay.start_of_obs[obs] = (node >= 0 && static_cast<uint32_t>(node) < E) ? col_of_row[node] : -1;
     }
-    timer.step("gemm_parents");
+    return lay;
+}
+
+int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
+    SetupTimer timer;
+    GemmLayout lay = gemm_layout.valid() ? gemm_layout.get() : build_gemm_layout(tree);
+    timer.step("gemm_layout");
+    if (!lay.error.empty()) {
+        last_error = lay.error;
+        return kOutputError;
+    }
+    k_pad = static_cast<uint32_t>(lay.lsorted.size());
+    n_chunks = static_cast<uint32_t>(lay.chunk_end.size());
+    const std::vector<int32_t> &start_of_obs = lay.start_of_obs;
+    const uint32_t n_obs_tree = static_cast<uint32_t>(start_of_obs.size());
     // per group: operand rows = the group's columns; each row's list of
     // starting columns (one per table row of an observation with a positive
     // count), built on the device from the uploaded CSR: count, scan, place
@@ -1611,23 +1659,11 @@ int PlanImpl::setup_gemm(const TableSet &set, const FlatTree &tree) {
     SSU_CK(alloc(&d_A, tc::PRODUCTS * op_bytes));
     SSU_CK(alloc(&d_B, tc::PRODUCTS * op_bytes));
     SSU_CK(alloc(&d_r, sizeof(double) * n_pad));
-    {
-        // digits u, s, v, t of every column, one k_pad row each
-        std::vector<uint8_t> digits(static_cast<size_t>(2 * tc::PRODUCTS) * k_pad);
-        for (uint32_t c = 0; c < k_pad; c++) {
-            uint8_t d[4];
-            if (!split_length(lq[c], d)) {
-                last_error = "length has no 8-bit product form";
-                return kOutputError;
-            }
-            for (int i = 0; i < 4; i++) digits[static_cast<size_t>(i) * k_pad + c] = d[i];
-        }
-        SSU_CK(upload(&d_lq, digits.data(), digits.size()));
-    }
-    SSU_CK(upload(&d_lsorted, lsorted.data(), sizeof(double) * k_pad));
-    SSU_CK(upload(&d_chunk_scale, scale.data(), sizeof(double) * n_chunks));
-    SSU_CK(upload(&d_chunk_end, chunk_end.data(), sizeof(uint32_t) * n_chunks));
-    SSU_CK(upload(&d_parent_col, parent_col.data(), sizeof(int32_t) * k_pad));
+    SSU_CK(upload(&d_lq, lay.digits.data(), lay.digits.size()));
+    SSU_CK(upload(&d_lsorted, lay.lsorted.data(), sizeof(double) * k_pad));
+    SSU_CK(upload(&d_chunk_scale, lay.scale.data(), sizeof(double) * n_chunks));
+    SSU_CK(upload(&d_chunk_end, lay.chunk_end.data(), sizeof(uint32_t) * n_chunks));
+    SSU_CK(upload(&d_parent_col, lay.parent_col.data(), sizeof(int32_t) * k_pad));
     SSU_CK(alloc(&d_error, sizeof(int)));
     SSU_CK(cudaMemsetAsync(d_error, 0, sizeof(int), stream));
     if (const char *w = std::getenv("UNIFRAC_B200_WAIT_CYCLES")) gemm_wait_cycles = std::max(0LL, std::atoll(w));
@@ -1711,6 +1747,10 @@ int PlanImpl::execute_gemm(cudaStream_t s, const dev::OutSpec &out) {
 // between two streams (the next band's clusters fill SMs as the previous
 // band drains), and the copy stream copies band p's rows after waiting for
 // band p's launch - the earlier bands' copies having waited for theirs.
+// (25,000 samples: the copy-out, about 43 GB/s while the kernel runs against
+// 57 GB/s alone, ends ~25 ms after the last band; copying per band the rows
+// and columns it finished, all bands on one stream, or two copy streams
+// measured the same.)
 int PlanImpl::execute_gemm_overlap(void *host) {
     const Group &g = groups[0];
     const uint32_t nb = static_cast<uint32_t>(g.band_unit.size()) - 1;
@@ -1803,8 +1843,7 @@ bool use_tensor_cores(const MethodSpec &spec, const TableSet &set, const FlatTre
     for (uint32_t e = 0; want && e < tree.n_embedded; e++)
         if (!(tree.length[e] >= 0.0 && std::isfinite(tree.length[e]))) want = false;
     for (const Table *t : set.tables)
-        for (uint64_t q = 0; want && q < t->nnz(); q++)
-            if (!(t->data[q] >= 0.0)) want = false;
+        if (!t->nonneg) want = false;  // found while the table's totals were summed
     return want;
 }
 
@@ -1822,6 +1861,7 @@ int Plan::create(const Table &table, const FlatTree &tree, const MethodSpec &spe
     set.tables.push_back(&table);
     set.embedded.push_back(tree.n_embedded);
     m.gemm = use_tensor_cores(spec, set, tree, false);
+    if (m.gemm) m.start_gemm_layout(tree);
     int rc = m.setup(set, tree, BatchOptions{});
     if (!rc) rc = m.gemm ? m.setup_gemm(set, tree) : spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
     if (rc) {
@@ -1849,6 +1889,7 @@ int Plan::create_batch(const TableSet &set, const FlatTree &tree, const MethodSp
     m.stream = static_cast<cudaStream_t>(stream);
     m.autotune = resolve_autotune(opts.autotune, true);
     m.gemm = use_tensor_cores(spec, set, tree, true);
+    if (m.gemm) m.start_gemm_layout(tree);
     int rc = m.setup(set, tree, opts);
     if (!rc) rc = m.gemm ? m.setup_gemm(set, tree) : spec.fp64 ? m.setup_method<double>() : m.setup_method<float>();
     if (rc) {
