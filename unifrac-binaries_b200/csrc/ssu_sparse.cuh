@@ -591,6 +591,7 @@ struct ScatterArgs {
     uint64_t ld;
     unsigned long long *Sq;
     double scale;  // 2^s
+    unsigned long long *next;  // task counter, zero at launch
 };
 
 template <typename T>
@@ -600,9 +601,15 @@ __global__ void __launch_bounds__(SC_WARPS * 32) sparse_pairs_kernel(const Scatt
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const uint32_t n_sparse = a.n_rows[1];
     const uint64_t tasks = static_cast<uint64_t>(n_sparse) * a.n_tables;
-    const uint64_t stride = static_cast<uint64_t>(gridDim.x) * SC_WARPS;
-    for (uint64_t task = static_cast<uint64_t>(blockIdx.x) * SC_WARPS + warp; task < tasks; task += stride) {
-        // table-major: the warps in flight share one table's sums in L2
+    for (;;) {
+        // tasks in table-major order, taken from a counter: the warps in
+        // flight hold a window of consecutive tasks, so they share one
+        // table's sums in L2 (a fixed grid stride lets warps with heavy rows
+        // fall behind until the tasks in flight span many tables)
+        unsigned long long task = 0;
+        if (lane == 0) task = atomicAdd(a.next, 1ull);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        if (task >= tasks) break;
         const uint32_t e = a.sparse_rows[task % n_sparse];
         const TableDesc td = a.tables[a.t0 + static_cast<uint32_t>(task / n_sparse)];
         const uint64_t w0 = td.base / 64;  // tables start on 128-column boundaries
