@@ -339,6 +339,7 @@ struct PlanImpl {
     bool hybrid_scatter = false;  // sparse rows as per-pair fixed-point sums (sparse_pairs_kernel)
     unsigned long long *d_Sq = nullptr;  // those sums; the fp64 result buffer doubles as them
     unsigned long long *d_sc_next = nullptr;  // the scatter's next (sparse row, table) task
+    uint64_t scatter_band_bytes = 40ull << 20;  // sums per scatter band (UNIFRAC_B200_SCATTER_BAND_BYTES, 0: one band)
     double sq_scale = 1.0;
     bool nonneg_data = true;  // no negative count in any table
     unsigned long long *d_masks = nullptr;
@@ -808,6 +809,8 @@ int PlanImpl::setup_hybrid() {
         else
             SSU_CK(alloc(&d_Sq, sizeof(unsigned long long) * std::max<uint64_t>(full_elems, 1)));
         SSU_CK(alloc(&d_sc_next, sizeof(unsigned long long)));
+        if (const char *b = std::getenv("UNIFRAC_B200_SCATTER_BAND_BYTES"))
+            scatter_band_bytes = std::strtoull(b, nullptr, 10);
     }
     const int smem = static_cast<int>(dev::hybrid_smem<T>());
     SSU_CK(cudaFuncSetAttribute(dev::pair_hybrid_kernel<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -898,6 +901,12 @@ int PlanImpl::hybrid_stage(cudaStream_t s, const Group &g, const dev::OutSpec &o
             SSU_CK(cudaMemsetAsync(d_sc_next, 0, sizeof(unsigned long long), s));
             sa.t0 = t;
             sa.n_tables = 1;
+            // bands of rows k whose sums fit L2 well (at most 16 bands)
+            uint64_t br = std::max<uint64_t>(nt, 1);
+            if (scatter_band_bytes && nt * nt * 8 > scatter_band_bytes)
+                br = std::max<uint64_t>({64, scatter_band_bytes / (8 * nt), (nt + 15) / 16});
+            sa.band_rows = static_cast<uint32_t>(br);
+            sa.n_bands = static_cast<uint32_t>((std::max<uint64_t>(nt, 1) + br - 1) / br);
             dev::sparse_pairs_kernel<T><<<static_cast<uint32_t>(n_sms) * 8, dev::SC_WARPS * 32, 0, s>>>(sa);
             launches++;
         }

@@ -592,6 +592,8 @@ struct ScatterArgs {
     unsigned long long *Sq;
     double scale;  // 2^s
     unsigned long long *next;  // task counter, zero at launch
+    uint32_t band_rows;        // rows k of the sums per band
+    uint32_t n_bands;          // bands per table (each table of the launch)
 };
 
 template <typename T>
@@ -600,26 +602,44 @@ __global__ void __launch_bounds__(SC_WARPS * 32) sparse_pairs_kernel(const Scatt
     __shared__ double val_s[SC_WARPS][2][SC_CAP];
     const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
     const uint32_t n_sparse = a.n_rows[1];
-    const uint64_t tasks = static_cast<uint64_t>(n_sparse) * a.n_tables;
+    const uint64_t per_table = static_cast<uint64_t>(n_sparse) * a.n_bands;
+    const uint64_t tasks = per_table * a.n_tables;
     for (;;) {
-        // tasks in table-major order, taken from a counter: the warps in
-        // flight hold a window of consecutive tasks, so they share one
-        // table's sums in L2 (a fixed grid stride lets warps with heavy rows
-        // fall behind until the tasks in flight span many tables)
+        // tasks (table, band, sparse row) in that order, taken from a counter:
+        // the warps in flight hold a window of consecutive tasks, so they
+        // share one band of one table's sums in L2 (a fixed grid stride lets
+        // warps with heavy rows fall behind until the tasks in flight span
+        // many bands)
         unsigned long long task = 0;
         if (lane == 0) task = atomicAdd(a.next, 1ull);
         task = __shfl_sync(0xffffffffu, task, 0);
         if (task >= tasks) break;
         const uint32_t e = a.sparse_rows[task % n_sparse];
-        const TableDesc td = a.tables[a.t0 + static_cast<uint32_t>(task / n_sparse)];
+        const TableDesc td = a.tables[a.t0 + static_cast<uint32_t>(task / per_table)];
+        const uint32_t band = static_cast<uint32_t>((task % per_table) / n_sparse);
+        const uint32_t klo = band * a.band_rows, khi = min(td.n, klo + a.band_rows);
         const uint64_t w0 = td.base / 64;  // tables start on 128-column boundaries
         const uint32_t nw = (td.n + 63) / 64;
         const unsigned long long *mrow = a.masks + w0 * a.E + e;
-        uint32_t P = 0;
-        for (uint32_t w = lane; w < nw; w += 32) P += __popcll(mrow[static_cast<uint64_t>(w) * a.E]);
+        // P present columns, Plo of them before the band, Phi before its end:
+        // the band's k are the list ranks [Plo, Phi)
+        uint32_t P = 0, Plo = 0, Phi = 0;
+        auto below = [](unsigned long long m, uint32_t c0, uint32_t lim) -> uint32_t {
+            return c0 + 64 <= lim ? __popcll(m) : c0 >= lim ? 0u : __popcll(m & ((1ull << (lim - c0)) - 1ull));
+        };
+        for (uint32_t w = lane; w < nw; w += 32) {
+            const unsigned long long m = mrow[static_cast<uint64_t>(w) * a.E];
+            P += __popcll(m);
+            Plo += below(m, w * 64, klo);
+            Phi += below(m, w * 64, khi);
+        }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) P += __shfl_xor_sync(0xffffffffu, P, o);
-        if (P < 2) continue;
+        for (int o = 16; o > 0; o >>= 1) {
+            P += __shfl_xor_sync(0xffffffffu, P, o);
+            Plo += __shfl_xor_sync(0xffffffffu, Plo, o);
+            Phi += __shfl_xor_sync(0xffffffffu, Phi, o);
+        }
+        if (Phi <= Plo || Plo + 1 >= P) continue;  // no k in the band, or no l after it
         const double L = static_cast<double>(a.len[e]) * a.scale;
         const T *row = a.U + static_cast<uint64_t>(e) * a.ld + td.base;
         unsigned long long *S = a.Sq + td.out_off;
@@ -651,8 +671,8 @@ __global__ void __launch_bounds__(SC_WARPS * 32) sparse_pairs_kernel(const Scatt
             }
             __syncwarp();
         };
-        for (uint32_t i0 = 0; i0 < P; i0 += SC_CAP) {
-            const uint32_t ni = min(static_cast<uint32_t>(SC_CAP), P - i0);
+        for (uint32_t i0 = Plo; i0 < Phi; i0 += SC_CAP) {
+            const uint32_t ni = min(static_cast<uint32_t>(SC_CAP), Phi - i0);
             collect(0, i0);
             for (uint32_t j0 = i0; j0 < P; j0 += SC_CAP) {
                 const bool same = j0 == i0;
