@@ -1,6 +1,11 @@
 // Host-side feature table: borrow, dense pair, filter, rarefy, totals.
 #include "ssu_table.hpp"
 
+#include <algorithm>
+#include <cmath>
+
+#include "ssu_host.hpp"
+
 
 namespace ssu {
 
@@ -10,11 +15,81 @@ void Table::adopt_owned() {
     data = own_data.data();
 }
 
+// Per-sample totals in observation order, with the shape checks.  Large
+// tables are summed by observation ranges on several threads first: when
+// every entry is an integer and the sum of magnitudes stays below 2^52,
+// every partial and final sum is an integer that fp64 holds exactly, so the
+// ranges' sums added in any order equal the observation-order sum bit for
+// bit (counts, presence and rarefied tables).  Other tables (proportions,
+// fractional abundances) are summed again in observation order.
 void Table::compute_totals() {
     totals.assign(n_samples, 0.0);
     nonneg = true;
     malformed = false;
     if (n_obs && indptr[0] != 0) malformed = true;
+    const uint64_t nnz_hint = n_obs ? indptr[n_obs] : 0;
+    const unsigned threads = host_threads(8);
+    if (threads > 1 && n_obs >= 1024 && nnz_hint >= (uint64_t(1) << 21)) {
+        struct Part {
+            std::vector<double> sum;
+            double mag = 0.0;
+            bool integral = true, nonneg = true, malformed = false;
+        };
+        std::vector<Part> parts(threads);
+        // ranges of about nnz / threads entries (cuts kept in order for any indptr)
+        std::vector<uint32_t> cut(threads + 1, 0);
+        cut[threads] = n_obs;
+        for (unsigned p = 1; p < threads; p++) {
+            const uint64_t target = nnz_hint * p / threads;
+            const uint32_t *at = std::lower_bound(indptr, indptr + n_obs, static_cast<uint32_t>(target));
+            cut[p] = std::max(cut[p - 1], static_cast<uint32_t>(at - indptr));
+        }
+        parallel_for(threads, threads, [&](unsigned p) {
+            // flags in locals: the parts share cache lines
+            std::vector<double> sum(n_samples, 0.0);
+            double mag = 0.0;
+            bool integral = true, nneg = true, bad = false;
+            for (uint32_t i = cut[p]; i < cut[p + 1]; i++) {
+                if (indptr[i + 1] < indptr[i]) {
+                    bad = true;
+                    continue;
+                }
+                for (uint32_t q = indptr[i]; q < indptr[i + 1]; q++) {
+                    const uint32_t j = indices[q];
+                    const double x = data[q];
+                    nneg = nneg && x >= 0.0;
+                    integral = integral && x == std::trunc(x);
+                    mag += std::fabs(x);
+                    if (j < n_samples)
+                        sum[j] += x;
+                    else
+                        bad = true;
+                }
+            }
+            Part &r = parts[p];
+            r.sum.swap(sum);
+            r.mag = mag;
+            r.integral = integral;
+            r.nonneg = nneg;
+            r.malformed = bad;
+        });
+        bool integral = true;
+        double mag = 0.0;
+        for (const Part &r : parts) {
+            malformed = malformed || r.malformed;
+            nonneg = nonneg && r.nonneg;
+            integral = integral && r.integral;
+            mag += r.mag;
+        }
+        if (integral && mag < 4503599627370496.0) {  // 2^52
+            for (const Part &r : parts)
+                for (uint32_t j = 0; j < n_samples; j++) totals[j] += r.sum[j];
+            return;
+        }
+        totals.assign(n_samples, 0.0);
+        nonneg = true;
+        malformed = n_obs && indptr[0] != 0;
+    }
     for (uint32_t i = 0; i < n_obs; i++) {
         if (indptr[i + 1] < indptr[i]) {
             malformed = true;
