@@ -11,14 +11,15 @@
 // Tile: 64 (k) x 64 (l) pairs; 16 consumer warps and a producer warpgroup
 // (one thread issues the copies; the group hands most of its registers to
 // the consumers through setmaxnreg, so accumulators and terms stay in
-// registers).  The embedded rows stream through in order, 16 consecutive
-// rows per stage: one 2-D TMA box (16 rows x 64 columns) per block (k, l)
-// and per array (proportions; counts for VAW) and one copy of the 16 branch
+// registers).  The embedded rows stream through in order, 32 consecutive
+// rows per stage: one 2-D TMA box (32 rows x 64 columns) per block (k, l)
+// and per array (proportions; counts for VAW) and one copy of the 32 branch
 // lengths - five copies a stage, not one per row - into a ring of
 // mbarrier-guarded stages (no multicast).  Each consumer warp waits only
 // for the stage it reads, so a warp with little work runs ahead.  Which
 // staged rows hold a tile row or column comes from the embedding's presence
-// words (one 64-bit word per row and 64 columns), read a stage ahead.  Row
+// words (one 64-bit word per row and 64 columns; lane n holds staged row
+// n's words of both blocks), read a stage ahead.  Row
 // pass: warp w owns rows 4w .. 4w + 3 (lanes over the 64 columns); column
 // pass: warp w owns columns 4w .. 4w + 3 (lanes over the 64 rows); both in
 // registers, one owner per element (deterministic sums); the two parts meet
@@ -43,7 +44,7 @@ struct UnionArgs {
     uint32_t n_tiles, n_splits;
     const TableDesc *tables;
     const T *tot;        // per-column totals (variance adjusted)
-    const T *len;        // per embedded row, zero-padded to a multiple of 16 rows
+    const T *len;        // per embedded row, zero-padded to a multiple of URS rows and one stage more
     const unsigned long long *masks;  // presence words: [ld / 64][E], bit c of word (w, e): U[e][64 w + c] > 0
     uint32_t E;
     uint64_t ld;
@@ -74,7 +75,11 @@ static_assert(UREG_CONSUMER * UCT + UREG_PRODUCER * 128 <= UREG_LAUNCH * UTHREAD
 static_assert(UREG_LAUNCH * UTHREADS <= 65536 && UREG_CONSUMER % 8 == 0 && UREG_PRODUCER % 8 == 0,
               "setmaxnreg counts are multiples of 8 within the register file");
 constexpr int UR = UT / UCW;              // rows (row pass) / columns (column pass) per warp
-constexpr int URS = 16;                   // embedded rows per ring stage (the box height)
+// embedded rows per ring stage (the box height): one per lane.  Measured on
+// the 64 uneven tables (five methods, one step): 32 rows 8.59 s, 16 rows
+// 9.28 s, 8 rows 11.07 s, 4 rows 15.27 s (per-stage waits, copy issue and
+// presence words outweigh the finer balance of short stages)
+constexpr int URS = 32;
 // A staged row with more than this many of the tile's 128 samples present
 // (about 31%) is evaluated for every pair of the warp's rows: past it the
 // item path issues more term slots (about 16 p per lane at presence p,
@@ -82,7 +87,7 @@ constexpr int URS = 16;                   // embedded rows per ring stage (the b
 constexpr int UDENSE_BITS = 40;
 constexpr int UFIN_THREADS = 256;
 
-// one staged box: 16 rows x 64 columns, densely packed
+// one staged box: URS rows x 64 columns, densely packed
 template <typename T>
 __host__ __device__ constexpr size_t union_box_bytes() {
     return sizeof(T) * URS * UT;
@@ -303,17 +308,18 @@ __global__ void __launch_bounds__(UTHREADS, 1)
             const int r0 = UR * warp, c0 = UR * warp;
             const double tk0 = CNT ? Ts[lane] : 0.0, tk1 = CNT ? Ts[lane + 32] : 0.0;
             const double tl0 = CNT ? Ts[UT + lane] : 0.0, tl1 = CNT ? Ts[UT + lane + 32] : 0.0;
-            // presence words of a stage: lane n < 16 the k block's word of
-            // staged row n, lane 16 + n the l block's
-            const uint64_t mword = (lane < 16 ? k0 : l0) / 64;
-            auto words_of = [&](uint32_t c) -> unsigned long long {
-                const uint32_t e = r_begin + c * URS + static_cast<uint32_t>(lane & 15);
-                return (c < n_chunks && e < r_end) ? a.masks[mword * a.E + e] : 0ull;
+            // presence words of a stage: lane n the k and l blocks' words of staged row n
+            auto words_of = [&](uint32_t c, unsigned long long &wk, unsigned long long &wl) {
+                const uint32_t e = r_begin + c * URS + static_cast<uint32_t>(lane);
+                const bool ok = c < n_chunks && lane < URS && e < r_end;
+                wk = ok ? a.masks[(k0 / 64) * static_cast<uint64_t>(a.E) + e] : 0ull;
+                wl = ok ? a.masks[(l0 / 64) * static_cast<uint64_t>(a.E) + e] : 0ull;
             };
-            unsigned long long wnext = words_of(0);
+            unsigned long long wk_next, wl_next;
+            words_of(0, wk_next, wl_next);
             for (uint32_t c = 0; c < n_chunks; c++) {
-                const unsigned long long word = wnext;
-                wnext = words_of(c + 1);  // in flight while this stage is evaluated
+                const unsigned long long wk = wk_next, wl = wl_next;
+                words_of(c + 1, wk_next, wl_next);  // in flight while this stage is evaluated
                 const uint32_t gc = g + c, st = gc % NS, use = gc / NS;
                 int ok = *vabort ? 0 : 1;
                 if (ok && !mbar_wait(full + st, use & 1, budget)) ok = 0;
@@ -321,26 +327,25 @@ __global__ void __launch_bounds__(UTHREADS, 1)
                     if (lane == 0 && !*vabort) union_fail(abort_flag, a.error, UNION_ERR_FULL_WAIT);
                     break;
                 }
-                const T *vk = reinterpret_cast<const T *>(ring + st * SB);  // [16][64] k block
-                const T *vl = vk + URS * UT;                                // [16][64] l block
+                const T *vk = reinterpret_cast<const T *>(ring + st * SB);  // [URS][64] k block
+                const T *vl = vk + URS * UT;                                // [URS][64] l block
                 const T *ck = vl + URS * UT;                                // counts (VAW)
                 const T *cl = ck + URS * UT;
-                const T *ls = vk + URS * UT * (CNT ? 4 : 2);                // [16] lengths
+                const T *ls = vk + URS * UT * (CNT ? 4 : 2);                // [URS] lengths
                 // bit n: staged row n has row r0 + rr (row pass) / column
                 // c0 + cc (column pass)
                 // staged rows dense in this tile (more than UDENSE_BITS of its
                 // 128 samples present): every pair of the warp's rows, below
                 uint32_t dm = 0;
                 if constexpr (op_dense_rows<Op>::value) {
-                    const int pc = __popcll(word);
-                    const int both = pc + __shfl_xor_sync(0xffffffffu, pc, 16);
-                    dm = __ballot_sync(0xffffffffu, lane < 16 && both > UDENSE_BITS) & 0xffffu;
+                    const int both = __popcll(wk) + __popcll(wl);
+                    dm = __ballot_sync(0xffffffffu, both > UDENSE_BITS);
                 }
                 uint32_t rm[UR], cm[UR];
 #pragma unroll
                 for (int q = 0; q < UR; q++) {
-                    rm[q] = __ballot_sync(0xffffffffu, lane < 16 && ((word >> (r0 + q)) & 1ull)) & 0xffffu & ~dm;
-                    cm[q] = (__ballot_sync(0xffffffffu, lane >= 16 && ((word >> (c0 + q)) & 1ull)) >> 16) & ~dm;
+                    rm[q] = __ballot_sync(0xffffffffu, (wk >> (r0 + q)) & 1ull) & ~dm;
+                    cm[q] = __ballot_sync(0xffffffffu, (wl >> (c0 + q)) & 1ull) & ~dm;
                 }
                 // dense staged rows: rows r0 .. r0 + 3 x columns lane, lane +
                 // 32, each pair's term (a pair with neither sample adds
