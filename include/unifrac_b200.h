@@ -397,9 +397,10 @@ SSU_EXTERN uint32_t ssu_b200_plan_n_samples(const ssu_b200_plan_t *plan);
 SSU_EXTERN uint64_t ssu_b200_plan_n_embedded(const ssu_b200_plan_t *plan);
 /* Kernel launches one execute issues. */
 SSU_EXTERN uint32_t ssu_b200_plan_launches(const ssu_b200_plan_t *plan);
-/* Tensor-core flops (2 x multiply-adds, padding and the hi/lo length planes
- * included) one execute issues on the unweighted tensor-core path; 0 for
- * plans on other kernels. */
+/* Tensor-core int8 operations (2 x multiply-adds; both byte products of
+ * each length, chunk padding and the units on the diagonal included) one
+ * execute issues on the unweighted tensor-core path; 0 for plans on other
+ * kernels. */
 SSU_EXTERN uint64_t ssu_b200_plan_tensor_flops(const ssu_b200_plan_t *plan);
 /* When enabled, execute brackets each stage with CUDA events on its stream;
  * ssu_b200_plan_stage_ms then reports {embed, pair-kernel, finalize} in ms for
