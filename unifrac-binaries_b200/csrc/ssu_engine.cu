@@ -1388,36 +1388,6 @@ int PlanImpl::run_windowed(int mode, void *d_out, uint32_t start, uint32_t stop)
 
 // --------------------------------------------------- tensor-core unweighted
 
-// q (< 2^23) as 256 u v + s t with u, v, s, t in [0, 255] and u v, s t <=
-// 32767: d = {u, s, v, t}.  p = u v runs down from q / 256 (s t = q - 256 p
-// up from q mod 256) until both are products of two bytes; every q < 2^23
-// has such a pair within 112 steps.  False if none is found.
-static bool split_length(uint32_t q, uint8_t d[4]) {
-    struct Factors {
-        uint16_t f[tc::MAX_PART + 1];  // u | v << 8 for p = u v, or 0xFFFF
-        Factors() {
-            std::fill(std::begin(f), std::end(f), static_cast<uint16_t>(0xFFFF));
-            f[0] = 0;
-            for (uint32_t u = 1; u < 256; u++)
-                for (uint32_t v = u; v < 256 && u * v <= static_cast<uint32_t>(tc::MAX_PART); v++)
-                    if (f[u * v] == 0xFFFF) f[u * v] = static_cast<uint16_t>(u | (v << 8));
-        }
-    };
-    static const Factors tab;
-    if (q >= (1u << tc::QBITS)) return false;
-    for (int64_t p = q >> 8, rest = q & 255; p >= 0 && rest <= tc::MAX_PART; p--, rest += 256) {
-        if (p > tc::MAX_PART) continue;
-        const uint16_t a = tab.f[p], b = tab.f[rest];
-        if (a == 0xFFFF || b == 0xFFFF) continue;
-        d[0] = static_cast<uint8_t>(a & 0xFF);
-        d[2] = static_cast<uint8_t>(a >> 8);
-        d[1] = static_cast<uint8_t>(b & 0xFF);
-        d[3] = static_cast<uint8_t>(b >> 8);
-        return true;
-    }
-    return false;
-}
-
 // Tensor-core work units: per table, the (256-row block, 128-column block)
 // pairs holding some pair k < l, ordered in bands of `band` row blocks walked
 // column by column.  Clusters start in launch order as SMs free up, so a
@@ -1514,7 +1484,7 @@ int PlanImpl::tune_band() {
 // columns) when the next length is below half the chunk's first, or at
 // MAX_CHUNK_KB blocks.  Chunk c is scaled by 2^s_c so that its largest
 // length lies in [2^22, 2^23); q = round(L 2^s_c) is then written as
-// 256 u v + s t with 8-bit digits (`split_length`).
+// 256 u v + s t with 8-bit digits (`digits::split_length`).
 GemmLayout build_gemm_layout(const FlatTree &tree) {
     GemmLayout lay;
     const uint32_t E = tree.n_embedded;
@@ -1581,7 +1551,7 @@ GemmLayout build_gemm_layout(const FlatTree &tree) {
     lay.digits.assign(static_cast<size_t>(2 * tc::PRODUCTS) * k_pad, 0);
     for (uint32_t c = 0; c < k_pad; c++) {
         uint8_t d[4];
-        if (!split_length(lq[c], d)) {
+        if (!digits::split_length(lq[c], d)) {
             lay.error = "length has no 8-bit product form";
             return lay;
         }

@@ -53,6 +53,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include "ssu_digits.hpp"
 #include "ssu_kernels.cuh"
 
 namespace ssu {
@@ -68,8 +69,8 @@ constexpr int UMMA_N = COLS;           // per product
 constexpr int B_ROWS = UMMA_N / 2;     // B rows of each product held by each CTA of the pair
 constexpr int STAGES = 4;
 constexpr int MAX_CHUNK_KB = 512;      // 512 x 128 x 32767 < 2^31: exact product sums
-constexpr int QBITS = 23;              // fixed-point bits of the largest length of a chunk
-constexpr int MAX_PART = 32767;        // largest u v and s t
+constexpr int QBITS = digits::kBits;   // fixed-point bits of the largest length of a chunk
+constexpr int MAX_PART = static_cast<int>(digits::kMaxPart);  // largest u v and s t
 constexpr int ACC_STRIDE = 256;        // TMEM columns between the two accumulators
 constexpr int TMEM_COLS = 512;
 constexpr int EPI_WARPS = 8;
