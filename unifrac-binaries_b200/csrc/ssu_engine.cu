@@ -12,10 +12,12 @@
 #include <cuda_runtime.h>
 #include <fstream>
 #include <map>
-#include <mutex>
 #include <future>
+#include <mutex>
+#include <thread>
 
 #include "ssu_gemm.cuh"
+#include "ssu_host.hpp"
 #include "ssu_kernels.cuh"
 #include "ssu_pairs.cuh"
 #include "ssu_sparse.cuh"
@@ -63,6 +65,116 @@ constexpr int kOutputError = 6;  // ComputeStatus output_error
 // One stream-ordered memory pool per device, owned by the library, that
 // keeps freed blocks cached (no release threshold): repeated calls reuse the
 // embedding and result buffers instead of re-mapping them.
+// Host -> device copies from pageable memory (the caller's table arrays)
+// through page-locked staging: up to four host threads each copy 8 MiB
+// pieces into two staging buffers of their own and issue an asynchronous
+// copy from each on a stream of their own (a buffer is refilled once its
+// last copy has landed), so host memory is read by several threads while
+// the copies run; the driver's own pageable path stages on the calling
+// thread (11-12 GB/s on the B200 hosts here).  The staging buffers are made
+// once per process, for the first device that uploads; other devices, a
+// second upload while one is running, and small uploads (below 32 MiB) take
+// the plain path.  On return the copies are ordered before later work on s.
+struct HostPiece {
+    void *dst;
+    const void *src;
+    size_t bytes;
+};
+class Staging {
+  public:
+    static constexpr size_t kPiece = size_t(8) << 20;
+    static constexpr int kWorkers = 4;
+
+    static Staging &get() {
+        static Staging st;
+        return st;
+    }
+    // 0 on success; any CUDA error code otherwise
+    cudaError_t upload(const std::vector<HostPiece> &pieces, cudaStream_t s, int dev) {
+        size_t total = 0;
+        for (const HostPiece &p : pieces) total += p.bytes;
+        std::unique_lock<std::mutex> lock(mu_, std::try_to_lock);
+        const unsigned workers = std::min<unsigned>(kWorkers, host_threads(kWorkers));
+        if (total < (size_t(32) << 20) || !lock.owns_lock() || workers < 2 || !ready(dev)) {
+            for (const HostPiece &p : pieces)
+                if (p.bytes) {
+                    const cudaError_t e = cudaMemcpyAsync(p.dst, p.src, p.bytes, cudaMemcpyHostToDevice, s);
+                    if (e != cudaSuccess) return e;
+                }
+            return cudaSuccess;
+        }
+        // the destinations are stream-ordered allocations on s: copies start after them
+        cudaError_t e0 = cudaEventRecord(start_, s);
+        for (unsigned w = 0; w < workers && e0 == cudaSuccess; w++) e0 = cudaStreamWaitEvent(streams_[w], start_, 0);
+        if (e0 != cudaSuccess) return e0;
+        std::vector<HostPiece> cuts;  // 8 MiB pieces, in order
+        for (const HostPiece &p : pieces)
+            for (size_t o = 0; o < p.bytes; o += kPiece)
+                cuts.push_back({static_cast<char *>(p.dst) + o, static_cast<const char *>(p.src) + o,
+                                std::min(kPiece, p.bytes - o)});
+        std::vector<cudaError_t> err(workers, cudaSuccess);
+        auto work = [&](unsigned w) {
+            cudaError_t e = cudaSetDevice(dev);
+            unsigned use = 0;
+            for (size_t i = w; i < cuts.size() && e == cudaSuccess; i += workers, use++) {
+                const unsigned b = w * 2 + (use & 1);
+                e = cudaEventSynchronize(landed_[b]);  // its previous copy has landed
+                if (e != cudaSuccess) break;
+                std::memcpy(buf_[b], cuts[i].src, cuts[i].bytes);
+                e = cudaMemcpyAsync(cuts[i].dst, buf_[b], cuts[i].bytes, cudaMemcpyHostToDevice, streams_[w]);
+                if (e == cudaSuccess) e = cudaEventRecord(landed_[b], streams_[w]);
+            }
+            err[w] = e;
+        };
+        std::vector<std::thread> pool;
+        for (unsigned w = 1; w < workers; w++) {
+            try {
+                pool.emplace_back(work, w);
+            } catch (const std::system_error &) {
+                err[w] = cudaErrorLaunchFailure;  // reported below; its pieces were not copied
+            }
+        }
+        work(0);
+        for (std::thread &t : pool) t.join();
+        for (unsigned w = 0; w < workers; w++)
+            if (err[w] != cudaSuccess) {
+                // nothing may still write the destinations once the caller frees them
+                for (unsigned v = 0; v < workers; v++) cudaStreamSynchronize(streams_[v]);
+                return err[w];
+            }
+        for (unsigned w = 0; w < workers; w++) {
+            cudaError_t e = cudaEventRecord(done_[w], streams_[w]);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(s, done_[w], 0);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+
+  private:
+    bool ready(int dev) {
+        if (dev_ >= 0) return dev_ == dev && ok_;
+        dev_ = dev;
+        ok_ = cudaEventCreateWithFlags(&start_, cudaEventDisableTiming) == cudaSuccess;
+        for (int w = 0; w < kWorkers && ok_; w++) {
+            ok_ = cudaStreamCreateWithFlags(&streams_[w], cudaStreamNonBlocking) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&done_[w], cudaEventDisableTiming) == cudaSuccess;
+            for (int b = 2 * w; b < 2 * w + 2 && ok_; b++)
+                ok_ = cudaHostAlloc(&buf_[b], kPiece, cudaHostAllocDefault) == cudaSuccess &&
+                      cudaEventCreateWithFlags(&landed_[b], cudaEventDisableTiming) == cudaSuccess;
+        }
+        if (!ok_) cudaGetLastError();  // the plain path stands in
+        return ok_;
+    }
+    std::mutex mu_;
+    int dev_ = -1;
+    bool ok_ = false;
+    cudaStream_t streams_[kWorkers] = {};
+    cudaEvent_t done_[kWorkers] = {};
+    void *buf_[2 * kWorkers] = {};
+    cudaEvent_t landed_[2 * kWorkers] = {};
+    cudaEvent_t start_ = nullptr;
+};
+
 cudaMemPool_t device_pool(int dev) {
     static std::mutex mu;
     static std::vector<cudaMemPool_t> pools;
@@ -515,17 +627,16 @@ int PlanImpl::setup(const TableSet &set, const FlatTree &tree, const BatchOption
     SSU_CK(alloc(&d_indptr, sizeof(uint32_t) * indptr_total));
     SSU_CK(alloc(&d_indices, sizeof(uint32_t) * nnz_total));
     SSU_CK(alloc(&d_data, sizeof(double) * nnz_total));
-    for (uint32_t t = 0; t < n_tables; t++) {
-        const Table &tb = *set.tables[t];
-        const dev::TableDesc &d = tdesc[t];
-        SSU_CK(cudaMemcpyAsync(d_indptr + d.indptr_off, tb.indptr, sizeof(uint32_t) * (tb.n_obs + 1),
-                               cudaMemcpyHostToDevice, stream));
-        if (tb.nnz()) {
-            SSU_CK(cudaMemcpyAsync(d_indices + d.nnz_off, tb.indices, sizeof(uint32_t) * tb.nnz(),
-                                   cudaMemcpyHostToDevice, stream));
-            SSU_CK(cudaMemcpyAsync(d_data + d.nnz_off, tb.data, sizeof(double) * tb.nnz(), cudaMemcpyHostToDevice,
-                                   stream));
+    {
+        std::vector<HostPiece> pieces;
+        for (uint32_t t = 0; t < n_tables; t++) {
+            const Table &tb = *set.tables[t];
+            const dev::TableDesc &d = tdesc[t];
+            pieces.push_back({d_indptr + d.indptr_off, tb.indptr, sizeof(uint32_t) * (tb.n_obs + 1)});
+            pieces.push_back({d_indices + d.nnz_off, tb.indices, sizeof(uint32_t) * tb.nnz()});
+            pieces.push_back({d_data + d.nnz_off, tb.data, sizeof(double) * tb.nnz()});
         }
+        SSU_CK(Staging::get().upload(pieces, stream, dev_id));
     }
 
     timer.step("csr_upload");
@@ -1479,39 +1590,41 @@ int PlanImpl::tune_band() {
 
 // Tree-only host part of the tensor-core setup (no CUDA call, so it runs on
 // a worker thread while the plan's CSR and tree are uploaded).
-// Embedded nodes by decreasing |length|, packed into chunks of whole
-// 128-node K blocks: a chunk closes (its last block padded with zero-length
-// columns) when the next length is below half the chunk's first, or at
-// MAX_CHUNK_KB blocks.  Chunk c is scaled by 2^s_c so that its largest
-// length lies in [2^22, 2^23); q = round(L 2^s_c) is then written as
-// 256 u v + s t with 8-bit digits (`digits::split_length`).
+// Embedded nodes grouped by the binary exponent of |length|, largest first,
+// packed into chunks of whole 128-node K blocks: a chunk closes (its last
+// block padded with zero-length columns) where the exponent changes or at
+// MAX_CHUNK_KB blocks.  Chunk c is scaled by 2^s_c so that its exponent's
+// largest length lies in [2^22, 2^23), which puts all its lengths there;
+// q = round(L 2^s_c) is then written as 256 u v + s t with 8-bit digits
+// (`digits::split_length`).
 GemmLayout build_gemm_layout(const FlatTree &tree) {
     GemmLayout lay;
     const uint32_t E = tree.n_embedded;
-    // stable order by decreasing |length|: an LSD radix sort of the
-    // complemented bit patterns, which order non-negative doubles
-    std::vector<uint32_t> order(E), tmp(E);
-    std::vector<uint64_t> key(E), key_tmp(E);
-    for (uint32_t e = 0; e < E; e++) {
-        order[e] = e;
-        const double a = std::fabs(tree.length[e]);
+    // order by binary exponent of |length|, largest first, by row within an
+    // exponent (one counting pass): every length of an exponent lies within a
+    // factor of two of the others, which is all the chunks need
+    constexpr int kExp = 2048;  // biased fp64 exponents; 0 holds zeros (and subnormals)
+    auto exponent = [](double a) {
         uint64_t b;
         std::memcpy(&b, &a, sizeof b);
-        key[e] = ~b;
+        return static_cast<int>((b >> 52) & 0x7FF);
+    };
+    std::vector<uint32_t> count(kExp, 0), order(E);
+    std::vector<double> emax(kExp, 0.0);
+    for (uint32_t e = 0; e < E; e++) {
+        const double a = std::fabs(tree.length[e]);
+        const int x = exponent(a);
+        count[x]++;
+        emax[x] = std::max(emax[x], a);
     }
-    std::vector<uint32_t> count(65537);
-    for (int shift = 0; shift < 64; shift += 16) {
-        std::fill(count.begin(), count.end(), 0u);
-        for (uint32_t i = 0; i < E; i++) count[((key[i] >> shift) & 0xFFFF) + 1]++;
-        if (std::count(count.begin(), count.end(), 0u) == 65536) continue;  // one digit value: order kept
-        for (int d = 0; d < 65536; d++) count[d + 1] += count[d];
-        for (uint32_t i = 0; i < E; i++) {
-            const uint32_t pos = count[(key[i] >> shift) & 0xFFFF]++;
-            key_tmp[pos] = key[i];
-            tmp[pos] = order[i];
+    {
+        uint32_t at = 0;
+        for (int x = kExp - 1; x >= 0; x--) {
+            const uint32_t c = count[x];
+            count[x] = at;
+            at += c;
         }
-        key.swap(key_tmp);
-        order.swap(tmp);
+        for (uint32_t e = 0; e < E; e++) order[count[exponent(std::fabs(tree.length[e]))]++] = e;
     }
     std::vector<int32_t> col_of_row(tree.n_nodes, -1);
     std::vector<uint32_t> lq;  // 23-bit fixed-point lengths
@@ -1525,24 +1638,32 @@ GemmLayout build_gemm_layout(const FlatTree &tree) {
         }
         lay.chunk_end.push_back(static_cast<uint32_t>(lay.lsorted.size() / tc::BLOCK_K));
     };
-    double first = -1.0;
+    // A chunk holds lengths of one exponent (at most MAX_CHUNK_KB blocks),
+    // scaled by 2^sig so that the exponent's largest lies in [2^22, 2^23):
+    // every length of the chunk then lies in [2^22, 2^23) too.
+    const double qmax = std::ldexp(1.0, tc::QBITS) - 1.0;
+    int cur = -1, sig = 0;
+    double pw = 1.0;
+    bool by_mul = true;
     size_t chunk_first = 0;
-    int sig = 0;
+    double first = -1.0;
     for (uint32_t i = 0; i < E; i++) {
         const double L = tree.length[order[i]];
-        const double a = std::fabs(L);
-        if (first < 0 || a < first / 2 || lay.lsorted.size() - chunk_first >= max_cols) {
-            if (first >= 0) pad_to_block();
-            first = a;
+        const int xe = exponent(std::fabs(L));
+        if (xe != cur || lay.lsorted.size() - chunk_first >= max_cols) {
+            if (cur >= 0) pad_to_block();
+            cur = xe;
+            first = emax[xe];
             chunk_first = lay.lsorted.size();
-            // the chunk's largest length to [2^22, 2^23)
-            sig = a > 0 ? (tc::QBITS - 1) - static_cast<int>(std::floor(std::log2(a))) : 0;
+            sig = first > 0 ? (tc::QBITS - 1) - static_cast<int>(std::floor(std::log2(first))) : 0;
             lay.scale.push_back(std::ldexp(1.0, -sig));
+            by_mul = sig >= -1022 && sig <= 1023;  // 2^sig itself a normal double
+            pw = by_mul ? std::ldexp(1.0, sig) : 1.0;
         }
         col_of_row[order[i]] = static_cast<int32_t>(lay.lsorted.size());
-        const double x = std::nearbyint(std::ldexp(L, sig));
+        const double x = by_mul ? L * pw : std::ldexp(L, sig);  // exact: a power of two
         lay.lsorted.push_back(L);
-        lq.push_back(static_cast<uint32_t>(std::min(std::max(x, 0.0), std::ldexp(1.0, tc::QBITS) - 1.0)));
+        lq.push_back(static_cast<uint32_t>(std::min(std::floor(std::max(x, 0.0) + 0.5), qmax)));
     }
     if (first < 0) lay.scale.push_back(1.0);  // no embedded node: one chunk of padding
     pad_to_block();

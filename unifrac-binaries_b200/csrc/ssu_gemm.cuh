@@ -25,14 +25,14 @@
 //   G[k][l] (chunk c) = 2^-s_c (256 P0[k][l] + P1[k][l]).
 // Two products of 8-bit operands carry the 23-bit lengths: two MMAs per
 // pair and node, where a 0/1 row operand against three byte planes of the
-// lengths takes three.  Nodes are sorted by decreasing length and packed
-// into chunks of whole 128-node K blocks whose lengths lie within a factor
-// of two of the chunk's largest (zero-length padding columns close a chunk);
-// chunk c's largest length lies in [2^22, 2^23) after scaling, so
-// q = round(L 2^s_c) keeps 22 significant bits of every length.  Each chunk
-// is accumulated in tensor memory (TMEM), then 256 P0 + P1 (exact in int64)
-// is promoted to fp64 registers scaled back by 2^-s_c.  The only rounding
-// before fp64 is the quantisation of each length (relative 2^-23 .. 2^-22).
+// lengths takes three.  Nodes are grouped by the binary exponent of their
+// length and packed into chunks of whole 128-node K blocks of one exponent
+// (zero-length padding columns close a chunk); scaled by 2^s_c every length
+// of chunk c lies in [2^22, 2^23), so q = round(L 2^s_c) keeps 23
+// significant bits.  Each chunk is accumulated in tensor memory (TMEM), then
+// 256 P0 + P1 (exact in int64) is promoted to fp64 registers scaled back by
+// 2^-s_c.  The only rounding before fp64 is the quantisation of each length
+// (relative at most 2^-23).
 //
 // Work unit: a cluster of two CTAs (cta_group::2) owns 256 rows k x 128
 // columns l of one table.  Per 32 nodes, two MMAs of M = 256 (128 rows per
