@@ -1655,7 +1655,9 @@ GemmLayout build_gemm_layout(const FlatTree &tree) {
             cur = xe;
             first = emax[xe];
             chunk_first = lay.lsorted.size();
-            sig = first > 0 ? (tc::QBITS - 1) - static_cast<int>(std::floor(std::log2(first))) : 0;
+            // floor(log2) of a normal double is its unbiased exponent, exactly
+            const int lg = xe > 0 ? xe - 1023 : (first > 0 ? static_cast<int>(std::floor(std::log2(first))) : 0);
+            sig = first > 0 ? (tc::QBITS - 1) - lg : 0;
             lay.scale.push_back(std::ldexp(1.0, -sig));
             by_mul = sig >= -1022 && sig <= 1023;  // 2^sig itself a normal double
             pw = by_mul ? std::ldexp(1.0, sig) : 1.0;
