@@ -1,6 +1,8 @@
 // Host-side phylogeny handling: BP trees, newick, shear, collapse, flatten.
 #include "ssu_tree.hpp"
 
+#include "ssu_host.hpp"
+
 #include <algorithm>
 #include <cstdlib>
 
@@ -198,22 +200,33 @@ TipMatch BPTree::match_tips(const NameMap &obs, uint32_t n_obs) const {
     m.tags.assign(n, -1);
     m.tree_id = open.data();
     m.tree_size = n;
-    std::vector<uint8_t> seen(n_obs, 0);
-    bool all = true;
-    for (uint32_t i = 0; i + 1 < n; i++) {
-        if (!leaf(i)) continue;
-        const int64_t row = obs.find(name[i]);
-        if (row < 0) {
-            all = false;
-            continue;
+    // the lookups (read-only on the map, disjoint tags) on up to four host
+    // threads for large trees, then the distinct rows counted in one pass
+    const unsigned threads = n >= (1u << 16) ? host_threads(4) : 1u;
+    const uint32_t span = (n + threads - 1) / threads;
+    std::vector<uint8_t> missing(threads, 0);
+    parallel_for(threads, threads, [&](unsigned p) {
+        const uint32_t lo = p * span, hi = std::min(n ? n - 1 : 0, lo + span);
+        bool miss = false;
+        for (uint32_t i = lo; i < hi; i++) {
+            if (!leaf(i)) continue;
+            const int64_t row = obs.find(name[i]);
+            if (row < 0)
+                miss = true;
+            else
+                m.tags[i] = static_cast<int32_t>(row);
         }
-        m.tags[i] = static_cast<int32_t>(row);
-        if (!seen[row]) {
+        missing[p] = miss ? 1 : 0;
+    });
+    std::vector<uint8_t> seen(n_obs, 0);
+    for (uint32_t i = 0; i + 1 < n; i++) {
+        const int32_t row = m.tags[i];
+        if (row >= 0 && !seen[row]) {
             seen[row] = 1;
             m.rows_matched++;
         }
     }
-    m.all_tips = all;
+    m.all_tips = std::find(missing.begin(), missing.end(), 1) == missing.end();
     return m;
 }
 
